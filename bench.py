@@ -1,0 +1,325 @@
+"""Benchmark of the FDTD time-step path.
+
+Workload (the configuration the headline metric is quoted on): 256^3 FP32 dispersive
+plasmonics -- Drude+Lorentz gold-like sphere, 12-cell CPML, TFSF broadband plane wave and
+DFT monitors on six box faces at 64 frequencies with FP64 sums.  One step = one full time
+step of the whole grid (H update with the deferred Sa/E2 sums, E update with CPML/ADE,
+TFSF injection, monitor gather; the DFT accumulation runs every 64 staged steps).
+
+  value   : Gcell-updates/s with all inputs resident in HBM, CUDA events on the library's
+            stream around the K timed steps (one mfd_run call), max over ranks.
+  e2e     : the same metric through the public API with host buffers: model upload
+            (mfd_create), K steps, and the read-back of the final fields, Sa/E2 and the DFT
+            spectra, wall-clock with the device synchronised.
+  roofline: the dominant kernel (E update), algorithmic bytes per launch / its mean launch
+            time from per-launch CUDA events in the timed region, against the measured HBM
+            copy bandwidth.
+
+Multi-GPU: replicas (the path does not shard); each rank runs the same workload on its own
+GPU, scaling "weak".  ``--impl reference`` times the CPU oracle (the restatement of the
+reference's CPU path) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "plasmonics_256: 256^3 FP32, Drude+Lorentz sphere r=60nm, 12-cell CPML, TFSF 600nm/3fs, 6x DFT faces x 64 freq FP64"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(model, meta, dtype):
+    """Algorithmic HBM bytes of one H launch and one E launch: every array read once and
+    written once, neighbours from on-chip reuse."""
+    T = np.dtype(dtype).itemsize
+    g = model.grid
+    N = g.Nx * g.Ny * g.Nz
+    geo = np.count_nonzero(model.geometry)
+    math_h = any(m.Mh != model.Mh for m in model.materials)
+    h = N * (3 * T + 6 * T + (1 if math_h else 0) + 2 * T + (2 * T if geo else 0))
+    e = N * (3 * T + 6 * T + 3 * T + (1 if geo else 0))
+    # CPML slabs: two psi per face cell, read + write, in each kernel
+    for f, L in enumerate(model.pml):
+        if L.nb:
+            axis = f // 2
+            n_axis = (g.Nx, g.Ny, g.Nz)[axis]
+            slab = N // n_axis * L.nb
+            h += slab * 2 * 2 * T
+            e += slab * 2 * 2 * T
+    # material state: E^n read + per pole P^n, P^{n-1} read and P^{n+1} write (3 components)
+    for imat, m in enumerate(model.materials, start=1):
+        cells = int(np.count_nonzero(model.geometry == imat))
+        if m.nq or m.isplasma:
+            e += cells * 3 * T
+        e += cells * m.nq * 3 * 3 * T
+        if m.isplasma:
+            e += cells * (3 * 3 * T + 3 * 2 * T + 2 * 2 * 8 + 2 * T)
+    return int(h), int(e)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"mfd_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if hasattr(self, "fh"):
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_gpu(args):
+    import maxwellfdtd_b200 as M
+    from maxwellfdtd_b200 import _abi, workloads
+    ws, rank, local = dist_setup()
+    torch = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    W, K = args.warmup, args.steps
+    nt = W + K + 2
+    model, mons = workloads.plasmonics_256(nt=nt, n=args.n)
+    dtype = np.float32
+    lib = M.load_library()
+    b, meta = model.build_desc(dtype, mons, device=local)
+    st = _abi.Stepper(lib, b, dtype)
+    N = model.grid.Nx * model.grid.Ny * model.grid.Nz
+    # warm-up
+    st.run(1, W)
+    kt0 = st.kernel_times()
+    if ws > 1:
+        dist.barrier()
+        torch.cuda.synchronize()
+    st.set_profiling(True)
+    with ClockSampler(local) as clk:
+        st.run(W + 1, W + K)        # timed: K steps, CUDA events on the library's stream
+    st.set_profiling(False)
+    ms = st.last_run_ms()
+    kt1 = st.kernel_times()
+    dev_bytes = st.device_bytes()
+    st.close()
+    ms_max = ms
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = N * K * ws / (ms_max * 1e-3) / 1e9
+    launches = int(sum(kt1[k][1] - kt0[k][1] for k in kt1))
+    h_bytes, e_bytes = algorithmic_bytes(model, meta, dtype)
+    e_ms = (kt1["E"][0] - kt0["E"][0]) / max(1, kt1["E"][1] - kt0["E"][1])
+    h_ms = (kt1["H"][0] - kt0["H"][0]) / max(1, kt1["H"][1] - kt0["H"][1])
+    peak, peak_kind = peaks()
+    e_gbs = e_bytes / (e_ms * 1e-3) / 1e9
+    h_gbs = h_bytes / (h_ms * 1e-3) / 1e9
+    per_kernel = {k: {"ms": round(kt1[k][0] - kt0[k][0], 4), "launches": int(kt1[k][1] - kt0[k][1])} for k in kt1}
+
+    # end to end through the public API with host buffers
+    t0 = time.perf_counter()
+    b2, meta2 = model.build_desc(dtype, mons, device=local)
+    t_desc = time.perf_counter() - t0
+    h2d = sum(a.nbytes for a in b2.keep if isinstance(a, np.ndarray))
+    t0 = time.perf_counter()
+    st2 = _abi.Stepper(lib, b2, dtype)
+    st2.run(1, K)
+    d2h = 0
+    for c in (6, 7, 8, 0, 1, 2):
+        d2h += st2.read_field(c).nbytes
+    d2h += st2.read_integral(_abi.MFD_INT_SA).nbytes + st2.read_integral(_abi.MFD_INT_E2).nbytes
+    for m, ms_ in enumerate(meta2["monitors"]):
+        for c in (0, 1, 2, 6, 7, 8):
+            d2h += st2.read_monitor(m, c, (ms_["dft"].Nw, len(ms_["cells"])), True).nbytes
+    t_e2e = time.perf_counter() - t0
+    st2.close()
+    if ws > 1:
+        t = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = N * K * ws / t_e2e / 1e9
+
+    out = None
+    if rank == 0:
+        cpu = None if (args.no_cpu or ws > 1) else cpu_baseline(args, model, mons)
+        out = {
+            "metric": "Gcell-updates/s",
+            "value": round(value, 3),
+            "unit": "Gcell-updates/s",
+            "n_gpus": ws,
+            "steps": K,
+            "warmup": W,
+            "ms_per_step": round(ms_max / K, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "cells": N, "steps_per_sim": 4000,
+                       "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (fields 604 MB)"},
+            "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d / K),
+                    "d2h_bytes_per_step": int(d2h / K), "includes": "mfd_create upload + K steps + read-back",
+                    "host_setup_s_excluded": round(t_desc, 3)},
+            "roofline": {"bound": "hbm", "kernel": "e3d_kernel (E update)", "achieved": round(e_gbs, 1),
+                         "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4), "traffic": None,
+                         "algorithmic_bytes_per_launch": e_bytes, "mean_launch_ms": round(e_ms, 5),
+                         "peak_kind": peak_kind,
+                         "h_kernel": {"achieved": round(h_gbs, 1), "frac": round(h_gbs / peak, 4),
+                                      "algorithmic_bytes_per_launch": h_bytes, "mean_launch_ms": round(h_ms, 5)}},
+            "kernels": per_kernel,
+            "gpu_launches": launches,
+            "device_bytes": dev_bytes,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def _oracle_lib():
+    from maxwellfdtd_b200 import _abi
+    so = os.path.join(ROOT, "oracle", "libmfd_oracle.so")
+    if not os.path.exists(so):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    return _abi.Library(so, "oracle_")
+
+
+def cpu_baseline(args, model, mons, steps=None):
+    """The oracle (the reference's CPU path restated in C++, OpenMP) on the same workload,
+    a bounded number of steps on all host cores."""
+    from maxwellfdtd_b200 import _abi
+    lib = _oracle_lib()
+    threads = lib.lib.oracle_set_threads(0)
+    steps = steps or args.cpu_steps
+    b, meta = model.build_desc(np.float32, mons)
+    st = _abi.Stepper(lib, b, np.float32)
+    st.run(1, 1)
+    t0 = time.perf_counter()
+    st.run(2, 1 + steps)
+    dt = time.perf_counter() - t0
+    st.close()
+    N = model.grid.Nx * model.grid.Ny * model.grid.Nz
+    return {"value": round(N * steps / dt / 1e9, 5), "unit": "Gcell-updates/s", "cores": int(threads),
+            "kind": "port", "sample": f"{steps} full steps of the {args.n}^3 workload ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    ws, rank, local = dist_setup()
+    if rank != 0:
+        return None
+    from maxwellfdtd_b200 import _abi, workloads
+    W, K = args.warmup, args.steps
+    # each step a bounded sample: full 256^3 steps on the host cores
+    nt = W + K + 2
+    model, mons = workloads.plasmonics_256(nt=nt, n=args.n)
+    lib = _oracle_lib()
+    threads = lib.lib.oracle_set_threads(0)
+    b, meta = model.build_desc(np.float32, mons)
+    st = _abi.Stepper(lib, b, np.float32)
+    st.run(1, W)
+    t0 = time.perf_counter()
+    st.run(W + 1, W + K)
+    dt = time.perf_counter() - t0
+    st.close()
+    N = model.grid.Nx * model.grid.Ny * model.grid.Nz
+    v = N * K / dt / 1e9
+    out = {"impl": "reference", "metric": "Gcell-updates/s", "value": round(v, 5), "unit": "Gcell-updates/s",
+           "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": round(dt * 1e3 / K, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "cells": N, "parallelism": "host cores"},
+           "cpu_baseline": {"value": round(v, 5), "unit": "Gcell-updates/s", "cores": int(threads), "kind": "port",
+                            "sample": f"{K} full steps of the {args.n}^3 workload after {W} warm-up steps"},
+           "e2e": {"value": round(v, 5), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        if args.steps > 20:
+            args.steps = 20   # each reference step is a full 256^3 step on the CPU
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,255 @@
+/*
+ * maxwellfdtd.h -- C ABI of the B200 FDTD time-stepper (libmaxwellfdtd_b200.so).
+ *
+ * This library replaces the time-step path of the Julia package MaxwellFDTD:
+ *
+ *   solve!(model; backend)         src/models.jl:166-242
+ *     adapt(backend, model)        src/models.jl:183        -> mfd_create
+ *     for it=1:Nt                  src/models.jl:199
+ *       step!(model, it)           src/models.jl:125-132    -> mfd_run (chunks of steps)
+ *         update_H!                src/models.jl:248-307, 450-536, 735-889
+ *         update_E!                src/models.jl:310-444, 539-726, 895-1175
+ *         add_source!              src/sources.jl:122-131, 235-244, 320-346, 469-497, 713-776
+ *       NaN/Inf guard              src/models.jl:202-209    -> MFD_ERR_NONFINITE
+ *       update_monitors!           src/outputs.jl:21-30     -> on-device monitors
+ *       update_integral_variables! src/outputs.jl:182-191, 318-327, 475-485 (fused)
+ *       write_tfsf_record          src/sources.jl:372-384, 534-550, 839-877 (on-device record)
+ *     write_fields / write_monitors / write_integral_variables read back through
+ *     mfd_read_field / mfd_read_monitor / mfd_read_integral.
+ *
+ * Conventions
+ *  - Grid arrays are dense, x fastest: cell (ix,iy,iz) (0-based) is at ix + nx*(iy + ny*iz).
+ *    This is the column-major layout of the reference's Julia arrays, so a Julia Array
+ *    passes with no transpose.  A 1-D model has nx = ny = 1 and uses z; a 2-D model
+ *    has ny = 1 and uses the x-z plane (reference Grid1D / Grid2D, src/grids.jl:182-258).
+ *  - Bulk arrays (fields, TFSF incident data, monitor outputs) are in the handle's
+ *    element type T (float for MFD_F32, double for MFD_F64).  Scalar coefficients and
+ *    the coefficient tables are passed as double and cast to T inside the library, as
+ *    the reference's adapt_storage does after computing them in Float64
+ *    (src/backends.jl:27-41).
+ *  - Step indices are 1-based, as in the reference loop `for it=1:Nt`.
+ *  - Every call returns an int status (MFD_OK = 0).  Nothing aborts or exits.  Details of
+ *    the last failure on a handle are in mfd_last_error().
+ *  - A handle is used by one host thread at a time.  Distinct handles may be driven from
+ *    different threads concurrently; each owns its CUDA stream and device memory.
+ */
+#ifndef MAXWELLFDTD_H
+#define MAXWELLFDTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define MFD_API __attribute__((visibility("default")))
+#else
+#define MFD_API
+#endif
+
+#define MFD_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------------------ */
+enum {
+    MFD_OK = 0,
+    MFD_ERR_INVALID = 1,    /* bad descriptor or argument                              */
+    MFD_ERR_OOM = 2,        /* device or host allocation failed                        */
+    MFD_ERR_CUDA = 3,       /* a CUDA runtime call failed                              */
+    MFD_ERR_NONFINITE = 4,  /* NaN or Inf found in Ex (reference models.jl:202-209)    */
+    MFD_ERR_TIMEOUT = 5,    /* a bounded host wait ran out                             */
+    MFD_ERR_ADMISSION = 6,  /* job does not fit the device-memory budget               */
+    MFD_ERR_NODEVICE = 7    /* no CUDA device available                                */
+};
+
+/* ---- element types ---------------------------------------------------------------- */
+enum { MFD_F32 = 0, MFD_F64 = 1 };
+
+/* ---- boundary conditions: the reference's bc2int codes (src/models.jl:1199-1217) ---- */
+enum { MFD_BC_PERIODIC = 1, MFD_BC_DIRICHLET = 2, MFD_BC_NEUMANN = 3 };
+
+/* ---- faces: index into bc[] and pml[] ----------------------------------------------- */
+enum { MFD_XL = 0, MFD_XR = 1, MFD_YL = 2, MFD_YR = 3, MFD_ZL = 4, MFD_ZR = 5 };
+
+/* ---- field components (the reference Field3D field order, src/fields.jl:67-90) ------ */
+enum {
+    MFD_HX = 0, MFD_HY = 1, MFD_HZ = 2,
+    MFD_DX = 3, MFD_DY = 4, MFD_DZ = 5,
+    MFD_EX = 6, MFD_EY = 7, MFD_EZ = 8
+};
+
+/* ---- integral outputs (reference Output.Sa/E2, model.JE, rho_end: outputs.jl:46-65) -- */
+enum { MFD_INT_SA = 0, MFD_INT_E2 = 1, MFD_INT_JE = 2, MFD_INT_RHO = 3 };
+
+/* ---- sources ------------------------------------------------------------------------ */
+enum { MFD_SRC_SOFT = 0, MFD_SRC_HARD = 1 };
+
+/* ---- monitors ----------------------------------------------------------------------- */
+enum { MFD_MON_FIELD = 0, MFD_MON_SPECTRAL = 1 };
+
+/* ---- plasma ionisation-rate closures (reference Plasma.ionrate, models.jl:1117) ------ */
+enum {
+    MFD_RATE_NONE = 0,
+    /* R(I) = 10^(order*log10(I) + log10c): the MPI form of
+       examples/5_nonlinear_propagation/3D_plasma.jl:67.  order*log10(I) is evaluated in T,
+       the sum and the power in double, as Julia's promotion does for that closure. */
+    MFD_RATE_POWER = 1,
+    /* log-log table, equally spaced log10(I) knots (IonizationRate.jl:13-52), in T. */
+    MFD_RATE_TABLE = 2
+};
+
+/* ---- TFSF incident-data arrays ----------------------------------------------------------
+ * 3-D: the 24 arrays of TFSFSource3D in its field order (src/sources.jl:556-587):
+ *   face 1yz: incHy, incHz, incEy, incEz;  face 2yz: same;  face x1z: incHx, incHz, incEx,
+ *   incEz;  face x2z: same;  face xy1: incHx, incHy, incEx, incEy;  face xy2: same.
+ * 2-D: the 8 arrays of TFSFSource2D (sources.jl:390-403):
+ *   1z: incHy, incEz; 2z: incHy, incEz; x1: incHy, incEx; x2: incHy, incEx.
+ * 1-D: the 4 arrays of TFSFSource1D (sources.jl:272-279): incHy_1, incEx_1, incHy_2, incEx_2.
+ * Each array is [nt][face extent] in T, the face extent laid out as in the reference
+ * (column-major (a, b, Nt) => C order [nt][b][a]). */
+#define MFD_TFSF_MAX_ARRAYS 24
+
+/* One CPML layer profile (reference PMLLayer, src/pml.jl:46-121).  nb = 0: no layer. */
+typedef struct mfd_pml_layer {
+    int32_t ib;        /* 1-based boundary index (PMLLayer.ib)                       */
+    int32_t nb;        /* number of grid points in the layer (PMLLayer.Nb)           */
+    const double* K;   /* [nb] kappa                                                 */
+    const double* A;   /* [nb]                                                       */
+    const double* B;   /* [nb]                                                       */
+} mfd_pml_layer;
+
+/* Per-material update coefficients (reference MaterialStruct3D, src/materials.jl:335-483). */
+typedef struct mfd_material {
+    double Mh, Me, Md1, Md2;
+    int32_t nq;                          /* ADE poles; 0 = no dispersion               */
+    const double* Aq;                    /* [nq]                                       */
+    const double* Bq;
+    const double* Cq;
+    int32_t kerr;                        /* iskerr                                     */
+    double Mk2, Mk3;
+    int32_t plasma;                      /* isplasma                                   */
+    double Rava, ksi, rho0, Ap, Bp, Cp, Ma;
+    int32_t rate_kind;                   /* MFD_RATE_*                                 */
+    double rate_order, rate_log10c;      /* MFD_RATE_POWER                             */
+    int32_t rate_n;                      /* MFD_RATE_TABLE: knots                      */
+    const double* rate_x;                /* [rate_n] log10(I), equally spaced          */
+    const double* rate_y;                /* [rate_n] log10(R)                          */
+} mfd_material;
+
+/* A soft or hard source (reference SoftSourceStruct / HardSourceStruct, sources.jl:41-244).
+ * The host has already redirected E components to D with coeff = EPS0 (sources.jl:61-69).
+ * The waveform is tabulated on the host in double: either wave[it][p] (general) or
+ * amp[p] * gt[it] (separable). */
+typedef struct mfd_source {
+    int32_t kind;            /* MFD_SRC_SOFT / MFD_SRC_HARD                          */
+    int32_t comp;            /* MFD_HX .. MFD_EZ                                     */
+    double coeff;            /* soft sources: FC += coeff * w                        */
+    int64_t npts;
+    const int64_t* cells;    /* [npts] 0-based linear cell indices                   */
+    const double* wave;      /* [nt][npts] or NULL                                   */
+    const double* amp;       /* [npts] when wave == NULL                             */
+    const double* gt;        /* [nt]   when wave == NULL                             */
+} mfd_source;
+
+/* TFSF replay source (reference TFSFSource{1,2,3}D + add_source!, sources.jl:272-776). */
+typedef struct mfd_tfsf {
+    int32_t enabled;
+    int32_t order;           /* point sources applied before it (sources act in tuple
+                                order, models.jl:128-130)                              */
+    int32_t i1[3];           /* 1-based (ix1, iy1, iz1)                               */
+    int32_t i2[3];           /* 1-based (ix2, iy2, iz2)                               */
+    const void* inc[MFD_TFSF_MAX_ARRAYS];
+} mfd_tfsf;
+
+/* Field or spectral monitor (reference monitors.jl:7-373, dft.jl:1-51). */
+typedef struct mfd_monitor {
+    int32_t kind;            /* MFD_MON_FIELD / MFD_MON_SPECTRAL                      */
+    int32_t sum;             /* issum                                                 */
+    int64_t npts;
+    const int64_t* cells;    /* [npts] 0-based linear cell indices                    */
+    int32_t nw;              /* spectral: number of frequencies                       */
+    const double* phasor;    /* spectral: [nt][nw][2] = exp(-i w (t_it - tshift))     */
+} mfd_monitor;
+
+/* Complete description of one model (reference Model, src/models.jl:1-122). */
+typedef struct mfd_desc {
+    int32_t abi_version;     /* MFD_ABI_VERSION                                       */
+    int32_t ndim;            /* 1, 2 or 3                                             */
+    int32_t dtype;           /* MFD_F32 / MFD_F64                                     */
+    int32_t nx, ny, nz;
+    double dx, dy, dz;
+    double dt;               /* time step (Float64 value; cast to T inside)           */
+    int64_t nt;              /* number of steps Nt                                    */
+    int32_t bc[6];           /* MFD_BC_* per face                                     */
+    mfd_pml_layer pml[6];    /* per face                                              */
+    double Mh0, Me0, Md10, Md20;   /* vacuum coefficients (models.jl:111-114)         */
+    const uint8_t* geometry; /* [nx*ny*nz] material index, 0 = vacuum; NULL = vacuum  */
+    int32_t nmat;            /* materials 1..nmat                                     */
+    const mfd_material* mats;
+    int32_t rho_fp64;        /* plasma density rho/drho kept in double for MFD_F32     */
+    int32_t nsrc;
+    const mfd_source* srcs;
+    mfd_tfsf tfsf;
+    int32_t nmon;
+    const mfd_monitor* mons;
+    int32_t tfsf_record;     /* record incident faces (prepare/write_tfsf_record)     */
+    int32_t rec_i1[3];       /* 1-based record box                                   */
+    int32_t rec_i2[3];
+    int32_t device;          /* CUDA device ordinal                                   */
+} mfd_desc;
+
+typedef struct mfd_handle mfd_handle;
+
+/* Model setup and device upload (replaces adapt(backend, model), models.jl:183). */
+MFD_API int mfd_create(const mfd_desc* desc, mfd_handle** out);
+MFD_API void mfd_destroy(mfd_handle* h);
+
+/* Run steps it_first..it_last (1-based, inclusive, consecutive with the previous call).
+ * Per step: update_H!, update_E!, add_source! for each source, then monitors, the
+ * integral sums and the TFSF record -- the reference's per-step order
+ * (models.jl:125-132, 199-234).  The NaN/Inf guard of models.jl:202-209 is evaluated on
+ * the device; MFD_ERR_NONFINITE is returned at the end of the call with the first bad
+ * step in mfd_status(). */
+MFD_API int mfd_run(mfd_handle* h, int64_t it_first, int64_t it_last);
+
+/* Number of steps completed and the first step whose Ex held NaN (bit 0) or Inf (bit 1). */
+MFD_API int mfd_status(const mfd_handle* h, int64_t* steps_done, int64_t* bad_step, int32_t* bad_kind);
+
+/* Dense field component (MFD_HX..MFD_EZ) to/from host memory, nx*ny*nz elements of T. */
+MFD_API int mfd_read_field(mfd_handle* h, int32_t comp, void* dst);
+MFD_API int mfd_write_field(mfd_handle* h, int32_t comp, const void* src);
+
+/* Integral outputs: Sa, E2, JE as nx*ny*nz of T; rho_end (sum over plasma materials of
+ * rho*rho0) as nx*ny*nz double. */
+MFD_API int mfd_read_integral(mfd_handle* h, int32_t which, void* dst);
+
+/* Monitor m, component comp.  Field monitor: T [nt][npts] ([nt] when sum).  Spectral
+ * monitor: double complex [nw][npts] ([nw] when sum) as interleaved (re, im). */
+MFD_API int mfd_read_monitor(mfd_handle* h, int32_t m, int32_t comp, void* dst);
+
+/* TFSF record array k (same order and layout as mfd_tfsf.inc), T [nt][face extent]. */
+MFD_API int mfd_read_tfsf_record(mfd_handle* h, int32_t k, void* dst);
+/* Element count of TFSF array k for the record box (0 if k is unused). */
+MFD_API int64_t mfd_tfsf_record_size(const mfd_handle* h, int32_t k);
+
+/* Device-time measurement: when on, every kernel launch of mfd_run is bracketed by CUDA
+ * events on the handle's stream and its duration is summed per kernel class. */
+MFD_API int mfd_set_profiling(mfd_handle* h, int32_t on);
+/* Kernel classes: 0 H update, 1 E update, 2 sources, 3 TFSF, 4 monitors, 5 DFT,
+ * 6 sums flush.  Fills ms[k], launches[k] for k < n; returns the number of classes. */
+MFD_API int mfd_kernel_times(const mfd_handle* h, double* ms, int64_t* launches, int32_t n);
+/* Device time of the last mfd_run call (CUDA events around the whole call), in ms. */
+MFD_API int mfd_last_run_ms(const mfd_handle* h, double* ms);
+/* Device bytes held by the handle. */
+MFD_API int64_t mfd_device_bytes(const mfd_handle* h);
+
+MFD_API const char* mfd_last_error(const mfd_handle* h);
+/* Error text of the last failed mfd_create (no handle exists then). */
+MFD_API const char* mfd_create_error(void);
+MFD_API int mfd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MAXWELLFDTD_H */

@@ -1,0 +1,218 @@
+"""ctypes mirror of include/maxwellfdtd.h and a thin wrapper over any library that exports
+that API under a symbol prefix (``mfd_`` for the CUDA library)."""
+import ctypes as C
+import os
+
+import numpy as np
+
+ABI_VERSION = 1
+
+MFD_OK, MFD_ERR_INVALID, MFD_ERR_OOM, MFD_ERR_CUDA, MFD_ERR_NONFINITE, MFD_ERR_TIMEOUT, \
+    MFD_ERR_ADMISSION, MFD_ERR_NODEVICE = range(8)
+MFD_F32, MFD_F64 = 0, 1
+MFD_INT_SA, MFD_INT_E2, MFD_INT_JE, MFD_INT_RHO = range(4)
+MFD_RATE_NONE, MFD_RATE_POWER, MFD_RATE_TABLE = range(3)
+
+_dp = C.POINTER(C.c_double)
+
+
+class PmlLayer(C.Structure):
+    _fields_ = [("ib", C.c_int32), ("nb", C.c_int32), ("K", _dp), ("A", _dp), ("B", _dp)]
+
+
+class Material(C.Structure):
+    _fields_ = [("Mh", C.c_double), ("Me", C.c_double), ("Md1", C.c_double), ("Md2", C.c_double),
+                ("nq", C.c_int32), ("Aq", _dp), ("Bq", _dp), ("Cq", _dp),
+                ("kerr", C.c_int32), ("Mk2", C.c_double), ("Mk3", C.c_double),
+                ("plasma", C.c_int32),
+                ("Rava", C.c_double), ("ksi", C.c_double), ("rho0", C.c_double), ("Ap", C.c_double),
+                ("Bp", C.c_double), ("Cp", C.c_double), ("Ma", C.c_double),
+                ("rate_kind", C.c_int32), ("rate_order", C.c_double), ("rate_log10c", C.c_double),
+                ("rate_n", C.c_int32), ("rate_x", _dp), ("rate_y", _dp)]
+
+
+class Source(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("comp", C.c_int32), ("coeff", C.c_double),
+                ("npts", C.c_int64), ("cells", C.POINTER(C.c_int64)),
+                ("wave", _dp), ("amp", _dp), ("gt", _dp)]
+
+
+class Tfsf(C.Structure):
+    _fields_ = [("enabled", C.c_int32), ("order", C.c_int32), ("i1", C.c_int32 * 3), ("i2", C.c_int32 * 3),
+                ("inc", C.c_void_p * 24)]
+
+
+class Monitor(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("sum", C.c_int32), ("npts", C.c_int64),
+                ("cells", C.POINTER(C.c_int64)), ("nw", C.c_int32), ("phasor", _dp)]
+
+
+class Desc(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("ndim", C.c_int32), ("dtype", C.c_int32),
+                ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+                ("dt", C.c_double), ("nt", C.c_int64),
+                ("bc", C.c_int32 * 6), ("pml", PmlLayer * 6),
+                ("Mh0", C.c_double), ("Me0", C.c_double), ("Md10", C.c_double), ("Md20", C.c_double),
+                ("geometry", C.POINTER(C.c_uint8)),
+                ("nmat", C.c_int32), ("mats", C.POINTER(Material)),
+                ("rho_fp64", C.c_int32),
+                ("nsrc", C.c_int32), ("srcs", C.POINTER(Source)),
+                ("tfsf", Tfsf),
+                ("nmon", C.c_int32), ("mons", C.POINTER(Monitor)),
+                ("tfsf_record", C.c_int32), ("rec_i1", C.c_int32 * 3), ("rec_i2", C.c_int32 * 3),
+                ("device", C.c_int32)]
+
+
+def dptr(a):
+    """double* of a contiguous float64 array (None -> NULL)."""
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+class DescBuilder:
+    """Owns every array the descriptor points to (keep it alive while the library reads it)."""
+
+    def __init__(self):
+        self.keep = []
+        self.desc = Desc()
+
+    def arr(self, a, dtype):
+        a = np.ascontiguousarray(a, dtype=dtype)
+        self.keep.append(a)
+        return a
+
+
+class StepperError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class Library:
+    """A loaded library exporting the maxwellfdtd C API with symbol prefix ``prefix``."""
+
+    def __init__(self, path, prefix="mfd_"):
+        self.path = os.path.abspath(path)
+        self.lib = C.CDLL(self.path, mode=C.RTLD_GLOBAL)
+        self.prefix = prefix
+        L, p = self.lib, prefix
+        vp = C.c_void_p
+
+        def fn(name, res, args):
+            f = getattr(L, p + name)
+            f.restype = res
+            f.argtypes = args
+            return f
+
+        self.create = fn("create", C.c_int, [C.POINTER(Desc), C.POINTER(vp)])
+        self.destroy = fn("destroy", None, [vp])
+        self.run = fn("run", C.c_int, [vp, C.c_int64, C.c_int64])
+        self.read_field = fn("read_field", C.c_int, [vp, C.c_int32, vp])
+        self.write_field = fn("write_field", C.c_int, [vp, C.c_int32, vp])
+        self.read_integral = fn("read_integral", C.c_int, [vp, C.c_int32, vp])
+        self.read_monitor = fn("read_monitor", C.c_int, [vp, C.c_int32, C.c_int32, vp])
+        self.read_tfsf_record = fn("read_tfsf_record", C.c_int, [vp, C.c_int32, vp])
+        self.tfsf_record_size = fn("tfsf_record_size", C.c_int64, [vp, C.c_int32])
+        self.status = fn("status", C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32)])
+        self.last_error = fn("last_error", C.c_char_p, [vp])
+        self.create_error = fn("create_error", C.c_char_p, [])
+        # device-side measurement entry points (CUDA library only)
+        self.has_timing = hasattr(L, p + "set_profiling")
+        if self.has_timing:
+            self.set_profiling = fn("set_profiling", C.c_int, [vp, C.c_int32])
+            self.kernel_times = fn("kernel_times", C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int32])
+            self.last_run_ms = fn("last_run_ms", C.c_int, [vp, C.POINTER(C.c_double)])
+            self.device_bytes = fn("device_bytes", C.c_int64, [vp])
+
+
+class Stepper:
+    """One model instance in a library (the handle)."""
+
+    def __init__(self, lib, builder, dtype):
+        self.lib = lib
+        self.builder = builder
+        self.dtype = np.dtype(dtype)
+        d = builder.desc
+        self.shape3 = (d.nx, d.ny, d.nz)
+        self.N = d.nx * d.ny * d.nz
+        h = C.c_void_p()
+        st = lib.create(C.byref(d), C.byref(h))
+        if st != MFD_OK:
+            raise StepperError(st, f"create failed ({st}): {lib.create_error().decode()}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != MFD_OK:
+            raise StepperError(st, self.lib.last_error(self.h).decode())
+
+    def run(self, a, b):
+        self._check(self.lib.run(self.h, int(a), int(b)))
+
+    def status(self):
+        d, b, k = C.c_int64(), C.c_int64(), C.c_int32()
+        self.lib.status(self.h, C.byref(d), C.byref(b), C.byref(k))
+        return d.value, b.value, k.value
+
+    def read_field(self, comp):
+        out = np.empty(self.N, dtype=self.dtype)
+        self._check(self.lib.read_field(self.h, int(comp), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def write_field(self, comp, values):
+        v = np.ascontiguousarray(values, dtype=self.dtype).ravel()
+        assert v.size == self.N
+        self._check(self.lib.write_field(self.h, int(comp), v.ctypes.data_as(C.c_void_p)))
+
+    def read_integral(self, which):
+        dt = np.float64 if which == MFD_INT_RHO else self.dtype
+        out = np.empty(self.N, dtype=dt)
+        self._check(self.lib.read_integral(self.h, int(which), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def read_monitor(self, m, comp, shape, spectral):
+        if spectral:
+            out = np.empty(shape, dtype=np.complex128)
+        else:
+            out = np.empty(shape, dtype=self.dtype)
+        self._check(self.lib.read_monitor(self.h, int(m), int(comp), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    KERNEL_CLASSES = ("H", "E", "sources", "tfsf", "monitors", "dft", "sums")
+
+    def set_profiling(self, on):
+        self._check(self.lib.set_profiling(self.h, int(bool(on))))
+
+    def kernel_times(self):
+        n = len(self.KERNEL_CLASSES)
+        ms = (C.c_double * n)()
+        cnt = (C.c_int64 * n)()
+        self.lib.kernel_times(self.h, ms, cnt, n)
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def last_run_ms(self):
+        v = C.c_double()
+        self._check(self.lib.last_run_ms(self.h, C.byref(v)))
+        return v.value
+
+    def device_bytes(self):
+        return int(self.lib.device_bytes(self.h))
+
+    def read_tfsf_record(self, k):
+        n = self.lib.tfsf_record_size(self.h, int(k))
+        out = np.empty(n, dtype=self.dtype)
+        self._check(self.lib.read_tfsf_record(self.h, int(k), out.ctypes.data_as(C.c_void_p)))
+        return out

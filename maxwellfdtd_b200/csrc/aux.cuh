@@ -1,0 +1,266 @@
+// aux.cuh -- per-step kernels around the Yee updates: point sources, TFSF injection, TFSF
+// record, monitors and the DFT accumulation.
+#pragma once
+
+#include "mfd_device.cuh"
+
+namespace mfd {
+
+// ------------------------------------------------------------------------------------------
+// Soft / hard point sources (sources.jl:77-131, 190-244).  The waveform is tabulated in
+// double; the add is done in double and rounded to T as the reference's mixed-type
+// expression FC + coeff*waveform(...) is.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) point_source_kernel(T* F, const long long* __restrict__ cells, long long npts,
+                                                           const double* __restrict__ wave, const double* __restrict__ amp,
+                                                           const double* __restrict__ gt, long long it0, int kind, T coeff) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= npts) return;
+    const double w = wave ? wave[it0 * npts + i] : amp[i] * gt[it0];
+    const long long c = cells[i];
+    if (kind == MFD_SRC_SOFT) F[c] = (T)((double)F[c] + (double)coeff * w);
+    else F[c] = (T)w;
+}
+
+// ------------------------------------------------------------------------------------------
+// Rectangle statements: F[comp][rect] op= coef * inc[k][it][local]  (TFSF add_source!,
+// sources.jl:320-346, 469-497, 713-776) or rec[k][it][local] = F[comp][rect] (TFSF record,
+// sources.jl:372-384, 534-550, 839-877).  Rectangles are 0-based inclusive.
+// ------------------------------------------------------------------------------------------
+#define MFD_MAX_STMT 36
+
+struct RectStmt {
+    int comp;
+    int x0, x1, y0, y1, z0, z1;
+    int k;            // incident / record array
+    int sign;         // +1 add, -1 subtract
+    int tprec;        // 1: coefficient and product in T; 0: in double
+    double coef;
+    double coefT;     // T-rounded coefficient for tprec
+    long long start;  // first work item of this statement
+    long long len;    // rectangle size (= array length per step)
+};
+
+template <typename T>
+struct RectParams {
+    int n;
+    long long total;
+    long long it0;    // 0-based step
+    Layout L;
+    T* F[9];
+    T* arr[24];       // TFSF: incident arrays; record: destination arrays
+    RectStmt s[MFD_MAX_STMT];
+};
+
+__device__ __forceinline__ bool rect_has(const RectStmt& s, int ix, int iy, int iz) {
+    return ix >= s.x0 && ix <= s.x1 && iy >= s.y0 && iy <= s.y1 && iz >= s.z0 && iz <= s.z1;
+}
+
+__device__ __forceinline__ long long rect_local(const RectStmt& s, int ix, int iy, int iz) {
+    const long long nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
+    return (ix - s.x0) + nxr * ((iy - s.y0) + nyr * (long long)(iz - s.z0));
+}
+
+// One thread per (statement, cell).  A cell reached by several statements of the same
+// component (edges of the 3-D TFSF box) is updated by the thread of its first statement,
+// which applies all of them in statement order -- the order of the reference's broadcasts.
+template <typename T>
+__global__ void __launch_bounds__(256) tfsf_kernel(const __grid_constant__ RectParams<T> p) {
+    const long long item = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (item >= p.total) return;
+    int si = 0;
+    while (si + 1 < p.n && p.s[si + 1].start <= item) ++si;
+    const RectStmt& s = p.s[si];
+    const long long local = item - s.start;
+    const long long nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
+    const int ix = s.x0 + (int)(local % nxr);
+    const long long rest = local / nxr;
+    const int iy = s.y0 + (int)(rest % nyr);
+    const int iz = s.z0 + (int)(rest / nyr);
+    for (int j = 0; j < si; ++j)
+        if (p.s[j].comp == s.comp && rect_has(p.s[j], ix, iy, iz)) return;
+    T* F = p.F[s.comp];
+    const long long c = ix + (long long)p.L.px * iy + p.L.sz * iz;
+    T v = F[c];
+    for (int j = si; j < p.n; ++j) {
+        const RectStmt& t = p.s[j];
+        if (t.comp != s.comp || !rect_has(t, ix, iy, iz)) continue;
+        const T inc = p.arr[t.k][p.it0 * t.len + rect_local(t, ix, iy, iz)];
+        if (t.tprec) {
+            const T u = (T)t.coefT * inc;
+            v = t.sign > 0 ? v + u : v - u;
+        } else {
+            const double u = t.coef * (double)inc;
+            v = (T)(t.sign > 0 ? (double)v + u : (double)v - u);
+        }
+    }
+    F[c] = v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) record_kernel(const __grid_constant__ RectParams<T> p) {
+    const long long item = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (item >= p.total) return;
+    int si = 0;
+    while (si + 1 < p.n && p.s[si + 1].start <= item) ++si;
+    const RectStmt& s = p.s[si];
+    const long long local = item - s.start;
+    const long long nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
+    const int ix = s.x0 + (int)(local % nxr);
+    const long long rest = local / nxr;
+    const int iy = s.y0 + (int)(rest % nyr);
+    const int iz = s.z0 + (int)(rest / nyr);
+    const long long c = ix + (long long)p.L.px * iy + p.L.sz * iz;
+    p.arr[s.k][p.it0 * s.len + local] = p.F[s.comp][c];
+}
+
+// ------------------------------------------------------------------------------------------
+// Monitors (monitors.jl, dft.jl).  Every step the gather kernel copies each monitor's point
+// values: field monitors without sum go straight to their full history [comp][nt][npts];
+// summed field monitors and spectral monitors go to a staging ring [slot][comp][npts] that
+// a flush kernel consumes every K steps.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+struct MonDev {
+    int kind, sum, nw;
+    long long npts;
+    const long long* cells;   // padded cell indices
+    T* hist;                  // field, no sum: [ncomp][nt][npts]; field sum: [ncomp][nt]
+    T* ring;                  // staging [K][ncomp][npts]
+    double2* S;               // spectral: [ncomp][nw][npts] or [ncomp][nw]
+    const double2* phasor;    // [nt][nw]  exp(-i w (t - tshift))
+    long long start;          // first gather item
+};
+
+template <typename T>
+struct MonParams {
+    int nmon, ncomp;
+    long long total, nt;
+    T* comp[6];               // field arrays of the monitored components
+    const MonDev<T>* mons;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) monitor_gather_kernel(const MonParams<T> p, long long it0, int slot) {
+    const long long item = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (item >= p.total) return;
+    int m = 0;
+    while (m + 1 < p.nmon && p.mons[m + 1].start <= item) ++m;
+    const MonDev<T>& M = p.mons[m];
+    const long long local = item - M.start;
+    const int k = (int)(local / M.npts);
+    const long long j = local - (long long)k * M.npts;
+    const T v = p.comp[k][M.cells[j]];
+    if (M.kind == MFD_MON_FIELD && !M.sum) M.hist[((long long)k * p.nt + it0) * M.npts + j] = v;
+    else M.ring[((long long)slot * p.ncomp + k) * M.npts + j] = v;
+}
+
+// Summed field monitor: hist[k][it] = sum over points (block reduction in T).
+template <typename T>
+__global__ void __launch_bounds__(256) monitor_fieldsum_kernel(const MonDev<T>* __restrict__ mon, int ncomp, long long nt,
+                                                               long long it0_first) {
+    __shared__ T red[256];
+    const MonDev<T>& M = *mon;
+    const int k = blockIdx.x, slot = blockIdx.y;
+    const T* src = M.ring + ((long long)slot * ncomp + k) * M.npts;
+    T acc = T(0);
+    for (long long j = threadIdx.x; j < M.npts; j += blockDim.x) acc += src[j];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) M.hist[(long long)k * nt + it0_first + slot] = red[0];
+}
+
+// Spectral monitor, per point: S[k][w][j] += F * (2 e_w(t) dt) for each staged step in
+// order (dft.jl:560-566).  A thread owns MFD_DFT_W frequencies of one point.
+#define MFD_DFT_W 8
+template <typename T>
+__global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __restrict__ mon, int ncomp, int nslots,
+                                                          long long it0_first, double dt) {
+    const MonDev<T>& M = *mon;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    const int w0 = blockIdx.z * MFD_DFT_W;
+    if (j >= M.npts) return;
+    const int nw = M.nw;
+    const int wn = min(MFD_DFT_W, nw - w0);
+    double sr[MFD_DFT_W], si[MFD_DFT_W];
+    double2* S = M.S + ((long long)k * nw + w0) * M.npts + j;
+#pragma unroll
+    for (int w = 0; w < MFD_DFT_W; ++w)
+        if (w < wn) { const double2 s = S[(long long)w * M.npts]; sr[w] = s.x; si[w] = s.y; }
+    for (int slot = 0; slot < nslots; ++slot) {
+        const double f = (double)M.ring[((long long)slot * ncomp + k) * M.npts + j];
+        const double2* e = M.phasor + (it0_first + slot) * nw + w0;
+#pragma unroll
+        for (int w = 0; w < MFD_DFT_W; ++w) {
+            if (w < wn) {
+                const double2 ew = e[w];
+                const double tr = (2 * ew.x) * dt, ti = (2 * ew.y) * dt;
+                sr[w] = sr[w] + f * tr;
+                si[w] = si[w] + f * ti;
+            }
+        }
+    }
+#pragma unroll
+    for (int w = 0; w < MFD_DFT_W; ++w)
+        if (w < wn) S[(long long)w * M.npts] = make_double2(sr[w], si[w]);
+}
+
+// Spectral monitor with sum: S[k][w] += 2 * sum_j(F_j e_w(t)) * dt (dft.jl:556-559).
+template <typename T>
+__global__ void __launch_bounds__(256) monitor_dftsum_kernel(const MonDev<T>* __restrict__ mon, int ncomp, int nslots,
+                                                             long long it0_first, double dt) {
+    __shared__ double rr[256], ri[256];
+    const MonDev<T>& M = *mon;
+    const int k = blockIdx.x, w = blockIdx.y;
+    double2 S = M.S[(long long)k * M.nw + w];
+    for (int slot = 0; slot < nslots; ++slot) {
+        const double2 e = M.phasor[(it0_first + slot) * M.nw + w];
+        const T* src = M.ring + ((long long)slot * ncomp + k) * M.npts;
+        double ar = 0, ai = 0;
+        for (long long j = threadIdx.x; j < M.npts; j += blockDim.x) {
+            const double f = (double)src[j];
+            ar += f * e.x;
+            ai += f * e.y;
+        }
+        rr[threadIdx.x] = ar;
+        ri[threadIdx.x] = ai;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) { rr[threadIdx.x] += rr[threadIdx.x + s]; ri[threadIdx.x] += ri[threadIdx.x + s]; }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            S.x = S.x + (2 * rr[0]) * dt;
+            S.y = S.y + (2 * ri[0]) * dt;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) M.S[(long long)k * M.nw + w] = S;
+}
+
+// ------------------------------------------------------------------------------------------
+// Material state -> dense outputs: JE (T) and rho_end = rho*rho0 (double) (outputs.jl:46-65)
+// ------------------------------------------------------------------------------------------
+template <typename T, typename R>
+__global__ void __launch_bounds__(256) scatter_state_kernel(const MatDev<T, R>* __restrict__ mats, const uint8_t* __restrict__ geom,
+                                                            Layout L, void* out, int which) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y, iz = blockIdx.z;
+    if (ix >= L.nx) return;
+    const long long c = ix + (long long)L.px * iy + L.sz * iz;
+    const int g = geom[c];
+    const MatDev<T, R>* m = g ? mats + (g - 1) : nullptr;
+    const bool pl = m && m->plasma;
+    long long bi = 0;
+    if (pl) bi = (long long)(ix - m->bx0) + (long long)m->bnx * ((long long)(iy - m->by0) + (long long)m->bny * (iz - m->bz0));
+    if (which == MFD_INT_JE) ((T*)out)[c] = pl ? m->JE[bi] : T(0);
+    else ((double*)out)[c] = pl ? 0.0 + (double)(m->rho[bi] * m->rho0) : 0.0;
+}
+
+}  // namespace mfd

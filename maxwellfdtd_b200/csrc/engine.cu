@@ -1,0 +1,1048 @@
+// engine.cu -- the handle behind the C ABI (include/maxwellfdtd.h): device memory, the
+// per-step launch sequence and host<->device transfers.
+//
+// Per step it (reference order, models.jl:125-132 and 199-234):
+//   H update  [+ Sa/E2 and NaN/Inf guard of step it-1]        h?d_kernel
+//   E update  (CPML, ADE, plasma, Kerr fused)                 e?d_kernel
+//   sources in tuple order (point sources, TFSF)             point_source_kernel, tfsf_kernel
+//   monitors                                                  monitor_gather_kernel (+ flush)
+//   TFSF record                                               record_kernel
+// and after the last step of a run: Sa/E2 + guard of that step (sums_kernel).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "aux.cuh"
+#include "yee.cuh"
+
+namespace mfd {
+
+constexpr double EPS0 = 8.8541878128e-12;
+constexpr double MU0 = 1.25663706212e-6;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define MFD_CK(call)                                                                              \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            throw ::mfd::Error(e_ == cudaErrorMemoryAllocation ? MFD_ERR_OOM : MFD_ERR_CUDA,      \
+                               std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+enum { KC_H = 0, KC_E, KC_SRC, KC_TFSF, KC_MON, KC_DFT, KC_SUMS, KC_N };
+
+struct HandleBase {
+    std::string err;
+    virtual ~HandleBase() = default;
+    virtual int run(int64_t a, int64_t b) = 0;
+    virtual int read_field(int comp, void* dst) = 0;
+    virtual int write_field(int comp, const void* src) = 0;
+    virtual int read_integral(int which, void* dst) = 0;
+    virtual int read_monitor(int m, int comp, void* dst) = 0;
+    virtual int read_record(int k, void* dst) = 0;
+    virtual int64_t record_size(int k) const = 0;
+    virtual void status(int64_t* d, int64_t* b, int32_t* k) const = 0;
+    virtual void set_profiling(bool on) = 0;
+    virtual int kernel_times(double* ms, int64_t* launches, int n) const = 0;
+    virtual double last_run_ms() const = 0;
+    virtual int64_t device_bytes() const = 0;
+};
+
+static double wait_timeout_s() {
+    const char* s = std::getenv("MFD_WAIT_TIMEOUT_S");
+    double v = s ? std::atof(s) : 0.0;
+    return v > 0 ? v : 3600.0;
+}
+
+// Bounded wait on a stream: polls instead of blocking so a run that does not finish turns
+// into MFD_ERR_TIMEOUT rather than a hung host thread.
+static void bounded_sync(cudaStream_t st) {
+    auto t0 = std::chrono::steady_clock::now();
+    const double limit = wait_timeout_s();
+    int spins = 0;
+    while (true) {
+        cudaError_t e = cudaStreamQuery(st);
+        if (e == cudaSuccess) return;
+        if (e != cudaErrorNotReady) throw Error(MFD_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+        double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit) throw Error(MFD_ERR_TIMEOUT, "device work did not finish within the wait limit");
+        if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(spins > 1000 ? 200 : 20));
+    }
+}
+
+static long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
+
+template <typename T, typename R>
+class Engine : public HandleBase {
+   public:
+    int ndim = 0, nx = 0, ny = 0, nz = 0, px = 0, dev = 0;
+    long long sz = 0, Np = 0, N = 0;
+    int64_t nt = 0;
+    T dx{}, dy{}, dz{}, dt{};
+    int bc[6] = {1, 1, 1, 1, 1, 1};
+    cudaStream_t st = nullptr;
+    std::vector<void*> allocs;
+    int64_t bytes = 0;
+
+    T* F[9] = {};
+    T* Sa = nullptr;
+    T* E2 = nullptr;
+    uint8_t* geom = nullptr;
+    bool any_geom = false, math_needed = false;
+    LayerDev<T> lay[6] = {};
+    T Mh0{}, Me0{}, Md10{}, Md20{};
+    int nmat = 0;
+    T* matMh = nullptr;
+    MatDev<T, R>* mats_dev = nullptr;
+    std::vector<MatDev<T, R>> mats_host;
+    bool any_plasma = false;
+
+    struct Src {
+        int kind, comp;
+        T coeff;
+        long long npts;
+        long long* cells;
+        double* wave;
+        double* amp;
+        double* gt;
+    };
+    std::vector<Src> srcs;
+    bool tfsf = false;
+    int tfsf_order = 0;
+    RectParams<T> tfsf_p{};
+    bool record = false;
+    RectParams<T> rec_p{};
+    int rec_narr = 0;
+
+    // monitors
+    int ncomp_mon = 0;
+    int mon_comps[6] = {};
+    std::vector<MonDev<T>> mons_host;
+    MonDev<T>* mons_dev = nullptr;
+    MonParams<T> mon_p{};
+    int ring_k = 0, ring_used = 0;
+    long long ring_first = 0;
+    bool need_ring = false;
+
+    int* d_flag = nullptr;
+    unsigned long long* d_bad = nullptr;
+    int* h_flag = nullptr;
+    unsigned long long* h_bad = nullptr;
+
+    int64_t done = 0, bad_step = 0;
+    int32_t bad_kind = 0;
+
+    // launch shapes
+    int bx3 = 32, by3 = 8, zc3 = 16;
+
+    // timing
+    bool profiling = false;
+    double k_ms[KC_N] = {};
+    int64_t k_n[KC_N] = {};
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pend;
+    std::vector<cudaEvent_t> ev_pool;
+    cudaEvent_t run_ev[2] = {nullptr, nullptr};
+    double run_ms = 0;
+
+    ~Engine() override {
+        cudaSetDevice(dev);
+        if (st) cudaStreamSynchronize(st);
+        for (void* p : allocs) cudaFree(p);
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        for (auto& pe : pend) { cudaEventDestroy(pe.second.first); cudaEventDestroy(pe.second.second); }
+        if (run_ev[0]) cudaEventDestroy(run_ev[0]);
+        if (run_ev[1]) cudaEventDestroy(run_ev[1]);
+        if (h_flag) cudaFreeHost(h_flag);
+        if (h_bad) cudaFreeHost(h_bad);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    template <typename U>
+    U* dalloc(size_t n) {
+        if (n == 0) n = 1;
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, n * sizeof(U));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(MFD_ERR_OOM, "cudaMalloc of " + std::to_string(n * sizeof(U)) + " bytes failed: " + cudaGetErrorString(e));
+        }
+        allocs.push_back(p);
+        bytes += (int64_t)(n * sizeof(U));
+        MFD_CK(cudaMemsetAsync(p, 0, n * sizeof(U), st));
+        return (U*)p;
+    }
+
+    template <typename U>
+    U* upload(const U* h, size_t n) {
+        U* d = dalloc<U>(n);
+        if (n) MFD_CK(cudaMemcpyAsync(d, h, n * sizeof(U), cudaMemcpyHostToDevice, st));
+        MFD_CK(cudaStreamSynchronize(st));   // the host buffer may be a temporary
+        return d;
+    }
+
+    template <typename U>
+    U* upload_cast(const double* h, size_t n) {
+        std::vector<U> tmp(h, h + n);
+        return upload(tmp.data(), n);
+    }
+
+    long long pad_index(long long c) const {   // dense x-fastest -> padded
+        return (c % nx) + (long long)px * (c / nx);
+    }
+
+    Layout layout() const { return Layout{nx, ny, nz, px, sz}; }
+
+    bool has_comp(int c) const {
+        if (ndim == 3) return true;
+        if (ndim == 2) return c == MFD_HY || c == MFD_DX || c == MFD_DZ || c == MFD_EX || c == MFD_EZ;
+        return c == MFD_HY || c == MFD_DX || c == MFD_EX;
+    }
+
+    // ---------------------------------------------------------------------------------
+    void init(const mfd_desc* d) {
+        dev = d->device;
+        MFD_CK(cudaSetDevice(dev));
+        MFD_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        MFD_CK(cudaEventCreate(&run_ev[0]));
+        MFD_CK(cudaEventCreate(&run_ev[1]));
+        ndim = d->ndim; nx = d->nx; ny = d->ny; nz = d->nz;
+        px = ndim == 1 ? 1 : (int)round_up(nx, 32);
+        sz = (long long)px * ny;
+        Np = sz * nz;
+        N = (long long)nx * ny * nz;
+        nt = d->nt;
+        dx = (T)d->dx; dy = (T)d->dy; dz = (T)d->dz; dt = (T)d->dt;
+        for (int f = 0; f < 6; ++f) bc[f] = d->bc[f];
+        Mh0 = (T)d->Mh0; Me0 = (T)d->Me0; Md10 = (T)d->Md10; Md20 = (T)d->Md20;
+        for (int c = 0; c < 9; ++c)
+            if (has_comp(c)) F[c] = dalloc<T>(Np);
+        Sa = dalloc<T>(Np);
+        // materials
+        nmat = d->nmat;
+        std::vector<uint8_t> gpad;
+        std::vector<int> bx0(nmat + 1, INT32_MAX), bx1(nmat + 1, -1), by0(nmat + 1, INT32_MAX), by1(nmat + 1, -1),
+            bz0(nmat + 1, INT32_MAX), bz1(nmat + 1, -1);
+        if (d->geometry) {
+            gpad.assign((size_t)Np, 0);
+            for (int iz = 0; iz < nz; ++iz)
+                for (int iy = 0; iy < ny; ++iy) {
+                    const uint8_t* row = d->geometry + (size_t)nx * (iy + (size_t)ny * iz);
+                    uint8_t* prow = gpad.data() + (size_t)px * iy + (size_t)sz * iz;
+                    for (int ix = 0; ix < nx; ++ix) {
+                        int g = row[ix];
+                        if (g > nmat) throw Error(MFD_ERR_INVALID, "geometry index beyond nmat");
+                        prow[ix] = (uint8_t)g;
+                        if (g) {
+                            any_geom = true;
+                            bx0[g] = std::min(bx0[g], ix); bx1[g] = std::max(bx1[g], ix);
+                            by0[g] = std::min(by0[g], iy); by1[g] = std::max(by1[g], iy);
+                            bz0[g] = std::min(bz0[g], iz); bz1[g] = std::max(bz1[g], iz);
+                        }
+                    }
+                }
+        }
+        if (any_geom) {
+            geom = upload(gpad.data(), gpad.size());
+            E2 = dalloc<T>(Np);
+        }
+        const int nc = ndim;   // field components per vector quantity
+        std::vector<T> mh(std::max(nmat, 1));
+        mats_host.resize(nmat);
+        for (int m = 0; m < nmat; ++m) {
+            const mfd_material& s = d->mats[m];
+            MatDev<T, R>& M = mats_host[m];
+            std::memset(&M, 0, sizeof(M));
+            M.Mh = (T)s.Mh; M.Me = (T)s.Me; M.Md1 = (T)s.Md1; M.Md2 = (T)s.Md2;
+            mh[m] = M.Mh;
+            if (M.Mh != Mh0) math_needed = true;
+            if (s.nq < 0 || s.nq > MFD_MAXQ) throw Error(MFD_ERR_INVALID, "a material has more than 16 ADE poles");
+            M.nq = s.nq;
+            for (int q = 0; q < s.nq; ++q) { M.Aq[q] = (T)s.Aq[q]; M.Bq[q] = (T)s.Bq[q]; M.Cq[q] = (T)s.Cq[q]; }
+            M.kerr = s.kerr ? 1 : 0; M.Mk2 = (T)s.Mk2; M.Mk3 = (T)s.Mk3;
+            M.plasma = s.plasma ? 1 : 0;
+            const int g = m + 1;
+            const bool present = bx1[g] >= 0;
+            if (present) {
+                M.bx0 = bx0[g]; M.by0 = by0[g]; M.bz0 = bz0[g];
+                M.bnx = bx1[g] - bx0[g] + 1; M.bny = by1[g] - by0[g] + 1; M.bnz = bz1[g] - bz0[g] + 1;
+                M.bsize = (long long)M.bnx * M.bny * M.bnz;
+            }
+            if (present && M.nq > 0) M.P = dalloc<T>((size_t)2 * M.nq * nc * M.bsize);
+            if (M.plasma) {
+                any_plasma = true;
+                M.Rava = (T)s.Rava; M.ksi = (T)s.ksi; M.rho0 = (T)s.rho0;
+                M.Ap = (T)s.Ap; M.Bp = (T)s.Bp; M.Cp = (T)s.Cp; M.Ma = (T)s.Ma;
+                M.rate_kind = s.rate_kind;
+                M.rate_order = (T)s.rate_order; M.rate_log10c = s.rate_log10c;
+                if (s.rate_kind == MFD_RATE_TABLE) {
+                    if (s.rate_n < 2) throw Error(MFD_ERR_INVALID, "rate table needs >= 2 knots");
+                    M.rate_n = s.rate_n;
+                    M.rate_x = upload_cast<T>(s.rate_x, s.rate_n);
+                    M.rate_y = upload_cast<T>(s.rate_y, s.rate_n);
+                }
+                if (present) {
+                    M.Pp = dalloc<T>((size_t)2 * nc * M.bsize);
+                    M.Pa = dalloc<T>((size_t)nc * M.bsize);
+                    M.rho = dalloc<R>(M.bsize);
+                    M.drho = dalloc<R>(M.bsize);
+                    M.JE = dalloc<T>(M.bsize);
+                }
+            }
+        }
+        if (nmat) {
+            matMh = upload(mh.data(), nmat);
+            mats_dev = upload(mats_host.data(), nmat);
+        }
+        // CPML
+        for (int f = 0; f < 6; ++f) {
+            const mfd_pml_layer& L = d->pml[f];
+            lay[f].ib = L.ib; lay[f].nb = L.nb;
+            if (L.nb <= 0) { lay[f].nb = 0; continue; }
+            const int axis = f / 2;
+            const int n = axis == 0 ? nx : axis == 1 ? ny : nz;
+            const bool used = ndim == 3 || (ndim == 2 && axis != 1) || (ndim == 1 && axis == 2);
+            if (!used) { lay[f].nb = 0; continue; }
+            if (L.ib < 1 || L.ib > n) throw Error(MFD_ERR_INVALID, "CPML boundary index out of range");
+            const bool left = (f % 2) == 0;
+            if (left ? (L.nb != L.ib) : (L.nb != n - L.ib + 1)) throw Error(MFD_ERR_INVALID, "CPML layer size does not match its boundary index");
+            lay[f].K = upload_cast<T>(L.K, L.nb);
+            lay[f].A = upload_cast<T>(L.A, L.nb);
+            lay[f].B = upload_cast<T>(L.B, L.nb);
+            long long cnt;
+            if (ndim == 3) cnt = axis == 0 ? (long long)L.nb * ny * nz : axis == 1 ? (long long)px * L.nb * nz : (long long)px * ny * L.nb;
+            else if (ndim == 2) cnt = axis == 0 ? (long long)L.nb * nz : (long long)px * L.nb;
+            else cnt = L.nb;
+            const int npsi = ndim == 3 ? 4 : 2;
+            for (int k = 0; k < npsi; ++k) lay[f].psi[k] = dalloc<T>(cnt);
+        }
+        // sources
+        for (int i = 0; i < d->nsrc; ++i) {
+            const mfd_source& s = d->srcs[i];
+            if (s.comp < 0 || s.comp > 8 || !has_comp(s.comp)) throw Error(MFD_ERR_INVALID, "source component not in this field");
+            if (s.npts < 1) throw Error(MFD_ERR_INVALID, "source without points");
+            Src S{};
+            S.kind = s.kind; S.comp = s.comp; S.coeff = (T)s.coeff; S.npts = s.npts;
+            std::vector<long long> cells(s.npts);
+            for (long long j = 0; j < s.npts; ++j) {
+                if (s.cells[j] < 0 || s.cells[j] >= N) throw Error(MFD_ERR_INVALID, "source cell out of range");
+                cells[j] = pad_index(s.cells[j]);
+            }
+            S.cells = upload(cells.data(), cells.size());
+            if (s.wave) S.wave = upload(s.wave, (size_t)nt * s.npts);
+            else {
+                if (!s.amp || !s.gt) throw Error(MFD_ERR_INVALID, "source needs wave or amp+gt");
+                S.amp = upload(s.amp, s.npts);
+                S.gt = upload(s.gt, nt);
+            }
+            srcs.push_back(S);
+        }
+        if (d->tfsf.enabled) init_tfsf(d);
+        if (d->tfsf_record) init_record(d);
+        init_monitors(d);
+        MFD_CK(cudaMalloc(&d_flag, sizeof(int)));
+        allocs.push_back(d_flag);
+        MFD_CK(cudaMalloc(&d_bad, sizeof(unsigned long long)));
+        allocs.push_back(d_bad);
+        MFD_CK(cudaHostAlloc(&h_flag, sizeof(int), cudaHostAllocDefault));
+        MFD_CK(cudaHostAlloc(&h_bad, sizeof(unsigned long long), cudaHostAllocDefault));
+        MFD_CK(cudaStreamSynchronize(st));
+        const char* tune = std::getenv("MFD_TILE3D");
+        if (tune) {
+            int a, b, c;
+            if (std::sscanf(tune, "%d,%d,%d", &a, &b, &c) == 3 && a > 0 && b > 0 && c > 0 && a * b <= 256 && a % 32 == 0) {
+                bx3 = a; by3 = b; zc3 = c;
+            }
+        }
+    }
+
+    // Statement lists: sources.jl:727-773 (3-D), 477-495 (2-D), 326-334 (1-D).
+    struct S6 { int comp, x0, x1, y0, y1, z0, z1, k, sign, kind; };   // kind 0: dt/MU0-type, 1: dt/EPS0-type, 2: D
+    void init_tfsf(const mfd_desc* d) {
+        tfsf = true;
+        tfsf_order = d->tfsf.order;
+        const int* i1 = d->tfsf.i1;
+        const int* i2 = d->tfsf.i2;
+        for (int a = 0; a < 3; ++a) {
+            const bool used = ndim == 3 || (ndim == 2 && a != 1) || (ndim == 1 && a == 2);
+            const int n = a == 0 ? nx : a == 1 ? ny : nz;
+            if (used && (i1[a] < 2 || i2[a] > n || i1[a] >= i2[a]))
+                throw Error(MFD_ERR_INVALID, "TFSF box must satisfy 2 <= i1 < i2 <= n on every axis");
+        }
+        // 0-based box
+        const int X1 = i1[0] - 1, X2 = i2[0] - 1, Y1 = i1[1] - 1, Y2 = i2[1] - 1, Z1 = i1[2] - 1, Z2 = i2[2] - 1;
+        std::vector<S6> v;
+        const double Cm = (double)dt / MU0, Ce = (double)dt / EPS0;
+        std::vector<double> coef;
+        std::vector<int> tp;
+        std::vector<T> coefT;
+        auto add = [&](int comp, int x0, int x1, int y0, int y1, int z0, int z1, int k, int sign, double c, int tprec, T cT) {
+            v.push_back(S6{comp, x0, x1, y0, y1, z0, z1, k, sign, 0});
+            coef.push_back(c); tp.push_back(tprec); coefT.push_back(cT);
+        };
+        if (ndim == 3) {
+            const double cmx = Cm / (double)dx, cmy = Cm / (double)dy, cmz = Cm / (double)dz;
+            const double cex = Ce / (double)dx, cey = Ce / (double)dy, cez = Ce / (double)dz;
+            const double cdx = EPS0 * Ce / (double)dx, cdy = EPS0 * Ce / (double)dy, cdz = EPS0 * Ce / (double)dz;
+            // 1yz
+            add(MFD_HY, X1 - 1, X1 - 1, Y1, Y2, Z1, Z2 - 1, 3, -1, cmx, 0, 0);
+            add(MFD_HZ, X1 - 1, X1 - 1, Y1, Y2 - 1, Z1, Z2, 2, +1, cmx, 0, 0);
+            add(MFD_EY, X1, X1, Y1, Y2 - 1, Z1, Z2, 1, +1, cex, 0, 0);
+            add(MFD_EZ, X1, X1, Y1, Y2, Z1, Z2 - 1, 0, -1, cex, 0, 0);
+            add(MFD_DY, X1, X1, Y1, Y2 - 1, Z1, Z2, 1, +1, cdx, 0, 0);
+            add(MFD_DZ, X1, X1, Y1, Y2, Z1, Z2 - 1, 0, -1, cdx, 0, 0);
+            // 2yz
+            add(MFD_HY, X2, X2, Y1, Y2, Z1, Z2 - 1, 7, +1, cmx, 0, 0);
+            add(MFD_HZ, X2, X2, Y1, Y2 - 1, Z1, Z2, 6, -1, cmx, 0, 0);
+            add(MFD_EY, X2, X2, Y1, Y2 - 1, Z1, Z2, 5, -1, cex, 0, 0);
+            add(MFD_EZ, X2, X2, Y1, Y2, Z1, Z2 - 1, 4, +1, cex, 0, 0);
+            add(MFD_DY, X2, X2, Y1, Y2 - 1, Z1, Z2, 5, -1, cdx, 0, 0);
+            add(MFD_DZ, X2, X2, Y1, Y2, Z1, Z2 - 1, 4, +1, cdx, 0, 0);
+            // x1z
+            add(MFD_HX, X1, X2, Y1 - 1, Y1 - 1, Z1, Z2 - 1, 11, +1, cmy, 0, 0);
+            add(MFD_HZ, X1, X2 - 1, Y1 - 1, Y1 - 1, Z1, Z2, 10, -1, cmy, 0, 0);
+            add(MFD_EX, X1, X2 - 1, Y1, Y1, Z1, Z2, 9, -1, cey, 0, 0);
+            add(MFD_EZ, X1, X2, Y1, Y1, Z1, Z2 - 1, 8, +1, cey, 0, 0);
+            add(MFD_DX, X1, X2 - 1, Y1, Y1, Z1, Z2, 9, -1, cdy, 0, 0);
+            add(MFD_DZ, X1, X2, Y1, Y1, Z1, Z2 - 1, 8, +1, cdy, 0, 0);
+            // x2z
+            add(MFD_HX, X1, X2, Y2, Y2, Z1, Z2 - 1, 15, -1, cmy, 0, 0);
+            add(MFD_HZ, X1, X2 - 1, Y2, Y2, Z1, Z2, 14, +1, cmy, 0, 0);
+            add(MFD_EX, X1, X2 - 1, Y2, Y2, Z1, Z2, 13, +1, cey, 0, 0);
+            add(MFD_EZ, X1, X2, Y2, Y2, Z1, Z2 - 1, 12, -1, cey, 0, 0);
+            add(MFD_DX, X1, X2 - 1, Y2, Y2, Z1, Z2, 13, +1, cdy, 0, 0);
+            add(MFD_DZ, X1, X2, Y2, Y2, Z1, Z2 - 1, 12, -1, cdy, 0, 0);
+            // xy1
+            add(MFD_HX, X1, X2, Y1, Y2 - 1, Z1 - 1, Z1 - 1, 19, -1, cmz, 0, 0);
+            add(MFD_HY, X1, X2 - 1, Y1, Y2, Z1 - 1, Z1 - 1, 18, +1, cmz, 0, 0);
+            add(MFD_EX, X1, X2 - 1, Y1, Y2, Z1, Z1, 17, +1, cez, 0, 0);
+            add(MFD_EY, X1, X2, Y1, Y2 - 1, Z1, Z1, 16, -1, cez, 0, 0);
+            add(MFD_DX, X1, X2 - 1, Y1, Y2, Z1, Z1, 17, +1, cdz, 0, 0);
+            add(MFD_DY, X1, X2, Y1, Y2 - 1, Z1, Z1, 16, -1, cdz, 0, 0);
+            // xy2
+            add(MFD_HX, X1, X2, Y1, Y2 - 1, Z2, Z2, 23, +1, cmz, 0, 0);
+            add(MFD_HY, X1, X2 - 1, Y1, Y2, Z2, Z2, 22, -1, cmz, 0, 0);
+            add(MFD_EX, X1, X2 - 1, Y1, Y2, Z2, Z2, 21, -1, cez, 0, 0);
+            add(MFD_EY, X1, X2, Y1, Y2 - 1, Z2, Z2, 20, +1, cez, 0, 0);
+            add(MFD_DX, X1, X2 - 1, Y1, Y2, Z2, Z2, 21, -1, cdz, 0, 0);
+            add(MFD_DY, X1, X2, Y1, Y2 - 1, Z2, Z2, 20, +1, cdz, 0, 0);
+        } else if (ndim == 2) {
+            const double cmx = (double)dt / (MU0 * (double)dx), cex = (double)dt / (EPS0 * (double)dx);
+            const double cmz = (double)dt / (MU0 * (double)dz), cez = (double)dt / (EPS0 * (double)dz);
+            const T cdx = dt / dx, cdz = dt / dz;
+            add(MFD_HY, X1 - 1, X1 - 1, 0, 0, Z1, Z2 - 1, 1, -1, cmx, 0, 0);
+            add(MFD_EZ, X1, X1, 0, 0, Z1, Z2 - 1, 0, -1, cex, 0, 0);
+            add(MFD_DZ, X1, X1, 0, 0, Z1, Z2 - 1, 0, -1, 0, 1, cdx);
+            add(MFD_HY, X2, X2, 0, 0, Z1, Z2 - 1, 3, +1, cmx, 0, 0);
+            add(MFD_EZ, X2, X2, 0, 0, Z1, Z2 - 1, 2, +1, cex, 0, 0);
+            add(MFD_DZ, X2, X2, 0, 0, Z1, Z2 - 1, 2, +1, 0, 1, cdx);
+            add(MFD_HY, X1, X2 - 1, 0, 0, Z1 - 1, Z1 - 1, 5, +1, cmz, 0, 0);
+            add(MFD_EX, X1, X2 - 1, 0, 0, Z1, Z1, 4, +1, cez, 0, 0);
+            add(MFD_DX, X1, X2 - 1, 0, 0, Z1, Z1, 4, +1, 0, 1, cdz);
+            add(MFD_HY, X1, X2 - 1, 0, 0, Z2, Z2, 7, -1, cmz, 0, 0);
+            add(MFD_EX, X1, X2 - 1, 0, 0, Z2, Z2, 6, -1, cez, 0, 0);
+            add(MFD_DX, X1, X2 - 1, 0, 0, Z2, Z2, 6, -1, 0, 1, cdz);
+        } else {
+            const double cm = (double)dt / (MU0 * (double)dz), ce = (double)dt / (EPS0 * (double)dz);
+            const T cd = dt / dz;
+            add(MFD_HY, 0, 0, 0, 0, Z1 - 1, Z1 - 1, 1, +1, cm, 0, 0);
+            add(MFD_EX, 0, 0, 0, 0, Z1, Z1, 0, +1, ce, 0, 0);
+            add(MFD_DX, 0, 0, 0, 0, Z1, Z1, 0, +1, 0, 1, cd);
+            add(MFD_HY, 0, 0, 0, 0, Z2, Z2, 3, -1, cm, 0, 0);
+            add(MFD_EX, 0, 0, 0, 0, Z2, Z2, 2, -1, ce, 0, 0);
+            add(MFD_DX, 0, 0, 0, 0, Z2, Z2, 2, -1, 0, 1, cd);
+        }
+        RectParams<T>& p = tfsf_p;
+        std::memset(&p, 0, sizeof(p));
+        p.n = (int)v.size();
+        p.L = layout();
+        for (int c = 0; c < 9; ++c) p.F[c] = F[c];
+        long long start = 0;
+        std::vector<long long> alen(24, -1);
+        for (int i = 0; i < p.n; ++i) {
+            RectStmt& s = p.s[i];
+            s.comp = v[i].comp; s.x0 = v[i].x0; s.x1 = v[i].x1; s.y0 = v[i].y0; s.y1 = v[i].y1; s.z0 = v[i].z0; s.z1 = v[i].z1;
+            s.k = v[i].k; s.sign = v[i].sign; s.tprec = tp[i]; s.coef = coef[i]; s.coefT = (double)coefT[i];
+            s.len = (long long)(s.x1 - s.x0 + 1) * (s.y1 - s.y0 + 1) * (s.z1 - s.z0 + 1);
+            s.start = start;
+            start += s.len;
+            alen[s.k] = s.len;
+        }
+        p.total = start;
+        const int narr = ndim == 3 ? 24 : ndim == 2 ? 8 : 4;
+        for (int k = 0; k < narr; ++k) {
+            if (!d->tfsf.inc[k]) throw Error(MFD_ERR_INVALID, "missing TFSF incident array");
+            p.arr[k] = upload((const T*)d->tfsf.inc[k], (size_t)alen[k] * nt);
+        }
+        MFD_CK(cudaStreamSynchronize(st));
+    }
+
+    // Record statements: sources.jl:372-384, 534-550, 839-877.
+    void init_record(const mfd_desc* d) {
+        record = true;
+        const int* i1 = d->rec_i1;
+        const int* i2 = d->rec_i2;
+        for (int a = 0; a < 3; ++a) {
+            const bool used = ndim == 3 || (ndim == 2 && a != 1) || (ndim == 1 && a == 2);
+            const int n = a == 0 ? nx : a == 1 ? ny : nz;
+            if (used && (i1[a] < 2 || i2[a] > n || i1[a] >= i2[a]))
+                throw Error(MFD_ERR_INVALID, "record box must satisfy 2 <= i1 < i2 <= n on every axis");
+        }
+        const int X1 = i1[0] - 1, X2 = i2[0] - 1, Y1 = i1[1] - 1, Y2 = i2[1] - 1, Z1 = i1[2] - 1, Z2 = i2[2] - 1;
+        std::vector<S6> v;
+        auto add = [&](int comp, int x0, int x1, int y0, int y1, int z0, int z1) {
+            v.push_back(S6{comp, x0, x1, y0, y1, z0, z1, (int)v.size(), 0, 0});
+        };
+        if (ndim == 3) {
+            add(MFD_HY, X1 - 1, X1 - 1, Y1, Y2, Z1, Z2 - 1); add(MFD_HZ, X1 - 1, X1 - 1, Y1, Y2 - 1, Z1, Z2);
+            add(MFD_EY, X1, X1, Y1, Y2 - 1, Z1, Z2); add(MFD_EZ, X1, X1, Y1, Y2, Z1, Z2 - 1);
+            add(MFD_HY, X2, X2, Y1, Y2, Z1, Z2 - 1); add(MFD_HZ, X2, X2, Y1, Y2 - 1, Z1, Z2);
+            add(MFD_EY, X2, X2, Y1, Y2 - 1, Z1, Z2); add(MFD_EZ, X2, X2, Y1, Y2, Z1, Z2 - 1);
+            add(MFD_HX, X1, X2, Y1 - 1, Y1 - 1, Z1, Z2 - 1); add(MFD_HZ, X1, X2 - 1, Y1 - 1, Y1 - 1, Z1, Z2);
+            add(MFD_EX, X1, X2 - 1, Y1, Y1, Z1, Z2); add(MFD_EZ, X1, X2, Y1, Y1, Z1, Z2 - 1);
+            add(MFD_HX, X1, X2, Y2, Y2, Z1, Z2 - 1); add(MFD_HZ, X1, X2 - 1, Y2, Y2, Z1, Z2);
+            add(MFD_EX, X1, X2 - 1, Y2, Y2, Z1, Z2); add(MFD_EZ, X1, X2, Y2, Y2, Z1, Z2 - 1);
+            add(MFD_HX, X1, X2, Y1, Y2 - 1, Z1 - 1, Z1 - 1); add(MFD_HY, X1, X2 - 1, Y1, Y2, Z1 - 1, Z1 - 1);
+            add(MFD_EX, X1, X2 - 1, Y1, Y2, Z1, Z1); add(MFD_EY, X1, X2, Y1, Y2 - 1, Z1, Z1);
+            add(MFD_HX, X1, X2, Y1, Y2 - 1, Z2, Z2); add(MFD_HY, X1, X2 - 1, Y1, Y2, Z2, Z2);
+            add(MFD_EX, X1, X2 - 1, Y1, Y2, Z2, Z2); add(MFD_EY, X1, X2, Y1, Y2 - 1, Z2, Z2);
+        } else if (ndim == 2) {
+            add(MFD_HY, X1 - 1, X1 - 1, 0, 0, Z1, Z2 - 1); add(MFD_EZ, X1, X1, 0, 0, Z1, Z2 - 1);
+            add(MFD_HY, X2, X2, 0, 0, Z1, Z2 - 1); add(MFD_EZ, X2, X2, 0, 0, Z1, Z2 - 1);
+            add(MFD_HY, X1, X2 - 1, 0, 0, Z1 - 1, Z1 - 1); add(MFD_EX, X1, X2 - 1, 0, 0, Z1, Z1);
+            add(MFD_HY, X1, X2 - 1, 0, 0, Z2, Z2); add(MFD_EX, X1, X2 - 1, 0, 0, Z2, Z2);
+        } else {
+            add(MFD_HY, 0, 0, 0, 0, Z1 - 1, Z1 - 1); add(MFD_EX, 0, 0, 0, 0, Z1, Z1);
+            add(MFD_HY, 0, 0, 0, 0, Z2, Z2); add(MFD_EX, 0, 0, 0, 0, Z2, Z2);
+        }
+        RectParams<T>& p = rec_p;
+        std::memset(&p, 0, sizeof(p));
+        p.n = (int)v.size();
+        rec_narr = p.n;
+        p.L = layout();
+        for (int c = 0; c < 9; ++c) p.F[c] = F[c];
+        long long start = 0;
+        for (int i = 0; i < p.n; ++i) {
+            RectStmt& s = p.s[i];
+            s.comp = v[i].comp; s.x0 = v[i].x0; s.x1 = v[i].x1; s.y0 = v[i].y0; s.y1 = v[i].y1; s.z0 = v[i].z0; s.z1 = v[i].z1;
+            s.k = i;
+            s.len = (long long)(s.x1 - s.x0 + 1) * (s.y1 - s.y0 + 1) * (s.z1 - s.z0 + 1);
+            s.start = start;
+            start += s.len;
+            p.arr[i] = dalloc<T>((size_t)s.len * nt);
+        }
+        p.total = start;
+    }
+
+    void init_monitors(const mfd_desc* d) {
+        if (d->nmon <= 0) return;
+        static const int c3[6] = {MFD_HX, MFD_HY, MFD_HZ, MFD_EX, MFD_EY, MFD_EZ};
+        static const int c2[3] = {MFD_HY, MFD_EX, MFD_EZ};
+        static const int c1[2] = {MFD_HY, MFD_EX};
+        ncomp_mon = ndim == 3 ? 6 : ndim == 2 ? 3 : 2;
+        for (int k = 0; k < ncomp_mon; ++k) mon_comps[k] = ndim == 3 ? c3[k] : ndim == 2 ? c2[k] : c1[k];
+        long long ring_vals = 0;
+        for (int m = 0; m < d->nmon; ++m) {
+            const mfd_monitor& a = d->mons[m];
+            if (a.npts < 1) throw Error(MFD_ERR_INVALID, "monitor without points");
+            if (a.kind == MFD_MON_SPECTRAL || a.sum) ring_vals += (long long)ncomp_mon * a.npts;
+        }
+        need_ring = ring_vals > 0;
+        if (need_ring) {
+            // staging depth: up to 64 steps, at most ~512 MB of staged values
+            long long cap = (512ll << 20) / ((long long)sizeof(T) * ring_vals);
+            ring_k = (int)std::max(1ll, std::min(64ll, cap));
+        }
+        long long start = 0;
+        for (int m = 0; m < d->nmon; ++m) {
+            const mfd_monitor& a = d->mons[m];
+            MonDev<T> M{};
+            M.kind = a.kind; M.sum = a.sum ? 1 : 0; M.npts = a.npts; M.nw = a.nw;
+            std::vector<long long> cells(a.npts);
+            for (long long j = 0; j < a.npts; ++j) {
+                if (a.cells[j] < 0 || a.cells[j] >= N) throw Error(MFD_ERR_INVALID, "monitor cell out of range");
+                cells[j] = pad_index(a.cells[j]);
+            }
+            M.cells = upload(cells.data(), cells.size());
+            if (a.kind == MFD_MON_FIELD) {
+                if (M.sum) M.hist = dalloc<T>((size_t)ncomp_mon * nt);
+                else M.hist = dalloc<T>((size_t)ncomp_mon * nt * a.npts);
+            } else {
+                if (a.nw < 1 || !a.phasor) throw Error(MFD_ERR_INVALID, "spectral monitor needs frequencies");
+                M.S = dalloc<double2>((size_t)ncomp_mon * a.nw * (M.sum ? 1 : a.npts));
+                M.phasor = (const double2*)upload(a.phasor, (size_t)nt * a.nw * 2);
+            }
+            if (a.kind == MFD_MON_SPECTRAL || M.sum) M.ring = dalloc<T>((size_t)ring_k * ncomp_mon * a.npts);
+            M.start = start;
+            start += (long long)ncomp_mon * a.npts;
+            mons_host.push_back(M);
+        }
+        mons_dev = upload(mons_host.data(), mons_host.size());
+        mon_p.nmon = (int)mons_host.size();
+        mon_p.ncomp = ncomp_mon;
+        mon_p.total = start;
+        mon_p.nt = nt;
+        for (int k = 0; k < ncomp_mon; ++k) mon_p.comp[k] = F[mon_comps[k]];
+        mon_p.mons = mons_dev;
+        MFD_CK(cudaStreamSynchronize(st));
+    }
+
+    // ---------------------------------------------------------------------------------
+    cudaEvent_t get_event() {
+        if (!ev_pool.empty()) { cudaEvent_t e = ev_pool.back(); ev_pool.pop_back(); return e; }
+        cudaEvent_t e;
+        MFD_CK(cudaEventCreate(&e));
+        return e;
+    }
+
+    template <typename F_>
+    void launch(int cls, F_&& f) {
+        if (profiling) {
+            cudaEvent_t a = get_event(), b = get_event();
+            MFD_CK(cudaEventRecord(a, st));
+            f();
+            MFD_CK(cudaEventRecord(b, st));
+            pend.push_back({cls, {a, b}});
+        } else {
+            f();
+        }
+        MFD_CK(cudaGetLastError());
+        k_n[cls]++;
+    }
+
+    void collect_times() {
+        for (auto& pe : pend) {
+            float ms = 0;
+            MFD_CK(cudaEventElapsedTime(&ms, pe.second.first, pe.second.second));
+            k_ms[pe.first] += ms;
+            ev_pool.push_back(pe.second.first);
+            ev_pool.push_back(pe.second.second);
+        }
+        pend.clear();
+    }
+
+    HParams<T> hparams(int accum, long long prev_step) {
+        HParams<T> p{};
+        p.L = layout();
+        p.dx = dx; p.dy = dy; p.dz = dz; p.dt = dt;
+        for (int f = 0; f < 6; ++f) { p.bc[f] = bc[f]; p.lay[f] = lay[f]; }
+        p.Mh0 = Mh0;
+        p.geom = geom;
+        p.matMh = matMh;
+        p.Hx = F[MFD_HX]; p.Hy = F[MFD_HY]; p.Hz = F[MFD_HZ];
+        p.Ex = F[MFD_EX]; p.Ey = F[MFD_EY]; p.Ez = F[MFD_EZ];
+        p.accum = accum;
+        p.sum_e2 = any_geom ? 1 : 0;
+        p.Sa = Sa; p.E2 = E2;
+        p.flag = d_flag; p.badstep = d_bad;
+        p.prev_step = prev_step;
+        return p;
+    }
+
+    EParams<T, R> eparams(int cur) {
+        EParams<T, R> p{};
+        p.L = layout();
+        p.dx = dx; p.dy = dy; p.dz = dz; p.dt = dt;
+        for (int f = 0; f < 6; ++f) { p.bc[f] = bc[f]; p.lay[f] = lay[f]; }
+        p.Me0 = Me0; p.Md10 = Md10; p.Md20 = Md20;
+        p.geom = geom;
+        p.mats = mats_dev;
+        p.Hx = F[MFD_HX]; p.Hy = F[MFD_HY]; p.Hz = F[MFD_HZ];
+        p.Dx = F[MFD_DX]; p.Dy = F[MFD_DY]; p.Dz = F[MFD_DZ];
+        p.Ex = F[MFD_EX]; p.Ey = F[MFD_EY]; p.Ez = F[MFD_EZ];
+        p.cur = cur;
+        return p;
+    }
+
+    void launch_H(int accum, long long prev_step) {
+        HParams<T> p = hparams(accum, prev_step);
+        launch(KC_H, [&] {
+            if (ndim == 3) {
+                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
+                if (math_needed) h3d_kernel<T, true><<<grd, blk, 0, st>>>(p, zc3);
+                else h3d_kernel<T, false><<<grd, blk, 0, st>>>(p, zc3);
+            } else if (ndim == 2) {
+                dim3 blk(32, 8), grd((nx + 31) / 32, (nz + 7) / 8);
+                if (math_needed) h2d_kernel<T, true><<<grd, blk, 0, st>>>(p);
+                else h2d_kernel<T, false><<<grd, blk, 0, st>>>(p);
+            } else {
+                dim3 blk(256), grd((nz + 255) / 256);
+                if (math_needed) h1d_kernel<T, true><<<grd, blk, 0, st>>>(p);
+                else h1d_kernel<T, false><<<grd, blk, 0, st>>>(p);
+            }
+        });
+    }
+
+    void launch_E(int cur) {
+        EParams<T, R> p = eparams(cur);
+        launch(KC_E, [&] {
+            if (ndim == 3) {
+                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
+                if (any_geom) e3d_kernel<T, R, true><<<grd, blk, 0, st>>>(p, zc3);
+                else e3d_kernel<T, R, false><<<grd, blk, 0, st>>>(p, zc3);
+            } else if (ndim == 2) {
+                dim3 blk(32, 8), grd((nx + 31) / 32, (nz + 7) / 8);
+                if (any_geom) e2d_kernel<T, R, true><<<grd, blk, 0, st>>>(p);
+                else e2d_kernel<T, R, false><<<grd, blk, 0, st>>>(p);
+            } else {
+                dim3 blk(256), grd((nz + 255) / 256);
+                if (any_geom) e1d_kernel<T, R, true><<<grd, blk, 0, st>>>(p);
+                else e1d_kernel<T, R, false><<<grd, blk, 0, st>>>(p);
+            }
+        });
+    }
+
+    void launch_sources(int64_t it) {
+        const long long it0 = it - 1;
+        for (size_t s = 0; s <= srcs.size(); ++s) {
+            if (tfsf && (int)s == tfsf_order) {
+                tfsf_p.it0 = it0;
+                launch(KC_TFSF, [&] {
+                    const long long nb = (tfsf_p.total + 255) / 256;
+                    tfsf_kernel<T><<<(unsigned)nb, 256, 0, st>>>(tfsf_p);
+                });
+            }
+            if (s < srcs.size()) {
+                const Src& S = srcs[s];
+                launch(KC_SRC, [&] {
+                    const long long nb = (S.npts + 255) / 256;
+                    point_source_kernel<T><<<(unsigned)nb, 256, 0, st>>>(F[S.comp], S.cells, S.npts, S.wave, S.amp, S.gt, it0, S.kind, S.coeff);
+                });
+            }
+        }
+    }
+
+    void flush_monitors() {
+        if (!need_ring || ring_used == 0) return;
+        const double dtd = (double)dt;
+        for (size_t m = 0; m < mons_host.size(); ++m) {
+            const MonDev<T>& M = mons_host[m];
+            const MonDev<T>* md = mons_dev + m;
+            if (M.kind == MFD_MON_FIELD && M.sum) {
+                launch(KC_DFT, [&] {
+                    monitor_fieldsum_kernel<T><<<dim3(ncomp_mon, ring_used), 256, 0, st>>>(md, ncomp_mon, nt, ring_first);
+                });
+            } else if (M.kind == MFD_MON_SPECTRAL && !M.sum) {
+                launch(KC_DFT, [&] {
+                    dim3 grd((unsigned)((M.npts + 255) / 256), ncomp_mon, (M.nw + MFD_DFT_W - 1) / MFD_DFT_W);
+                    monitor_dft_kernel<T><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first, dtd);
+                });
+            } else if (M.kind == MFD_MON_SPECTRAL) {
+                launch(KC_DFT, [&] {
+                    monitor_dftsum_kernel<T><<<dim3(ncomp_mon, M.nw), 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first, dtd);
+                });
+            }
+        }
+        ring_used = 0;
+    }
+
+    void launch_monitors(int64_t it) {
+        if (mons_host.empty()) return;
+        if (need_ring && ring_used == 0) ring_first = it - 1;
+        const int slot = ring_used;
+        launch(KC_MON, [&] {
+            const long long nb = (mon_p.total + 255) / 256;
+            monitor_gather_kernel<T><<<(unsigned)nb, 256, 0, st>>>(mon_p, it - 1, slot);
+        });
+        if (need_ring) {
+            ring_used++;
+            if (ring_used == ring_k) flush_monitors();
+        }
+    }
+
+    void launch_record(int64_t it) {
+        rec_p.it0 = it - 1;
+        launch(KC_MON, [&] {
+            const long long nb = (rec_p.total + 255) / 256;
+            record_kernel<T><<<(unsigned)nb, 256, 0, st>>>(rec_p);
+        });
+    }
+
+    void launch_sums(int64_t step) {
+        HParams<T> p = hparams(1, step);
+        launch(KC_SUMS, [&] {
+            dim3 grd((nx + 255) / 256, ny, nz);
+            sums_kernel<T><<<grd, 256, 0, st>>>(p, ndim);
+        });
+    }
+
+    int run(int64_t a, int64_t b) override {
+        if (bad_step) { err = "the model holds non-finite fields from step " + std::to_string(bad_step); return MFD_ERR_NONFINITE; }
+        if (a != done + 1 || b < a - 1 || b > nt) { err = "steps must be consecutive and within 1..Nt"; return MFD_ERR_INVALID; }
+        if (b < a) return MFD_OK;
+        MFD_CK(cudaSetDevice(dev));
+        MFD_CK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+        MFD_CK(cudaMemsetAsync(d_bad, 0xff, sizeof(unsigned long long), st));
+        MFD_CK(cudaEventRecord(run_ev[0], st));
+        for (int64_t it = a; it <= b; ++it) {
+            launch_H(it > a ? 1 : 0, it - 1);
+            launch_E((int)((it - 1) & 1));
+            launch_sources(it);
+            launch_monitors(it);
+            if (record) launch_record(it);
+        }
+        flush_monitors();
+        launch_sums(b);
+        MFD_CK(cudaEventRecord(run_ev[1], st));
+        MFD_CK(cudaMemcpyAsync(h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        MFD_CK(cudaMemcpyAsync(h_bad, d_bad, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        bounded_sync(st);
+        float ms = 0;
+        MFD_CK(cudaEventElapsedTime(&ms, run_ev[0], run_ev[1]));
+        run_ms = ms;
+        if (profiling) collect_times();
+        done = b;
+        if (*h_flag) {
+            bad_kind = *h_flag;
+            bad_step = (int64_t)*h_bad;
+            err = (bad_kind & 1) ? "Something went wrong. I found NaN field values."
+                                 : "Something went wrong. I found Inf field values.";
+            err += " (step " + std::to_string(bad_step) + ")";
+            return MFD_ERR_NONFINITE;
+        }
+        return MFD_OK;
+    }
+
+    void copy_out(const void* dsrc, void* hdst, size_t esize) {
+        MFD_CK(cudaSetDevice(dev));
+        MFD_CK(cudaMemcpy2DAsync(hdst, (size_t)nx * esize, dsrc, (size_t)px * esize, (size_t)nx * esize, (size_t)ny * nz,
+                                 cudaMemcpyDeviceToHost, st));
+        bounded_sync(st);
+    }
+
+    int read_field(int comp, void* dst) override {
+        if (comp < 0 || comp > 8 || !F[comp]) { err = "bad component"; return MFD_ERR_INVALID; }
+        copy_out(F[comp], dst, sizeof(T));
+        return MFD_OK;
+    }
+
+    int write_field(int comp, const void* src) override {
+        if (comp < 0 || comp > 8 || !F[comp]) { err = "bad component"; return MFD_ERR_INVALID; }
+        MFD_CK(cudaSetDevice(dev));
+        MFD_CK(cudaMemcpy2DAsync(F[comp], (size_t)px * sizeof(T), src, (size_t)nx * sizeof(T), (size_t)nx * sizeof(T),
+                                 (size_t)ny * nz, cudaMemcpyHostToDevice, st));
+        bounded_sync(st);
+        return MFD_OK;
+    }
+
+    int read_integral(int which, void* dst) override {
+        MFD_CK(cudaSetDevice(dev));
+        if (which == MFD_INT_SA) { copy_out(Sa, dst, sizeof(T)); return MFD_OK; }
+        if (which == MFD_INT_E2) {
+            if (E2) copy_out(E2, dst, sizeof(T));
+            else std::memset(dst, 0, (size_t)N * sizeof(T));
+            return MFD_OK;
+        }
+        if (which == MFD_INT_JE || which == MFD_INT_RHO) {
+            const size_t es = which == MFD_INT_JE ? sizeof(T) : sizeof(double);
+            if (!any_plasma || !any_geom) { std::memset(dst, 0, (size_t)N * es); return MFD_OK; }
+            void* tmp = nullptr;
+            MFD_CK(cudaMallocAsync(&tmp, (size_t)Np * es, st));
+            dim3 grd((nx + 255) / 256, ny, nz);
+            scatter_state_kernel<T, R><<<grd, 256, 0, st>>>(mats_dev, geom, layout(), tmp, which);
+            MFD_CK(cudaGetLastError());
+            try {
+                copy_out(tmp, dst, es);
+            } catch (...) {
+                cudaFreeAsync(tmp, st);
+                throw;
+            }
+            MFD_CK(cudaFreeAsync(tmp, st));
+            bounded_sync(st);
+            return MFD_OK;
+        }
+        err = "bad integral";
+        return MFD_ERR_INVALID;
+    }
+
+    int read_monitor(int m, int comp, void* dst) override {
+        if (m < 0 || m >= (int)mons_host.size()) { err = "bad monitor"; return MFD_ERR_INVALID; }
+        int k = -1;
+        for (int j = 0; j < ncomp_mon; ++j) if (mon_comps[j] == comp) k = j;
+        if (k < 0) { err = "bad monitor component"; return MFD_ERR_INVALID; }
+        const MonDev<T>& M = mons_host[m];
+        MFD_CK(cudaSetDevice(dev));
+        if (M.kind == MFD_MON_FIELD) {
+            const size_t n = M.sum ? (size_t)nt : (size_t)nt * M.npts;
+            MFD_CK(cudaMemcpyAsync(dst, M.hist + (size_t)k * n, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+        } else {
+            const size_t n = (size_t)M.nw * (M.sum ? 1 : M.npts);
+            MFD_CK(cudaMemcpyAsync(dst, M.S + (size_t)k * n, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        }
+        bounded_sync(st);
+        return MFD_OK;
+    }
+
+    int read_record(int k, void* dst) override {
+        if (!record || k < 0 || k >= rec_narr) { err = "no such record array"; return MFD_ERR_INVALID; }
+        MFD_CK(cudaSetDevice(dev));
+        MFD_CK(cudaMemcpyAsync(dst, rec_p.arr[k], (size_t)rec_p.s[k].len * nt * sizeof(T), cudaMemcpyDeviceToHost, st));
+        bounded_sync(st);
+        return MFD_OK;
+    }
+
+    int64_t record_size(int k) const override {
+        if (!record || k < 0 || k >= rec_narr) return 0;
+        return (int64_t)rec_p.s[k].len * nt;
+    }
+
+    void status(int64_t* d, int64_t* b, int32_t* k) const override {
+        if (d) *d = done;
+        if (b) *b = bad_step;
+        if (k) *k = bad_kind;
+    }
+
+    void set_profiling(bool on) override { profiling = on; }
+
+    int kernel_times(double* ms, int64_t* launches, int n) const override {
+        for (int k = 0; k < n && k < KC_N; ++k) {
+            if (ms) ms[k] = k_ms[k];
+            if (launches) launches[k] = k_n[k];
+        }
+        return KC_N;
+    }
+
+    double last_run_ms() const override { return run_ms; }
+    int64_t device_bytes() const override { return bytes; }
+};
+
+thread_local std::string g_create_error;
+
+}  // namespace mfd
+
+using namespace mfd;
+
+struct mfd_handle {
+    std::unique_ptr<HandleBase> impl;
+};
+
+static int validate_desc(const mfd_desc* d) {
+    if (!d) { g_create_error = "null descriptor"; return MFD_ERR_INVALID; }
+    if (d->abi_version != MFD_ABI_VERSION) { g_create_error = "ABI version mismatch"; return MFD_ERR_INVALID; }
+    if (d->ndim < 1 || d->ndim > 3 || d->nx < 1 || d->ny < 1 || d->nz < 1 || d->nt < 1) { g_create_error = "bad dims"; return MFD_ERR_INVALID; }
+    if (d->ndim == 1 && (d->nx != 1 || d->ny != 1)) { g_create_error = "1-D model needs nx = ny = 1"; return MFD_ERR_INVALID; }
+    if (d->ndim == 2 && d->ny != 1) { g_create_error = "2-D model needs ny = 1"; return MFD_ERR_INVALID; }
+    if (d->dtype != MFD_F32 && d->dtype != MFD_F64) { g_create_error = "bad dtype"; return MFD_ERR_INVALID; }
+    if (d->nmat < 0 || d->nmat > 255) { g_create_error = "at most 255 materials"; return MFD_ERR_INVALID; }
+    if ((long long)d->nx * d->ny * d->nz > (1ll << 34)) { g_create_error = "grid too large"; return MFD_ERR_INVALID; }
+    return MFD_OK;
+}
+
+extern "C" {
+
+int mfd_abi_version(void) { return MFD_ABI_VERSION; }
+
+int mfd_create(const mfd_desc* desc, mfd_handle** out) {
+    if (!out) return MFD_ERR_INVALID;
+    *out = nullptr;
+    int st = validate_desc(desc);
+    if (st) return st;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g_create_error = "no CUDA device";
+        return MFD_ERR_NODEVICE;
+    }
+    if (desc->device < 0 || desc->device >= ndev) { g_create_error = "bad device ordinal"; return MFD_ERR_INVALID; }
+    std::unique_ptr<mfd_handle> h(new mfd_handle);
+    try {
+        if (desc->dtype == MFD_F64) {
+            auto e = std::make_unique<Engine<double, double>>();
+            e->init(desc);
+            h->impl = std::move(e);
+        } else if (desc->rho_fp64) {
+            auto e = std::make_unique<Engine<float, double>>();
+            e->init(desc);
+            h->impl = std::move(e);
+        } else {
+            auto e = std::make_unique<Engine<float, float>>();
+            e->init(desc);
+            h->impl = std::move(e);
+        }
+    } catch (const Error& e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_create_error = "out of host memory";
+        return MFD_ERR_OOM;
+    }
+    *out = h.release();
+    return MFD_OK;
+}
+
+void mfd_destroy(mfd_handle* h) { delete h; }
+
+#define MFD_GUARD(h, expr)                                   \
+    do {                                                     \
+        if (!(h) || !(h)->impl) return MFD_ERR_INVALID;      \
+        try {                                                \
+            return (expr);                                   \
+        } catch (const Error& e) {                           \
+            (h)->impl->err = e.what();                       \
+            return e.code;                                   \
+        } catch (const std::bad_alloc&) {                    \
+            (h)->impl->err = "out of host memory";           \
+            return MFD_ERR_OOM;                              \
+        }                                                    \
+    } while (0)
+
+int mfd_run(mfd_handle* h, int64_t a, int64_t b) { MFD_GUARD(h, h->impl->run(a, b)); }
+int mfd_read_field(mfd_handle* h, int32_t comp, void* dst) { MFD_GUARD(h, h->impl->read_field(comp, dst)); }
+int mfd_write_field(mfd_handle* h, int32_t comp, const void* src) { MFD_GUARD(h, h->impl->write_field(comp, src)); }
+int mfd_read_integral(mfd_handle* h, int32_t which, void* dst) { MFD_GUARD(h, h->impl->read_integral(which, dst)); }
+int mfd_read_monitor(mfd_handle* h, int32_t m, int32_t comp, void* dst) { MFD_GUARD(h, h->impl->read_monitor(m, comp, dst)); }
+int mfd_read_tfsf_record(mfd_handle* h, int32_t k, void* dst) { MFD_GUARD(h, h->impl->read_record(k, dst)); }
+
+int64_t mfd_tfsf_record_size(const mfd_handle* h, int32_t k) {
+    if (!h || !h->impl) return 0;
+    return h->impl->record_size(k);
+}
+
+int mfd_status(const mfd_handle* h, int64_t* d, int64_t* b, int32_t* k) {
+    if (!h || !h->impl) return MFD_ERR_INVALID;
+    h->impl->status(d, b, k);
+    return MFD_OK;
+}
+
+int mfd_set_profiling(mfd_handle* h, int32_t on) {
+    if (!h || !h->impl) return MFD_ERR_INVALID;
+    h->impl->set_profiling(on != 0);
+    return MFD_OK;
+}
+
+int mfd_kernel_times(const mfd_handle* h, double* ms, int64_t* launches, int32_t n) {
+    if (!h || !h->impl) return MFD_ERR_INVALID;
+    return h->impl->kernel_times(ms, launches, n);
+}
+
+int mfd_last_run_ms(const mfd_handle* h, double* ms) {
+    if (!h || !h->impl || !ms) return MFD_ERR_INVALID;
+    *ms = h->impl->last_run_ms();
+    return MFD_OK;
+}
+
+int64_t mfd_device_bytes(const mfd_handle* h) {
+    if (!h || !h->impl) return 0;
+    return h->impl->device_bytes();
+}
+
+const char* mfd_last_error(const mfd_handle* h) {
+    if (!h || !h->impl) return "invalid handle";
+    return h->impl->err.c_str();
+}
+
+const char* mfd_create_error(void) { return g_create_error.c_str(); }
+
+}  // extern "C"

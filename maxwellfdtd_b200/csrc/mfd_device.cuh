@@ -1,0 +1,208 @@
+// mfd_device.cuh -- device-side data layout and per-cell physics of the B200 FDTD stepper.
+//
+// HBM layout (one handle):
+//  * every grid array (9 field components, Sa, E2, the uint8 material map) is x-fastest with
+//    the x row padded to a pitch px (a multiple of 32 elements) so rows start on 128-byte
+//    (float) / 256-byte (double) boundaries: cell (ix,iy,iz) -> ix + px*(iy + ny*iz);
+//  * CPML psi arrays exist only inside their slabs: x faces [iz][iy][p] (p < nb), y faces
+//    [iz][p][ix], z faces [p][iy][ix] (pitch px);
+//  * polarisation / plasma state exists only inside the bounding box of each material's
+//    cells, x-fastest, with two ping-pong buffers per recursion instead of the reference's
+//    three dense arrays P, oldP1, oldP2 (materials.jl:424-426):
+//      P^{n+1} = Aq P^n + Bq P^{n-1} + Cq E^n  is written over P^{n-1}.
+//
+// The arithmetic of every cell update follows the reference kernels operation by operation
+// (src/models.jl) with the same operand types; kernels are compiled with --fmad=false so no
+// a*b+c is fused, as Julia does not fuse either.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+#include "../../include/maxwellfdtd.h"
+
+#define MFD_MAXQ 16
+
+namespace mfd {
+
+template <typename T> struct Eps;
+template <> struct Eps<float> { static __device__ __forceinline__ float v() { return FLT_EPSILON; } };
+template <> struct Eps<double> { static __device__ __forceinline__ double v() { return DBL_EPSILON; } };
+
+struct Layout {
+    int nx, ny, nz;
+    int px;            // x pitch (elements)
+    long long sz;      // px*ny (z-plane stride)
+};
+
+template <typename T>
+struct LayerDev {
+    int ib, nb;        // 1-based boundary index, points in layer (0 = none)
+    const T* K;
+    const T* A;
+    const T* B;
+    T* psi[4];         // 3-D: x faces Hyx,Hzx,Eyx,Ezx; y: Hxy,Hzy,Exy,Ezy; z: Hxz,Hyz,Exz,Eyz
+                       // 2-D: x faces Hyx,Ezx; z faces Hyz,Exz.  1-D: z faces Hyz,Exz.
+};
+
+// Material coefficients + pointers to its compact state (materials.jl:335-483).
+template <typename T, typename R>
+struct MatDev {
+    T Mh, Me, Md1, Md2;
+    int nq, kerr, plasma, rate_kind;
+    T Aq[MFD_MAXQ], Bq[MFD_MAXQ], Cq[MFD_MAXQ];
+    T Mk2, Mk3;
+    T Rava, ksi, rho0, Ap, Bp, Cp, Ma;
+    T rate_order;
+    double rate_log10c;
+    int rate_n;
+    const T* rate_x;
+    const T* rate_y;
+    int bx0, by0, bz0, bnx, bny, bnz;   // bounding box of the material's cells
+    long long bsize;
+    T* P;       // [2][nq][nc][bsize]
+    T* Pp;      // [2][nc][bsize]
+    T* Pa;      // [nc][bsize]
+    R* rho;     // [bsize]
+    R* drho;    // [bsize]
+    T* JE;      // [bsize]
+};
+
+// Neighbour value across a grid face (models.jl:755-808, 920-973): periodic wraps,
+// Dirichlet is zero, Neumann repeats the cell's own value.
+template <typename T>
+__device__ __forceinline__ T bc_value(int bc, T wrapped, T self) {
+    return bc == MFD_BC_PERIODIC ? wrapped : (bc == MFD_BC_DIRICHLET ? T(0) : self);
+}
+
+// IonizationRate functor in T precision (IonizationRate.jl:42-52).
+template <typename T>
+__device__ __forceinline__ T rate_table(const T* __restrict__ X, const T* __restrict__ Y, int n, T x) {
+    if (x <= T(0)) return T(0);
+    T xi = log10(x);
+    int i;
+    if (xi <= X[0]) i = 0;
+    else if (xi >= X[n - 1]) i = n - 2;
+    else {
+        int lo = 0, hi = n - 1;     // first j with X[j] >= xi, then i = j - 1
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (X[mid] < xi) lo = mid + 1; else hi = mid;
+        }
+        i = lo - 1;
+    }
+    T dydx = (Y[i + 1] - Y[i]) / (X[i + 1] - X[i]);
+    T yl = Y[i] + dydx * (xi - X[i]);
+    return pow(T(10), yl);
+}
+
+template <typename T, typename R, typename Q>
+__device__ __forceinline__ void plasma_density(R& rho, R& drho, Q R1, T R2, T dt) {
+    // models.jl:1116-1125: exact integration of drho/dt = R1 (1 - rho) - R2 rho over dt
+    R r = rho;
+    if (R2 == T(0)) {
+        r = 1 - (1 - r) * exp(-R1 * dt);
+    } else {
+        auto R12 = R1 - R2;
+        r = R1 / R12 * 1 - (R1 / R12 * 1 - r) * exp(-R12 * dt);
+    }
+    rho = r;
+    drho = R1 * (1 - r);
+}
+
+// Material response of one cell after its D update: ADE poles, plasma, Kerr, E from D
+// (models.jl:1042-1154; 2-D 622-712; 1-D 365-431).  NC field components; E[k] points to
+// the k-th E component (x, [y,] z order), Dv[k] the updated D values.
+template <typename T, typename R, int NC>
+__device__ __forceinline__ void material_cell(const MatDev<T, R>* __restrict__ m, int ix, int iy, int iz,
+                                              T* const* E, long long c, const T* Dv, int cur, T dt) {
+    const T Me = m->Me;
+    T sumP[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) sumP[k] = T(0);
+    const int nq = m->nq;
+    const bool plasma = m->plasma != 0;
+    T En[NC];
+    long long bi = 0;
+    if (nq > 0 || plasma) {
+#pragma unroll
+        for (int k = 0; k < NC; ++k) En[k] = E[k][c];
+        bi = (long long)(ix - m->bx0) + (long long)m->bnx * ((long long)(iy - m->by0) + (long long)m->bny * (iz - m->bz0));
+    }
+    const long long bs = m->bsize;
+    for (int q = 0; q < nq; ++q) {
+        const T Aq = m->Aq[q], Bq = m->Bq[q], Cq = m->Cq[q];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            T* Pc = m->P + ((long long)(cur * nq + q) * NC + k) * bs;
+            T* Po = m->P + ((long long)((1 - cur) * nq + q) * NC + k) * bs;
+            T pn = Pc[bi], pm = Po[bi];
+            T pnew = Aq * pn + Bq * pm + Cq * En[k];
+            Po[bi] = pnew;
+            sumP[k] += pnew;
+        }
+    }
+    if (plasma) {
+        T E2 = En[0] * En[0];
+#pragma unroll
+        for (int k = 1; k < NC; ++k) E2 = E2 + En[k] * En[k];
+        T II = m->ksi * E2;
+        R rho = m->rho[bi];
+        R drho = m->drho[bi];
+        T Ppn[NC], Ppm[NC], Ppnew[NC];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            T* Pc = m->Pp + ((long long)cur * NC + k) * bs;
+            T* Po = m->Pp + ((long long)(1 - cur) * NC + k) * bs;
+            Ppn[k] = Pc[bi];
+            Ppm[k] = Po[bi];
+            Ppnew[k] = m->Ap * Ppn[k] + m->Bp * Ppm[k] + m->Cp * rho * m->rho0 * En[k];
+            Po[bi] = Ppnew[k];
+        }
+#pragma unroll
+        for (int k = 0; k < NC; ++k) sumP[k] += Ppnew[k];
+        T invE2 = (E2 >= Eps<T>::v()) ? T(1) / E2 : T(0);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            T* pa = m->Pa + (long long)k * bs;
+            T v = pa[bi] + m->Ma * drho * m->rho0 * En[k] * invE2;
+            pa[bi] = v;
+            sumP[k] += v;
+        }
+        if (m->rate_kind == MFD_RATE_TABLE) {
+            T R1 = rate_table<T>(m->rate_x, m->rate_y, m->rate_n, II);
+            plasma_density<T, R, T>(rho, drho, R1, m->Rava * E2, dt);
+        } else if (m->rate_kind == MFD_RATE_POWER) {
+            T lg = log10(II);
+            T a = m->rate_order * lg;
+            double R1 = pow(10.0, (double)a + m->rate_log10c);
+            plasma_density<T, R, double>(rho, drho, R1, m->Rava * E2, dt);
+        } else {
+            plasma_density<T, R, T>(rho, drho, T(0), m->Rava * E2, dt);
+        }
+        m->rho[bi] = rho;
+        m->drho[bi] = drho;
+        T acc = (Ppnew[0] - Ppm[0]) / (2 * dt) * En[0];
+#pragma unroll
+        for (int k = 1; k < NC; ++k) acc = acc + (Ppnew[k] - Ppm[k]) / (2 * dt) * En[k];
+        m->JE[bi] = m->JE[bi] + acc * dt;
+    }
+    if (m->kerr) {
+        const T Mk2 = m->Mk2, Mk3 = m->Mk3;
+        const T Me2 = Me * Me, Me3 = Me * Me * Me;
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            T X = Dv[k] - sumP[k];
+            T X2 = X * X;
+            // Kerr by Meep (models.jl:1143-1149)
+            E[k][c] = (1 + 1 * Mk2 * Me2 * X + 2 * Mk3 * Me3 * X2) /
+                      (1 + 2 * Mk2 * Me2 * X + 3 * Mk3 * Me3 * X2) * X * Me;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NC; ++k) E[k][c] = (Dv[k] - sumP[k]) * Me;
+    }
+}
+
+}  // namespace mfd

@@ -1,0 +1,653 @@
+// yee.cuh -- Yee H and E update kernels (1-D, 2-D, 3-D) for sm_100a.
+//
+// 3-D kernels march along z: a thread owns one (ix, iy) column of a z-chunk and keeps the
+// z-neighbour plane in registers (E at iz+1 for the H update, H at iz-1 for the E update),
+// so each plane of the read-only field is fetched from memory once per chunk; x and y
+// neighbours come from the same or adjacent warps through L1.  The CPML psi recursions are
+// fused into the curls, the material response (ADE poles, plasma, Kerr) into the E update,
+// and the running sums Sa/E2 of the previous step plus the NaN/Inf guard on Ex into the H
+// update, which reads every E and H value of the cell anyway.
+//
+// Reference kernels: src/models.jl:248-437 (1-D), 450-719 (2-D), 735-1162 (3-D).
+#pragma once
+
+#include "mfd_device.cuh"
+
+namespace mfd {
+
+template <typename T>
+struct HParams {
+    Layout L;
+    T dx, dy, dz, dt;
+    int bc[6];
+    LayerDev<T> lay[6];
+    T Mh0;
+    const uint8_t* __restrict__ geom;
+    const T* __restrict__ matMh;     // Mh of material g at matMh[g-1]
+    T* Hx; T* Hy; T* Hz;
+    const T* __restrict__ Ex; const T* __restrict__ Ey; const T* __restrict__ Ez;
+    // running sums of the previous step (outputs.jl:475-485) and NaN/Inf guard (models.jl:202-209)
+    int accum;
+    int sum_e2;
+    T* Sa; T* E2;
+    int* flag;
+    unsigned long long* badstep;
+    long long prev_step;
+};
+
+template <typename T, typename R>
+struct EParams {
+    Layout L;
+    T dx, dy, dz, dt;
+    int bc[6];
+    LayerDev<T> lay[6];
+    T Me0, Md10, Md20;
+    const uint8_t* __restrict__ geom;
+    const MatDev<T, R>* __restrict__ mats;
+    const T* __restrict__ Hx; const T* __restrict__ Hy; const T* __restrict__ Hz;
+    T* Dx; T* Dy; T* Dz;
+    T* Ex; T* Ey; T* Ez;
+    int cur;    // ping-pong buffer holding P^n
+};
+
+template <typename T>
+__device__ __forceinline__ void guard(const HParams<T>& p, T ex) {
+    int bad = (isnan(ex) ? 1 : 0) | (isinf(ex) ? 2 : 0);
+    if (bad) {
+        atomicOr(p.flag, bad);
+        atomicMin(p.badstep, (unsigned long long)p.prev_step);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// 3-D
+// ------------------------------------------------------------------------------------------
+template <typename T, bool MATH>
+__global__ void __launch_bounds__(256) h3d_kernel(const __grid_constant__ HParams<T> p, const int zc) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
+    if (ix >= nx || iy >= ny) return;
+    const int z0 = blockIdx.z * zc;
+    const int z1 = min(z0 + zc, nz);
+    const long long sy = p.L.px, sz = p.L.sz;
+    long long c = ix + sy * iy + sz * z0;
+    const T dx = p.dx, dy = p.dy, dz = p.dz;
+    T ex = p.Ex[c], ey = p.Ey[c];
+    const bool xr = ix == nx - 1, yr = iy == ny - 1;
+    const long long wx = -(long long)(nx - 1), wy = -(long long)(ny - 1) * sy, wz = -(long long)(nz - 1) * sz;
+    for (int iz = z0; iz < z1; ++iz, c += sz) {
+        const T ez = p.Ez[c];
+        T ey_xp, ez_xp, ex_yp, ez_yp, ex_zp, ey_zp;
+        if (!xr) { ey_xp = p.Ey[c + 1]; ez_xp = p.Ez[c + 1]; }
+        else {
+            const int b = p.bc[MFD_XR];
+            ey_xp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ey[c + wx] : T(0), ey);
+            ez_xp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ez[c + wx] : T(0), ez);
+        }
+        if (!yr) { ex_yp = p.Ex[c + sy]; ez_yp = p.Ez[c + sy]; }
+        else {
+            const int b = p.bc[MFD_YR];
+            ex_yp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ex[c + wy] : T(0), ex);
+            ez_yp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ez[c + wy] : T(0), ez);
+        }
+        if (iz < nz - 1) { ex_zp = p.Ex[c + sz]; ey_zp = p.Ey[c + sz]; }
+        else {
+            const int b = p.bc[MFD_ZR];
+            ex_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ex[c + wz] : T(0), ex);
+            ey_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ey[c + wz] : T(0), ey);
+        }
+        T hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
+        if (p.accum) {
+            const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
+            p.Sa[c] = p.Sa[c] + sqrt(a * a + b * b + d * d) * p.dt;
+            if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
+            guard(p, ex);
+        }
+        T Mh = p.Mh0;
+        if (MATH) {
+            const int g = p.geom[c];
+            if (g) Mh = p.matMh[g - 1];
+        }
+        T dExy = (ex_yp - ex) / dy;
+        T dExz = (ex_zp - ex) / dz;
+        T dEyx = (ey_xp - ey) / dx;
+        T dEyz = (ey_zp - ey) / dz;
+        T dEzx = (ez_xp - ez) / dx;
+        T dEzy = (ez_yp - ez) / dy;
+        // CPML (models.jl:811-871)
+        {
+            const LayerDev<T>& l = p.lay[MFD_XL];
+            if (l.nb && ix < l.ib) {
+                const int q = ix;
+                const long long k = q + (long long)l.nb * (iy + (long long)ny * iz);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pEyx = B * l.psi[2][k] + A * dEyx;
+                const T pEzx = B * l.psi[3][k] + A * dEzx;
+                l.psi[2][k] = pEyx; l.psi[3][k] = pEzx;
+                hy += Mh * pEzx;
+                hz -= Mh * pEyx;
+                dEyx = dEyx / K;
+                dEzx = dEzx / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_XR];
+            if (l.nb && ix >= l.ib - 1) {
+                const int q = ix - (l.ib - 1);
+                const long long k = q + (long long)l.nb * (iy + (long long)ny * iz);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pEyx = B * l.psi[2][k] + A * dEyx;
+                const T pEzx = B * l.psi[3][k] + A * dEzx;
+                l.psi[2][k] = pEyx; l.psi[3][k] = pEzx;
+                hy += Mh * pEzx;
+                hz -= Mh * pEyx;
+                dEyx = dEyx / K;
+                dEzx = dEzx / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_YL];
+            if (l.nb && iy < l.ib) {
+                const int q = iy;
+                const long long k = ix + sy * (q + (long long)l.nb * iz);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pExy = B * l.psi[2][k] + A * dExy;
+                const T pEzy = B * l.psi[3][k] + A * dEzy;
+                l.psi[2][k] = pExy; l.psi[3][k] = pEzy;
+                hx -= Mh * pEzy;
+                hz += Mh * pExy;
+                dExy = dExy / K;
+                dEzy = dEzy / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_YR];
+            if (l.nb && iy >= l.ib - 1) {
+                const int q = iy - (l.ib - 1);
+                const long long k = ix + sy * (q + (long long)l.nb * iz);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pExy = B * l.psi[2][k] + A * dExy;
+                const T pEzy = B * l.psi[3][k] + A * dEzy;
+                l.psi[2][k] = pExy; l.psi[3][k] = pEzy;
+                hx -= Mh * pEzy;
+                hz += Mh * pExy;
+                dExy = dExy / K;
+                dEzy = dEzy / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_ZL];
+            if (l.nb && iz < l.ib) {
+                const int q = iz;
+                const long long k = ix + sy * (iy + (long long)ny * q);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pExz = B * l.psi[2][k] + A * dExz;
+                const T pEyz = B * l.psi[3][k] + A * dEyz;
+                l.psi[2][k] = pExz; l.psi[3][k] = pEyz;
+                hx += Mh * pEyz;
+                hy -= Mh * pExz;
+                dExz = dExz / K;
+                dEyz = dEyz / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_ZR];
+            if (l.nb && iz >= l.ib - 1) {
+                const int q = iz - (l.ib - 1);
+                const long long k = ix + sy * (iy + (long long)ny * q);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pExz = B * l.psi[2][k] + A * dExz;
+                const T pEyz = B * l.psi[3][k] + A * dEyz;
+                l.psi[2][k] = pExz; l.psi[3][k] = pEyz;
+                hx += Mh * pEyz;
+                hy -= Mh * pExz;
+                dExz = dExz / K;
+                dEyz = dEyz / K;
+            }
+        }
+        hx -= Mh * (dEzy - dEyz);
+        hy -= Mh * (dExz - dEzx);
+        hz -= Mh * (dEyx - dExy);
+        p.Hx[c] = hx; p.Hy[c] = hy; p.Hz[c] = hz;
+        ex = ex_zp;
+        ey = ey_zp;
+    }
+}
+
+template <typename T, typename R, bool MAT>
+__global__ void __launch_bounds__(256) e3d_kernel(const __grid_constant__ EParams<T, R> p, const int zc) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
+    if (ix >= nx || iy >= ny) return;
+    const int z0 = blockIdx.z * zc;
+    const int z1 = min(z0 + zc, nz);
+    const long long sy = p.L.px, sz = p.L.sz;
+    long long c = ix + sy * iy + sz * z0;
+    const T dx = p.dx, dy = p.dy, dz = p.dz;
+    const bool xl = ix == 0, yl = iy == 0;
+    const long long wx = (long long)(nx - 1), wy = (long long)(ny - 1) * sy, wz = (long long)(nz - 1) * sz;
+    T hx_zm, hy_zm;
+    if (z0 > 0) { hx_zm = p.Hx[c - sz]; hy_zm = p.Hy[c - sz]; }
+    else {
+        const int b = p.bc[MFD_ZL];
+        hx_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hx[c + wz] : T(0), p.Hx[c]);
+        hy_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + wz] : T(0), p.Hy[c]);
+    }
+    T* const Ep[3] = {p.Ex, p.Ey, p.Ez};
+    for (int iz = z0; iz < z1; ++iz, c += sz) {
+        const T hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
+        T hy_xm, hz_xm, hx_ym, hz_ym;
+        if (!xl) { hy_xm = p.Hy[c - 1]; hz_xm = p.Hz[c - 1]; }
+        else {
+            const int b = p.bc[MFD_XL];
+            hy_xm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + wx] : T(0), hy);
+            hz_xm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hz[c + wx] : T(0), hz);
+        }
+        if (!yl) { hx_ym = p.Hx[c - sy]; hz_ym = p.Hz[c - sy]; }
+        else {
+            const int b = p.bc[MFD_YL];
+            hx_ym = bc_value(b, b == MFD_BC_PERIODIC ? p.Hx[c + wy] : T(0), hx);
+            hz_ym = bc_value(b, b == MFD_BC_PERIODIC ? p.Hz[c + wy] : T(0), hz);
+        }
+        T dHxy = (hx - hx_ym) / dy;
+        T dHxz = (hx - hx_zm) / dz;
+        T dHyx = (hy - hy_xm) / dx;
+        T dHyz = (hy - hy_zm) / dz;
+        T dHzx = (hz - hz_xm) / dx;
+        T dHzy = (hz - hz_ym) / dy;
+        int g = 0;
+        T Md1 = p.Md10, Md2 = p.Md20;
+        if (MAT) {
+            g = p.geom[c];
+            if (g) { Md1 = p.mats[g - 1].Md1; Md2 = p.mats[g - 1].Md2; }
+        }
+        T Dv[3] = {p.Dx[c], p.Dy[c], p.Dz[c]};
+        // CPML (models.jl:975-1035)
+        {
+            const LayerDev<T>& l = p.lay[MFD_XL];
+            if (l.nb && ix < l.ib) {
+                const int q = ix;
+                const long long k = q + (long long)l.nb * (iy + (long long)ny * iz);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pHyx = B * l.psi[0][k] + A * dHyx;
+                const T pHzx = B * l.psi[1][k] + A * dHzx;
+                l.psi[0][k] = pHyx; l.psi[1][k] = pHzx;
+                Dv[1] -= Md2 * pHzx;
+                Dv[2] += Md2 * pHyx;
+                dHyx = dHyx / K;
+                dHzx = dHzx / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_XR];
+            if (l.nb && ix >= l.ib - 1) {
+                const int q = ix - (l.ib - 1);
+                const long long k = q + (long long)l.nb * (iy + (long long)ny * iz);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pHyx = B * l.psi[0][k] + A * dHyx;
+                const T pHzx = B * l.psi[1][k] + A * dHzx;
+                l.psi[0][k] = pHyx; l.psi[1][k] = pHzx;
+                Dv[1] -= Md2 * pHzx;
+                Dv[2] += Md2 * pHyx;
+                dHyx = dHyx / K;
+                dHzx = dHzx / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_YL];
+            if (l.nb && iy < l.ib) {
+                const int q = iy;
+                const long long k = ix + sy * (q + (long long)l.nb * iz);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pHxy = B * l.psi[0][k] + A * dHxy;
+                const T pHzy = B * l.psi[1][k] + A * dHzy;
+                l.psi[0][k] = pHxy; l.psi[1][k] = pHzy;
+                Dv[0] += Md2 * pHzy;
+                Dv[2] -= Md2 * pHxy;
+                dHxy = dHxy / K;
+                dHzy = dHzy / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_YR];
+            if (l.nb && iy >= l.ib - 1) {
+                const int q = iy - (l.ib - 1);
+                const long long k = ix + sy * (q + (long long)l.nb * iz);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pHxy = B * l.psi[0][k] + A * dHxy;
+                const T pHzy = B * l.psi[1][k] + A * dHzy;
+                l.psi[0][k] = pHxy; l.psi[1][k] = pHzy;
+                Dv[0] += Md2 * pHzy;
+                Dv[2] -= Md2 * pHxy;
+                dHxy = dHxy / K;
+                dHzy = dHzy / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_ZL];
+            if (l.nb && iz < l.ib) {
+                const int q = iz;
+                const long long k = ix + sy * (iy + (long long)ny * q);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pHxz = B * l.psi[0][k] + A * dHxz;
+                const T pHyz = B * l.psi[1][k] + A * dHyz;
+                l.psi[0][k] = pHxz; l.psi[1][k] = pHyz;
+                Dv[0] -= Md2 * pHyz;
+                Dv[1] += Md2 * pHxz;
+                dHxz = dHxz / K;
+                dHyz = dHyz / K;
+            }
+        }
+        {
+            const LayerDev<T>& l = p.lay[MFD_ZR];
+            if (l.nb && iz >= l.ib - 1) {
+                const int q = iz - (l.ib - 1);
+                const long long k = ix + sy * (iy + (long long)ny * q);
+                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const T pHxz = B * l.psi[0][k] + A * dHxz;
+                const T pHyz = B * l.psi[1][k] + A * dHyz;
+                l.psi[0][k] = pHxz; l.psi[1][k] = pHyz;
+                Dv[0] -= Md2 * pHyz;
+                Dv[1] += Md2 * pHxz;
+                dHxz = dHxz / K;
+                dHyz = dHyz / K;
+            }
+        }
+        Dv[0] = Md1 * Dv[0] + Md2 * (dHzy - dHyz);
+        Dv[1] = Md1 * Dv[1] + Md2 * (dHxz - dHzx);
+        Dv[2] = Md1 * Dv[2] + Md2 * (dHyx - dHxy);
+        p.Dx[c] = Dv[0]; p.Dy[c] = Dv[1]; p.Dz[c] = Dv[2];
+        if (MAT && g) {
+            material_cell<T, R, 3>(p.mats + (g - 1), ix, iy, iz, Ep, c, Dv, p.cur, p.dt);
+        } else {
+            p.Ex[c] = Dv[0] * p.Me0;
+            p.Ey[c] = Dv[1] * p.Me0;
+            p.Ez[c] = Dv[2] * p.Me0;
+        }
+        hx_zm = hx;
+        hy_zm = hy;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// 2-D (x-z plane): one thread per cell
+// ------------------------------------------------------------------------------------------
+template <typename T, bool MATH>
+__global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParams<T> p) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.L.nx, nz = p.L.nz;
+    if (ix >= nx || iz >= nz) return;
+    const long long sz = p.L.sz;
+    const long long c = ix + sz * iz;
+    const T ex = p.Ex[c], ez = p.Ez[c];
+    T ez_xp, ex_zp;
+    if (ix < nx - 1) ez_xp = p.Ez[c + 1];
+    else { const int b = p.bc[MFD_XR]; ez_xp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ez[c - (nx - 1)] : T(0), ez); }
+    if (iz < nz - 1) ex_zp = p.Ex[c + sz];
+    else { const int b = p.bc[MFD_ZR]; ex_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ex[c - (long long)(nz - 1) * sz] : T(0), ex); }
+    T hy = p.Hy[c];
+    if (p.accum) {
+        const T a = -ez * hy, b = ex * hy;
+        p.Sa[c] = p.Sa[c] + sqrt(a * a + b * b) * p.dt;
+        if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ez * ez) * p.dt;
+        guard(p, ex);
+    }
+    T Mh = p.Mh0;
+    if (MATH) { const int g = p.geom[c]; if (g) Mh = p.matMh[g - 1]; }
+    T dExz = (ex_zp - ex) / p.dz;
+    T dEzx = (ez_xp - ez) / p.dx;
+    {
+        const LayerDev<T>& l = p.lay[MFD_XL];
+        if (l.nb && ix < l.ib) {
+            const int q = ix;
+            const long long k = q + (long long)l.nb * iz;
+            const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEzx;
+            l.psi[1][k] = ps;
+            hy += Mh * ps;
+            dEzx = dEzx / l.K[q];
+        }
+    }
+    {
+        const LayerDev<T>& l = p.lay[MFD_XR];
+        if (l.nb && ix >= l.ib - 1) {
+            const int q = ix - (l.ib - 1);
+            const long long k = q + (long long)l.nb * iz;
+            const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEzx;
+            l.psi[1][k] = ps;
+            hy += Mh * ps;
+            dEzx = dEzx / l.K[q];
+        }
+    }
+    {
+        const LayerDev<T>& l = p.lay[MFD_ZL];
+        if (l.nb && iz < l.ib) {
+            const int q = iz;
+            const long long k = ix + (long long)p.L.px * q;
+            const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dExz;
+            l.psi[1][k] = ps;
+            hy -= Mh * ps;
+            dExz = dExz / l.K[q];
+        }
+    }
+    {
+        const LayerDev<T>& l = p.lay[MFD_ZR];
+        if (l.nb && iz >= l.ib - 1) {
+            const int q = iz - (l.ib - 1);
+            const long long k = ix + (long long)p.L.px * q;
+            const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dExz;
+            l.psi[1][k] = ps;
+            hy -= Mh * ps;
+            dExz = dExz / l.K[q];
+        }
+    }
+    hy -= Mh * (dExz - dEzx);
+    p.Hy[c] = hy;
+}
+
+template <typename T, typename R, bool MAT>
+__global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParams<T, R> p) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.L.nx, nz = p.L.nz;
+    if (ix >= nx || iz >= nz) return;
+    const long long sz = p.L.sz;
+    const long long c = ix + sz * iz;
+    const T hy = p.Hy[c];
+    T hy_xm, hy_zm;
+    if (ix > 0) hy_xm = p.Hy[c - 1];
+    else { const int b = p.bc[MFD_XL]; hy_xm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + (nx - 1)] : T(0), hy); }
+    if (iz > 0) hy_zm = p.Hy[c - sz];
+    else { const int b = p.bc[MFD_ZL]; hy_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + (long long)(nz - 1) * sz] : T(0), hy); }
+    T dHyx = (hy - hy_xm) / p.dx;
+    T dHyz = (hy - hy_zm) / p.dz;
+    int g = 0;
+    T Md1 = p.Md10, Md2 = p.Md20;
+    if (MAT) {
+        g = p.geom[c];
+        if (g) { Md1 = p.mats[g - 1].Md1; Md2 = p.mats[g - 1].Md2; }
+    }
+    T Dv[2] = {p.Dx[c], p.Dz[c]};
+    {
+        const LayerDev<T>& l = p.lay[MFD_XL];
+        if (l.nb && ix < l.ib) {
+            const int q = ix;
+            const long long k = q + (long long)l.nb * iz;
+            const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyx;
+            l.psi[0][k] = ps;
+            Dv[1] += Md2 * ps;
+            dHyx = dHyx / l.K[q];
+        }
+    }
+    {
+        const LayerDev<T>& l = p.lay[MFD_XR];
+        if (l.nb && ix >= l.ib - 1) {
+            const int q = ix - (l.ib - 1);
+            const long long k = q + (long long)l.nb * iz;
+            const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyx;
+            l.psi[0][k] = ps;
+            Dv[1] += Md2 * ps;
+            dHyx = dHyx / l.K[q];
+        }
+    }
+    {
+        const LayerDev<T>& l = p.lay[MFD_ZL];
+        if (l.nb && iz < l.ib) {
+            const int q = iz;
+            const long long k = ix + (long long)p.L.px * q;
+            const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyz;
+            l.psi[0][k] = ps;
+            Dv[0] -= Md2 * ps;
+            dHyz = dHyz / l.K[q];
+        }
+    }
+    {
+        const LayerDev<T>& l = p.lay[MFD_ZR];
+        if (l.nb && iz >= l.ib - 1) {
+            const int q = iz - (l.ib - 1);
+            const long long k = ix + (long long)p.L.px * q;
+            const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyz;
+            l.psi[0][k] = ps;
+            Dv[0] -= Md2 * ps;
+            dHyz = dHyz / l.K[q];
+        }
+    }
+    Dv[0] = Md1 * Dv[0] + Md2 * (T(0) - dHyz);
+    Dv[1] = Md1 * Dv[1] + Md2 * (dHyx - T(0));
+    p.Dx[c] = Dv[0]; p.Dz[c] = Dv[1];
+    if (MAT && g) {
+        T* const Ep[2] = {p.Ex, p.Ez};
+        material_cell<T, R, 2>(p.mats + (g - 1), ix, 0, iz, Ep, c, Dv, p.cur, p.dt);
+    } else {
+        p.Ex[c] = Dv[0] * p.Me0;
+        p.Ez[c] = Dv[1] * p.Me0;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// 1-D (z)
+// ------------------------------------------------------------------------------------------
+template <typename T, bool MATH>
+__global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParams<T> p) {
+    const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nz = p.L.nz;
+    if (iz >= nz) return;
+    const long long c = iz;
+    const T ex = p.Ex[c];
+    T ex_zp;
+    if (iz < nz - 1) ex_zp = p.Ex[c + 1];
+    else { const int b = p.bc[MFD_ZR]; ex_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ex[0] : T(0), ex); }
+    T hy = p.Hy[c];
+    if (p.accum) {
+        const T a = ex * hy;
+        p.Sa[c] = p.Sa[c] + sqrt(a * a) * p.dt;
+        if (p.sum_e2) p.E2[c] = p.E2[c] + ex * ex * p.dt;
+        guard(p, ex);
+    }
+    T Mh = p.Mh0;
+    if (MATH) { const int g = p.geom[c]; if (g) Mh = p.matMh[g - 1]; }
+    T dExz = (ex_zp - ex) / p.dz;
+    {
+        const LayerDev<T>& l = p.lay[MFD_ZL];
+        if (l.nb && iz < l.ib) {
+            const int q = iz;
+            const T ps = l.B[q] * l.psi[1][q] + l.A[q] * dExz;
+            l.psi[1][q] = ps;
+            hy -= Mh * ps;
+            dExz = dExz / l.K[q];
+        }
+    }
+    {
+        const LayerDev<T>& l = p.lay[MFD_ZR];
+        if (l.nb && iz >= l.ib - 1) {
+            const int q = iz - (l.ib - 1);
+            const T ps = l.B[q] * l.psi[1][q] + l.A[q] * dExz;
+            l.psi[1][q] = ps;
+            hy -= Mh * ps;
+            dExz = dExz / l.K[q];
+        }
+    }
+    hy -= Mh * (T(0) + dExz);
+    p.Hy[c] = hy;
+}
+
+template <typename T, typename R, bool MAT>
+__global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParams<T, R> p) {
+    const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nz = p.L.nz;
+    if (iz >= nz) return;
+    const long long c = iz;
+    const T hy = p.Hy[c];
+    T hy_zm;
+    if (iz > 0) hy_zm = p.Hy[c - 1];
+    else { const int b = p.bc[MFD_ZL]; hy_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[nz - 1] : T(0), hy); }
+    T dHyz = (hy - hy_zm) / p.dz;
+    int g = 0;
+    T Md1 = p.Md10, Md2 = p.Md20;
+    if (MAT) {
+        g = p.geom[c];
+        if (g) { Md1 = p.mats[g - 1].Md1; Md2 = p.mats[g - 1].Md2; }
+    }
+    T Dv[1] = {p.Dx[c]};
+    {
+        const LayerDev<T>& l = p.lay[MFD_ZL];
+        if (l.nb && iz < l.ib) {
+            const int q = iz;
+            const T ps = l.B[q] * l.psi[0][q] + l.A[q] * dHyz;
+            l.psi[0][q] = ps;
+            Dv[0] -= Md2 * ps;
+            dHyz = dHyz / l.K[q];
+        }
+    }
+    {
+        const LayerDev<T>& l = p.lay[MFD_ZR];
+        if (l.nb && iz >= l.ib - 1) {
+            const int q = iz - (l.ib - 1);
+            const T ps = l.B[q] * l.psi[0][q] + l.A[q] * dHyz;
+            l.psi[0][q] = ps;
+            Dv[0] -= Md2 * ps;
+            dHyz = dHyz / l.K[q];
+        }
+    }
+    Dv[0] = Md1 * Dv[0] + Md2 * (T(0) - dHyz);
+    p.Dx[c] = Dv[0];
+    if (MAT && g) {
+        T* const Ep[1] = {p.Ex};
+        material_cell<T, R, 1>(p.mats + (g - 1), 0, 0, iz, Ep, c, Dv, p.cur, p.dt);
+    } else {
+        p.Ex[c] = Dv[0] * p.Me0;
+    }
+}
+
+// Running sums and NaN/Inf guard for the last step of a run (the H kernel of the next step
+// does this for every other step).
+template <typename T>
+__global__ void __launch_bounds__(256) sums_kernel(const __grid_constant__ HParams<T> p, const int ndim) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y;
+    const int iz = blockIdx.z;
+    if (ix >= p.L.nx) return;
+    const long long c = ix + (long long)p.L.px * iy + p.L.sz * iz;
+    const T ex = p.Ex[c];
+    if (ndim == 3) {
+        const T ey = p.Ey[c], ez = p.Ez[c], hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
+        const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
+        p.Sa[c] = p.Sa[c] + sqrt(a * a + b * b + d * d) * p.dt;
+        if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
+    } else if (ndim == 2) {
+        const T ez = p.Ez[c], hy = p.Hy[c];
+        const T a = -ez * hy, b = ex * hy;
+        p.Sa[c] = p.Sa[c] + sqrt(a * a + b * b) * p.dt;
+        if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ez * ez) * p.dt;
+    } else {
+        const T hy = p.Hy[c];
+        const T a = ex * hy;
+        p.Sa[c] = p.Sa[c] + sqrt(a * a) * p.dt;
+        if (p.sum_e2) p.E2[c] = p.E2[c] + ex * ex * p.dt;
+    }
+    guard(p, ex);
+}
+
+}  // namespace mfd

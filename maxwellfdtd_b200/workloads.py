@@ -1,0 +1,120 @@
+"""Synthetic workloads of the benchmark configurations, built through the public API.
+
+plasmonics_256: 256^3 grid, dx = 2 nm, 12-cell CPML, a gold-like sphere (radius 60 nm,
+eps_inf = 9, Drude wp = 1.37e16 rad/s, gamma = 1.07e14 1/s, one Lorentz pole deps = 1.1,
+w0 = 4.2e15 rad/s, gamma = 1.0e15 1/s i.e. delta = gamma/2), an x-polarised broadband TFSF
+plane wave along +z (600 nm, 3 fs), and DFT monitors on the six faces of a 160^3 box at 64
+wavelengths 400-900 nm with double-precision sums.  The incident TFSF data are the
+analytic plane wave sampled at the Yee positions, standing in for a vacuum record run.
+
+dielectric_100: 100^3 grid, dx = 20 nm, 10-cell CPML, Float64, a dielectric sphere
+(radius 500 nm, eps = 2.25), a TFSF x-polarised Gaussian pulse (800 nm, 10 fs intensity
+FWHM) along +z, and one point monitor.
+"""
+import numpy as np
+
+from . import (C0, EPS0, MU0, Grid, DrudeSusceptibility, FieldMonitor, LorentzSusceptibility, Material, Model,
+               SpectralMonitor, TFSFSource)
+from .model import time_range, time_step
+from .sources import TFSF_NAMES_3D
+
+
+def _plane_wave_tfsf(grid, i1, i2, t, f, zs, dt):
+    """TFSF record data of an x-polarised plane wave along +z: Ex = f(t - (z - zs)/c),
+    Hy = Ex/eta0 sampled half a cell up and half a step earlier."""
+    eta0 = np.sqrt(MU0 / EPS0)
+    (ix1, iy1, iz1), (ix2, iy2, iz2) = i1, i2
+    Nxi, Nyi, Nzi = ix2 - ix1, iy2 - iy1, iz2 - iz1
+    z = grid.z
+    dz = grid.dz
+    nt = len(t)
+    te = t + dt          # E at the end of step it
+    th = t + dt / 2      # H half a step earlier
+
+    def Ex(zv):
+        return f(te[:, None] - (zv[None, :] - zs) / C0)
+
+    def Hy(zv):
+        return f(th[:, None] - (zv[None, :] + dz / 2 - zs) / C0) / eta0
+
+    d = {"t": np.asarray(t), "box": np.array([grid.x[ix1 - 1], grid.x[ix2 - 1], grid.y[iy1 - 1], grid.y[iy2 - 1],
+                                              grid.z[iz1 - 1], grid.z[iz2 - 1]]),
+         "x": grid.x[ix1 - 1:ix2], "y": grid.y[iy1 - 1:iy2], "z": grid.z[iz1 - 1:iz2]}
+    zh = z[iz1 - 1:iz2 - 1]      # iz1 .. iz2-1
+    zf = z[iz1 - 1:iz2]          # iz1 .. iz2
+    shapes = {}
+    for k, name in enumerate(TFSF_NAMES_3D):
+        face, j = k // 4, k % 4
+        if face < 2:
+            a, b = (Nyi + 1, Nzi) if j in (0, 3) else (Nyi, Nzi + 1)
+        elif face < 4:
+            a, b = (Nxi + 1, Nzi) if j in (0, 3) else (Nxi, Nzi + 1)
+        else:
+            a, b = (Nxi + 1, Nyi) if j in (0, 3) else (Nxi, Nyi + 1)
+        shapes[name] = (nt, b, a)
+        d[name] = np.zeros((nt, b, a), dtype=np.float32)
+    for name in ("incHy_1yz", "incHy_2yz"):          # (Nyi+1, Nzi): z in iz1..iz2-1
+        d[name][:] = Hy(zh)[:, :, None]
+    for name in ("incEx_x1z", "incEx_x2z"):          # (Nxi, Nzi+1): z in iz1..iz2
+        d[name][:] = Ex(zf)[:, :, None]
+    d["incHy_xy1"][:] = Hy(z[iz1 - 2:iz1 - 1])[:, :, None]
+    d["incEx_xy1"][:] = Ex(z[iz1 - 1:iz1])[:, :, None]
+    d["incHy_xy2"][:] = Hy(z[iz2 - 1:iz2])[:, :, None]
+    d["incEx_xy2"][:] = Ex(z[iz2 - 1:iz2])[:, :, None]
+    return d
+
+
+def plasmonics_256(nt=4000, n=256, with_monitors=True):
+    dx = 2e-9
+    L = (n - 1) * dx / 2
+    grid = Grid(xmin=-L, xmax=L, Nx=n, ymin=-L, ymax=L, Ny=n, zmin=-L, zmax=L, Nz=n)
+    r = 60e-9
+    gold = Material(geometry=lambda x, y, z: x * x + y * y + z * z <= r * r, eps=9.0,
+                    chi=[DrudeSusceptibility(wp=1.37e16, gamma=1.07e14),
+                         LorentzSusceptibility(deps=1.1, w0=4.2e15, delta=0.5e15)])
+    dt = time_step(grid, 0.5)
+    t = time_range(dt, (nt - 0.5) * dt)
+    tau = 3e-15
+    t0 = 3 * tau
+    w0 = 2 * np.pi * C0 / 600e-9
+    f = lambda s: np.exp(-2 * np.log(2) * (s - t0) ** 2 / tau ** 2) * np.cos(w0 * (s - t0))
+    m = 20                                   # TFSF box faces 20 cells in from the edges
+    i1, i2 = (m, m, m), (n + 1 - m, n + 1 - m, n + 1 - m)
+    data = _plane_wave_tfsf(grid, i1, i2, t, f, grid.z[i1[2] - 1], dt)
+    model = Model(grid, TFSFSource(data=data), tmax=(nt - 0.5) * dt, pml=12 * dx, material=gold)
+    mons = None
+    if with_monitors:
+        h = 80 * dx + dx / 2                # faces on grid planes (coordinates are odd multiples of dx/2)
+        lam = np.linspace(400e-9, 900e-9, 64)
+        w = 2 * np.pi * C0 / lam
+        eps = dx / 2
+        box = lambda a: (np.abs(a) <= h + eps)
+        faces = [
+            lambda x, y, z: (np.abs(x + h) < eps) & box(y) & box(z),
+            lambda x, y, z: (np.abs(x - h) < eps) & box(y) & box(z),
+            lambda x, y, z: (np.abs(y + h) < eps) & box(x) & box(z),
+            lambda x, y, z: (np.abs(y - h) < eps) & box(x) & box(z),
+            lambda x, y, z: (np.abs(z + h) < eps) & box(x) & box(y),
+            lambda x, y, z: (np.abs(z - h) < eps) & box(x) & box(y),
+        ]
+        mons = [SpectralMonitor(fc, w=w) for fc in faces]
+    return model, mons
+
+
+def dielectric_100(nt=1000, n=100):
+    dx = 20e-9
+    L = (n - 1) * dx / 2
+    grid = Grid(xmin=-L, xmax=L, Nx=n, ymin=-L, ymax=L, Ny=n, zmin=-L, zmax=L, Nz=n)
+    r = 500e-9
+    mat = Material(geometry=lambda x, y, z: x * x + y * y + z * z <= r * r, eps=2.25)
+    dt = time_step(grid, 0.5)
+    t = time_range(dt, (nt - 0.5) * dt)
+    fwhm = 10e-15
+    t0 = 3 * fwhm
+    w0 = 2 * np.pi * C0 / 800e-9
+    f = lambda s: np.exp(-2 * np.log(2) * (s - t0) ** 2 / fwhm ** 2) * np.cos(w0 * (s - t0))
+    m = 11
+    i1, i2 = (m, m, m), (n + 1 - m, n + 1 - m, n + 1 - m)
+    data = _plane_wave_tfsf(grid, i1, i2, t, f, grid.z[i1[2] - 1], dt)
+    model = Model(grid, TFSFSource(data=data), tmax=(nt - 0.5) * dt, pml=10 * dx, material=mat)
+    return model, [FieldMonitor((0.0, 0.0, 0.0))]

@@ -1,0 +1,127 @@
+"""The C ABI: the CUDA library loads without a GPU and exports every function declared in
+include/maxwellfdtd.h; the ctypes mirror has the same struct layout as the C compiler;
+mfd_create reports a clear error (no crash) when there is no device or the descriptor is bad."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import maxwellfdtd_b200 as M
+from maxwellfdtd_b200 import _abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "maxwellfdtd.h")
+
+
+def declared_functions():
+    with open(HEADER) as f:
+        src = f.read()
+    return sorted(set(re.findall(r"MFD_API\s+[\w\s\*]+?\b(mfd_\w+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def cuda_lib():
+    from maxwellfdtd_b200 import build
+    build.build()
+    return C.CDLL(build.OUT)
+
+
+def test_library_exports_every_declared_function(cuda_lib):
+    names = declared_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(cuda_lib, n)]
+    assert not missing, missing
+
+
+def test_oracle_exports_the_same_api(oracle_lib):
+    for n in declared_functions():
+        short = n[len("mfd_"):]
+        if short in ("set_profiling", "kernel_times", "last_run_ms", "device_bytes", "abi_version"):
+            continue
+        assert hasattr(oracle_lib.lib, "oracle_" + short), short
+
+
+def _c_layout():
+    prog = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "maxwellfdtd.h"
+#define F(s, m) printf(#s "." #m " %zu\n", offsetof(s, m));
+int main(void) {
+  printf("mfd_pml_layer %zu\n", sizeof(mfd_pml_layer));
+  printf("mfd_material %zu\n", sizeof(mfd_material));
+  printf("mfd_source %zu\n", sizeof(mfd_source));
+  printf("mfd_tfsf %zu\n", sizeof(mfd_tfsf));
+  printf("mfd_monitor %zu\n", sizeof(mfd_monitor));
+  printf("mfd_desc %zu\n", sizeof(mfd_desc));
+  F(mfd_desc, dt) F(mfd_desc, nt) F(mfd_desc, bc) F(mfd_desc, pml) F(mfd_desc, Mh0) F(mfd_desc, geometry)
+  F(mfd_desc, nmat) F(mfd_desc, mats) F(mfd_desc, rho_fp64) F(mfd_desc, nsrc) F(mfd_desc, srcs)
+  F(mfd_desc, tfsf) F(mfd_desc, nmon) F(mfd_desc, mons) F(mfd_desc, tfsf_record) F(mfd_desc, rec_i1)
+  F(mfd_desc, rec_i2) F(mfd_desc, device)
+  F(mfd_material, nq) F(mfd_material, Aq) F(mfd_material, kerr) F(mfd_material, plasma) F(mfd_material, Rava)
+  F(mfd_material, rate_kind) F(mfd_material, rate_order) F(mfd_material, rate_n) F(mfd_material, rate_y)
+  F(mfd_source, coeff) F(mfd_source, npts) F(mfd_source, cells) F(mfd_source, gt)
+  F(mfd_tfsf, order) F(mfd_tfsf, i1) F(mfd_tfsf, i2) F(mfd_tfsf, inc)
+  F(mfd_monitor, npts) F(mfd_monitor, cells) F(mfd_monitor, nw) F(mfd_monitor, phasor)
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "lay.c")
+        exe = os.path.join(d, "lay")
+        with open(src, "w") as f:
+            f.write(prog)
+        subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), src, "-o", exe])
+        out = subprocess.check_output([exe]).decode()
+    return {l.split()[0]: int(l.split()[1]) for l in out.strip().splitlines()}
+
+
+def test_ctypes_layout_matches_c():
+    lay = _c_layout()
+    types = {"mfd_pml_layer": _abi.PmlLayer, "mfd_material": _abi.Material, "mfd_source": _abi.Source,
+             "mfd_tfsf": _abi.Tfsf, "mfd_monitor": _abi.Monitor, "mfd_desc": _abi.Desc}
+    for k, v in lay.items():
+        if "." in k:
+            s, m = k.split(".")
+            assert getattr(types[s], m).offset == v, k
+        else:
+            assert C.sizeof(types[k]) == v, k
+
+
+def _tiny_model():
+    g = M.Grid(zmin=0, zmax=1e-6, Nz=21)
+    src = M.SoftSource(geometry=(0.5e-6,), waveform=lambda z, t: np.sin(1e15 * t), component="Ex")
+    return M.Model(g, src, tmax=1e-15, pml=0.1e-6)
+
+
+def test_create_without_device_or_with_bad_desc_returns_status(cuda_lib):
+    lib = _abi.Library(os.path.join(ROOT, "maxwellfdtd_b200", "libmaxwellfdtd_b200.so"), "mfd_")
+    b, _ = _tiny_model().build_desc(np.float32)
+    b.desc.abi_version = 999
+    h = C.c_void_p()
+    st = lib.create(C.byref(b.desc), C.byref(h))
+    assert st == _abi.MFD_ERR_INVALID
+    assert "ABI" in lib.create_error().decode()
+    b.desc.abi_version = _abi.ABI_VERSION
+    st = lib.create(C.byref(b.desc), C.byref(h))
+    assert st in (_abi.MFD_OK, _abi.MFD_ERR_NODEVICE)
+    if st == _abi.MFD_OK:
+        lib.destroy(h)
+
+
+def test_oracle_rejects_bad_descriptors(oracle_lib):
+    m = _tiny_model()
+    b, _ = m.build_desc(np.float64)
+    b.desc.ndim = 2    # 2-D with ny = 1 but nx = 1 is fine; make nz invalid instead
+    b.desc.nz = 0
+    h = C.c_void_p()
+    assert oracle_lib.create(C.byref(b.desc), C.byref(h)) == _abi.MFD_ERR_INVALID
+    b, _ = m.build_desc(np.float64)
+    b.desc.tfsf.enabled = 1
+    b.desc.tfsf.i1[2], b.desc.tfsf.i2[2] = 1, 5
+    assert oracle_lib.create(C.byref(b.desc), C.byref(h)) == _abi.MFD_ERR_INVALID
+    assert "TFSF box" in oracle_lib.create_error().decode()

@@ -1,0 +1,116 @@
+"""GPU parity: the CUDA library against the CPU oracle on identical descriptors.
+
+Paths without transcendental functions are compared bit for bit (the kernels follow the
+reference's operation order with no FMA contraction; both sides use IEEE division and
+square root).  Plasma (log10/pow/exp) and the summed monitors (a different summation
+order) are compared within the north-star tolerances: relative L2 <= 1e-5 in Float32 and
+<= 1e-12 in Float64.
+"""
+import numpy as np
+import pytest
+
+import cases as C
+import maxwellfdtd_b200 as M
+from maxwellfdtd_b200 import _abi
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.float32: 1e-5, np.float64: 1e-12}
+
+
+def _rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if np.iscomplexobj(a) or np.iscomplexobj(b):
+        a = np.concatenate([np.real(a).ravel(), np.imag(a).ravel()])
+        b = np.concatenate([np.real(b).ravel(), np.imag(b).ravel()])
+    a = a.astype(np.float64)
+    b = b.astype(np.float64)
+    den = max(np.linalg.norm(a), np.linalg.norm(b))
+    return 0.0 if den == 0 else float(np.linalg.norm(a - b) / den)
+
+
+def _compare(ref, got, dtype, exact=True, loose=()):
+    assert set(ref) == set(got), set(ref) ^ set(got)
+    for k in ref:
+        a, b = ref[k], got[k]
+        assert np.shape(a) == np.shape(b), k
+        is_loose = (not exact) or any(s in k for s in loose)
+        if is_loose:
+            assert _rel(a, b) <= TOL[dtype], f"{k}: rel L2 {_rel(a, b):.3g}"
+        else:
+            if not np.array_equal(np.asarray(a), np.asarray(b), equal_nan=True):
+                diff = np.nanmax(np.abs(np.asarray(a, dtype=np.complex128) - np.asarray(b, dtype=np.complex128)))
+                raise AssertionError(f"{k}: not bit-exact (max abs diff {diff:.3g}, rel L2 {_rel(a, b):.3g})")
+
+
+DTYPES = [np.float64, np.float32]
+SUMMED = ("monitors/2/", "monitors/5/")   # FieldMonitor(sum) and SpectralMonitor(sum)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("ndim", [1, 2, 3])
+@pytest.mark.parametrize("builder", ["vacuum", "bcs", "materials", "sources"])
+def test_parity_exact(builder, ndim, dtype, oracle_lib, gpu_lib):
+    model = getattr(C, "model_" + builder)(ndim)
+    mons = C.monitors(ndim) if builder in ("vacuum", "materials") else None
+    ref = C.run_all(model, oracle_lib, dtype, mons)
+    got = C.run_all(model, gpu_lib, dtype, mons)
+    _compare(ref, got, dtype, exact=True, loose=SUMMED)
+
+
+@pytest.mark.parametrize("dtype,rho_fp64", [(np.float64, True), (np.float32, True), (np.float32, False)])
+@pytest.mark.parametrize("ndim", [1, 2, 3])
+@pytest.mark.parametrize("rate", ["power", "table"])
+def test_parity_plasma(rate, ndim, dtype, rho_fp64, oracle_lib, gpu_lib):
+    model = C.model_plasma(ndim, rate)
+    ref = C.run_all(model, oracle_lib, dtype, rho_fp64=rho_fp64)
+    got = C.run_all(model, gpu_lib, dtype, rho_fp64=rho_fp64)
+    assert np.max(ref["rho_end"]) > 0, "the case must ionise"
+    _compare(ref, got, dtype, exact=False)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("ndim", [1, 2, 3])
+def test_parity_tfsf_record_replay(ndim, dtype, oracle_lib, gpu_lib):
+    rec_model = C.model_tfsf_record(ndim)
+    box = C.tfsf_box(ndim)
+    ref = C.run_all(rec_model, oracle_lib, dtype, tfsf_box_=box)
+    got = C.run_all(rec_model, gpu_lib, dtype, tfsf_box_=box)
+    _compare(ref, got, dtype, exact=True)
+    record = {k[4:]: v for k, v in ref.items() if k.startswith("rec/")}
+    rep = C.model_tfsf_replay(ndim, record)
+    ref2 = C.run_all(rep, oracle_lib, dtype, C.monitors(ndim))
+    got2 = C.run_all(rep, gpu_lib, dtype, C.monitors(ndim))
+    _compare(ref2, got2, dtype, exact=True, loose=SUMMED)
+    assert np.abs(got2["field/Ex"]).max() > 0
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_chunked_runs_equal_single_run(ndim, gpu_lib):
+    """Splitting a run into several mfd_run calls changes nothing (the deferred Sa/E2
+    accumulation and the monitor staging are flushed at every call boundary)."""
+    model = C.model_materials(ndim)
+    one = C.run_all(model, gpu_lib, np.float32, chunks=[])
+    many = C.run_all(model, gpu_lib, np.float32, chunks=[1, 7, 13, 2])
+    _compare(one, many, np.float32, exact=True)
+
+
+def test_nonfinite_guard_matches_oracle(oracle_lib, gpu_lib):
+    """An unstable model (Courant number 1.5) blows up; both report the same first step
+    with a non-finite Ex (models.jl:202-209)."""
+    g = C.grid3((16, 16, 16))
+    src = M.SoftSource(geometry=(0.0, 0.0, 0.0), waveform=lambda x, y, z, t: 1e30 * C.pulse(t), component="Ex")
+    model = M.Model(g, src, tmax=1e-13, CN=1.5, pml=0)
+    results = []
+    for lib in (oracle_lib, gpu_lib):
+        b, _ = model.build_desc(np.float32, None)
+        st = _abi.Stepper(lib, b, np.float32)
+        with pytest.raises(_abi.StepperError) as ei:
+            st.run(1, model.Nt)
+        assert ei.value.code == _abi.MFD_ERR_NONFINITE
+        assert "Something went wrong" in str(ei.value)
+        results.append(st.status()[1:])
+        st.close()
+    assert results[0] == results[1], results
+    assert results[0][0] > 1
