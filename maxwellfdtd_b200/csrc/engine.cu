@@ -12,10 +12,13 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <thread>
@@ -85,6 +88,92 @@ static void bounded_sync(cudaStream_t st) {
 
 static long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
 
+// Exhaustive check of the constant-divisor fast path (see DivC in mfd_device.cuh): for every
+// significand x in [1, 2), the correction step must reproduce IEEE x/d bit for bit.
+__global__ void verify_div_kernel(const float* __restrict__ ds, const float* __restrict__ rs, int* fails) {
+    const int j = blockIdx.y;
+    const float d = ds[j], r = rs[j];
+    int bad = 0;
+    for (unsigned m = blockIdx.x * blockDim.x + threadIdx.x; m < (1u << 23); m += gridDim.x * blockDim.x) {
+        const float x = __int_as_float(0x3f800000u | m);
+        const float q0 = __fmul_rn(x, r);
+        const float e = __fmaf_rn(-q0, d, x);
+        const float q = __fmaf_rn(e, r, q0);
+        bad += __float_as_int(q) != __float_as_int(__fdiv_rn(x, d));
+    }
+    if (bad) atomicAdd(&fails[j], bad);
+}
+
+// Divisor descriptors, verified once per process and divisor value.
+class DivisorCache {
+   public:
+    static DivisorCache& get() {
+        static DivisorCache c;
+        return c;
+    }
+    // Fills ok for each float divisor; runs the device check for values not seen yet.
+    void verify(std::vector<DivC<float>>& dv, cudaStream_t st) {
+        std::lock_guard<std::mutex> lk(mu_);
+        std::vector<float> todo_d, todo_r;
+        for (auto& D : dv) {
+            uint32_t key;
+            std::memcpy(&key, &D.d, 4);
+            if (!known_.count(key) && std::find(todo_d.begin(), todo_d.end(), D.d) == todo_d.end()) {
+                todo_d.push_back(D.d);
+                todo_r.push_back(D.r);
+            }
+        }
+        if (!todo_d.empty()) {
+            const int n = (int)todo_d.size();
+            float *dd = nullptr, *dr = nullptr;
+            int* df = nullptr;
+            MFD_CK(cudaMalloc(&dd, n * sizeof(float)));
+            MFD_CK(cudaMalloc(&dr, n * sizeof(float)));
+            MFD_CK(cudaMalloc(&df, n * sizeof(int)));
+            MFD_CK(cudaMemcpyAsync(dd, todo_d.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+            MFD_CK(cudaMemcpyAsync(dr, todo_r.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+            MFD_CK(cudaMemsetAsync(df, 0, n * sizeof(int), st));
+            verify_div_kernel<<<dim3(128, n), 256, 0, st>>>(dd, dr, df);
+            MFD_CK(cudaGetLastError());
+            std::vector<int> fails(n);
+            MFD_CK(cudaMemcpyAsync(fails.data(), df, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+            MFD_CK(cudaStreamSynchronize(st));
+            cudaFree(dd);
+            cudaFree(dr);
+            cudaFree(df);
+            for (int j = 0; j < n; ++j) {
+                uint32_t key;
+                std::memcpy(&key, &todo_d[j], 4);
+                known_[key] = fails[j] == 0;
+            }
+        }
+        for (auto& D : dv) {
+            uint32_t key;
+            std::memcpy(&key, &D.d, 4);
+            D.ok = D.ok && known_[key] ? 1 : 0;
+        }
+    }
+
+   private:
+    std::mutex mu_;
+    std::map<uint32_t, bool> known_;
+};
+
+template <typename T>
+static DivC<T> make_div(T d) {
+    DivC<T> D{};
+    D.d = d;
+    D.r = T(1) / d;
+    D.ok = 0;
+    if (sizeof(T) == 4 && d > T(0) && std::isnormal((double)d)) {
+        const double r = (double)D.r;
+        D.lo = (T)std::max(std::ldexp(1.0, -76), std::ldexp(1.0, -100) / r);
+        D.hi = (T)std::min(std::ldexp(1.0, 100), std::ldexp(1.0, 100) / r);
+        D.ok = (D.lo <= T(1) && D.hi >= T(2)) ? 1 : 0;   // the checked binade lies in the band
+    }
+    return D;
+}
+
 template <typename T, typename R>
 class Engine : public HandleBase {
    public:
@@ -92,6 +181,7 @@ class Engine : public HandleBase {
     long long sz = 0, Np = 0, N = 0;
     int64_t nt = 0;
     T dx{}, dy{}, dz{}, dt{};
+    DivC<T> ddx{}, ddy{}, ddz{};
     int bc[6] = {1, 1, 1, 1, 1, 1};
     cudaStream_t st = nullptr;
     std::vector<void*> allocs;
@@ -137,10 +227,8 @@ class Engine : public HandleBase {
     long long ring_first = 0;
     bool need_ring = false;
 
-    int* d_flag = nullptr;
-    unsigned long long* d_bad = nullptr;
-    int* h_flag = nullptr;
-    unsigned long long* h_bad = nullptr;
+    int* d_flags = nullptr;     // [nt] per-step NaN/Inf flags of Ex
+    int* h_flags = nullptr;     // pinned copy
 
     int64_t done = 0, bad_step = 0;
     int32_t bad_kind = 0;
@@ -165,8 +253,7 @@ class Engine : public HandleBase {
         for (auto& pe : pend) { cudaEventDestroy(pe.second.first); cudaEventDestroy(pe.second.second); }
         if (run_ev[0]) cudaEventDestroy(run_ev[0]);
         if (run_ev[1]) cudaEventDestroy(run_ev[1]);
-        if (h_flag) cudaFreeHost(h_flag);
-        if (h_bad) cudaFreeHost(h_bad);
+        if (h_flags) cudaFreeHost(h_flags);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -203,7 +290,12 @@ class Engine : public HandleBase {
         return (c % nx) + (long long)px * (c / nx);
     }
 
-    Layout layout() const { return Layout{nx, ny, nz, px, sz}; }
+    Layout layout() const { return Layout{nx, ny, nz, px, (int)sz}; }
+
+    void verify_divs(std::vector<DivC<T>>& dv) {
+        if (sizeof(T) != 4) return;
+        DivisorCache::get().verify(reinterpret_cast<std::vector<DivC<float>>&>(dv), st);
+    }
 
     bool has_comp(int c) const {
         if (ndim == 3) return true;
@@ -225,6 +317,12 @@ class Engine : public HandleBase {
         N = (long long)nx * ny * nz;
         nt = d->nt;
         dx = (T)d->dx; dy = (T)d->dy; dz = (T)d->dz; dt = (T)d->dt;
+        if (Np >= (1ll << 31)) throw Error(MFD_ERR_INVALID, "grid too large: padded cell count must stay below 2^31");
+        {
+            std::vector<DivC<T>> dv = {make_div<T>(dx), make_div<T>(dy), make_div<T>(dz)};
+            verify_divs(dv);
+            ddx = dv[0]; ddy = dv[1]; ddz = dv[2];
+        }
         for (int f = 0; f < 6; ++f) bc[f] = d->bc[f];
         Mh0 = (T)d->Mh0; Me0 = (T)d->Me0; Md10 = (T)d->Md10; Md20 = (T)d->Md20;
         for (int c = 0; c < 9; ++c)
@@ -318,7 +416,12 @@ class Engine : public HandleBase {
             if (L.ib < 1 || L.ib > n) throw Error(MFD_ERR_INVALID, "CPML boundary index out of range");
             const bool left = (f % 2) == 0;
             if (left ? (L.nb != L.ib) : (L.nb != n - L.ib + 1)) throw Error(MFD_ERR_INVALID, "CPML layer size does not match its boundary index");
-            lay[f].K = upload_cast<T>(L.K, L.nb);
+            {
+                std::vector<DivC<T>> kv;
+                for (int i = 0; i < L.nb; ++i) kv.push_back(make_div<T>((T)L.K[i]));
+                verify_divs(kv);
+                lay[f].K = upload(kv.data(), kv.size());
+            }
             lay[f].A = upload_cast<T>(L.A, L.nb);
             lay[f].B = upload_cast<T>(L.B, L.nb);
             long long cnt;
@@ -352,12 +455,8 @@ class Engine : public HandleBase {
         if (d->tfsf.enabled) init_tfsf(d);
         if (d->tfsf_record) init_record(d);
         init_monitors(d);
-        MFD_CK(cudaMalloc(&d_flag, sizeof(int)));
-        allocs.push_back(d_flag);
-        MFD_CK(cudaMalloc(&d_bad, sizeof(unsigned long long)));
-        allocs.push_back(d_bad);
-        MFD_CK(cudaHostAlloc(&h_flag, sizeof(int), cudaHostAllocDefault));
-        MFD_CK(cudaHostAlloc(&h_bad, sizeof(unsigned long long), cudaHostAllocDefault));
+        d_flags = dalloc<int>((size_t)nt);
+        MFD_CK(cudaHostAlloc(&h_flags, (size_t)nt * sizeof(int), cudaHostAllocDefault));
         MFD_CK(cudaStreamSynchronize(st));
         const char* tune = std::getenv("MFD_TILE3D");
         if (tune) {
@@ -636,7 +735,7 @@ class Engine : public HandleBase {
     HParams<T> hparams(int accum, long long prev_step) {
         HParams<T> p{};
         p.L = layout();
-        p.dx = dx; p.dy = dy; p.dz = dz; p.dt = dt;
+        p.ddx = ddx; p.ddy = ddy; p.ddz = ddz; p.dt = dt;
         for (int f = 0; f < 6; ++f) { p.bc[f] = bc[f]; p.lay[f] = lay[f]; }
         p.Mh0 = Mh0;
         p.geom = geom;
@@ -646,7 +745,7 @@ class Engine : public HandleBase {
         p.accum = accum;
         p.sum_e2 = any_geom ? 1 : 0;
         p.Sa = Sa; p.E2 = E2;
-        p.flag = d_flag; p.badstep = d_bad;
+        p.flags = d_flags;
         p.prev_step = prev_step;
         return p;
     }
@@ -654,7 +753,7 @@ class Engine : public HandleBase {
     EParams<T, R> eparams(int cur) {
         EParams<T, R> p{};
         p.L = layout();
-        p.dx = dx; p.dy = dy; p.dz = dz; p.dt = dt;
+        p.ddx = ddx; p.ddy = ddy; p.ddz = ddz; p.dt = dt;
         for (int f = 0; f < 6; ++f) { p.bc[f] = bc[f]; p.lay[f] = lay[f]; }
         p.Me0 = Me0; p.Md10 = Md10; p.Md20 = Md20;
         p.geom = geom;
@@ -783,8 +882,6 @@ class Engine : public HandleBase {
         if (a != done + 1 || b < a - 1 || b > nt) { err = "steps must be consecutive and within 1..Nt"; return MFD_ERR_INVALID; }
         if (b < a) return MFD_OK;
         MFD_CK(cudaSetDevice(dev));
-        MFD_CK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
-        MFD_CK(cudaMemsetAsync(d_bad, 0xff, sizeof(unsigned long long), st));
         MFD_CK(cudaEventRecord(run_ev[0], st));
         for (int64_t it = a; it <= b; ++it) {
             launch_H(it > a ? 1 : 0, it - 1);
@@ -796,17 +893,20 @@ class Engine : public HandleBase {
         flush_monitors();
         launch_sums(b);
         MFD_CK(cudaEventRecord(run_ev[1], st));
-        MFD_CK(cudaMemcpyAsync(h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-        MFD_CK(cudaMemcpyAsync(h_bad, d_bad, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        MFD_CK(cudaMemcpyAsync(h_flags + (a - 1), d_flags + (a - 1), (size_t)(b - a + 1) * sizeof(int),
+                               cudaMemcpyDeviceToHost, st));
         bounded_sync(st);
         float ms = 0;
         MFD_CK(cudaEventElapsedTime(&ms, run_ev[0], run_ev[1]));
         run_ms = ms;
         if (profiling) collect_times();
         done = b;
-        if (*h_flag) {
-            bad_kind = *h_flag;
-            bad_step = (int64_t)*h_bad;
+        int64_t first = 0;
+        for (int64_t it = a; it <= b && !first; ++it)
+            if (h_flags[it - 1]) first = it;
+        if (first) {
+            bad_kind = h_flags[first - 1];
+            bad_step = first;
             err = (bad_kind & 1) ? "Something went wrong. I found NaN field values."
                                  : "Something went wrong. I found Inf field values.";
             err += " (step " + std::to_string(bad_step) + ")";

@@ -33,13 +33,57 @@ template <> struct Eps<double> { static __device__ __forceinline__ double v() { 
 struct Layout {
     int nx, ny, nz;
     int px;            // x pitch (elements)
-    long long sz;      // px*ny (z-plane stride)
+    int sz;            // px*ny (z-plane stride); padded grids stay below 2^31 cells
 };
+
+// Division by a positive grid constant (dx, dy, dz, CPML kappa).
+//
+// The reference divides by these constants in every cell (models.jl:803-808, 968-973,
+// 819-820 ...).  An IEEE division costs a long instruction sequence, and a much longer one
+// for the zero or tiny numerators that fill most of a grid early in a run.  For a constant
+// divisor d the library uses Markstein's correction step (P. W. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990):
+//     r = RN(1/d),  q0 = RN(x r),  e = RN(x - q0 d) (fma),  q = RN(q0 + e r) (fma).
+// Scaling x by 2^k scales q0, e and q by 2^k exactly while all of them stay normal, so the
+// result equals RN(x/d) for every x in the band [lo, hi] (where they do) as soon as it does
+// for every significand of one binade.  The engine checks exactly that on the device, for
+// each divisor, against IEEE division over all 2^23 significands in [1, 2) before the first
+// step; a divisor that fails (or any double-precision divisor) keeps IEEE division
+// (ok = 0), as do numerators outside the band.
+template <typename T>
+struct DivC {
+    T d, r;          // divisor and its correctly rounded reciprocal
+    T lo, hi;        // |x| band in which the correction step is exact
+    int ok;          // verified for every significand
+};
+
+template <typename T>
+__device__ __forceinline__ T cdiv(T x, const DivC<T>& D) {
+    return x / D.d;
+}
+
+template <>
+__device__ __forceinline__ float cdiv<float>(float x, const DivC<float>& D) {
+    const float ax = fabsf(x);
+    if (ax == 0.0f) return x;   // 0/d keeps the sign of x (d > 0)
+    if (D.ok && ax >= D.lo && ax <= D.hi) {
+        const float q0 = __fmul_rn(x, D.r);
+        const float e = __fmaf_rn(-q0, D.d, x);
+        return __fmaf_rn(e, D.r, q0);
+    }
+    return __fdiv_rn(x, D.d);
+}
+
+// sqrt of a sum of squares; zero (most cells early in a run) skips the special-case path.
+template <typename T>
+__device__ __forceinline__ T sqrt0(T v) {
+    return v == T(0) ? T(0) : sqrt(v);
+}
 
 template <typename T>
 struct LayerDev {
     int ib, nb;        // 1-based boundary index, points in layer (0 = none)
-    const T* K;
+    const DivC<T>* K;  // kappa as a divisor
     const T* A;
     const T* B;
     T* psi[4];         // 3-D: x faces Hyx,Hzx,Eyx,Ezx; y: Hxy,Hzy,Exy,Ezy; z: Hxz,Hyz,Exz,Eyz

@@ -18,7 +18,8 @@ namespace mfd {
 template <typename T>
 struct HParams {
     Layout L;
-    T dx, dy, dz, dt;
+    DivC<T> ddx, ddy, ddz;
+    T dt;
     int bc[6];
     LayerDev<T> lay[6];
     T Mh0;
@@ -30,15 +31,15 @@ struct HParams {
     int accum;
     int sum_e2;
     T* Sa; T* E2;
-    int* flag;
-    unsigned long long* badstep;
+    int* flags;            // per-step NaN (bit 0) / Inf (bit 1) flags of Ex, index step-1
     long long prev_step;
 };
 
 template <typename T, typename R>
 struct EParams {
     Layout L;
-    T dx, dy, dz, dt;
+    DivC<T> ddx, ddy, ddz;
+    T dt;
     int bc[6];
     LayerDev<T> lay[6];
     T Me0, Md10, Md20;
@@ -52,30 +53,26 @@ struct EParams {
 
 template <typename T>
 __device__ __forceinline__ void guard(const HParams<T>& p, T ex) {
-    int bad = (isnan(ex) ? 1 : 0) | (isinf(ex) ? 2 : 0);
-    if (bad) {
-        atomicOr(p.flag, bad);
-        atomicMin(p.badstep, (unsigned long long)p.prev_step);
-    }
+    const int bad = (isnan(ex) ? 1 : 0) | (isinf(ex) ? 2 : 0);
+    if (bad) atomicOr(p.flags + (p.prev_step - 1), bad);
 }
 
 // ------------------------------------------------------------------------------------------
 // 3-D
 // ------------------------------------------------------------------------------------------
 template <typename T, bool MATH>
-__global__ void __launch_bounds__(256) h3d_kernel(const __grid_constant__ HParams<T> p, const int zc) {
+__global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HParams<T> p, const int zc) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
     if (ix >= nx || iy >= ny) return;
     const int z0 = blockIdx.z * zc;
     const int z1 = min(z0 + zc, nz);
-    const long long sy = p.L.px, sz = p.L.sz;
-    long long c = ix + sy * iy + sz * z0;
-    const T dx = p.dx, dy = p.dy, dz = p.dz;
-    T ex = p.Ex[c], ey = p.Ey[c];
+    const int sy = p.L.px, sz = p.L.sz;
+    int c = ix + sy * iy + sz * z0;
+        T ex = p.Ex[c], ey = p.Ey[c];
     const bool xr = ix == nx - 1, yr = iy == ny - 1;
-    const long long wx = -(long long)(nx - 1), wy = -(long long)(ny - 1) * sy, wz = -(long long)(nz - 1) * sz;
+    const int wx = -(nx - 1), wy = -(ny - 1) * sy, wz = -(nz - 1) * sz;
     for (int iz = z0; iz < z1; ++iz, c += sz) {
         const T ez = p.Ez[c];
         T ey_xp, ez_xp, ex_yp, ez_yp, ex_zp, ey_zp;
@@ -100,7 +97,7 @@ __global__ void __launch_bounds__(256) h3d_kernel(const __grid_constant__ HParam
         T hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
         if (p.accum) {
             const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
-            p.Sa[c] = p.Sa[c] + sqrt(a * a + b * b + d * d) * p.dt;
+            p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b + d * d) * p.dt;
             if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
             guard(p, ex);
         }
@@ -109,101 +106,107 @@ __global__ void __launch_bounds__(256) h3d_kernel(const __grid_constant__ HParam
             const int g = p.geom[c];
             if (g) Mh = p.matMh[g - 1];
         }
-        T dExy = (ex_yp - ex) / dy;
-        T dExz = (ex_zp - ex) / dz;
-        T dEyx = (ey_xp - ey) / dx;
-        T dEyz = (ey_zp - ey) / dz;
-        T dEzx = (ez_xp - ez) / dx;
-        T dEzy = (ez_yp - ez) / dy;
+        T dExy = cdiv(ex_yp - ex, p.ddy);
+        T dExz = cdiv(ex_zp - ex, p.ddz);
+        T dEyx = cdiv(ey_xp - ey, p.ddx);
+        T dEyz = cdiv(ey_zp - ey, p.ddz);
+        T dEzx = cdiv(ez_xp - ez, p.ddx);
+        T dEzy = cdiv(ez_yp - ez, p.ddy);
         // CPML (models.jl:811-871)
         {
             const LayerDev<T>& l = p.lay[MFD_XL];
             if (l.nb && ix < l.ib) {
                 const int q = ix;
-                const long long k = q + (long long)l.nb * (iy + (long long)ny * iz);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = q + l.nb * (iy + ny * iz);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pEyx = B * l.psi[2][k] + A * dEyx;
                 const T pEzx = B * l.psi[3][k] + A * dEzx;
                 l.psi[2][k] = pEyx; l.psi[3][k] = pEzx;
                 hy += Mh * pEzx;
                 hz -= Mh * pEyx;
-                dEyx = dEyx / K;
-                dEzx = dEzx / K;
+                dEyx = cdiv(dEyx, K);
+                dEzx = cdiv(dEzx, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_XR];
             if (l.nb && ix >= l.ib - 1) {
                 const int q = ix - (l.ib - 1);
-                const long long k = q + (long long)l.nb * (iy + (long long)ny * iz);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = q + l.nb * (iy + ny * iz);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pEyx = B * l.psi[2][k] + A * dEyx;
                 const T pEzx = B * l.psi[3][k] + A * dEzx;
                 l.psi[2][k] = pEyx; l.psi[3][k] = pEzx;
                 hy += Mh * pEzx;
                 hz -= Mh * pEyx;
-                dEyx = dEyx / K;
-                dEzx = dEzx / K;
+                dEyx = cdiv(dEyx, K);
+                dEzx = cdiv(dEzx, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_YL];
             if (l.nb && iy < l.ib) {
                 const int q = iy;
-                const long long k = ix + sy * (q + (long long)l.nb * iz);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = ix + sy * (q + l.nb * iz);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pExy = B * l.psi[2][k] + A * dExy;
                 const T pEzy = B * l.psi[3][k] + A * dEzy;
                 l.psi[2][k] = pExy; l.psi[3][k] = pEzy;
                 hx -= Mh * pEzy;
                 hz += Mh * pExy;
-                dExy = dExy / K;
-                dEzy = dEzy / K;
+                dExy = cdiv(dExy, K);
+                dEzy = cdiv(dEzy, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_YR];
             if (l.nb && iy >= l.ib - 1) {
                 const int q = iy - (l.ib - 1);
-                const long long k = ix + sy * (q + (long long)l.nb * iz);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = ix + sy * (q + l.nb * iz);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pExy = B * l.psi[2][k] + A * dExy;
                 const T pEzy = B * l.psi[3][k] + A * dEzy;
                 l.psi[2][k] = pExy; l.psi[3][k] = pEzy;
                 hx -= Mh * pEzy;
                 hz += Mh * pExy;
-                dExy = dExy / K;
-                dEzy = dEzy / K;
+                dExy = cdiv(dExy, K);
+                dEzy = cdiv(dEzy, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_ZL];
             if (l.nb && iz < l.ib) {
                 const int q = iz;
-                const long long k = ix + sy * (iy + (long long)ny * q);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = ix + sy * (iy + ny * q);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pExz = B * l.psi[2][k] + A * dExz;
                 const T pEyz = B * l.psi[3][k] + A * dEyz;
                 l.psi[2][k] = pExz; l.psi[3][k] = pEyz;
                 hx += Mh * pEyz;
                 hy -= Mh * pExz;
-                dExz = dExz / K;
-                dEyz = dEyz / K;
+                dExz = cdiv(dExz, K);
+                dEyz = cdiv(dEyz, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_ZR];
             if (l.nb && iz >= l.ib - 1) {
                 const int q = iz - (l.ib - 1);
-                const long long k = ix + sy * (iy + (long long)ny * q);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = ix + sy * (iy + ny * q);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pExz = B * l.psi[2][k] + A * dExz;
                 const T pEyz = B * l.psi[3][k] + A * dEyz;
                 l.psi[2][k] = pExz; l.psi[3][k] = pEyz;
                 hx += Mh * pEyz;
                 hy -= Mh * pExz;
-                dExz = dExz / K;
-                dEyz = dEyz / K;
+                dExz = cdiv(dExz, K);
+                dEyz = cdiv(dEyz, K);
             }
         }
         hx -= Mh * (dEzy - dEyz);
@@ -216,18 +219,17 @@ __global__ void __launch_bounds__(256) h3d_kernel(const __grid_constant__ HParam
 }
 
 template <typename T, typename R, bool MAT>
-__global__ void __launch_bounds__(256) e3d_kernel(const __grid_constant__ EParams<T, R> p, const int zc) {
+__global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EParams<T, R> p, const int zc) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
     if (ix >= nx || iy >= ny) return;
     const int z0 = blockIdx.z * zc;
     const int z1 = min(z0 + zc, nz);
-    const long long sy = p.L.px, sz = p.L.sz;
-    long long c = ix + sy * iy + sz * z0;
-    const T dx = p.dx, dy = p.dy, dz = p.dz;
-    const bool xl = ix == 0, yl = iy == 0;
-    const long long wx = (long long)(nx - 1), wy = (long long)(ny - 1) * sy, wz = (long long)(nz - 1) * sz;
+    const int sy = p.L.px, sz = p.L.sz;
+    int c = ix + sy * iy + sz * z0;
+        const bool xl = ix == 0, yl = iy == 0;
+    const int wx = nx - 1, wy = (ny - 1) * sy, wz = (nz - 1) * sz;
     T hx_zm, hy_zm;
     if (z0 > 0) { hx_zm = p.Hx[c - sz]; hy_zm = p.Hy[c - sz]; }
     else {
@@ -251,12 +253,12 @@ __global__ void __launch_bounds__(256) e3d_kernel(const __grid_constant__ EParam
             hx_ym = bc_value(b, b == MFD_BC_PERIODIC ? p.Hx[c + wy] : T(0), hx);
             hz_ym = bc_value(b, b == MFD_BC_PERIODIC ? p.Hz[c + wy] : T(0), hz);
         }
-        T dHxy = (hx - hx_ym) / dy;
-        T dHxz = (hx - hx_zm) / dz;
-        T dHyx = (hy - hy_xm) / dx;
-        T dHyz = (hy - hy_zm) / dz;
-        T dHzx = (hz - hz_xm) / dx;
-        T dHzy = (hz - hz_ym) / dy;
+        T dHxy = cdiv(hx - hx_ym, p.ddy);
+        T dHxz = cdiv(hx - hx_zm, p.ddz);
+        T dHyx = cdiv(hy - hy_xm, p.ddx);
+        T dHyz = cdiv(hy - hy_zm, p.ddz);
+        T dHzx = cdiv(hz - hz_xm, p.ddx);
+        T dHzy = cdiv(hz - hz_ym, p.ddy);
         int g = 0;
         T Md1 = p.Md10, Md2 = p.Md20;
         if (MAT) {
@@ -269,90 +271,96 @@ __global__ void __launch_bounds__(256) e3d_kernel(const __grid_constant__ EParam
             const LayerDev<T>& l = p.lay[MFD_XL];
             if (l.nb && ix < l.ib) {
                 const int q = ix;
-                const long long k = q + (long long)l.nb * (iy + (long long)ny * iz);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = q + l.nb * (iy + ny * iz);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pHyx = B * l.psi[0][k] + A * dHyx;
                 const T pHzx = B * l.psi[1][k] + A * dHzx;
                 l.psi[0][k] = pHyx; l.psi[1][k] = pHzx;
                 Dv[1] -= Md2 * pHzx;
                 Dv[2] += Md2 * pHyx;
-                dHyx = dHyx / K;
-                dHzx = dHzx / K;
+                dHyx = cdiv(dHyx, K);
+                dHzx = cdiv(dHzx, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_XR];
             if (l.nb && ix >= l.ib - 1) {
                 const int q = ix - (l.ib - 1);
-                const long long k = q + (long long)l.nb * (iy + (long long)ny * iz);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = q + l.nb * (iy + ny * iz);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pHyx = B * l.psi[0][k] + A * dHyx;
                 const T pHzx = B * l.psi[1][k] + A * dHzx;
                 l.psi[0][k] = pHyx; l.psi[1][k] = pHzx;
                 Dv[1] -= Md2 * pHzx;
                 Dv[2] += Md2 * pHyx;
-                dHyx = dHyx / K;
-                dHzx = dHzx / K;
+                dHyx = cdiv(dHyx, K);
+                dHzx = cdiv(dHzx, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_YL];
             if (l.nb && iy < l.ib) {
                 const int q = iy;
-                const long long k = ix + sy * (q + (long long)l.nb * iz);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = ix + sy * (q + l.nb * iz);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pHxy = B * l.psi[0][k] + A * dHxy;
                 const T pHzy = B * l.psi[1][k] + A * dHzy;
                 l.psi[0][k] = pHxy; l.psi[1][k] = pHzy;
                 Dv[0] += Md2 * pHzy;
                 Dv[2] -= Md2 * pHxy;
-                dHxy = dHxy / K;
-                dHzy = dHzy / K;
+                dHxy = cdiv(dHxy, K);
+                dHzy = cdiv(dHzy, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_YR];
             if (l.nb && iy >= l.ib - 1) {
                 const int q = iy - (l.ib - 1);
-                const long long k = ix + sy * (q + (long long)l.nb * iz);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = ix + sy * (q + l.nb * iz);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pHxy = B * l.psi[0][k] + A * dHxy;
                 const T pHzy = B * l.psi[1][k] + A * dHzy;
                 l.psi[0][k] = pHxy; l.psi[1][k] = pHzy;
                 Dv[0] += Md2 * pHzy;
                 Dv[2] -= Md2 * pHxy;
-                dHxy = dHxy / K;
-                dHzy = dHzy / K;
+                dHxy = cdiv(dHxy, K);
+                dHzy = cdiv(dHzy, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_ZL];
             if (l.nb && iz < l.ib) {
                 const int q = iz;
-                const long long k = ix + sy * (iy + (long long)ny * q);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = ix + sy * (iy + ny * q);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pHxz = B * l.psi[0][k] + A * dHxz;
                 const T pHyz = B * l.psi[1][k] + A * dHyz;
                 l.psi[0][k] = pHxz; l.psi[1][k] = pHyz;
                 Dv[0] -= Md2 * pHyz;
                 Dv[1] += Md2 * pHxz;
-                dHxz = dHxz / K;
-                dHyz = dHyz / K;
+                dHxz = cdiv(dHxz, K);
+                dHyz = cdiv(dHyz, K);
             }
         }
         {
             const LayerDev<T>& l = p.lay[MFD_ZR];
             if (l.nb && iz >= l.ib - 1) {
                 const int q = iz - (l.ib - 1);
-                const long long k = ix + sy * (iy + (long long)ny * q);
-                const T B = l.B[q], A = l.A[q], K = l.K[q];
+                const int k = ix + sy * (iy + ny * q);
+                const T B = l.B[q], A = l.A[q];
+                const DivC<T> K = l.K[q];
                 const T pHxz = B * l.psi[0][k] + A * dHxz;
                 const T pHyz = B * l.psi[1][k] + A * dHyz;
                 l.psi[0][k] = pHxz; l.psi[1][k] = pHyz;
                 Dv[0] -= Md2 * pHyz;
                 Dv[1] += Md2 * pHxz;
-                dHxz = dHxz / K;
-                dHyz = dHyz / K;
+                dHxz = cdiv(dHxz, K);
+                dHyz = cdiv(dHyz, K);
             }
         }
         Dv[0] = Md1 * Dv[0] + Md2 * (dHzy - dHyz);
@@ -380,67 +388,67 @@ __global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParam
     const int iz = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, nz = p.L.nz;
     if (ix >= nx || iz >= nz) return;
-    const long long sz = p.L.sz;
-    const long long c = ix + sz * iz;
+    const int sz = p.L.sz;
+    const int c = ix + sz * iz;
     const T ex = p.Ex[c], ez = p.Ez[c];
     T ez_xp, ex_zp;
     if (ix < nx - 1) ez_xp = p.Ez[c + 1];
     else { const int b = p.bc[MFD_XR]; ez_xp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ez[c - (nx - 1)] : T(0), ez); }
     if (iz < nz - 1) ex_zp = p.Ex[c + sz];
-    else { const int b = p.bc[MFD_ZR]; ex_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ex[c - (long long)(nz - 1) * sz] : T(0), ex); }
+    else { const int b = p.bc[MFD_ZR]; ex_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ex[c - (nz - 1) * sz] : T(0), ex); }
     T hy = p.Hy[c];
     if (p.accum) {
         const T a = -ez * hy, b = ex * hy;
-        p.Sa[c] = p.Sa[c] + sqrt(a * a + b * b) * p.dt;
+        p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b) * p.dt;
         if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ez * ez) * p.dt;
         guard(p, ex);
     }
     T Mh = p.Mh0;
     if (MATH) { const int g = p.geom[c]; if (g) Mh = p.matMh[g - 1]; }
-    T dExz = (ex_zp - ex) / p.dz;
-    T dEzx = (ez_xp - ez) / p.dx;
+    T dExz = cdiv(ex_zp - ex, p.ddz);
+    T dEzx = cdiv(ez_xp - ez, p.ddx);
     {
         const LayerDev<T>& l = p.lay[MFD_XL];
         if (l.nb && ix < l.ib) {
             const int q = ix;
-            const long long k = q + (long long)l.nb * iz;
+            const int k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEzx;
             l.psi[1][k] = ps;
             hy += Mh * ps;
-            dEzx = dEzx / l.K[q];
+            dEzx = cdiv(dEzx, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_XR];
         if (l.nb && ix >= l.ib - 1) {
             const int q = ix - (l.ib - 1);
-            const long long k = q + (long long)l.nb * iz;
+            const int k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEzx;
             l.psi[1][k] = ps;
             hy += Mh * ps;
-            dEzx = dEzx / l.K[q];
+            dEzx = cdiv(dEzx, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_ZL];
         if (l.nb && iz < l.ib) {
             const int q = iz;
-            const long long k = ix + (long long)p.L.px * q;
+            const int k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dExz;
             l.psi[1][k] = ps;
             hy -= Mh * ps;
-            dExz = dExz / l.K[q];
+            dExz = cdiv(dExz, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_ZR];
         if (l.nb && iz >= l.ib - 1) {
             const int q = iz - (l.ib - 1);
-            const long long k = ix + (long long)p.L.px * q;
+            const int k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dExz;
             l.psi[1][k] = ps;
             hy -= Mh * ps;
-            dExz = dExz / l.K[q];
+            dExz = cdiv(dExz, l.K[q]);
         }
     }
     hy -= Mh * (dExz - dEzx);
@@ -453,16 +461,16 @@ __global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParam
     const int iz = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, nz = p.L.nz;
     if (ix >= nx || iz >= nz) return;
-    const long long sz = p.L.sz;
-    const long long c = ix + sz * iz;
+    const int sz = p.L.sz;
+    const int c = ix + sz * iz;
     const T hy = p.Hy[c];
     T hy_xm, hy_zm;
     if (ix > 0) hy_xm = p.Hy[c - 1];
     else { const int b = p.bc[MFD_XL]; hy_xm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + (nx - 1)] : T(0), hy); }
     if (iz > 0) hy_zm = p.Hy[c - sz];
-    else { const int b = p.bc[MFD_ZL]; hy_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + (long long)(nz - 1) * sz] : T(0), hy); }
-    T dHyx = (hy - hy_xm) / p.dx;
-    T dHyz = (hy - hy_zm) / p.dz;
+    else { const int b = p.bc[MFD_ZL]; hy_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + (nz - 1) * sz] : T(0), hy); }
+    T dHyx = cdiv(hy - hy_xm, p.ddx);
+    T dHyz = cdiv(hy - hy_zm, p.ddz);
     int g = 0;
     T Md1 = p.Md10, Md2 = p.Md20;
     if (MAT) {
@@ -474,44 +482,44 @@ __global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParam
         const LayerDev<T>& l = p.lay[MFD_XL];
         if (l.nb && ix < l.ib) {
             const int q = ix;
-            const long long k = q + (long long)l.nb * iz;
+            const int k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyx;
             l.psi[0][k] = ps;
             Dv[1] += Md2 * ps;
-            dHyx = dHyx / l.K[q];
+            dHyx = cdiv(dHyx, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_XR];
         if (l.nb && ix >= l.ib - 1) {
             const int q = ix - (l.ib - 1);
-            const long long k = q + (long long)l.nb * iz;
+            const int k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyx;
             l.psi[0][k] = ps;
             Dv[1] += Md2 * ps;
-            dHyx = dHyx / l.K[q];
+            dHyx = cdiv(dHyx, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_ZL];
         if (l.nb && iz < l.ib) {
             const int q = iz;
-            const long long k = ix + (long long)p.L.px * q;
+            const int k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyz;
             l.psi[0][k] = ps;
             Dv[0] -= Md2 * ps;
-            dHyz = dHyz / l.K[q];
+            dHyz = cdiv(dHyz, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_ZR];
         if (l.nb && iz >= l.ib - 1) {
             const int q = iz - (l.ib - 1);
-            const long long k = ix + (long long)p.L.px * q;
+            const int k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyz;
             l.psi[0][k] = ps;
             Dv[0] -= Md2 * ps;
-            dHyz = dHyz / l.K[q];
+            dHyz = cdiv(dHyz, l.K[q]);
         }
     }
     Dv[0] = Md1 * Dv[0] + Md2 * (T(0) - dHyz);
@@ -534,7 +542,7 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
     const int iz = blockIdx.x * blockDim.x + threadIdx.x;
     const int nz = p.L.nz;
     if (iz >= nz) return;
-    const long long c = iz;
+    const int c = iz;
     const T ex = p.Ex[c];
     T ex_zp;
     if (iz < nz - 1) ex_zp = p.Ex[c + 1];
@@ -542,13 +550,13 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
     T hy = p.Hy[c];
     if (p.accum) {
         const T a = ex * hy;
-        p.Sa[c] = p.Sa[c] + sqrt(a * a) * p.dt;
+        p.Sa[c] = p.Sa[c] + sqrt0(a * a) * p.dt;
         if (p.sum_e2) p.E2[c] = p.E2[c] + ex * ex * p.dt;
         guard(p, ex);
     }
     T Mh = p.Mh0;
     if (MATH) { const int g = p.geom[c]; if (g) Mh = p.matMh[g - 1]; }
-    T dExz = (ex_zp - ex) / p.dz;
+    T dExz = cdiv(ex_zp - ex, p.ddz);
     {
         const LayerDev<T>& l = p.lay[MFD_ZL];
         if (l.nb && iz < l.ib) {
@@ -556,7 +564,7 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
             const T ps = l.B[q] * l.psi[1][q] + l.A[q] * dExz;
             l.psi[1][q] = ps;
             hy -= Mh * ps;
-            dExz = dExz / l.K[q];
+            dExz = cdiv(dExz, l.K[q]);
         }
     }
     {
@@ -566,7 +574,7 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
             const T ps = l.B[q] * l.psi[1][q] + l.A[q] * dExz;
             l.psi[1][q] = ps;
             hy -= Mh * ps;
-            dExz = dExz / l.K[q];
+            dExz = cdiv(dExz, l.K[q]);
         }
     }
     hy -= Mh * (T(0) + dExz);
@@ -578,12 +586,12 @@ __global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParam
     const int iz = blockIdx.x * blockDim.x + threadIdx.x;
     const int nz = p.L.nz;
     if (iz >= nz) return;
-    const long long c = iz;
+    const int c = iz;
     const T hy = p.Hy[c];
     T hy_zm;
     if (iz > 0) hy_zm = p.Hy[c - 1];
     else { const int b = p.bc[MFD_ZL]; hy_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[nz - 1] : T(0), hy); }
-    T dHyz = (hy - hy_zm) / p.dz;
+    T dHyz = cdiv(hy - hy_zm, p.ddz);
     int g = 0;
     T Md1 = p.Md10, Md2 = p.Md20;
     if (MAT) {
@@ -598,7 +606,7 @@ __global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParam
             const T ps = l.B[q] * l.psi[0][q] + l.A[q] * dHyz;
             l.psi[0][q] = ps;
             Dv[0] -= Md2 * ps;
-            dHyz = dHyz / l.K[q];
+            dHyz = cdiv(dHyz, l.K[q]);
         }
     }
     {
@@ -608,7 +616,7 @@ __global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParam
             const T ps = l.B[q] * l.psi[0][q] + l.A[q] * dHyz;
             l.psi[0][q] = ps;
             Dv[0] -= Md2 * ps;
-            dHyz = dHyz / l.K[q];
+            dHyz = cdiv(dHyz, l.K[q]);
         }
     }
     Dv[0] = Md1 * Dv[0] + Md2 * (T(0) - dHyz);
@@ -629,22 +637,22 @@ __global__ void __launch_bounds__(256) sums_kernel(const __grid_constant__ HPara
     const int iy = blockIdx.y;
     const int iz = blockIdx.z;
     if (ix >= p.L.nx) return;
-    const long long c = ix + (long long)p.L.px * iy + p.L.sz * iz;
+    const int c = ix + p.L.px * iy + p.L.sz * iz;
     const T ex = p.Ex[c];
     if (ndim == 3) {
         const T ey = p.Ey[c], ez = p.Ez[c], hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
         const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
-        p.Sa[c] = p.Sa[c] + sqrt(a * a + b * b + d * d) * p.dt;
+        p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b + d * d) * p.dt;
         if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
     } else if (ndim == 2) {
         const T ez = p.Ez[c], hy = p.Hy[c];
         const T a = -ez * hy, b = ex * hy;
-        p.Sa[c] = p.Sa[c] + sqrt(a * a + b * b) * p.dt;
+        p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b) * p.dt;
         if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ez * ez) * p.dt;
     } else {
         const T hy = p.Hy[c];
         const T a = ex * hy;
-        p.Sa[c] = p.Sa[c] + sqrt(a * a) * p.dt;
+        p.Sa[c] = p.Sa[c] + sqrt0(a * a) * p.dt;
         if (p.sum_e2) p.E2[c] = p.E2[c] + ex * ex * p.dt;
     }
     guard(p, ex);

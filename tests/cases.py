@@ -114,7 +114,7 @@ def model_materials(ndim, nsteps=70):
 
 def model_plasma(ndim, rate="power", nsteps=60):
     g = _grid(ndim)
-    E0 = 8e9
+    E0 = 1.3e10
     src = M.SoftSource(geometry=_plane(ndim, -250e-9), waveform=_src_wave(ndim, E0), component="Ex")
     dt = 0.5 / C0 / np.sqrt(ndim / (50e-9) ** 2)
     w0 = 2 * np.pi * C0 / 800e-9
@@ -122,7 +122,7 @@ def model_plasma(ndim, rate="power", nsteps=60):
         ionrate = M.PowerLawRate(order=8, sigma=1e-130)
     else:
         I = np.logspace(12, 20, 81)
-        ionrate = M.IonizationRate(np.stack([I, 1e-130 * I ** 8 + 1.0], axis=1))
+        ionrate = M.IonizationRate(np.stack([I, 1e-130 * I ** 8], axis=1))
     pl = M.Plasma(ionrate=ionrate, rho0=2.1e28, nuc=1 / 1e-15, frequency=w0, Uiev=9.0, mr=0.64)
     chi3 = 4 / 3 * 1.45 ** 2 * EPS0 * C0 * 2.5e-20
     mat = M.Material(geometry=_ball(ndim, 250e-9), eps=1.45 ** 2, chi3=chi3, plasma=pl,
