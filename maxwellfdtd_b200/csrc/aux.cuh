@@ -38,14 +38,14 @@ struct RectStmt {
     int tprec;        // 1: coefficient and product in T; 0: in double
     double coef;
     double coefT;     // T-rounded coefficient for tprec
-    long long start;  // first work item of this statement
     long long len;    // rectangle size (= array length per step)
+    unsigned long long prev;   // earlier statements of the same component whose rectangle meets this one
+    unsigned long long next;   // later ones
 };
 
 template <typename T>
 struct RectParams {
     int n;
-    long long total;
     long long it0;    // 0-based step
     Layout L;
     T* F[9];
@@ -62,56 +62,52 @@ __device__ __forceinline__ long long rect_local(const RectStmt& s, int ix, int i
     return (ix - s.x0) + nxr * ((iy - s.y0) + nyr * (long long)(iz - s.z0));
 }
 
-// One thread per (statement, cell).  A cell reached by several statements of the same
+template <typename T>
+__device__ __forceinline__ T tfsf_apply(const RectStmt& t, T v, T inc) {
+    if (t.tprec) {
+        const T u = (T)t.coefT * inc;
+        return t.sign > 0 ? v + u : v - u;
+    }
+    const double u = t.coef * (double)inc;
+    return (T)(t.sign > 0 ? (double)v + u : (double)v - u);
+}
+
+// Grid row blockIdx.y = statement.  A cell reached by several statements of the same
 // component (edges of the 3-D TFSF box) is updated by the thread of its first statement,
 // which applies all of them in statement order -- the order of the reference's broadcasts.
 template <typename T>
 __global__ void __launch_bounds__(256) tfsf_kernel(const __grid_constant__ RectParams<T> p) {
-    const long long item = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (item >= p.total) return;
-    int si = 0;
-    while (si + 1 < p.n && p.s[si + 1].start <= item) ++si;
-    const RectStmt& s = p.s[si];
-    const long long local = item - s.start;
-    const long long nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
+    const RectStmt& s = p.s[blockIdx.y];
+    const long long local = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (local >= s.len) return;
+    const int nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
     const int ix = s.x0 + (int)(local % nxr);
     const long long rest = local / nxr;
     const int iy = s.y0 + (int)(rest % nyr);
     const int iz = s.z0 + (int)(rest / nyr);
-    for (int j = 0; j < si; ++j)
-        if (p.s[j].comp == s.comp && rect_has(p.s[j], ix, iy, iz)) return;
+    for (unsigned long long m = s.prev; m; m &= m - 1)
+        if (rect_has(p.s[__ffsll((long long)m) - 1], ix, iy, iz)) return;
     T* F = p.F[s.comp];
-    const long long c = ix + (long long)p.L.px * iy + p.L.sz * iz;
-    T v = F[c];
-    for (int j = si; j < p.n; ++j) {
-        const RectStmt& t = p.s[j];
-        if (t.comp != s.comp || !rect_has(t, ix, iy, iz)) continue;
-        const T inc = p.arr[t.k][p.it0 * t.len + rect_local(t, ix, iy, iz)];
-        if (t.tprec) {
-            const T u = (T)t.coefT * inc;
-            v = t.sign > 0 ? v + u : v - u;
-        } else {
-            const double u = t.coef * (double)inc;
-            v = (T)(t.sign > 0 ? (double)v + u : (double)v - u);
-        }
+    const int c = ix + p.L.px * iy + p.L.sz * iz;
+    T v = tfsf_apply(s, F[c], p.arr[s.k][p.it0 * s.len + local]);
+    for (unsigned long long m = s.next; m; m &= m - 1) {
+        const RectStmt& t = p.s[__ffsll((long long)m) - 1];
+        if (rect_has(t, ix, iy, iz)) v = tfsf_apply(t, v, p.arr[t.k][p.it0 * t.len + rect_local(t, ix, iy, iz)]);
     }
     F[c] = v;
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) record_kernel(const __grid_constant__ RectParams<T> p) {
-    const long long item = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (item >= p.total) return;
-    int si = 0;
-    while (si + 1 < p.n && p.s[si + 1].start <= item) ++si;
-    const RectStmt& s = p.s[si];
-    const long long local = item - s.start;
-    const long long nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
+    const RectStmt& s = p.s[blockIdx.y];
+    const long long local = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (local >= s.len) return;
+    const int nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
     const int ix = s.x0 + (int)(local % nxr);
     const long long rest = local / nxr;
     const int iy = s.y0 + (int)(rest % nyr);
     const int iz = s.z0 + (int)(rest / nyr);
-    const long long c = ix + (long long)p.L.px * iy + p.L.sz * iz;
+    const int c = ix + p.L.px * iy + p.L.sz * iz;
     p.arr[s.k][p.it0 * s.len + local] = p.F[s.comp][c];
 }
 
@@ -125,32 +121,28 @@ template <typename T>
 struct MonDev {
     int kind, sum, nw;
     long long npts;
-    const long long* cells;   // padded cell indices
+    const int* cells;         // padded cell indices
     T* hist;                  // field, no sum: [ncomp][nt][npts]; field sum: [ncomp][nt]
     T* ring;                  // staging [K][ncomp][npts]
     double2* S;               // spectral: [ncomp][nw][npts] or [ncomp][nw]
-    const double2* phasor;    // [nt][nw]  exp(-i w (t - tshift))
-    long long start;          // first gather item
+    const double2* phasor;    // [nt][nw]: exp(-i w (t - tshift)) with sum, 2 exp(...) dt without
 };
 
 template <typename T>
 struct MonParams {
     int nmon, ncomp;
-    long long total, nt;
-    T* comp[6];               // field arrays of the monitored components
+    long long nt;
+    const T* comp[6];         // field arrays of the monitored components
     const MonDev<T>* mons;
 };
 
+// Grid row blockIdx.y = monitor * ncomp + component.
 template <typename T>
-__global__ void __launch_bounds__(256) monitor_gather_kernel(const MonParams<T> p, long long it0, int slot) {
-    const long long item = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (item >= p.total) return;
-    int m = 0;
-    while (m + 1 < p.nmon && p.mons[m + 1].start <= item) ++m;
+__global__ void __launch_bounds__(256) monitor_gather_kernel(const __grid_constant__ MonParams<T> p, long long it0, int slot) {
+    const int m = blockIdx.y / p.ncomp, k = blockIdx.y - m * p.ncomp;
     const MonDev<T>& M = p.mons[m];
-    const long long local = item - M.start;
-    const int k = (int)(local / M.npts);
-    const long long j = local - (long long)k * M.npts;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= M.npts) return;
     const T v = p.comp[k][M.cells[j]];
     if (M.kind == MFD_MON_FIELD && !M.sum) M.hist[((long long)k * p.nt + it0) * M.npts + j] = v;
     else M.ring[((long long)slot * p.ncomp + k) * M.npts + j] = v;
@@ -180,7 +172,7 @@ __global__ void __launch_bounds__(256) monitor_fieldsum_kernel(const MonDev<T>* 
 #define MFD_DFT_W 8
 template <typename T>
 __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __restrict__ mon, int ncomp, int nslots,
-                                                          long long it0_first, double dt) {
+                                                          long long it0_first) {
     const MonDev<T>& M = *mon;
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
@@ -195,14 +187,13 @@ __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __res
         if (w < wn) { const double2 s = S[(long long)w * M.npts]; sr[w] = s.x; si[w] = s.y; }
     for (int slot = 0; slot < nslots; ++slot) {
         const double f = (double)M.ring[((long long)slot * ncomp + k) * M.npts + j];
-        const double2* e = M.phasor + (it0_first + slot) * nw + w0;
+        const double2* e = M.phasor + (it0_first + slot) * nw + w0;   // 2 exp(...) dt, tabulated
 #pragma unroll
         for (int w = 0; w < MFD_DFT_W; ++w) {
             if (w < wn) {
-                const double2 ew = e[w];
-                const double tr = (2 * ew.x) * dt, ti = (2 * ew.y) * dt;
-                sr[w] = sr[w] + f * tr;
-                si[w] = si[w] + f * ti;
+                const double2 tw = e[w];
+                sr[w] = sr[w] + f * tw.x;
+                si[w] = si[w] + f * tw.y;
             }
         }
     }
@@ -242,6 +233,14 @@ __global__ void __launch_bounds__(256) monitor_dftsum_kernel(const MonDev<T>* __
         __syncthreads();
     }
     if (threadIdx.x == 0) M.S[(long long)k * M.nw + w] = S;
+}
+
+// The per-step DFT factor 2 exp(-i w (t - tshift)) dt of dft.jl:562, from the phasor table.
+__global__ void dft_factor_kernel(double2* ph, long long n, double dt) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double2 e = ph[i];
+    ph[i] = make_double2((2 * e.x) * dt, (2 * e.y) * dt);
 }
 
 // ------------------------------------------------------------------------------------------

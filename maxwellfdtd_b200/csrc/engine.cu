@@ -213,6 +213,7 @@ class Engine : public HandleBase {
     bool tfsf = false;
     int tfsf_order = 0;
     RectParams<T> tfsf_p{};
+    long long tfsf_maxlen = 0, rec_maxlen = 0;
     bool record = false;
     RectParams<T> rec_p{};
     int rec_narr = 0;
@@ -224,6 +225,7 @@ class Engine : public HandleBase {
     MonDev<T>* mons_dev = nullptr;
     MonParams<T> mon_p{};
     int ring_k = 0, ring_used = 0;
+    long long mon_maxpts = 0;
     long long ring_first = 0;
     bool need_ring = false;
 
@@ -563,28 +565,47 @@ class Engine : public HandleBase {
             add(MFD_EX, 0, 0, 0, 0, Z2, Z2, 2, -1, ce, 0, 0);
             add(MFD_DX, 0, 0, 0, 0, Z2, Z2, 2, -1, 0, 1, cd);
         }
-        RectParams<T>& p = tfsf_p;
-        std::memset(&p, 0, sizeof(p));
-        p.n = (int)v.size();
-        p.L = layout();
-        for (int c = 0; c < 9; ++c) p.F[c] = F[c];
-        long long start = 0;
-        std::vector<long long> alen(24, -1);
-        for (int i = 0; i < p.n; ++i) {
-            RectStmt& s = p.s[i];
-            s.comp = v[i].comp; s.x0 = v[i].x0; s.x1 = v[i].x1; s.y0 = v[i].y0; s.y1 = v[i].y1; s.z0 = v[i].z0; s.z1 = v[i].z1;
-            s.k = v[i].k; s.sign = v[i].sign; s.tprec = tp[i]; s.coef = coef[i]; s.coefT = (double)coefT[i];
-            s.len = (long long)(s.x1 - s.x0 + 1) * (s.y1 - s.y0 + 1) * (s.z1 - s.z0 + 1);
-            s.start = start;
-            start += s.len;
-            alen[s.k] = s.len;
-        }
-        p.total = start;
+        // An incident array that is zero at every step changes nothing (F +- c*0 == F up to
+        // the sign of a zero): its statements are dropped and the array is not uploaded.
         const int narr = ndim == 3 ? 24 : ndim == 2 ? 8 : 4;
+        std::vector<long long> alen(24, -1);
+        for (size_t i = 0; i < v.size(); ++i)
+            alen[v[i].k] = (long long)(v[i].x1 - v[i].x0 + 1) * (v[i].y1 - v[i].y0 + 1) * (v[i].z1 - v[i].z0 + 1);
+        std::vector<bool> nonzero(24, false);
         for (int k = 0; k < narr; ++k) {
             if (!d->tfsf.inc[k]) throw Error(MFD_ERR_INVALID, "missing TFSF incident array");
-            p.arr[k] = upload((const T*)d->tfsf.inc[k], (size_t)alen[k] * nt);
+            const T* a = (const T*)d->tfsf.inc[k];
+            const size_t n = (size_t)alen[k] * nt;
+            for (size_t i = 0; i < n && !nonzero[k]; ++i) nonzero[k] = a[i] != T(0);
         }
+        RectParams<T>& p = tfsf_p;
+        std::memset(&p, 0, sizeof(p));
+        p.L = layout();
+        for (int c = 0; c < 9; ++c) p.F[c] = F[c];
+        int n = 0;
+        for (size_t i = 0; i < v.size(); ++i) {
+            if (!nonzero[v[i].k]) continue;
+            RectStmt& s = p.s[n++];
+            s.comp = v[i].comp; s.x0 = v[i].x0; s.x1 = v[i].x1; s.y0 = v[i].y0; s.y1 = v[i].y1; s.z0 = v[i].z0; s.z1 = v[i].z1;
+            s.k = v[i].k; s.sign = v[i].sign; s.tprec = tp[i]; s.coef = coef[i]; s.coefT = (double)coefT[i];
+            s.len = alen[s.k];
+        }
+        p.n = n;
+        auto meets = [](const RectStmt& a, const RectStmt& b) {
+            return a.comp == b.comp && a.x0 <= b.x1 && b.x0 <= a.x1 && a.y0 <= b.y1 && b.y0 <= a.y1 && a.z0 <= b.z1 && b.z0 <= a.z1;
+        };
+        tfsf_maxlen = 0;
+        for (int i = 0; i < n; ++i) {
+            p.s[i].prev = p.s[i].next = 0;
+            for (int j = 0; j < n; ++j) {
+                if (j == i || !meets(p.s[i], p.s[j])) continue;
+                if (j < i) p.s[i].prev |= 1ull << j; else p.s[i].next |= 1ull << j;
+            }
+            tfsf_maxlen = std::max(tfsf_maxlen, p.s[i].len);
+        }
+        for (int k = 0; k < narr; ++k)
+            if (nonzero[k]) p.arr[k] = upload((const T*)d->tfsf.inc[k], (size_t)alen[k] * nt);
+        tfsf = n > 0;
         MFD_CK(cudaStreamSynchronize(st));
     }
 
@@ -632,17 +653,14 @@ class Engine : public HandleBase {
         rec_narr = p.n;
         p.L = layout();
         for (int c = 0; c < 9; ++c) p.F[c] = F[c];
-        long long start = 0;
         for (int i = 0; i < p.n; ++i) {
             RectStmt& s = p.s[i];
             s.comp = v[i].comp; s.x0 = v[i].x0; s.x1 = v[i].x1; s.y0 = v[i].y0; s.y1 = v[i].y1; s.z0 = v[i].z0; s.z1 = v[i].z1;
             s.k = i;
             s.len = (long long)(s.x1 - s.x0 + 1) * (s.y1 - s.y0 + 1) * (s.z1 - s.z0 + 1);
-            s.start = start;
-            start += s.len;
+            rec_maxlen = std::max(rec_maxlen, s.len);
             p.arr[i] = dalloc<T>((size_t)s.len * nt);
         }
-        p.total = start;
     }
 
     void init_monitors(const mfd_desc* d) {
@@ -664,15 +682,15 @@ class Engine : public HandleBase {
             long long cap = (512ll << 20) / ((long long)sizeof(T) * ring_vals);
             ring_k = (int)std::max(1ll, std::min(64ll, cap));
         }
-        long long start = 0;
         for (int m = 0; m < d->nmon; ++m) {
             const mfd_monitor& a = d->mons[m];
             MonDev<T> M{};
             M.kind = a.kind; M.sum = a.sum ? 1 : 0; M.npts = a.npts; M.nw = a.nw;
-            std::vector<long long> cells(a.npts);
+            mon_maxpts = std::max(mon_maxpts, (long long)a.npts);
+            std::vector<int> cells(a.npts);
             for (long long j = 0; j < a.npts; ++j) {
                 if (a.cells[j] < 0 || a.cells[j] >= N) throw Error(MFD_ERR_INVALID, "monitor cell out of range");
-                cells[j] = pad_index(a.cells[j]);
+                cells[j] = (int)pad_index(a.cells[j]);
             }
             M.cells = upload(cells.data(), cells.size());
             if (a.kind == MFD_MON_FIELD) {
@@ -681,17 +699,20 @@ class Engine : public HandleBase {
             } else {
                 if (a.nw < 1 || !a.phasor) throw Error(MFD_ERR_INVALID, "spectral monitor needs frequencies");
                 M.S = dalloc<double2>((size_t)ncomp_mon * a.nw * (M.sum ? 1 : a.npts));
-                M.phasor = (const double2*)upload(a.phasor, (size_t)nt * a.nw * 2);
+                double2* ph = (double2*)upload(a.phasor, (size_t)nt * a.nw * 2);
+                if (!M.sum) {   // tabulate 2 exp(...) dt once (dft.jl:562)
+                    const long long n = (long long)nt * a.nw;
+                    dft_factor_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ph, n, (double)dt);
+                    MFD_CK(cudaGetLastError());
+                }
+                M.phasor = ph;
             }
             if (a.kind == MFD_MON_SPECTRAL || M.sum) M.ring = dalloc<T>((size_t)ring_k * ncomp_mon * a.npts);
-            M.start = start;
-            start += (long long)ncomp_mon * a.npts;
             mons_host.push_back(M);
         }
         mons_dev = upload(mons_host.data(), mons_host.size());
         mon_p.nmon = (int)mons_host.size();
         mon_p.ncomp = ncomp_mon;
-        mon_p.total = start;
         mon_p.nt = nt;
         for (int k = 0; k < ncomp_mon; ++k) mon_p.comp[k] = F[mon_comps[k]];
         mon_p.mons = mons_dev;
@@ -809,8 +830,8 @@ class Engine : public HandleBase {
             if (tfsf && (int)s == tfsf_order) {
                 tfsf_p.it0 = it0;
                 launch(KC_TFSF, [&] {
-                    const long long nb = (tfsf_p.total + 255) / 256;
-                    tfsf_kernel<T><<<(unsigned)nb, 256, 0, st>>>(tfsf_p);
+                    const long long nb = (tfsf_maxlen + 255) / 256;
+                    tfsf_kernel<T><<<dim3((unsigned)nb, tfsf_p.n), 256, 0, st>>>(tfsf_p);
                 });
             }
             if (s < srcs.size()) {
@@ -836,7 +857,7 @@ class Engine : public HandleBase {
             } else if (M.kind == MFD_MON_SPECTRAL && !M.sum) {
                 launch(KC_DFT, [&] {
                     dim3 grd((unsigned)((M.npts + 255) / 256), ncomp_mon, (M.nw + MFD_DFT_W - 1) / MFD_DFT_W);
-                    monitor_dft_kernel<T><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first, dtd);
+                    monitor_dft_kernel<T><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first);
                 });
             } else if (M.kind == MFD_MON_SPECTRAL) {
                 launch(KC_DFT, [&] {
@@ -852,8 +873,8 @@ class Engine : public HandleBase {
         if (need_ring && ring_used == 0) ring_first = it - 1;
         const int slot = ring_used;
         launch(KC_MON, [&] {
-            const long long nb = (mon_p.total + 255) / 256;
-            monitor_gather_kernel<T><<<(unsigned)nb, 256, 0, st>>>(mon_p, it - 1, slot);
+            const long long nb = (mon_maxpts + 255) / 256;
+            monitor_gather_kernel<T><<<dim3((unsigned)nb, mon_p.nmon * ncomp_mon), 256, 0, st>>>(mon_p, it - 1, slot);
         });
         if (need_ring) {
             ring_used++;
@@ -864,8 +885,8 @@ class Engine : public HandleBase {
     void launch_record(int64_t it) {
         rec_p.it0 = it - 1;
         launch(KC_MON, [&] {
-            const long long nb = (rec_p.total + 255) / 256;
-            record_kernel<T><<<(unsigned)nb, 256, 0, st>>>(rec_p);
+            const long long nb = (rec_maxlen + 255) / 256;
+            record_kernel<T><<<dim3((unsigned)nb, rec_p.n), 256, 0, st>>>(rec_p);
         });
     }
 

@@ -59,7 +59,43 @@ __device__ __forceinline__ void guard(const HParams<T>& p, T ex) {
 
 // ------------------------------------------------------------------------------------------
 // 3-D
+//
+// Software-pipelined z march: all loads of plane iz+1 are issued before the arithmetic and
+// stores of plane iz, so two planes of memory traffic are in flight per thread.  Boundary
+// conditions are folded into per-thread neighbour offsets (periodic: the wrapped cell;
+// Neumann: the cell itself; Dirichlet: the cell itself, zeroed after the load), so the
+// prefetch never depends on values of the current plane.
 // ------------------------------------------------------------------------------------------
+template <typename T>
+struct HLoad {
+    T ez, eyx, ezx, exy, ezy, exz, eyz, hx, hy, hz, sa, e2;
+    int g;
+};
+
+template <typename T, bool MATH>
+__device__ __forceinline__ HLoad<T> h3d_load(const HParams<T>& p, int c, int iz, int ox, int oy, int ozw) {
+    HLoad<T> v;
+    const int oz = iz < p.L.nz - 1 ? p.L.sz : ozw;
+    v.ez = p.Ez[c];
+    v.eyx = p.Ey[c + ox];
+    v.ezx = p.Ez[c + ox];
+    v.exy = p.Ex[c + oy];
+    v.ezy = p.Ez[c + oy];
+    v.exz = p.Ex[c + oz];
+    v.eyz = p.Ey[c + oz];
+    v.hx = p.Hx[c];
+    v.hy = p.Hy[c];
+    v.hz = p.Hz[c];
+    if (p.accum) {
+        v.sa = p.Sa[c];
+        v.e2 = p.sum_e2 ? p.E2[c] : T(0);
+    } else {
+        v.sa = v.e2 = T(0);
+    }
+    v.g = MATH ? (int)p.geom[c] : 0;
+    return v;
+}
+
 template <typename T, bool MATH>
 __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HParams<T> p, const int zc) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -69,43 +105,32 @@ __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HPa
     const int z0 = blockIdx.z * zc;
     const int z1 = min(z0 + zc, nz);
     const int sy = p.L.px, sz = p.L.sz;
-    int c = ix + sy * iy + sz * z0;
-        T ex = p.Ex[c], ey = p.Ey[c];
+    const int bxr = p.bc[MFD_XR], byr = p.bc[MFD_YR], bzr = p.bc[MFD_ZR];
     const bool xr = ix == nx - 1, yr = iy == ny - 1;
-    const int wx = -(nx - 1), wy = -(ny - 1) * sy, wz = -(nz - 1) * sz;
+    const int ox = !xr ? 1 : (bxr == MFD_BC_PERIODIC ? -(nx - 1) : 0);
+    const int oy = !yr ? sy : (byr == MFD_BC_PERIODIC ? -(ny - 1) * sy : 0);
+    const int ozw = bzr == MFD_BC_PERIODIC ? -(nz - 1) * sz : 0;
+    const bool zx = xr && bxr == MFD_BC_DIRICHLET, zy = yr && byr == MFD_BC_DIRICHLET;
+    int c = ix + sy * iy + sz * z0;
+    T ex = p.Ex[c], ey = p.Ey[c];
+    HLoad<T> cur = h3d_load<T, MATH>(p, c, z0, ox, oy, ozw);
     for (int iz = z0; iz < z1; ++iz, c += sz) {
-        const T ez = p.Ez[c];
-        T ey_xp, ez_xp, ex_yp, ez_yp, ex_zp, ey_zp;
-        if (!xr) { ey_xp = p.Ey[c + 1]; ez_xp = p.Ez[c + 1]; }
-        else {
-            const int b = p.bc[MFD_XR];
-            ey_xp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ey[c + wx] : T(0), ey);
-            ez_xp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ez[c + wx] : T(0), ez);
-        }
-        if (!yr) { ex_yp = p.Ex[c + sy]; ez_yp = p.Ez[c + sy]; }
-        else {
-            const int b = p.bc[MFD_YR];
-            ex_yp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ex[c + wy] : T(0), ex);
-            ez_yp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ez[c + wy] : T(0), ez);
-        }
-        if (iz < nz - 1) { ex_zp = p.Ex[c + sz]; ey_zp = p.Ey[c + sz]; }
-        else {
-            const int b = p.bc[MFD_ZR];
-            ex_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ex[c + wz] : T(0), ex);
-            ey_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ey[c + wz] : T(0), ey);
-        }
-        T hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
+        HLoad<T> nxt;
+        if (iz + 1 < z1) nxt = h3d_load<T, MATH>(p, c + sz, iz + 1, ox, oy, ozw);
+        const T ez = cur.ez;
+        const T ey_xp = zx ? T(0) : cur.eyx, ez_xp = zx ? T(0) : cur.ezx;
+        const T ex_yp = zy ? T(0) : cur.exy, ez_yp = zy ? T(0) : cur.ezy;
+        const bool zz = iz == nz - 1 && bzr == MFD_BC_DIRICHLET;
+        const T ex_zp = zz ? T(0) : cur.exz, ey_zp = zz ? T(0) : cur.eyz;
+        T hx = cur.hx, hy = cur.hy, hz = cur.hz;
         if (p.accum) {
             const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
-            p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b + d * d) * p.dt;
-            if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
+            p.Sa[c] = cur.sa + sqrt0(a * a + b * b + d * d) * p.dt;
+            if (p.sum_e2) p.E2[c] = cur.e2 + (ex * ex + ey * ey + ez * ez) * p.dt;
             guard(p, ex);
         }
         T Mh = p.Mh0;
-        if (MATH) {
-            const int g = p.geom[c];
-            if (g) Mh = p.matMh[g - 1];
-        }
+        if (MATH && cur.g) Mh = p.matMh[cur.g - 1];
         T dExy = cdiv(ex_yp - ex, p.ddy);
         T dExz = cdiv(ex_zp - ex, p.ddz);
         T dEyx = cdiv(ey_xp - ey, p.ddx);
@@ -119,14 +144,13 @@ __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HPa
                 const int q = ix;
                 const int k = q + l.nb * (iy + ny * iz);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pEyx = B * l.psi[2][k] + A * dEyx;
                 const T pEzx = B * l.psi[3][k] + A * dEzx;
                 l.psi[2][k] = pEyx; l.psi[3][k] = pEzx;
                 hy += Mh * pEzx;
                 hz -= Mh * pEyx;
-                dEyx = cdiv(dEyx, K);
-                dEzx = cdiv(dEzx, K);
+                dEyx = cdiv(dEyx, l.K[q]);
+                dEzx = cdiv(dEzx, l.K[q]);
             }
         }
         {
@@ -135,14 +159,13 @@ __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HPa
                 const int q = ix - (l.ib - 1);
                 const int k = q + l.nb * (iy + ny * iz);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pEyx = B * l.psi[2][k] + A * dEyx;
                 const T pEzx = B * l.psi[3][k] + A * dEzx;
                 l.psi[2][k] = pEyx; l.psi[3][k] = pEzx;
                 hy += Mh * pEzx;
                 hz -= Mh * pEyx;
-                dEyx = cdiv(dEyx, K);
-                dEzx = cdiv(dEzx, K);
+                dEyx = cdiv(dEyx, l.K[q]);
+                dEzx = cdiv(dEzx, l.K[q]);
             }
         }
         {
@@ -151,14 +174,13 @@ __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HPa
                 const int q = iy;
                 const int k = ix + sy * (q + l.nb * iz);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pExy = B * l.psi[2][k] + A * dExy;
                 const T pEzy = B * l.psi[3][k] + A * dEzy;
                 l.psi[2][k] = pExy; l.psi[3][k] = pEzy;
                 hx -= Mh * pEzy;
                 hz += Mh * pExy;
-                dExy = cdiv(dExy, K);
-                dEzy = cdiv(dEzy, K);
+                dExy = cdiv(dExy, l.K[q]);
+                dEzy = cdiv(dEzy, l.K[q]);
             }
         }
         {
@@ -167,14 +189,13 @@ __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HPa
                 const int q = iy - (l.ib - 1);
                 const int k = ix + sy * (q + l.nb * iz);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pExy = B * l.psi[2][k] + A * dExy;
                 const T pEzy = B * l.psi[3][k] + A * dEzy;
                 l.psi[2][k] = pExy; l.psi[3][k] = pEzy;
                 hx -= Mh * pEzy;
                 hz += Mh * pExy;
-                dExy = cdiv(dExy, K);
-                dEzy = cdiv(dEzy, K);
+                dExy = cdiv(dExy, l.K[q]);
+                dEzy = cdiv(dEzy, l.K[q]);
             }
         }
         {
@@ -183,14 +204,13 @@ __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HPa
                 const int q = iz;
                 const int k = ix + sy * (iy + ny * q);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pExz = B * l.psi[2][k] + A * dExz;
                 const T pEyz = B * l.psi[3][k] + A * dEyz;
                 l.psi[2][k] = pExz; l.psi[3][k] = pEyz;
                 hx += Mh * pEyz;
                 hy -= Mh * pExz;
-                dExz = cdiv(dExz, K);
-                dEyz = cdiv(dEyz, K);
+                dExz = cdiv(dExz, l.K[q]);
+                dEyz = cdiv(dEyz, l.K[q]);
             }
         }
         {
@@ -199,23 +219,46 @@ __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HPa
                 const int q = iz - (l.ib - 1);
                 const int k = ix + sy * (iy + ny * q);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pExz = B * l.psi[2][k] + A * dExz;
                 const T pEyz = B * l.psi[3][k] + A * dEyz;
                 l.psi[2][k] = pExz; l.psi[3][k] = pEyz;
                 hx += Mh * pEyz;
                 hy -= Mh * pExz;
-                dExz = cdiv(dExz, K);
-                dEyz = cdiv(dEyz, K);
+                dExz = cdiv(dExz, l.K[q]);
+                dEyz = cdiv(dEyz, l.K[q]);
             }
         }
         hx -= Mh * (dEzy - dEyz);
         hy -= Mh * (dExz - dEzx);
         hz -= Mh * (dEyx - dExy);
         p.Hx[c] = hx; p.Hy[c] = hy; p.Hz[c] = hz;
-        ex = ex_zp;
-        ey = ey_zp;
+        ex = cur.exz;
+        ey = cur.eyz;
+        cur = nxt;
     }
+}
+
+template <typename T>
+struct ELoad {
+    T hx, hy, hz, hyx, hzx, hxy, hzy, dx, dy, dz;
+    int g;
+};
+
+template <typename T, typename R, bool MAT>
+__device__ __forceinline__ ELoad<T> e3d_load(const EParams<T, R>& p, int c, int ox, int oy) {
+    ELoad<T> v;
+    v.hx = p.Hx[c];
+    v.hy = p.Hy[c];
+    v.hz = p.Hz[c];
+    v.hyx = p.Hy[c + ox];
+    v.hzx = p.Hz[c + ox];
+    v.hxy = p.Hx[c + oy];
+    v.hzy = p.Hz[c + oy];
+    v.dx = p.Dx[c];
+    v.dy = p.Dy[c];
+    v.dz = p.Dz[c];
+    v.g = MAT ? (int)p.geom[c] : 0;
+    return v;
 }
 
 template <typename T, typename R, bool MAT>
@@ -227,45 +270,39 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
     const int z0 = blockIdx.z * zc;
     const int z1 = min(z0 + zc, nz);
     const int sy = p.L.px, sz = p.L.sz;
+    const int bxl = p.bc[MFD_XL], byl = p.bc[MFD_YL], bzl = p.bc[MFD_ZL];
+    const bool xl = ix == 0, yl = iy == 0;
+    const int ox = !xl ? -1 : (bxl == MFD_BC_PERIODIC ? nx - 1 : 0);
+    const int oy = !yl ? -sy : (byl == MFD_BC_PERIODIC ? (ny - 1) * sy : 0);
+    const bool zx = xl && bxl == MFD_BC_DIRICHLET, zy = yl && byl == MFD_BC_DIRICHLET;
     int c = ix + sy * iy + sz * z0;
-        const bool xl = ix == 0, yl = iy == 0;
-    const int wx = nx - 1, wy = (ny - 1) * sy, wz = (nz - 1) * sz;
     T hx_zm, hy_zm;
-    if (z0 > 0) { hx_zm = p.Hx[c - sz]; hy_zm = p.Hy[c - sz]; }
-    else {
-        const int b = p.bc[MFD_ZL];
-        hx_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hx[c + wz] : T(0), p.Hx[c]);
-        hy_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + wz] : T(0), p.Hy[c]);
+    if (z0 > 0) {
+        hx_zm = p.Hx[c - sz];
+        hy_zm = p.Hy[c - sz];
+    } else {
+        const int oz = bzl == MFD_BC_PERIODIC ? (nz - 1) * sz : 0;
+        hx_zm = bzl == MFD_BC_DIRICHLET ? T(0) : p.Hx[c + oz];
+        hy_zm = bzl == MFD_BC_DIRICHLET ? T(0) : p.Hy[c + oz];
     }
     T* const Ep[3] = {p.Ex, p.Ey, p.Ez};
+    ELoad<T> cur = e3d_load<T, R, MAT>(p, c, ox, oy);
     for (int iz = z0; iz < z1; ++iz, c += sz) {
-        const T hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
-        T hy_xm, hz_xm, hx_ym, hz_ym;
-        if (!xl) { hy_xm = p.Hy[c - 1]; hz_xm = p.Hz[c - 1]; }
-        else {
-            const int b = p.bc[MFD_XL];
-            hy_xm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + wx] : T(0), hy);
-            hz_xm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hz[c + wx] : T(0), hz);
-        }
-        if (!yl) { hx_ym = p.Hx[c - sy]; hz_ym = p.Hz[c - sy]; }
-        else {
-            const int b = p.bc[MFD_YL];
-            hx_ym = bc_value(b, b == MFD_BC_PERIODIC ? p.Hx[c + wy] : T(0), hx);
-            hz_ym = bc_value(b, b == MFD_BC_PERIODIC ? p.Hz[c + wy] : T(0), hz);
-        }
+        ELoad<T> nxt;
+        if (iz + 1 < z1) nxt = e3d_load<T, R, MAT>(p, c + sz, ox, oy);
+        const T hx = cur.hx, hy = cur.hy, hz = cur.hz;
+        const T hy_xm = zx ? T(0) : cur.hyx, hz_xm = zx ? T(0) : cur.hzx;
+        const T hx_ym = zy ? T(0) : cur.hxy, hz_ym = zy ? T(0) : cur.hzy;
         T dHxy = cdiv(hx - hx_ym, p.ddy);
         T dHxz = cdiv(hx - hx_zm, p.ddz);
         T dHyx = cdiv(hy - hy_xm, p.ddx);
         T dHyz = cdiv(hy - hy_zm, p.ddz);
         T dHzx = cdiv(hz - hz_xm, p.ddx);
         T dHzy = cdiv(hz - hz_ym, p.ddy);
-        int g = 0;
+        const int g = cur.g;
         T Md1 = p.Md10, Md2 = p.Md20;
-        if (MAT) {
-            g = p.geom[c];
-            if (g) { Md1 = p.mats[g - 1].Md1; Md2 = p.mats[g - 1].Md2; }
-        }
-        T Dv[3] = {p.Dx[c], p.Dy[c], p.Dz[c]};
+        if (MAT && g) { Md1 = p.mats[g - 1].Md1; Md2 = p.mats[g - 1].Md2; }
+        T Dv[3] = {cur.dx, cur.dy, cur.dz};
         // CPML (models.jl:975-1035)
         {
             const LayerDev<T>& l = p.lay[MFD_XL];
@@ -273,14 +310,13 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
                 const int q = ix;
                 const int k = q + l.nb * (iy + ny * iz);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pHyx = B * l.psi[0][k] + A * dHyx;
                 const T pHzx = B * l.psi[1][k] + A * dHzx;
                 l.psi[0][k] = pHyx; l.psi[1][k] = pHzx;
                 Dv[1] -= Md2 * pHzx;
                 Dv[2] += Md2 * pHyx;
-                dHyx = cdiv(dHyx, K);
-                dHzx = cdiv(dHzx, K);
+                dHyx = cdiv(dHyx, l.K[q]);
+                dHzx = cdiv(dHzx, l.K[q]);
             }
         }
         {
@@ -289,14 +325,13 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
                 const int q = ix - (l.ib - 1);
                 const int k = q + l.nb * (iy + ny * iz);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pHyx = B * l.psi[0][k] + A * dHyx;
                 const T pHzx = B * l.psi[1][k] + A * dHzx;
                 l.psi[0][k] = pHyx; l.psi[1][k] = pHzx;
                 Dv[1] -= Md2 * pHzx;
                 Dv[2] += Md2 * pHyx;
-                dHyx = cdiv(dHyx, K);
-                dHzx = cdiv(dHzx, K);
+                dHyx = cdiv(dHyx, l.K[q]);
+                dHzx = cdiv(dHzx, l.K[q]);
             }
         }
         {
@@ -305,14 +340,13 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
                 const int q = iy;
                 const int k = ix + sy * (q + l.nb * iz);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pHxy = B * l.psi[0][k] + A * dHxy;
                 const T pHzy = B * l.psi[1][k] + A * dHzy;
                 l.psi[0][k] = pHxy; l.psi[1][k] = pHzy;
                 Dv[0] += Md2 * pHzy;
                 Dv[2] -= Md2 * pHxy;
-                dHxy = cdiv(dHxy, K);
-                dHzy = cdiv(dHzy, K);
+                dHxy = cdiv(dHxy, l.K[q]);
+                dHzy = cdiv(dHzy, l.K[q]);
             }
         }
         {
@@ -321,14 +355,13 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
                 const int q = iy - (l.ib - 1);
                 const int k = ix + sy * (q + l.nb * iz);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pHxy = B * l.psi[0][k] + A * dHxy;
                 const T pHzy = B * l.psi[1][k] + A * dHzy;
                 l.psi[0][k] = pHxy; l.psi[1][k] = pHzy;
                 Dv[0] += Md2 * pHzy;
                 Dv[2] -= Md2 * pHxy;
-                dHxy = cdiv(dHxy, K);
-                dHzy = cdiv(dHzy, K);
+                dHxy = cdiv(dHxy, l.K[q]);
+                dHzy = cdiv(dHzy, l.K[q]);
             }
         }
         {
@@ -337,14 +370,13 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
                 const int q = iz;
                 const int k = ix + sy * (iy + ny * q);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pHxz = B * l.psi[0][k] + A * dHxz;
                 const T pHyz = B * l.psi[1][k] + A * dHyz;
                 l.psi[0][k] = pHxz; l.psi[1][k] = pHyz;
                 Dv[0] -= Md2 * pHyz;
                 Dv[1] += Md2 * pHxz;
-                dHxz = cdiv(dHxz, K);
-                dHyz = cdiv(dHyz, K);
+                dHxz = cdiv(dHxz, l.K[q]);
+                dHyz = cdiv(dHyz, l.K[q]);
             }
         }
         {
@@ -353,14 +385,13 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
                 const int q = iz - (l.ib - 1);
                 const int k = ix + sy * (iy + ny * q);
                 const T B = l.B[q], A = l.A[q];
-                const DivC<T> K = l.K[q];
                 const T pHxz = B * l.psi[0][k] + A * dHxz;
                 const T pHyz = B * l.psi[1][k] + A * dHyz;
                 l.psi[0][k] = pHxz; l.psi[1][k] = pHyz;
                 Dv[0] -= Md2 * pHyz;
                 Dv[1] += Md2 * pHxz;
-                dHxz = cdiv(dHxz, K);
-                dHyz = cdiv(dHyz, K);
+                dHxz = cdiv(dHxz, l.K[q]);
+                dHyz = cdiv(dHyz, l.K[q]);
             }
         }
         Dv[0] = Md1 * Dv[0] + Md2 * (dHzy - dHyz);
@@ -376,6 +407,7 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
         }
         hx_zm = hx;
         hy_zm = hy;
+        cur = nxt;
     }
 }
 

@@ -244,8 +244,9 @@ def library_path():
 
 
 def load_library(path=None):
-    """The CUDA library (fails loudly when it has not been built: there is no CPU path)."""
-    path = path or library_path()
+    """The CUDA library (fails loudly when it has not been built: there is no CPU path).
+    MFD_LIBRARY names another build of the same library."""
+    path = path or os.environ.get("MFD_LIBRARY") or library_path()
     if path not in _LIB_CACHE:
         if not os.path.exists(path):
             raise RuntimeError(f"CUDA library {path} is not built; run __graft_entry__.build()")
