@@ -237,7 +237,7 @@ MFD_API int64_t mfd_tfsf_record_size(const mfd_handle* h, int32_t k);
  * events on the handle's stream and its duration is summed per kernel class. */
 MFD_API int mfd_set_profiling(mfd_handle* h, int32_t on);
 /* Kernel classes: 0 H update, 1 E update, 2 sources, 3 TFSF, 4 monitors, 5 DFT,
- * 6 sums flush.  Fills ms[k], launches[k] for k < n; returns the number of classes. */
+ * 6 sums flush, 7 material response.  Fills ms[k], launches[k] for k < n; returns the number of classes. */
 MFD_API int mfd_kernel_times(const mfd_handle* h, double* ms, int64_t* launches, int32_t n);
 /* Device time of the last mfd_run call (CUDA events around the whole call), in ms. */
 MFD_API int mfd_last_run_ms(const mfd_handle* h, double* ms);

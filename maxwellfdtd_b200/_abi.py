@@ -191,7 +191,7 @@ class Stepper:
         self._check(self.lib.read_monitor(self.h, int(m), int(comp), out.ctypes.data_as(C.c_void_p)))
         return out
 
-    KERNEL_CLASSES = ("H", "E", "sources", "tfsf", "monitors", "dft", "sums")
+    KERNEL_CLASSES = ("H", "E", "sources", "tfsf", "monitors", "dft", "sums", "material")
 
     def set_profiling(self, on):
         self._check(self.lib.set_profiling(self.h, int(bool(on))))

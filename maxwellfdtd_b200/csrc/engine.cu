@@ -26,6 +26,7 @@
 
 #include "aux.cuh"
 #include "yee.cuh"
+#include "yee3d_tma.cuh"
 
 namespace mfd {
 
@@ -45,7 +46,7 @@ struct Error : std::runtime_error {
                                std::string(#call) + ": " + cudaGetErrorString(e_));               \
     } while (0)
 
-enum { KC_H = 0, KC_E, KC_SRC, KC_TFSF, KC_MON, KC_DFT, KC_SUMS, KC_N };
+enum { KC_H = 0, KC_E, KC_SRC, KC_TFSF, KC_MON, KC_DFT, KC_SUMS, KC_MAT, KC_N };
 
 struct HandleBase {
     std::string err;
@@ -159,6 +160,25 @@ class DivisorCache {
     std::map<uint32_t, bool> known_;
 };
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (EncodeTiledFn) nullptr;
+        }
+        return (EncodeTiledFn)p;
+    }();
+    return fn;
+}
+
 template <typename T>
 static DivC<T> make_div(T d) {
     DivC<T> D{};
@@ -170,6 +190,12 @@ static DivC<T> make_div(T d) {
         D.lo = (T)std::max(std::ldexp(1.0, -76), std::ldexp(1.0, -100) / r);
         D.hi = (T)std::min(std::ldexp(1.0, 100), std::ldexp(1.0, 100) / r);
         D.ok = (D.lo <= T(1) && D.hi >= T(2)) ? 1 : 0;   // the checked binade lies in the band
+        const float lo = (float)D.lo, hi = (float)D.hi;
+        uint32_t a, b;
+        std::memcpy(&a, &lo, 4);
+        std::memcpy(&b, &hi, 4);
+        D.lob = a;
+        D.span = b - a;
     }
     return D;
 }
@@ -182,6 +208,8 @@ class Engine : public HandleBase {
     int64_t nt = 0;
     T dx{}, dy{}, dz{}, dt{};
     DivC<T> ddx{}, ddy{}, ddz{};
+    bool fastdiv = false;        // every divisor passed the device check
+    Div3 d3{};                   // grid constants for the branch-free 3-D division (single precision)
     int bc[6] = {1, 1, 1, 1, 1, 1};
     cudaStream_t st = nullptr;
     std::vector<void*> allocs;
@@ -198,6 +226,7 @@ class Engine : public HandleBase {
     T* matMh = nullptr;
     MatDev<T, R>* mats_dev = nullptr;
     std::vector<MatDev<T, R>> mats_host;
+    std::vector<int> response_mats;   // present materials whose E comes from material_kernel
     bool any_plasma = false;
 
     struct Src {
@@ -237,6 +266,13 @@ class Engine : public HandleBase {
 
     // launch shapes
     int bx3 = 32, by3 = 8, zc3 = 16;
+    // TMA-fed 3-D kernels (single precision)
+    bool use_tma = false;
+    int tma_zc = 16;
+    HTmaParams htma{};
+    ETmaParams<R> etma{};
+    int* d_timeout = nullptr;   // set by a kernel whose bounded wait ran out
+    int* h_timeout = nullptr;
 
     // timing
     bool profiling = false;
@@ -256,6 +292,7 @@ class Engine : public HandleBase {
         if (run_ev[0]) cudaEventDestroy(run_ev[0]);
         if (run_ev[1]) cudaEventDestroy(run_ev[1]);
         if (h_flags) cudaFreeHost(h_flags);
+        if (h_timeout) cudaFreeHost(h_timeout);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -324,6 +361,15 @@ class Engine : public HandleBase {
             std::vector<DivC<T>> dv = {make_div<T>(dx), make_div<T>(dy), make_div<T>(dz)};
             verify_divs(dv);
             ddx = dv[0]; ddy = dv[1]; ddz = dv[2];
+            fastdiv = sizeof(T) == 4 && ddx.ok && ddy.ok && ddz.ok;
+            if constexpr (sizeof(T) == 4) {   // band common to the three divisors (div6)
+                d3.dx = ddx.d; d3.dy = ddy.d; d3.dz = ddz.d;
+                d3.rx = ddx.r; d3.ry = ddy.r; d3.rz = ddz.r;
+                const unsigned lob = std::max(ddx.lob, std::max(ddy.lob, ddz.lob));
+                const unsigned hib = std::min(ddx.lob + ddx.span, std::min(ddy.lob + ddy.span, ddz.lob + ddz.span));
+                d3.lob1 = lob - 1u;
+                d3.hib = hib;
+            }
         }
         for (int f = 0; f < 6; ++f) bc[f] = d->bc[f];
         Mh0 = (T)d->Mh0; Me0 = (T)d->Me0; Md10 = (T)d->Md10; Md20 = (T)d->Md20;
@@ -373,8 +419,10 @@ class Engine : public HandleBase {
             for (int q = 0; q < s.nq; ++q) { M.Aq[q] = (T)s.Aq[q]; M.Bq[q] = (T)s.Bq[q]; M.Cq[q] = (T)s.Cq[q]; }
             M.kerr = s.kerr ? 1 : 0; M.Mk2 = (T)s.Mk2; M.Mk3 = (T)s.Mk3;
             M.plasma = s.plasma ? 1 : 0;
+            M.simple = (M.nq == 0 && !M.plasma && !M.kerr) ? 1 : 0;
             const int g = m + 1;
             const bool present = bx1[g] >= 0;
+            if (present && !M.simple) response_mats.push_back(g);
             if (present) {
                 M.bx0 = bx0[g]; M.by0 = by0[g]; M.bz0 = bz0[g];
                 M.bnx = bx1[g] - bx0[g] + 1; M.bny = by1[g] - by0[g] + 1; M.bnz = bz1[g] - bz0[g] + 1;
@@ -422,6 +470,7 @@ class Engine : public HandleBase {
                 std::vector<DivC<T>> kv;
                 for (int i = 0; i < L.nb; ++i) kv.push_back(make_div<T>((T)L.K[i]));
                 verify_divs(kv);
+                for (auto& D : kv) fastdiv = fastdiv && D.ok;
                 lay[f].K = upload(kv.data(), kv.size());
             }
             lay[f].A = upload_cast<T>(L.A, L.nb);
@@ -467,6 +516,51 @@ class Engine : public HandleBase {
                 bx3 = a; by3 = b; zc3 = c;
             }
         }
+        d_timeout = dalloc<int>(1);
+        MFD_CK(cudaHostAlloc(&h_timeout, sizeof(int), cudaHostAllocDefault));
+        init_tma();
+    }
+
+    // Tensor maps of the TMA-fed 3-D kernels: dims (nx, ny, nz) so cells beyond the grid are
+    // out of bounds (zero-filled); strides of the padded layout (multiples of 16 bytes).
+    bool make_map(CUtensorMap* m, const void* base, bool u8, unsigned bx, unsigned by) {
+        EncodeTiledFn fn = encode_tiled();
+        if (!fn) return false;
+        const size_t es = u8 ? 1 : sizeof(T);
+        cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+        cuuint64_t strides[2] = {(cuuint64_t)px * es, (cuuint64_t)sz * es};
+        cuuint32_t box[3] = {bx, by, 1};
+        cuuint32_t estr[3] = {1, 1, 1};
+        return fn(m, u8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+
+    void init_tma() {
+        if (ndim != 3 || sizeof(T) != 4 || !std::getenv("MFD_TMA")) return;
+        if (const char* z = std::getenv("MFD_TMA_ZC")) tma_zc = std::max(1, std::atoi(z));
+        const uint8_t* gm = geom ? geom : (const uint8_t*)F[MFD_HX];
+        const void* e2 = E2 ? (const void*)E2 : (const void*)Sa;
+        bool ok = true;
+        ok = ok && make_map(&htma.mEx, F[MFD_EX], false, 32, 9);
+        ok = ok && make_map(&htma.mEy, F[MFD_EY], false, 36, 8);
+        ok = ok && make_map(&htma.mEz, F[MFD_EZ], false, 36, 9);
+        ok = ok && make_map(&htma.mHx, F[MFD_HX], false, 32, 8);
+        ok = ok && make_map(&htma.mHy, F[MFD_HY], false, 32, 8);
+        ok = ok && make_map(&htma.mHz, F[MFD_HZ], false, 32, 8);
+        ok = ok && make_map(&htma.mSa, Sa, false, 32, 8);
+        ok = ok && make_map(&htma.mE2, e2, false, 32, 8);
+        ok = ok && make_map(&htma.mG, gm, geom != nullptr, 32, 8);
+        ok = ok && make_map(&etma.mHx, F[MFD_HX], false, 32, 9);
+        ok = ok && make_map(&etma.mHy, F[MFD_HY], false, 36, 8);
+        ok = ok && make_map(&etma.mHz, F[MFD_HZ], false, 36, 9);
+        ok = ok && make_map(&etma.mDx, F[MFD_DX], false, 32, 8);
+        ok = ok && make_map(&etma.mDy, F[MFD_DY], false, 32, 8);
+        ok = ok && make_map(&etma.mDz, F[MFD_DZ], false, 32, 8);
+        ok = ok && make_map(&etma.mG, gm, geom != nullptr, 32, 8);
+        htma.timeout = d_timeout;
+        etma.timeout = d_timeout;
+        use_tma = ok;
     }
 
     // Statement lists: sources.jl:727-773 (3-D), 477-495 (2-D), 326-334 (1-D).
@@ -771,7 +865,7 @@ class Engine : public HandleBase {
         return p;
     }
 
-    EParams<T, R> eparams(int cur) {
+    EParams<T, R> eparams() {
         EParams<T, R> p{};
         p.L = layout();
         p.ddx = ddx; p.ddy = ddy; p.ddz = ddz; p.dt = dt;
@@ -782,46 +876,135 @@ class Engine : public HandleBase {
         p.Hx = F[MFD_HX]; p.Hy = F[MFD_HY]; p.Hz = F[MFD_HZ];
         p.Dx = F[MFD_DX]; p.Dy = F[MFD_DY]; p.Dz = F[MFD_DZ];
         p.Ex = F[MFD_EX]; p.Ey = F[MFD_EY]; p.Ez = F[MFD_EZ];
-        p.cur = cur;
         return p;
+    }
+
+    template <bool MATH, bool FAST>
+    void launch_H_t(const HParams<T>& p) {
+        if (ndim == 3) {
+            dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
+            h3d_kernel<T, MATH, FAST><<<grd, blk, 0, st>>>(p, zc3);
+        } else if (ndim == 2) {
+            dim3 blk(32, 8), grd((nx + 31) / 32, (nz + 7) / 8);
+            h2d_kernel<T, MATH, FAST><<<grd, blk, 0, st>>>(p);
+        } else {
+            dim3 blk(256), grd((nz + 255) / 256);
+            h1d_kernel<T, MATH, FAST><<<grd, blk, 0, st>>>(p);
+        }
+    }
+
+    template <bool MATH, bool FAST>
+    void launch_H_tma() {
+        dim3 blk(TMA_BX, TMA_BY), grd((nx + TMA_BX - 1) / TMA_BX, (ny + TMA_BY - 1) / TMA_BY, (nz + tma_zc - 1) / tma_zc);
+        h3d_tma_kernel<MATH, FAST><<<grd, blk, TMA_STAGES * HStage::BYTES, st>>>(htma, tma_zc);
+    }
+
+    template <bool MAT, bool FAST>
+    void launch_E_tma() {
+        dim3 blk(TMA_BX, TMA_BY), grd((nx + TMA_BX - 1) / TMA_BX, (ny + TMA_BY - 1) / TMA_BY, (nz + tma_zc - 1) / tma_zc);
+        e3d_tma_kernel<R, MAT, FAST><<<grd, blk, TMA_STAGES * EStage::BYTES, st>>>(etma, tma_zc);
+    }
+
+    template <bool MATH, bool FAST, bool ACC, bool E2S>
+    void launch_H_f32(const HParams<float>& p) {
+        dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
+        h3d_f32_kernel<MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, zc3);
+    }
+
+    template <bool MATH, bool FAST>
+    void launch_H_f32_acc(const HParams<float>& p) {
+        if (!p.accum) launch_H_f32<MATH, FAST, false, false>(p);
+        else if (p.sum_e2) launch_H_f32<MATH, FAST, true, true>(p);
+        else launch_H_f32<MATH, FAST, true, false>(p);
+    }
+
+    template <bool MAT, bool FAST>
+    void launch_E_f32(const EParams<float, R>& p) {
+        dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
+        e3d_f32_kernel<R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, zc3);
     }
 
     void launch_H(int accum, long long prev_step) {
         HParams<T> p = hparams(accum, prev_step);
-        launch(KC_H, [&] {
-            if (ndim == 3) {
-                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
-                if (math_needed) h3d_kernel<T, true><<<grd, blk, 0, st>>>(p, zc3);
-                else h3d_kernel<T, false><<<grd, blk, 0, st>>>(p, zc3);
-            } else if (ndim == 2) {
-                dim3 blk(32, 8), grd((nx + 31) / 32, (nz + 7) / 8);
-                if (math_needed) h2d_kernel<T, true><<<grd, blk, 0, st>>>(p);
-                else h2d_kernel<T, false><<<grd, blk, 0, st>>>(p);
-            } else {
-                dim3 blk(256), grd((nz + 255) / 256);
-                if (math_needed) h1d_kernel<T, true><<<grd, blk, 0, st>>>(p);
-                else h1d_kernel<T, false><<<grd, blk, 0, st>>>(p);
+        if constexpr (sizeof(T) == 4) {
+            if (ndim == 3 && !use_tma) {
+                const HParams<float>& pf = reinterpret_cast<const HParams<float>&>(p);
+                launch(KC_H, [&] {
+                    if (math_needed) { if (fastdiv) launch_H_f32_acc<true, true>(pf); else launch_H_f32_acc<true, false>(pf); }
+                    else { if (fastdiv) launch_H_f32_acc<false, true>(pf); else launch_H_f32_acc<false, false>(pf); }
+                });
+                return;
             }
+            if (use_tma) {
+                std::memcpy(&htma.p, &p, sizeof(p));
+                launch(KC_H, [&] {
+                    if (math_needed) { if (fastdiv) launch_H_tma<true, true>(); else launch_H_tma<true, false>(); }
+                    else { if (fastdiv) launch_H_tma<false, true>(); else launch_H_tma<false, false>(); }
+                });
+                return;
+            }
+        }
+        launch(KC_H, [&] {
+            if (math_needed) { if (fastdiv) launch_H_t<true, true>(p); else launch_H_t<true, false>(p); }
+            else { if (fastdiv) launch_H_t<false, true>(p); else launch_H_t<false, false>(p); }
         });
     }
 
+    template <bool MAT, bool FAST>
+    void launch_E_t(const EParams<T, R>& p) {
+        if (ndim == 3) {
+            dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
+            e3d_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p, zc3);
+        } else if (ndim == 2) {
+            dim3 blk(32, 8), grd((nx + 31) / 32, (nz + 7) / 8);
+            e2d_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p);
+        } else {
+            dim3 blk(256), grd((nz + 255) / 256);
+            e1d_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p);
+        }
+    }
+
     void launch_E(int cur) {
-        EParams<T, R> p = eparams(cur);
-        launch(KC_E, [&] {
-            if (ndim == 3) {
-                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
-                if (any_geom) e3d_kernel<T, R, true><<<grd, blk, 0, st>>>(p, zc3);
-                else e3d_kernel<T, R, false><<<grd, blk, 0, st>>>(p, zc3);
-            } else if (ndim == 2) {
-                dim3 blk(32, 8), grd((nx + 31) / 32, (nz + 7) / 8);
-                if (any_geom) e2d_kernel<T, R, true><<<grd, blk, 0, st>>>(p);
-                else e2d_kernel<T, R, false><<<grd, blk, 0, st>>>(p);
-            } else {
-                dim3 blk(256), grd((nz + 255) / 256);
-                if (any_geom) e1d_kernel<T, R, true><<<grd, blk, 0, st>>>(p);
-                else e1d_kernel<T, R, false><<<grd, blk, 0, st>>>(p);
+        EParams<T, R> p = eparams();
+        bool done_tma = false;
+        if constexpr (sizeof(T) == 4) {
+            if (ndim == 3 && !use_tma) {
+                const EParams<float, R>& pf = reinterpret_cast<const EParams<float, R>&>(p);
+                launch(KC_E, [&] {
+                    if (any_geom) { if (fastdiv) launch_E_f32<true, true>(pf); else launch_E_f32<true, false>(pf); }
+                    else { if (fastdiv) launch_E_f32<false, true>(pf); else launch_E_f32<false, false>(pf); }
+                });
+                done_tma = true;
+            } else if (use_tma) {
+                std::memcpy(&etma.p, &p, sizeof(p));
+                launch(KC_E, [&] {
+                    if (any_geom) { if (fastdiv) launch_E_tma<true, true>(); else launch_E_tma<true, false>(); }
+                    else { if (fastdiv) launch_E_tma<false, true>(); else launch_E_tma<false, false>(); }
+                });
+                done_tma = true;
             }
-        });
+        }
+        if (!done_tma)
+            launch(KC_E, [&] {
+                if (any_geom) { if (fastdiv) launch_E_t<true, true>(p); else launch_E_t<true, false>(p); }
+                else { if (fastdiv) launch_E_t<false, true>(p); else launch_E_t<false, false>(p); }
+            });
+        // E of dispersive / plasma / Kerr cells (material_kernel)
+        for (int g : response_mats) {
+            const MatDev<T, R>& m = mats_host[g - 1];
+            launch(KC_MAT, [&] {
+                dim3 grd((m.bnx + 127) / 128, m.bny, m.bnz);
+                if (ndim == 3)
+                    material_kernel<T, R, 3><<<grd, 128, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], F[MFD_DY], F[MFD_DZ],
+                                                                  F[MFD_EX], F[MFD_EY], F[MFD_EZ], cur, dt);
+                else if (ndim == 2)
+                    material_kernel<T, R, 2><<<grd, 128, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], nullptr, F[MFD_DZ],
+                                                                  F[MFD_EX], nullptr, F[MFD_EZ], cur, dt);
+                else
+                    material_kernel<T, R, 1><<<grd, 128, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], nullptr, nullptr,
+                                                                  F[MFD_EX], nullptr, nullptr, cur, dt);
+            });
+        }
     }
 
     void launch_sources(int64_t it) {
@@ -916,7 +1099,14 @@ class Engine : public HandleBase {
         MFD_CK(cudaEventRecord(run_ev[1], st));
         MFD_CK(cudaMemcpyAsync(h_flags + (a - 1), d_flags + (a - 1), (size_t)(b - a + 1) * sizeof(int),
                                cudaMemcpyDeviceToHost, st));
+        MFD_CK(cudaMemcpyAsync(h_timeout, d_timeout, sizeof(int), cudaMemcpyDeviceToHost, st));
         bounded_sync(st);
+        if (*h_timeout) {
+            done = b;
+            bad_step = b;
+            err = "a kernel's bounded wait on its TMA copies ran out";
+            return MFD_ERR_TIMEOUT;
+        }
         float ms = 0;
         MFD_CK(cudaEventElapsedTime(&ms, run_ev[0], run_ev[1]));
         run_ms = ms;

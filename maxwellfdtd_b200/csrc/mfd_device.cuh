@@ -50,28 +50,76 @@ struct Layout {
 // each divisor, against IEEE division over all 2^23 significands in [1, 2) before the first
 // step; a divisor that fails (or any double-precision divisor) keeps IEEE division
 // (ok = 0), as do numerators outside the band.
+// Kernels take FAST = true only when every divisor of the model passed the check; the
+// band test is one unsigned compare on the bit pattern (lob = bits(lo), span = bits(hi) -
+// bits(lo)).  A zero numerator returns x (0/d keeps the sign of x since d > 0).
 template <typename T>
 struct DivC {
     T d, r;          // divisor and its correctly rounded reciprocal
     T lo, hi;        // |x| band in which the correction step is exact
+    unsigned lob, span;
     int ok;          // verified for every significand
 };
 
-template <typename T>
+template <bool FAST, typename T>
 __device__ __forceinline__ T cdiv(T x, const DivC<T>& D) {
     return x / D.d;
 }
 
 template <>
-__device__ __forceinline__ float cdiv<float>(float x, const DivC<float>& D) {
-    const float ax = fabsf(x);
-    if (ax == 0.0f) return x;   // 0/d keeps the sign of x (d > 0)
-    if (D.ok && ax >= D.lo && ax <= D.hi) {
+__device__ __forceinline__ float cdiv<true, float>(float x, const DivC<float>& D) {
+    const unsigned ax = __float_as_uint(x) & 0x7fffffffu;
+    if (ax - D.lob <= D.span) {
         const float q0 = __fmul_rn(x, D.r);
         const float e = __fmaf_rn(-q0, D.d, x);
         return __fmaf_rn(e, D.r, q0);
     }
+    if (ax == 0u) return x;
     return __fdiv_rn(x, D.d);
+}
+
+// The six curl derivatives of a cell divide by the three grid constants.  Div3 holds the
+// three divisors and reciprocals and the band common to the three (lob1 = bits(lo) - 1,
+// hib = bits(hi)), so one integer min/max reduction checks all six numerators: a nonzero
+// |x| outside the band, or an unverified divisor, takes the IEEE division in one rarely
+// taken branch.  copysign(q, x) makes zero numerators exact too (q = RN(x/d) has the sign
+// of x since d > 0).
+struct Div3 {
+    float dx, dy, dz, rx, ry, rz;
+    unsigned lob1, hib;
+};
+
+__device__ __forceinline__ float qcorr(float x, float d, float r) {
+    const float q0 = __fmul_rn(x, r);
+    const float e = __fmaf_rn(-q0, d, x);
+    return copysignf(__fmaf_rn(e, r, q0), x);
+}
+
+// q[i] = RN(x[i] / d[i]) for the six derivatives, d = (dy, dz, dx, dz, dx, dy) in the order
+// (x-y, x-z, y-x, y-z, z-x, z-y) of the curl.
+template <bool FAST>
+__device__ __forceinline__ void div6(const Div3& D, const float (&x)[6], float (&q)[6]) {
+    const float d[6] = {D.dy, D.dz, D.dx, D.dz, D.dx, D.dy};
+    if (FAST) {
+        const float r[6] = {D.ry, D.rz, D.rx, D.rz, D.rx, D.ry};
+        unsigned mn = 0xffffffffu, mx = 0u;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            q[i] = qcorr(x[i], d[i], r[i]);
+            const unsigned ax = __float_as_uint(x[i]) & 0x7fffffffu;
+            mn = min(mn, ax - 1u);   // zero wraps to the maximum: excluded from the lower bound
+            mx = max(mx, ax);
+        }
+        if (mn >= D.lob1 && mx <= D.hib) return;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const unsigned ax = __float_as_uint(x[i]) & 0x7fffffffu;
+            if (ax != 0u && (ax - 1u < D.lob1 || ax > D.hib)) q[i] = __fdiv_rn(x[i], d[i]);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) q[i] = __fdiv_rn(x[i], d[i]);
+    }
 }
 
 // sqrt of a sum of squares; zero (most cells early in a run) skips the special-case path.
@@ -103,6 +151,7 @@ struct MatDev {
     int rate_n;
     const T* rate_x;
     const T* rate_y;
+    int simple;                         // no poles, plasma or Kerr: E = D Me in the stencil
     int bx0, by0, bz0, bnx, bny, bnz;   // bounding box of the material's cells
     long long bsize;
     T* P;       // [2][nq][nc][bsize]

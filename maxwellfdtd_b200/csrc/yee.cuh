@@ -1,14 +1,22 @@
-// yee.cuh -- Yee H and E update kernels (1-D, 2-D, 3-D) for sm_100a.
+// yee.cuh -- Yee H and E update kernels (1-D, 2-D, 3-D) and the material kernel, sm_100a.
 //
-// 3-D kernels march along z: a thread owns one (ix, iy) column of a z-chunk and keeps the
-// z-neighbour plane in registers (E at iz+1 for the H update, H at iz-1 for the E update),
-// so each plane of the read-only field is fetched from memory once per chunk; x and y
-// neighbours come from the same or adjacent warps through L1.  The CPML psi recursions are
-// fused into the curls, the material response (ADE poles, plasma, Kerr) into the E update,
-// and the running sums Sa/E2 of the previous step plus the NaN/Inf guard on Ex into the H
-// update, which reads every E and H value of the cell anyway.
+// 3-D kernels march along z: a thread owns one (ix, iy) column of a z-chunk.  The march is
+// software-pipelined: all loads of plane iz+1 are issued before the arithmetic and stores of
+// plane iz, so two planes of traffic are in flight per thread, and the z-neighbour plane is
+// carried in registers (E at iz+1 for the H update, H at iz-1 for the E update).  x and y
+// neighbours come from the same or adjacent warps through L1.  Boundary conditions are
+// folded into per-thread neighbour offsets (periodic: the wrapped cell; Neumann: the cell
+// itself; Dirichlet: the cell itself, zeroed after the load).
 //
-// Reference kernels: src/models.jl:248-437 (1-D), 450-719 (2-D), 735-1162 (3-D).
+// Fused into the H update: the CPML psi recursions of the E curl, and -- for the previous
+// step -- the running sums Sa/E2 (outputs.jl:475-485) and the NaN/Inf guard on Ex
+// (models.jl:202-209), since it reads every E and H value of the cell anyway.
+// Fused into the E update: the CPML psi recursions of the H curl, the D update and E = D Me
+// for vacuum and plain dielectrics.  Cells of dispersive, plasma or Kerr materials get E
+// from material_kernel, which runs over each such material's bounding box right after.
+//
+// Every cell update follows the reference kernels (src/models.jl:248-437 1-D, 450-719 2-D,
+// 735-1162 3-D) operation by operation with the same operand types.
 #pragma once
 
 #include "mfd_device.cuh"
@@ -27,9 +35,8 @@ struct HParams {
     const T* __restrict__ matMh;     // Mh of material g at matMh[g-1]
     T* Hx; T* Hy; T* Hz;
     const T* __restrict__ Ex; const T* __restrict__ Ey; const T* __restrict__ Ez;
-    // running sums of the previous step (outputs.jl:475-485) and NaN/Inf guard (models.jl:202-209)
-    int accum;
-    int sum_e2;
+    int accum;             // add the running sums of the previous step
+    int sum_e2;            // E2 is kept (any material cell)
     T* Sa; T* E2;
     int* flags;            // per-step NaN (bit 0) / Inf (bit 1) flags of Ex, index step-1
     long long prev_step;
@@ -48,7 +55,6 @@ struct EParams {
     const T* __restrict__ Hx; const T* __restrict__ Hy; const T* __restrict__ Hz;
     T* Dx; T* Dy; T* Dz;
     T* Ex; T* Ey; T* Ez;
-    int cur;    // ping-pong buffer holding P^n
 };
 
 template <typename T>
@@ -57,14 +63,44 @@ __device__ __forceinline__ void guard(const HParams<T>& p, T ex) {
     if (bad) atomicOr(p.flags + (p.prev_step - 1), bad);
 }
 
+template <typename T>
+__device__ __forceinline__ bool in_layers(const LayerDev<T>& lo, const LayerDev<T>& hi, int i) {
+    return (lo.nb && i < lo.ib) || (hi.nb && i >= hi.ib - 1);
+}
+
+// CPML of the E curl in the H update, one face (models.jl:811-871).  The face's psi pair
+// (psi[2], psi[3]) follows derivatives (da, db); S = +1: h1 += Mh pb, h2 -= Mh pa;
+// S = -1: h1 -= Mh pb, h2 += Mh pa.  Then da, db are divided by kappa.
+template <int S, bool FAST, typename T>
+__device__ __forceinline__ void cpml_h(const LayerDev<T>& l, int q, int k, T Mh, T& da, T& db, T& h1, T& h2) {
+    const T B = l.B[q], A = l.A[q];
+    const T pa = B * l.psi[2][k] + A * da;
+    const T pb = B * l.psi[3][k] + A * db;
+    l.psi[2][k] = pa;
+    l.psi[3][k] = pb;
+    if (S > 0) { h1 += Mh * pb; h2 -= Mh * pa; }
+    else { h1 -= Mh * pb; h2 += Mh * pa; }
+    da = cdiv<FAST>(da, l.K[q]);
+    db = cdiv<FAST>(db, l.K[q]);
+}
+
+// CPML of the H curl in the E update, one face (models.jl:975-1035), psi pair (psi[0],
+// psi[1]); S = +1: D1 += Md2 pb, D2 -= Md2 pa; S = -1: D1 -= Md2 pb, D2 += Md2 pa.
+template <int S, bool FAST, typename T>
+__device__ __forceinline__ void cpml_e(const LayerDev<T>& l, int q, int k, T Md2, T& da, T& db, T& d1, T& d2) {
+    const T B = l.B[q], A = l.A[q];
+    const T pa = B * l.psi[0][k] + A * da;
+    const T pb = B * l.psi[1][k] + A * db;
+    l.psi[0][k] = pa;
+    l.psi[1][k] = pb;
+    if (S > 0) { d1 += Md2 * pb; d2 -= Md2 * pa; }
+    else { d1 -= Md2 * pb; d2 += Md2 * pa; }
+    da = cdiv<FAST>(da, l.K[q]);
+    db = cdiv<FAST>(db, l.K[q]);
+}
+
 // ------------------------------------------------------------------------------------------
 // 3-D
-//
-// Software-pipelined z march: all loads of plane iz+1 are issued before the arithmetic and
-// stores of plane iz, so two planes of memory traffic are in flight per thread.  Boundary
-// conditions are folded into per-thread neighbour offsets (periodic: the wrapped cell;
-// Neumann: the cell itself; Dirichlet: the cell itself, zeroed after the load), so the
-// prefetch never depends on values of the current plane.
 // ------------------------------------------------------------------------------------------
 template <typename T>
 struct HLoad {
@@ -96,8 +132,8 @@ __device__ __forceinline__ HLoad<T> h3d_load(const HParams<T>& p, int c, int iz,
     return v;
 }
 
-template <typename T, bool MATH>
-__global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HParams<T> p, const int zc) {
+template <typename T, bool MATH, bool FAST>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) h3d_kernel(const __grid_constant__ HParams<T> p, const int zc) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -111,6 +147,7 @@ __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HPa
     const int oy = !yr ? sy : (byr == MFD_BC_PERIODIC ? -(ny - 1) * sy : 0);
     const int ozw = bzr == MFD_BC_PERIODIC ? -(nz - 1) * sz : 0;
     const bool zx = xr && bxr == MFD_BC_DIRICHLET, zy = yr && byr == MFD_BC_DIRICHLET;
+    const bool cxy = in_layers(p.lay[MFD_XL], p.lay[MFD_XR], ix) || in_layers(p.lay[MFD_YL], p.lay[MFD_YR], iy);
     int c = ix + sy * iy + sz * z0;
     T ex = p.Ex[c], ey = p.Ey[c];
     HLoad<T> cur = h3d_load<T, MATH>(p, c, z0, ox, oy, ozw);
@@ -131,101 +168,29 @@ __global__ void __launch_bounds__(256, 4) h3d_kernel(const __grid_constant__ HPa
         }
         T Mh = p.Mh0;
         if (MATH && cur.g) Mh = p.matMh[cur.g - 1];
-        T dExy = cdiv(ex_yp - ex, p.ddy);
-        T dExz = cdiv(ex_zp - ex, p.ddz);
-        T dEyx = cdiv(ey_xp - ey, p.ddx);
-        T dEyz = cdiv(ey_zp - ey, p.ddz);
-        T dEzx = cdiv(ez_xp - ez, p.ddx);
-        T dEzy = cdiv(ez_yp - ez, p.ddy);
-        // CPML (models.jl:811-871)
-        {
-            const LayerDev<T>& l = p.lay[MFD_XL];
-            if (l.nb && ix < l.ib) {
-                const int q = ix;
-                const int k = q + l.nb * (iy + ny * iz);
-                const T B = l.B[q], A = l.A[q];
-                const T pEyx = B * l.psi[2][k] + A * dEyx;
-                const T pEzx = B * l.psi[3][k] + A * dEzx;
-                l.psi[2][k] = pEyx; l.psi[3][k] = pEzx;
-                hy += Mh * pEzx;
-                hz -= Mh * pEyx;
-                dEyx = cdiv(dEyx, l.K[q]);
-                dEzx = cdiv(dEzx, l.K[q]);
+        T dExy = cdiv<FAST>(ex_yp - ex, p.ddy);
+        T dExz = cdiv<FAST>(ex_zp - ex, p.ddz);
+        T dEyx = cdiv<FAST>(ey_xp - ey, p.ddx);
+        T dEyz = cdiv<FAST>(ey_zp - ey, p.ddz);
+        T dEzx = cdiv<FAST>(ez_xp - ez, p.ddx);
+        T dEzy = cdiv<FAST>(ez_yp - ez, p.ddy);
+        if (cxy || in_layers(p.lay[MFD_ZL], p.lay[MFD_ZR], iz)) {
+            const LayerDev<T>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL], &lyr = p.lay[MFD_YR],
+                             &lzl = p.lay[MFD_ZL], &lzr = p.lay[MFD_ZR];
+            if (lxl.nb && ix < lxl.ib) cpml_h<+1, FAST>(lxl, ix, ix + lxl.nb * (iy + ny * iz), Mh, dEyx, dEzx, hy, hz);
+            if (lxr.nb && ix >= lxr.ib - 1) {
+                const int q = ix - (lxr.ib - 1);
+                cpml_h<+1, FAST>(lxr, q, q + lxr.nb * (iy + ny * iz), Mh, dEyx, dEzx, hy, hz);
             }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_XR];
-            if (l.nb && ix >= l.ib - 1) {
-                const int q = ix - (l.ib - 1);
-                const int k = q + l.nb * (iy + ny * iz);
-                const T B = l.B[q], A = l.A[q];
-                const T pEyx = B * l.psi[2][k] + A * dEyx;
-                const T pEzx = B * l.psi[3][k] + A * dEzx;
-                l.psi[2][k] = pEyx; l.psi[3][k] = pEzx;
-                hy += Mh * pEzx;
-                hz -= Mh * pEyx;
-                dEyx = cdiv(dEyx, l.K[q]);
-                dEzx = cdiv(dEzx, l.K[q]);
+            if (lyl.nb && iy < lyl.ib) cpml_h<-1, FAST>(lyl, iy, ix + sy * (iy + lyl.nb * iz), Mh, dExy, dEzy, hx, hz);
+            if (lyr.nb && iy >= lyr.ib - 1) {
+                const int q = iy - (lyr.ib - 1);
+                cpml_h<-1, FAST>(lyr, q, ix + sy * (q + lyr.nb * iz), Mh, dExy, dEzy, hx, hz);
             }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_YL];
-            if (l.nb && iy < l.ib) {
-                const int q = iy;
-                const int k = ix + sy * (q + l.nb * iz);
-                const T B = l.B[q], A = l.A[q];
-                const T pExy = B * l.psi[2][k] + A * dExy;
-                const T pEzy = B * l.psi[3][k] + A * dEzy;
-                l.psi[2][k] = pExy; l.psi[3][k] = pEzy;
-                hx -= Mh * pEzy;
-                hz += Mh * pExy;
-                dExy = cdiv(dExy, l.K[q]);
-                dEzy = cdiv(dEzy, l.K[q]);
-            }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_YR];
-            if (l.nb && iy >= l.ib - 1) {
-                const int q = iy - (l.ib - 1);
-                const int k = ix + sy * (q + l.nb * iz);
-                const T B = l.B[q], A = l.A[q];
-                const T pExy = B * l.psi[2][k] + A * dExy;
-                const T pEzy = B * l.psi[3][k] + A * dEzy;
-                l.psi[2][k] = pExy; l.psi[3][k] = pEzy;
-                hx -= Mh * pEzy;
-                hz += Mh * pExy;
-                dExy = cdiv(dExy, l.K[q]);
-                dEzy = cdiv(dEzy, l.K[q]);
-            }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_ZL];
-            if (l.nb && iz < l.ib) {
-                const int q = iz;
-                const int k = ix + sy * (iy + ny * q);
-                const T B = l.B[q], A = l.A[q];
-                const T pExz = B * l.psi[2][k] + A * dExz;
-                const T pEyz = B * l.psi[3][k] + A * dEyz;
-                l.psi[2][k] = pExz; l.psi[3][k] = pEyz;
-                hx += Mh * pEyz;
-                hy -= Mh * pExz;
-                dExz = cdiv(dExz, l.K[q]);
-                dEyz = cdiv(dEyz, l.K[q]);
-            }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_ZR];
-            if (l.nb && iz >= l.ib - 1) {
-                const int q = iz - (l.ib - 1);
-                const int k = ix + sy * (iy + ny * q);
-                const T B = l.B[q], A = l.A[q];
-                const T pExz = B * l.psi[2][k] + A * dExz;
-                const T pEyz = B * l.psi[3][k] + A * dEyz;
-                l.psi[2][k] = pExz; l.psi[3][k] = pEyz;
-                hx += Mh * pEyz;
-                hy -= Mh * pExz;
-                dExz = cdiv(dExz, l.K[q]);
-                dEyz = cdiv(dEyz, l.K[q]);
+            if (lzl.nb && iz < lzl.ib) cpml_h<+1, FAST>(lzl, iz, ix + sy * (iy + ny * iz), Mh, dExz, dEyz, hx, hy);
+            if (lzr.nb && iz >= lzr.ib - 1) {
+                const int q = iz - (lzr.ib - 1);
+                cpml_h<+1, FAST>(lzr, q, ix + sy * (iy + ny * q), Mh, dExz, dEyz, hx, hy);
             }
         }
         hx -= Mh * (dEzy - dEyz);
@@ -261,8 +226,8 @@ __device__ __forceinline__ ELoad<T> e3d_load(const EParams<T, R>& p, int c, int 
     return v;
 }
 
-template <typename T, typename R, bool MAT>
-__global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EParams<T, R> p, const int zc) {
+template <typename T, typename R, bool MAT, bool FAST>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) e3d_kernel(const __grid_constant__ EParams<T, R> p, const int zc) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -275,6 +240,7 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
     const int ox = !xl ? -1 : (bxl == MFD_BC_PERIODIC ? nx - 1 : 0);
     const int oy = !yl ? -sy : (byl == MFD_BC_PERIODIC ? (ny - 1) * sy : 0);
     const bool zx = xl && bxl == MFD_BC_DIRICHLET, zy = yl && byl == MFD_BC_DIRICHLET;
+    const bool cxy = in_layers(p.lay[MFD_XL], p.lay[MFD_XR], ix) || in_layers(p.lay[MFD_YL], p.lay[MFD_YR], iy);
     int c = ix + sy * iy + sz * z0;
     T hx_zm, hy_zm;
     if (z0 > 0) {
@@ -285,7 +251,6 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
         hx_zm = bzl == MFD_BC_DIRICHLET ? T(0) : p.Hx[c + oz];
         hy_zm = bzl == MFD_BC_DIRICHLET ? T(0) : p.Hy[c + oz];
     }
-    T* const Ep[3] = {p.Ex, p.Ey, p.Ez};
     ELoad<T> cur = e3d_load<T, R, MAT>(p, c, ox, oy);
     for (int iz = z0; iz < z1; ++iz, c += sz) {
         ELoad<T> nxt;
@@ -293,117 +258,265 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
         const T hx = cur.hx, hy = cur.hy, hz = cur.hz;
         const T hy_xm = zx ? T(0) : cur.hyx, hz_xm = zx ? T(0) : cur.hzx;
         const T hx_ym = zy ? T(0) : cur.hxy, hz_ym = zy ? T(0) : cur.hzy;
-        T dHxy = cdiv(hx - hx_ym, p.ddy);
-        T dHxz = cdiv(hx - hx_zm, p.ddz);
-        T dHyx = cdiv(hy - hy_xm, p.ddx);
-        T dHyz = cdiv(hy - hy_zm, p.ddz);
-        T dHzx = cdiv(hz - hz_xm, p.ddx);
-        T dHzy = cdiv(hz - hz_ym, p.ddy);
+        T dHxy = cdiv<FAST>(hx - hx_ym, p.ddy);
+        T dHxz = cdiv<FAST>(hx - hx_zm, p.ddz);
+        T dHyx = cdiv<FAST>(hy - hy_xm, p.ddx);
+        T dHyz = cdiv<FAST>(hy - hy_zm, p.ddz);
+        T dHzx = cdiv<FAST>(hz - hz_xm, p.ddx);
+        T dHzy = cdiv<FAST>(hz - hz_ym, p.ddy);
         const int g = cur.g;
-        T Md1 = p.Md10, Md2 = p.Md20;
-        if (MAT && g) { Md1 = p.mats[g - 1].Md1; Md2 = p.mats[g - 1].Md2; }
-        T Dv[3] = {cur.dx, cur.dy, cur.dz};
-        // CPML (models.jl:975-1035)
-        {
-            const LayerDev<T>& l = p.lay[MFD_XL];
-            if (l.nb && ix < l.ib) {
-                const int q = ix;
-                const int k = q + l.nb * (iy + ny * iz);
-                const T B = l.B[q], A = l.A[q];
-                const T pHyx = B * l.psi[0][k] + A * dHyx;
-                const T pHzx = B * l.psi[1][k] + A * dHzx;
-                l.psi[0][k] = pHyx; l.psi[1][k] = pHzx;
-                Dv[1] -= Md2 * pHzx;
-                Dv[2] += Md2 * pHyx;
-                dHyx = cdiv(dHyx, l.K[q]);
-                dHzx = cdiv(dHzx, l.K[q]);
-            }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_XR];
-            if (l.nb && ix >= l.ib - 1) {
-                const int q = ix - (l.ib - 1);
-                const int k = q + l.nb * (iy + ny * iz);
-                const T B = l.B[q], A = l.A[q];
-                const T pHyx = B * l.psi[0][k] + A * dHyx;
-                const T pHzx = B * l.psi[1][k] + A * dHzx;
-                l.psi[0][k] = pHyx; l.psi[1][k] = pHzx;
-                Dv[1] -= Md2 * pHzx;
-                Dv[2] += Md2 * pHyx;
-                dHyx = cdiv(dHyx, l.K[q]);
-                dHzx = cdiv(dHzx, l.K[q]);
-            }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_YL];
-            if (l.nb && iy < l.ib) {
-                const int q = iy;
-                const int k = ix + sy * (q + l.nb * iz);
-                const T B = l.B[q], A = l.A[q];
-                const T pHxy = B * l.psi[0][k] + A * dHxy;
-                const T pHzy = B * l.psi[1][k] + A * dHzy;
-                l.psi[0][k] = pHxy; l.psi[1][k] = pHzy;
-                Dv[0] += Md2 * pHzy;
-                Dv[2] -= Md2 * pHxy;
-                dHxy = cdiv(dHxy, l.K[q]);
-                dHzy = cdiv(dHzy, l.K[q]);
-            }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_YR];
-            if (l.nb && iy >= l.ib - 1) {
-                const int q = iy - (l.ib - 1);
-                const int k = ix + sy * (q + l.nb * iz);
-                const T B = l.B[q], A = l.A[q];
-                const T pHxy = B * l.psi[0][k] + A * dHxy;
-                const T pHzy = B * l.psi[1][k] + A * dHzy;
-                l.psi[0][k] = pHxy; l.psi[1][k] = pHzy;
-                Dv[0] += Md2 * pHzy;
-                Dv[2] -= Md2 * pHxy;
-                dHxy = cdiv(dHxy, l.K[q]);
-                dHzy = cdiv(dHzy, l.K[q]);
-            }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_ZL];
-            if (l.nb && iz < l.ib) {
-                const int q = iz;
-                const int k = ix + sy * (iy + ny * q);
-                const T B = l.B[q], A = l.A[q];
-                const T pHxz = B * l.psi[0][k] + A * dHxz;
-                const T pHyz = B * l.psi[1][k] + A * dHyz;
-                l.psi[0][k] = pHxz; l.psi[1][k] = pHyz;
-                Dv[0] -= Md2 * pHyz;
-                Dv[1] += Md2 * pHxz;
-                dHxz = cdiv(dHxz, l.K[q]);
-                dHyz = cdiv(dHyz, l.K[q]);
-            }
-        }
-        {
-            const LayerDev<T>& l = p.lay[MFD_ZR];
-            if (l.nb && iz >= l.ib - 1) {
-                const int q = iz - (l.ib - 1);
-                const int k = ix + sy * (iy + ny * q);
-                const T B = l.B[q], A = l.A[q];
-                const T pHxz = B * l.psi[0][k] + A * dHxz;
-                const T pHyz = B * l.psi[1][k] + A * dHyz;
-                l.psi[0][k] = pHxz; l.psi[1][k] = pHyz;
-                Dv[0] -= Md2 * pHyz;
-                Dv[1] += Md2 * pHxz;
-                dHxz = cdiv(dHxz, l.K[q]);
-                dHyz = cdiv(dHyz, l.K[q]);
-            }
-        }
-        Dv[0] = Md1 * Dv[0] + Md2 * (dHzy - dHyz);
-        Dv[1] = Md1 * Dv[1] + Md2 * (dHxz - dHzx);
-        Dv[2] = Md1 * Dv[2] + Md2 * (dHyx - dHxy);
-        p.Dx[c] = Dv[0]; p.Dy[c] = Dv[1]; p.Dz[c] = Dv[2];
+        T Md1 = p.Md10, Md2 = p.Md20, Me = p.Me0;
+        bool simple = true;
         if (MAT && g) {
-            material_cell<T, R, 3>(p.mats + (g - 1), ix, iy, iz, Ep, c, Dv, p.cur, p.dt);
-        } else {
-            p.Ex[c] = Dv[0] * p.Me0;
-            p.Ey[c] = Dv[1] * p.Me0;
-            p.Ez[c] = Dv[2] * p.Me0;
+            const MatDev<T, R>& m = p.mats[g - 1];
+            Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
+        }
+        T D0 = cur.dx, D1 = cur.dy, D2 = cur.dz;
+        if (cxy || in_layers(p.lay[MFD_ZL], p.lay[MFD_ZR], iz)) {
+            const LayerDev<T>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL], &lyr = p.lay[MFD_YR],
+                             &lzl = p.lay[MFD_ZL], &lzr = p.lay[MFD_ZR];
+            if (lxl.nb && ix < lxl.ib) cpml_e<-1, FAST>(lxl, ix, ix + lxl.nb * (iy + ny * iz), Md2, dHyx, dHzx, D1, D2);
+            if (lxr.nb && ix >= lxr.ib - 1) {
+                const int q = ix - (lxr.ib - 1);
+                cpml_e<-1, FAST>(lxr, q, q + lxr.nb * (iy + ny * iz), Md2, dHyx, dHzx, D1, D2);
+            }
+            if (lyl.nb && iy < lyl.ib) cpml_e<+1, FAST>(lyl, iy, ix + sy * (iy + lyl.nb * iz), Md2, dHxy, dHzy, D0, D2);
+            if (lyr.nb && iy >= lyr.ib - 1) {
+                const int q = iy - (lyr.ib - 1);
+                cpml_e<+1, FAST>(lyr, q, ix + sy * (q + lyr.nb * iz), Md2, dHxy, dHzy, D0, D2);
+            }
+            if (lzl.nb && iz < lzl.ib) cpml_e<-1, FAST>(lzl, iz, ix + sy * (iy + ny * iz), Md2, dHxz, dHyz, D0, D1);
+            if (lzr.nb && iz >= lzr.ib - 1) {
+                const int q = iz - (lzr.ib - 1);
+                cpml_e<-1, FAST>(lzr, q, ix + sy * (iy + ny * q), Md2, dHxz, dHyz, D0, D1);
+            }
+        }
+        D0 = Md1 * D0 + Md2 * (dHzy - dHyz);
+        D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
+        D2 = Md1 * D2 + Md2 * (dHyx - dHxy);
+        p.Dx[c] = D0; p.Dy[c] = D1; p.Dz[c] = D2;
+        if (simple) {   // E = (D - 0) Me (models.jl:1136-1153 with no polarisation)
+            p.Ex[c] = D0 * Me;
+            p.Ey[c] = D1 * Me;
+            p.Ez[c] = D2 * Me;
+        }
+        hx_zm = hx;
+        hy_zm = hy;
+        cur = nxt;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// 3-D, single precision: the same updates as h3d_kernel / e3d_kernel with the instruction
+// count cut down -- the six derivative divisions are branch-free (div6), the run-level
+// flags (accumulate sums, E2 kept) are template parameters, loop invariants are hoisted
+// into registers, and the z march is unrolled twice so the prefetched plane is renamed
+// instead of copied.
+// ------------------------------------------------------------------------------------------
+template <bool MATH, bool FAST, bool ACC, bool E2S>
+__global__ void __launch_bounds__(256, 4) h3d_f32_kernel(const __grid_constant__ HParams<float> p, const Div3 D3,
+                                                         const int zc) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
+    if (ix >= nx || iy >= ny) return;
+    const int z0 = blockIdx.z * zc;
+    const int z1 = min(z0 + zc, nz);
+    const int sy = p.L.px, sz = p.L.sz;
+    const int bxr = p.bc[MFD_XR], byr = p.bc[MFD_YR], bzr = p.bc[MFD_ZR];
+    const bool xr = ix == nx - 1, yr = iy == ny - 1;
+    const int ox = !xr ? 1 : (bxr == MFD_BC_PERIODIC ? -(nx - 1) : 0);
+    const int oy = !yr ? sy : (byr == MFD_BC_PERIODIC ? -(ny - 1) * sy : 0);
+    const int ozw = bzr == MFD_BC_PERIODIC ? -(nz - 1) * sz : 0;
+    const int zlast_zero = bzr == MFD_BC_DIRICHLET ? nz - 1 : -1;   // plane whose z+1 neighbour is zero
+    const bool zx = xr && bxr == MFD_BC_DIRICHLET, zy = yr && byr == MFD_BC_DIRICHLET;
+    const bool cxy = in_layers(p.lay[MFD_XL], p.lay[MFD_XR], ix) || in_layers(p.lay[MFD_YL], p.lay[MFD_YR], iy);
+    const int zl = p.lay[MFD_ZL].nb ? p.lay[MFD_ZL].ib : 0;          // iz < zl: left z layer
+    const int zr = p.lay[MFD_ZR].nb ? p.lay[MFD_ZR].ib - 1 : nz;     // iz >= zr: right z layer
+    const float dt = p.dt, Mh0 = p.Mh0;
+    const float* __restrict__ Ex = p.Ex;
+    const float* __restrict__ Ey = p.Ey;
+    const float* __restrict__ Ez = p.Ez;
+    float* Hx = p.Hx;
+    float* Hy = p.Hy;
+    float* Hz = p.Hz;
+    float* Sa = p.Sa;
+    float* E2 = p.E2;
+    int c = ix + sy * iy + sz * z0;
+    float ex = Ex[c], ey = Ey[c];
+    auto load = [&](int cc, int iz) {
+        HLoad<float> v;
+        const int oz = iz < nz - 1 ? sz : ozw;
+        v.ez = Ez[cc];
+        v.eyx = Ey[cc + ox];
+        v.ezx = Ez[cc + ox];
+        v.exy = Ex[cc + oy];
+        v.ezy = Ez[cc + oy];
+        v.exz = Ex[cc + oz];
+        v.eyz = Ey[cc + oz];
+        v.hx = Hx[cc];
+        v.hy = Hy[cc];
+        v.hz = Hz[cc];
+        v.sa = ACC ? Sa[cc] : 0.0f;
+        v.e2 = (ACC && E2S) ? E2[cc] : 0.0f;
+        v.g = MATH ? (int)p.geom[cc] : 0;
+        return v;
+    };
+    HLoad<float> cur = load(c, z0);
+#pragma unroll 2
+    for (int iz = z0; iz < z1; ++iz, c += sz) {
+        HLoad<float> nxt;
+        if (iz + 1 < z1) nxt = load(c + sz, iz + 1);
+        const float ez = cur.ez;
+        const float ey_xp = zx ? 0.0f : cur.eyx, ez_xp = zx ? 0.0f : cur.ezx;
+        const float ex_yp = zy ? 0.0f : cur.exy, ez_yp = zy ? 0.0f : cur.ezy;
+        const bool zz = iz == zlast_zero;
+        const float ex_zp = zz ? 0.0f : cur.exz, ey_zp = zz ? 0.0f : cur.eyz;
+        float hx = cur.hx, hy = cur.hy, hz = cur.hz;
+        if (ACC) {
+            const float a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
+            Sa[c] = cur.sa + sqrt0(a * a + b * b + d * d) * dt;
+            if (E2S) E2[c] = cur.e2 + (ex * ex + ey * ey + ez * ez) * dt;
+            if (!(fabsf(ex) <= FLT_MAX)) guard(p, ex);
+        }
+        float Mh = Mh0;
+        if (MATH && cur.g) Mh = p.matMh[cur.g - 1];
+        const float num[6] = {ex_yp - ex, ex_zp - ex, ey_xp - ey, ey_zp - ey, ez_xp - ez, ez_yp - ez};
+        float q[6];
+        div6<FAST>(D3, num, q);
+        float dExy = q[0], dExz = q[1], dEyx = q[2], dEyz = q[3], dEzx = q[4], dEzy = q[5];
+        if (cxy || iz < zl || iz >= zr) {
+            const LayerDev<float>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL],
+                                  &lyr = p.lay[MFD_YR], &lzl = p.lay[MFD_ZL], &lzr = p.lay[MFD_ZR];
+            if (lxl.nb && ix < lxl.ib) cpml_h<+1, FAST>(lxl, ix, ix + lxl.nb * (iy + ny * iz), Mh, dEyx, dEzx, hy, hz);
+            if (lxr.nb && ix >= lxr.ib - 1) {
+                const int qq = ix - (lxr.ib - 1);
+                cpml_h<+1, FAST>(lxr, qq, qq + lxr.nb * (iy + ny * iz), Mh, dEyx, dEzx, hy, hz);
+            }
+            if (lyl.nb && iy < lyl.ib) cpml_h<-1, FAST>(lyl, iy, ix + sy * (iy + lyl.nb * iz), Mh, dExy, dEzy, hx, hz);
+            if (lyr.nb && iy >= lyr.ib - 1) {
+                const int qq = iy - (lyr.ib - 1);
+                cpml_h<-1, FAST>(lyr, qq, ix + sy * (qq + lyr.nb * iz), Mh, dExy, dEzy, hx, hz);
+            }
+            if (lzl.nb && iz < lzl.ib) cpml_h<+1, FAST>(lzl, iz, ix + sy * (iy + ny * iz), Mh, dExz, dEyz, hx, hy);
+            if (lzr.nb && iz >= lzr.ib - 1) {
+                const int qq = iz - (lzr.ib - 1);
+                cpml_h<+1, FAST>(lzr, qq, ix + sy * (iy + ny * qq), Mh, dExz, dEyz, hx, hy);
+            }
+        }
+        hx -= Mh * (dEzy - dEyz);
+        hy -= Mh * (dExz - dEzx);
+        hz -= Mh * (dEyx - dExy);
+        Hx[c] = hx;
+        Hy[c] = hy;
+        Hz[c] = hz;
+        ex = cur.exz;
+        ey = cur.eyz;
+        cur = nxt;
+    }
+}
+
+template <typename R, bool MAT, bool FAST>
+__global__ void __launch_bounds__(256, 4) e3d_f32_kernel(const __grid_constant__ EParams<float, R> p, const Div3 D3,
+                                                         const int zc) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
+    if (ix >= nx || iy >= ny) return;
+    const int z0 = blockIdx.z * zc;
+    const int z1 = min(z0 + zc, nz);
+    const int sy = p.L.px, sz = p.L.sz;
+    const int bxl = p.bc[MFD_XL], byl = p.bc[MFD_YL], bzl = p.bc[MFD_ZL];
+    const bool xl = ix == 0, yl = iy == 0;
+    const int ox = !xl ? -1 : (bxl == MFD_BC_PERIODIC ? nx - 1 : 0);
+    const int oy = !yl ? -sy : (byl == MFD_BC_PERIODIC ? (ny - 1) * sy : 0);
+    const bool zx = xl && bxl == MFD_BC_DIRICHLET, zy = yl && byl == MFD_BC_DIRICHLET;
+    const bool cxy = in_layers(p.lay[MFD_XL], p.lay[MFD_XR], ix) || in_layers(p.lay[MFD_YL], p.lay[MFD_YR], iy);
+    const int zl = p.lay[MFD_ZL].nb ? p.lay[MFD_ZL].ib : 0;
+    const int zr = p.lay[MFD_ZR].nb ? p.lay[MFD_ZR].ib - 1 : nz;
+    const float Md10 = p.Md10, Md20 = p.Md20, Me0 = p.Me0;
+    const float* __restrict__ Hx = p.Hx;
+    const float* __restrict__ Hy = p.Hy;
+    const float* __restrict__ Hz = p.Hz;
+    float* Dx = p.Dx;
+    float* Dy = p.Dy;
+    float* Dz = p.Dz;
+    float* Ex = p.Ex;
+    float* Ey = p.Ey;
+    float* Ez = p.Ez;
+    int c = ix + sy * iy + sz * z0;
+    float hx_zm, hy_zm;
+    if (z0 > 0) {
+        hx_zm = Hx[c - sz];
+        hy_zm = Hy[c - sz];
+    } else {
+        const int oz = bzl == MFD_BC_PERIODIC ? (nz - 1) * sz : 0;
+        hx_zm = bzl == MFD_BC_DIRICHLET ? 0.0f : Hx[c + oz];
+        hy_zm = bzl == MFD_BC_DIRICHLET ? 0.0f : Hy[c + oz];
+    }
+    auto load = [&](int cc) {
+        ELoad<float> v;
+        v.hx = Hx[cc];
+        v.hy = Hy[cc];
+        v.hz = Hz[cc];
+        v.hyx = Hy[cc + ox];
+        v.hzx = Hz[cc + ox];
+        v.hxy = Hx[cc + oy];
+        v.hzy = Hz[cc + oy];
+        v.dx = Dx[cc];
+        v.dy = Dy[cc];
+        v.dz = Dz[cc];
+        v.g = MAT ? (int)p.geom[cc] : 0;
+        return v;
+    };
+    ELoad<float> cur = load(c);
+#pragma unroll 2
+    for (int iz = z0; iz < z1; ++iz, c += sz) {
+        ELoad<float> nxt;
+        if (iz + 1 < z1) nxt = load(c + sz);
+        const float hx = cur.hx, hy = cur.hy, hz = cur.hz;
+        const float hy_xm = zx ? 0.0f : cur.hyx, hz_xm = zx ? 0.0f : cur.hzx;
+        const float hx_ym = zy ? 0.0f : cur.hxy, hz_ym = zy ? 0.0f : cur.hzy;
+        const float num[6] = {hx - hx_ym, hx - hx_zm, hy - hy_xm, hy - hy_zm, hz - hz_xm, hz - hz_ym};
+        float q[6];
+        div6<FAST>(D3, num, q);
+        float dHxy = q[0], dHxz = q[1], dHyx = q[2], dHyz = q[3], dHzx = q[4], dHzy = q[5];
+        float Md1 = Md10, Md2 = Md20, Me = Me0;
+        bool simple = true;
+        if (MAT && cur.g) {
+            const MatDev<float, R>& m = p.mats[cur.g - 1];
+            Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
+        }
+        float D0 = cur.dx, D1 = cur.dy, D2 = cur.dz;
+        if (cxy || iz < zl || iz >= zr) {
+            const LayerDev<float>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL],
+                                  &lyr = p.lay[MFD_YR], &lzl = p.lay[MFD_ZL], &lzr = p.lay[MFD_ZR];
+            if (lxl.nb && ix < lxl.ib) cpml_e<-1, FAST>(lxl, ix, ix + lxl.nb * (iy + ny * iz), Md2, dHyx, dHzx, D1, D2);
+            if (lxr.nb && ix >= lxr.ib - 1) {
+                const int qq = ix - (lxr.ib - 1);
+                cpml_e<-1, FAST>(lxr, qq, qq + lxr.nb * (iy + ny * iz), Md2, dHyx, dHzx, D1, D2);
+            }
+            if (lyl.nb && iy < lyl.ib) cpml_e<+1, FAST>(lyl, iy, ix + sy * (iy + lyl.nb * iz), Md2, dHxy, dHzy, D0, D2);
+            if (lyr.nb && iy >= lyr.ib - 1) {
+                const int qq = iy - (lyr.ib - 1);
+                cpml_e<+1, FAST>(lyr, qq, ix + sy * (qq + lyr.nb * iz), Md2, dHxy, dHzy, D0, D2);
+            }
+            if (lzl.nb && iz < lzl.ib) cpml_e<-1, FAST>(lzl, iz, ix + sy * (iy + ny * iz), Md2, dHxz, dHyz, D0, D1);
+            if (lzr.nb && iz >= lzr.ib - 1) {
+                const int qq = iz - (lzr.ib - 1);
+                cpml_e<-1, FAST>(lzr, qq, ix + sy * (iy + ny * qq), Md2, dHxz, dHyz, D0, D1);
+            }
+        }
+        D0 = Md1 * D0 + Md2 * (dHzy - dHyz);
+        D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
+        D2 = Md1 * D2 + Md2 * (dHyx - dHxy);
+        Dx[c] = D0;
+        Dy[c] = D1;
+        Dz[c] = D2;
+        if (simple) {
+            Ex[c] = D0 * Me;
+            Ey[c] = D1 * Me;
+            Ez[c] = D2 * Me;
         }
         hx_zm = hx;
         hy_zm = hy;
@@ -414,7 +527,7 @@ __global__ void __launch_bounds__(256, 4) e3d_kernel(const __grid_constant__ EPa
 // ------------------------------------------------------------------------------------------
 // 2-D (x-z plane): one thread per cell
 // ------------------------------------------------------------------------------------------
-template <typename T, bool MATH>
+template <typename T, bool MATH, bool FAST>
 __global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParams<T> p) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iz = blockIdx.y * blockDim.y + threadIdx.y;
@@ -437,57 +550,53 @@ __global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParam
     }
     T Mh = p.Mh0;
     if (MATH) { const int g = p.geom[c]; if (g) Mh = p.matMh[g - 1]; }
-    T dExz = cdiv(ex_zp - ex, p.ddz);
-    T dEzx = cdiv(ez_xp - ez, p.ddx);
+    T dExz = cdiv<FAST>(ex_zp - ex, p.ddz);
+    T dEzx = cdiv<FAST>(ez_xp - ez, p.ddx);
     {
         const LayerDev<T>& l = p.lay[MFD_XL];
         if (l.nb && ix < l.ib) {
-            const int q = ix;
-            const int k = q + l.nb * iz;
+            const int q = ix, k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEzx;
             l.psi[1][k] = ps;
             hy += Mh * ps;
-            dEzx = cdiv(dEzx, l.K[q]);
+            dEzx = cdiv<FAST>(dEzx, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_XR];
         if (l.nb && ix >= l.ib - 1) {
-            const int q = ix - (l.ib - 1);
-            const int k = q + l.nb * iz;
+            const int q = ix - (l.ib - 1), k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEzx;
             l.psi[1][k] = ps;
             hy += Mh * ps;
-            dEzx = cdiv(dEzx, l.K[q]);
+            dEzx = cdiv<FAST>(dEzx, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_ZL];
         if (l.nb && iz < l.ib) {
-            const int q = iz;
-            const int k = ix + p.L.px * q;
+            const int q = iz, k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dExz;
             l.psi[1][k] = ps;
             hy -= Mh * ps;
-            dExz = cdiv(dExz, l.K[q]);
+            dExz = cdiv<FAST>(dExz, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_ZR];
         if (l.nb && iz >= l.ib - 1) {
-            const int q = iz - (l.ib - 1);
-            const int k = ix + p.L.px * q;
+            const int q = iz - (l.ib - 1), k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dExz;
             l.psi[1][k] = ps;
             hy -= Mh * ps;
-            dExz = cdiv(dExz, l.K[q]);
+            dExz = cdiv<FAST>(dExz, l.K[q]);
         }
     }
     hy -= Mh * (dExz - dEzx);
     p.Hy[c] = hy;
 }
 
-template <typename T, typename R, bool MAT>
+template <typename T, typename R, bool MAT, bool FAST>
 __global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParams<T, R> p) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iz = blockIdx.y * blockDim.y + threadIdx.y;
@@ -501,75 +610,72 @@ __global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParam
     else { const int b = p.bc[MFD_XL]; hy_xm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + (nx - 1)] : T(0), hy); }
     if (iz > 0) hy_zm = p.Hy[c - sz];
     else { const int b = p.bc[MFD_ZL]; hy_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[c + (nz - 1) * sz] : T(0), hy); }
-    T dHyx = cdiv(hy - hy_xm, p.ddx);
-    T dHyz = cdiv(hy - hy_zm, p.ddz);
-    int g = 0;
-    T Md1 = p.Md10, Md2 = p.Md20;
+    T dHyx = cdiv<FAST>(hy - hy_xm, p.ddx);
+    T dHyz = cdiv<FAST>(hy - hy_zm, p.ddz);
+    T Md1 = p.Md10, Md2 = p.Md20, Me = p.Me0;
+    bool simple = true;
     if (MAT) {
-        g = p.geom[c];
-        if (g) { Md1 = p.mats[g - 1].Md1; Md2 = p.mats[g - 1].Md2; }
+        const int g = p.geom[c];
+        if (g) {
+            const MatDev<T, R>& m = p.mats[g - 1];
+            Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
+        }
     }
-    T Dv[2] = {p.Dx[c], p.Dz[c]};
+    T D0 = p.Dx[c], D2 = p.Dz[c];
     {
         const LayerDev<T>& l = p.lay[MFD_XL];
         if (l.nb && ix < l.ib) {
-            const int q = ix;
-            const int k = q + l.nb * iz;
+            const int q = ix, k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyx;
             l.psi[0][k] = ps;
-            Dv[1] += Md2 * ps;
-            dHyx = cdiv(dHyx, l.K[q]);
+            D2 += Md2 * ps;
+            dHyx = cdiv<FAST>(dHyx, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_XR];
         if (l.nb && ix >= l.ib - 1) {
-            const int q = ix - (l.ib - 1);
-            const int k = q + l.nb * iz;
+            const int q = ix - (l.ib - 1), k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyx;
             l.psi[0][k] = ps;
-            Dv[1] += Md2 * ps;
-            dHyx = cdiv(dHyx, l.K[q]);
+            D2 += Md2 * ps;
+            dHyx = cdiv<FAST>(dHyx, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_ZL];
         if (l.nb && iz < l.ib) {
-            const int q = iz;
-            const int k = ix + p.L.px * q;
+            const int q = iz, k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyz;
             l.psi[0][k] = ps;
-            Dv[0] -= Md2 * ps;
-            dHyz = cdiv(dHyz, l.K[q]);
+            D0 -= Md2 * ps;
+            dHyz = cdiv<FAST>(dHyz, l.K[q]);
         }
     }
     {
         const LayerDev<T>& l = p.lay[MFD_ZR];
         if (l.nb && iz >= l.ib - 1) {
-            const int q = iz - (l.ib - 1);
-            const int k = ix + p.L.px * q;
+            const int q = iz - (l.ib - 1), k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyz;
             l.psi[0][k] = ps;
-            Dv[0] -= Md2 * ps;
-            dHyz = cdiv(dHyz, l.K[q]);
+            D0 -= Md2 * ps;
+            dHyz = cdiv<FAST>(dHyz, l.K[q]);
         }
     }
-    Dv[0] = Md1 * Dv[0] + Md2 * (T(0) - dHyz);
-    Dv[1] = Md1 * Dv[1] + Md2 * (dHyx - T(0));
-    p.Dx[c] = Dv[0]; p.Dz[c] = Dv[1];
-    if (MAT && g) {
-        T* const Ep[2] = {p.Ex, p.Ez};
-        material_cell<T, R, 2>(p.mats + (g - 1), ix, 0, iz, Ep, c, Dv, p.cur, p.dt);
-    } else {
-        p.Ex[c] = Dv[0] * p.Me0;
-        p.Ez[c] = Dv[1] * p.Me0;
+    D0 = Md1 * D0 + Md2 * (T(0) - dHyz);
+    D2 = Md1 * D2 + Md2 * (dHyx - T(0));
+    p.Dx[c] = D0;
+    p.Dz[c] = D2;
+    if (simple) {
+        p.Ex[c] = D0 * Me;
+        p.Ez[c] = D2 * Me;
     }
 }
 
 // ------------------------------------------------------------------------------------------
 // 1-D (z)
 // ------------------------------------------------------------------------------------------
-template <typename T, bool MATH>
+template <typename T, bool MATH, bool FAST>
 __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParams<T> p) {
     const int iz = blockIdx.x * blockDim.x + threadIdx.x;
     const int nz = p.L.nz;
@@ -588,7 +694,7 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
     }
     T Mh = p.Mh0;
     if (MATH) { const int g = p.geom[c]; if (g) Mh = p.matMh[g - 1]; }
-    T dExz = cdiv(ex_zp - ex, p.ddz);
+    T dExz = cdiv<FAST>(ex_zp - ex, p.ddz);
     {
         const LayerDev<T>& l = p.lay[MFD_ZL];
         if (l.nb && iz < l.ib) {
@@ -596,7 +702,7 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
             const T ps = l.B[q] * l.psi[1][q] + l.A[q] * dExz;
             l.psi[1][q] = ps;
             hy -= Mh * ps;
-            dExz = cdiv(dExz, l.K[q]);
+            dExz = cdiv<FAST>(dExz, l.K[q]);
         }
     }
     {
@@ -606,14 +712,14 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
             const T ps = l.B[q] * l.psi[1][q] + l.A[q] * dExz;
             l.psi[1][q] = ps;
             hy -= Mh * ps;
-            dExz = cdiv(dExz, l.K[q]);
+            dExz = cdiv<FAST>(dExz, l.K[q]);
         }
     }
     hy -= Mh * (T(0) + dExz);
     p.Hy[c] = hy;
 }
 
-template <typename T, typename R, bool MAT>
+template <typename T, typename R, bool MAT, bool FAST>
 __global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParams<T, R> p) {
     const int iz = blockIdx.x * blockDim.x + threadIdx.x;
     const int nz = p.L.nz;
@@ -623,22 +729,25 @@ __global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParam
     T hy_zm;
     if (iz > 0) hy_zm = p.Hy[c - 1];
     else { const int b = p.bc[MFD_ZL]; hy_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hy[nz - 1] : T(0), hy); }
-    T dHyz = cdiv(hy - hy_zm, p.ddz);
-    int g = 0;
-    T Md1 = p.Md10, Md2 = p.Md20;
+    T dHyz = cdiv<FAST>(hy - hy_zm, p.ddz);
+    T Md1 = p.Md10, Md2 = p.Md20, Me = p.Me0;
+    bool simple = true;
     if (MAT) {
-        g = p.geom[c];
-        if (g) { Md1 = p.mats[g - 1].Md1; Md2 = p.mats[g - 1].Md2; }
+        const int g = p.geom[c];
+        if (g) {
+            const MatDev<T, R>& m = p.mats[g - 1];
+            Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
+        }
     }
-    T Dv[1] = {p.Dx[c]};
+    T D0 = p.Dx[c];
     {
         const LayerDev<T>& l = p.lay[MFD_ZL];
         if (l.nb && iz < l.ib) {
             const int q = iz;
             const T ps = l.B[q] * l.psi[0][q] + l.A[q] * dHyz;
             l.psi[0][q] = ps;
-            Dv[0] -= Md2 * ps;
-            dHyz = cdiv(dHyz, l.K[q]);
+            D0 -= Md2 * ps;
+            dHyz = cdiv<FAST>(dHyz, l.K[q]);
         }
     }
     {
@@ -647,18 +756,43 @@ __global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParam
             const int q = iz - (l.ib - 1);
             const T ps = l.B[q] * l.psi[0][q] + l.A[q] * dHyz;
             l.psi[0][q] = ps;
-            Dv[0] -= Md2 * ps;
-            dHyz = cdiv(dHyz, l.K[q]);
+            D0 -= Md2 * ps;
+            dHyz = cdiv<FAST>(dHyz, l.K[q]);
         }
     }
-    Dv[0] = Md1 * Dv[0] + Md2 * (T(0) - dHyz);
-    p.Dx[c] = Dv[0];
-    if (MAT && g) {
-        T* const Ep[1] = {p.Ex};
-        material_cell<T, R, 1>(p.mats + (g - 1), 0, 0, iz, Ep, c, Dv, p.cur, p.dt);
+    D0 = Md1 * D0 + Md2 * (T(0) - dHyz);
+    p.Dx[c] = D0;
+    if (simple) p.Ex[c] = D0 * Me;
+}
+
+// ------------------------------------------------------------------------------------------
+// Material response (ADE poles, plasma, Kerr; models.jl:1042-1154, 622-712, 365-431) for the
+// cells of material g inside its bounding box: reads the new D and the old E of the cell.
+// ------------------------------------------------------------------------------------------
+template <typename T, typename R, int NC>
+__global__ void __launch_bounds__(128) material_kernel(const MatDev<T, R>* __restrict__ mats, int g,
+                                                      const uint8_t* __restrict__ geom, Layout L,
+                                                      const T* D0, const T* D1, const T* D2, T* E0, T* E1, T* E2,
+                                                      int cur, T dt) {
+    const MatDev<T, R>* m = mats + (g - 1);
+    const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bx >= m->bnx) return;
+    const int ix = m->bx0 + bx, iy = m->by0 + (int)blockIdx.y, iz = m->bz0 + (int)blockIdx.z;
+    const int c = ix + L.px * iy + L.sz * iz;
+    if (geom[c] != g) return;
+    T Dv[NC];
+    T* Ep[NC];
+    if (NC == 3) {
+        Dv[0] = D0[c]; Dv[1 % NC] = D1[c]; Dv[2 % NC] = D2[c];
+        Ep[0] = E0; Ep[1 % NC] = E1; Ep[2 % NC] = E2;
+    } else if (NC == 2) {   // x and z
+        Dv[0] = D0[c]; Dv[1 % NC] = D2[c];
+        Ep[0] = E0; Ep[1 % NC] = E2;
     } else {
-        p.Ex[c] = Dv[0] * p.Me0;
+        Dv[0] = D0[c];
+        Ep[0] = E0;
     }
+    material_cell<T, R, NC>(m, ix, iy, iz, Ep, c, Dv, cur, dt);
 }
 
 // Running sums and NaN/Inf guard for the last step of a run (the H kernel of the next step
