@@ -27,6 +27,7 @@
 #include "aux.cuh"
 #include "yee.cuh"
 #include "yee3d_tma.cuh"
+#include "yee3d_split.cuh"
 
 namespace mfd {
 
@@ -266,6 +267,11 @@ class Engine : public HandleBase {
 
     // launch shapes
     int bx3 = 32, by3 = 8, zc3 = 16;
+    // single-precision 3-D updates split into core rows and CPML slabs (yee3d_split.cuh)
+    bool use_split = false;
+    SplitBox sbox{};
+    long long slab_rows = 0;
+    int kcount = 1;             // kernels issued by the current launch() call
     // TMA-fed 3-D kernels (single precision)
     bool use_tma = false;
     int tma_zc = 16;
@@ -516,6 +522,7 @@ class Engine : public HandleBase {
                 bx3 = a; by3 = b; zc3 = c;
             }
         }
+        init_split();
         d_timeout = dalloc<int>(1);
         MFD_CK(cudaHostAlloc(&h_timeout, sizeof(int), cudaHostAllocDefault));
         init_tma();
@@ -534,6 +541,21 @@ class Engine : public HandleBase {
         return fn(m, u8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims,
                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+
+    // The split needs layers that do not overlap in any dimension; MFD_KERNEL3D=unsplit
+    // keeps the single-kernel updates (for comparison).
+    void init_split() {
+        if (ndim != 3 || sizeof(T) != 4) return;
+        if (const char* k = std::getenv("MFD_KERNEL3D"))
+            if (!std::strcmp(k, "unsplit")) return;
+        const int xl = lay[MFD_XL].nb ? lay[MFD_XL].ib : 0, xr = lay[MFD_XR].nb ? lay[MFD_XR].ib - 1 : nx;
+        const int yl = lay[MFD_YL].nb ? lay[MFD_YL].ib : 0, yr = lay[MFD_YR].nb ? lay[MFD_YR].ib - 1 : ny;
+        const int zl = lay[MFD_ZL].nb ? lay[MFD_ZL].ib : 0, zr = lay[MFD_ZR].nb ? lay[MFD_ZR].ib - 1 : nz;
+        if (xl > xr || yl > yr || zl > zr) return;
+        sbox = SplitBox{yl, yr, zl, zr, zc3, (zl + nz - zr) * ny};
+        slab_rows = (long long)sbox.nzr + (long long)(zr - zl) * (yl + ny - yr);
+        use_split = true;
     }
 
     void init_tma() {
@@ -823,6 +845,7 @@ class Engine : public HandleBase {
 
     template <typename F_>
     void launch(int cls, F_&& f) {
+        kcount = 1;
         if (profiling) {
             cudaEvent_t a = get_event(), b = get_event();
             MFD_CK(cudaEventRecord(a, st));
@@ -833,7 +856,7 @@ class Engine : public HandleBase {
             f();
         }
         MFD_CK(cudaGetLastError());
-        k_n[cls]++;
+        k_n[cls] += kcount;
     }
 
     void collect_times() {
@@ -907,6 +930,20 @@ class Engine : public HandleBase {
 
     template <bool MATH, bool FAST, bool ACC, bool E2S>
     void launch_H_f32(const HParams<float>& p) {
+        if (use_split) {
+            kcount = 0;
+            if (sbox.yr > sbox.yl && sbox.zr > sbox.zl) {
+                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (sbox.zr - sbox.zl + zc3 - 1) / zc3);
+                h3d_core_kernel<MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, sbox);
+                kcount++;
+            }
+            if (slab_rows) {
+                dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
+                h3d_slab_kernel<MATH, FAST, ACC, E2S><<<grd, 128, 0, st>>>(p, d3, sbox);
+                kcount++;
+            }
+            return;
+        }
         dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
         h3d_f32_kernel<MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, zc3);
     }
@@ -920,6 +957,20 @@ class Engine : public HandleBase {
 
     template <bool MAT, bool FAST>
     void launch_E_f32(const EParams<float, R>& p) {
+        if (use_split) {
+            kcount = 0;
+            if (sbox.yr > sbox.yl && sbox.zr > sbox.zl) {
+                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (sbox.zr - sbox.zl + zc3 - 1) / zc3);
+                e3d_core_kernel<R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sbox);
+                kcount++;
+            }
+            if (slab_rows) {
+                dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
+                e3d_slab_kernel<R, MAT, FAST><<<grd, 128, 0, st>>>(p, d3, sbox);
+                kcount++;
+            }
+            return;
+        }
         dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
         e3d_f32_kernel<R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, zc3);
     }

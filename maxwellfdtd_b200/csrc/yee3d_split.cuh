@@ -1,0 +1,408 @@
+// yee3d_split.cuh -- single-precision 3-D updates split by CPML region (sm_100a).
+//
+// A 3-D grid with CPML layers on the y and z faces is cut into
+//   core  : rows outside the y and z layers (all x), marched along z by h3d_core_kernel /
+//           e3d_core_kernel.  The only layers a core cell can be in are the x layers, and
+//           for a given column that membership, the layer's coefficients and its psi stride
+//           are fixed, so they are loaded once and the psi pair of the next plane is
+//           prefetched with the fields: a layer cell costs its psi traffic and a few flops;
+//   slab  : every cell of the y and z layers (h3d_slab_kernel / e3d_slab_kernel), one cell
+//           per thread with all of its loads issued together, general CPML (any faces).
+// The per-cell arithmetic is that of h3d_f32_kernel / e3d_f32_kernel (yee.cuh), operation
+// for operation and with the faces in the same order, so results are bit-identical.  The
+// split needs layers that do not overlap in any dimension (checked on the host, which
+// otherwise launches the unsplit kernels).
+#pragma once
+
+#include "yee.cuh"
+
+namespace mfd {
+
+// Rows of the core box and the slab region.  Cells with iz < zl or iz >= zr are in a z layer,
+// iy < yl or iy >= yr in a y layer (zl <= zr, yl <= yr).  Slab rows are numbered z-layer
+// rows first (plane-major: nzr = (zl + nz - zr) * ny of them), then y-layer rows of the
+// core planes (zr - zl planes of yl + ny - yr rows).
+struct SplitBox {
+    int yl, yr, zl, zr;
+    int zc;     // planes per core block
+    int nzr;    // slab rows in z layers
+};
+
+__device__ __forceinline__ void slab_row(const SplitBox& s, int ny, int r, int& iy, int& iz) {
+    if (r < s.nzr) {
+        const int pz = r / ny;
+        iy = r - pz * ny;
+        iz = pz < s.zl ? pz : s.zr + (pz - s.zl);
+    } else {
+        const int nys = s.yl + (ny - s.yr);
+        const int r2 = r - s.nzr;
+        const int zz = r2 / nys, yy = r2 - zz * nys;
+        iz = s.zl + zz;
+        iy = yy < s.yl ? yy : s.yr + (yy - s.yl);
+    }
+}
+
+// x-layer state of one column: which face (none / left / right), its coefficients and psi.
+struct XCol {
+    bool in;
+    int q, nb;
+    float A, B;
+    DivC<float> K;
+    float* pa;
+    float* pb;
+};
+
+__device__ __forceinline__ XCol xcol(const LayerDev<float>& lxl, const LayerDev<float>& lxr, int ix, int ia, int ib) {
+    XCol x;
+    const bool l = lxl.nb && ix < lxl.ib;
+    const bool r = lxr.nb && ix >= lxr.ib - 1;
+    x.in = l || r;
+    x.q = l ? ix : ix - (lxr.ib - 1);
+    x.nb = l ? lxl.nb : lxr.nb;
+    x.pa = l ? lxl.psi[ia] : lxr.psi[ia];
+    x.pb = l ? lxl.psi[ib] : lxr.psi[ib];
+    if (x.in) {
+        const LayerDev<float>& lx = l ? lxl : lxr;
+        x.A = lx.A[x.q];
+        x.B = lx.B[x.q];
+        x.K = lx.K[x.q];
+    } else {
+        x.A = x.B = 0.0f;
+        x.K = DivC<float>{};
+    }
+    return x;
+}
+
+struct HCoreLoad {
+    float ez, eyx, ezx, exy, ezy, exz, eyz, hx, hy, hz, sa, e2, pa, pb;
+    int g;
+};
+
+template <bool MATH, bool FAST, bool ACC, bool E2S>
+__global__ void __launch_bounds__(256, 4) h3d_core_kernel(const __grid_constant__ HParams<float> p, const Div3 D3,
+                                                          const SplitBox s) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = s.yl + blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
+    if (ix >= nx || iy >= s.yr) return;
+    const int z0 = s.zl + blockIdx.z * s.zc;
+    const int z1 = min(z0 + s.zc, s.zr);
+    const int sy = p.L.px, sz = p.L.sz;
+    const int bxr = p.bc[MFD_XR], byr = p.bc[MFD_YR], bzr = p.bc[MFD_ZR];
+    const bool xr = ix == nx - 1, yr = iy == ny - 1;
+    const int ox = !xr ? 1 : (bxr == MFD_BC_PERIODIC ? -(nx - 1) : 0);
+    const int oy = !yr ? sy : (byr == MFD_BC_PERIODIC ? -(ny - 1) * sy : 0);
+    const int ozw = bzr == MFD_BC_PERIODIC ? -(nz - 1) * sz : 0;
+    const int zlast_zero = bzr == MFD_BC_DIRICHLET ? nz - 1 : -1;
+    const bool zx = xr && bxr == MFD_BC_DIRICHLET, zy = yr && byr == MFD_BC_DIRICHLET;
+    const XCol X = xcol(p.lay[MFD_XL], p.lay[MFD_XR], ix, 2, 3);   // H uses psi pair (2, 3)
+    const int kstep = X.nb * ny;
+    int k = X.q + X.nb * (iy + ny * z0);
+    const float dt = p.dt, Mh0 = p.Mh0;
+    const float* __restrict__ Ex = p.Ex;
+    const float* __restrict__ Ey = p.Ey;
+    const float* __restrict__ Ez = p.Ez;
+    float* Hx = p.Hx;
+    float* Hy = p.Hy;
+    float* Hz = p.Hz;
+    float* Sa = p.Sa;
+    float* E2 = p.E2;
+    int c = ix + sy * iy + sz * z0;
+    float ex = Ex[c], ey = Ey[c];
+    auto load = [&](int cc, int iz, int kk) {
+        HCoreLoad v;
+        const int oz = iz < nz - 1 ? sz : ozw;
+        v.ez = Ez[cc];
+        v.eyx = Ey[cc + ox];
+        v.ezx = Ez[cc + ox];
+        v.exy = Ex[cc + oy];
+        v.ezy = Ez[cc + oy];
+        v.exz = Ex[cc + oz];
+        v.eyz = Ey[cc + oz];
+        v.hx = Hx[cc];
+        v.hy = Hy[cc];
+        v.hz = Hz[cc];
+        v.sa = ACC ? Sa[cc] : 0.0f;
+        v.e2 = (ACC && E2S) ? E2[cc] : 0.0f;
+        v.g = MATH ? (int)p.geom[cc] : 0;
+        v.pa = X.in ? X.pa[kk] : 0.0f;
+        v.pb = X.in ? X.pb[kk] : 0.0f;
+        return v;
+    };
+    HCoreLoad cur = load(c, z0, k);
+    for (int iz = z0; iz < z1; ++iz, c += sz, k += kstep) {
+        HCoreLoad nxt;
+        if (iz + 1 < z1) nxt = load(c + sz, iz + 1, k + kstep);
+        const float ez = cur.ez;
+        const float ey_xp = zx ? 0.0f : cur.eyx, ez_xp = zx ? 0.0f : cur.ezx;
+        const float ex_yp = zy ? 0.0f : cur.exy, ez_yp = zy ? 0.0f : cur.ezy;
+        const bool zz = iz == zlast_zero;
+        const float ex_zp = zz ? 0.0f : cur.exz, ey_zp = zz ? 0.0f : cur.eyz;
+        float hx = cur.hx, hy = cur.hy, hz = cur.hz;
+        if (ACC) {
+            const float a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
+            Sa[c] = cur.sa + sqrt0(a * a + b * b + d * d) * dt;
+            if (E2S) E2[c] = cur.e2 + (ex * ex + ey * ey + ez * ez) * dt;
+            if (!(fabsf(ex) <= FLT_MAX)) guard(p, ex);
+        }
+        float Mh = Mh0;
+        if (MATH && cur.g) Mh = p.matMh[cur.g - 1];
+        const float num[6] = {ex_yp - ex, ex_zp - ex, ey_xp - ey, ey_zp - ey, ez_xp - ez, ez_yp - ez};
+        float q[6];
+        div6<FAST>(D3, num, q);
+        const float dExy = q[0], dExz = q[1], dEyz = q[3], dEzy = q[5];
+        float dEyx = q[2], dEzx = q[4];
+        if (X.in) {   // cpml_h<+1> of the column's x face
+            const float pa = X.B * cur.pa + X.A * dEyx;
+            const float pb = X.B * cur.pb + X.A * dEzx;
+            X.pa[k] = pa;
+            X.pb[k] = pb;
+            hy += Mh * pb;
+            hz -= Mh * pa;
+            dEyx = cdiv<FAST>(dEyx, X.K);
+            dEzx = cdiv<FAST>(dEzx, X.K);
+        }
+        hx -= Mh * (dEzy - dEyz);
+        hy -= Mh * (dExz - dEzx);
+        hz -= Mh * (dEyx - dExy);
+        Hx[c] = hx;
+        Hy[c] = hy;
+        Hz[c] = hz;
+        ex = cur.exz;
+        ey = cur.eyz;
+        cur = nxt;
+    }
+}
+
+template <bool MATH, bool FAST, bool ACC, bool E2S>
+__global__ void __launch_bounds__(128) h3d_slab_kernel(const __grid_constant__ HParams<float> p, const Div3 D3,
+                                                       const SplitBox s) {
+    const int ix = blockIdx.y * blockDim.x + threadIdx.x;
+    const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
+    if (ix >= nx) return;
+    int iy, iz;
+    slab_row(s, ny, (int)blockIdx.x, iy, iz);
+    const int sy = p.L.px, sz = p.L.sz;
+    const int bxr = p.bc[MFD_XR], byr = p.bc[MFD_YR], bzr = p.bc[MFD_ZR];
+    const bool xr = ix == nx - 1, yr = iy == ny - 1, zr = iz == nz - 1;
+    const int ox = !xr ? 1 : (bxr == MFD_BC_PERIODIC ? -(nx - 1) : 0);
+    const int oy = !yr ? sy : (byr == MFD_BC_PERIODIC ? -(ny - 1) * sy : 0);
+    const int oz = !zr ? sz : (bzr == MFD_BC_PERIODIC ? -(nz - 1) * sz : 0);
+    const bool zx = xr && bxr == MFD_BC_DIRICHLET, zy = yr && byr == MFD_BC_DIRICHLET, zz = zr && bzr == MFD_BC_DIRICHLET;
+    const int c = ix + sy * iy + sz * iz;
+    const float ex = p.Ex[c], ey = p.Ey[c], ez = p.Ez[c];
+    const float ey_xp = zx ? 0.0f : p.Ey[c + ox], ez_xp = zx ? 0.0f : p.Ez[c + ox];
+    const float ex_yp = zy ? 0.0f : p.Ex[c + oy], ez_yp = zy ? 0.0f : p.Ez[c + oy];
+    const float ex_zp = zz ? 0.0f : p.Ex[c + oz], ey_zp = zz ? 0.0f : p.Ey[c + oz];
+    float hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
+    if (ACC) {
+        const float a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
+        p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b + d * d) * p.dt;
+        if (E2S) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
+        if (!(fabsf(ex) <= FLT_MAX)) guard(p, ex);
+    }
+    float Mh = p.Mh0;
+    if (MATH) {
+        const int g = p.geom[c];
+        if (g) Mh = p.matMh[g - 1];
+    }
+    const float num[6] = {ex_yp - ex, ex_zp - ex, ey_xp - ey, ey_zp - ey, ez_xp - ez, ez_yp - ez};
+    float q[6];
+    div6<FAST>(D3, num, q);
+    float dExy = q[0], dExz = q[1], dEyx = q[2], dEyz = q[3], dEzx = q[4], dEzy = q[5];
+    const LayerDev<float>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL], &lyr = p.lay[MFD_YR],
+                          &lzl = p.lay[MFD_ZL], &lzr = p.lay[MFD_ZR];
+    if (lxl.nb && ix < lxl.ib) cpml_h<+1, FAST>(lxl, ix, ix + lxl.nb * (iy + ny * iz), Mh, dEyx, dEzx, hy, hz);
+    if (lxr.nb && ix >= lxr.ib - 1) {
+        const int qq = ix - (lxr.ib - 1);
+        cpml_h<+1, FAST>(lxr, qq, qq + lxr.nb * (iy + ny * iz), Mh, dEyx, dEzx, hy, hz);
+    }
+    if (lyl.nb && iy < lyl.ib) cpml_h<-1, FAST>(lyl, iy, ix + sy * (iy + lyl.nb * iz), Mh, dExy, dEzy, hx, hz);
+    if (lyr.nb && iy >= lyr.ib - 1) {
+        const int qq = iy - (lyr.ib - 1);
+        cpml_h<-1, FAST>(lyr, qq, ix + sy * (qq + lyr.nb * iz), Mh, dExy, dEzy, hx, hz);
+    }
+    if (lzl.nb && iz < lzl.ib) cpml_h<+1, FAST>(lzl, iz, ix + sy * (iy + ny * iz), Mh, dExz, dEyz, hx, hy);
+    if (lzr.nb && iz >= lzr.ib - 1) {
+        const int qq = iz - (lzr.ib - 1);
+        cpml_h<+1, FAST>(lzr, qq, ix + sy * (iy + ny * qq), Mh, dExz, dEyz, hx, hy);
+    }
+    hx -= Mh * (dEzy - dEyz);
+    hy -= Mh * (dExz - dEzx);
+    hz -= Mh * (dEyx - dExy);
+    p.Hx[c] = hx;
+    p.Hy[c] = hy;
+    p.Hz[c] = hz;
+}
+
+struct ECoreLoad {
+    float hx, hy, hz, hyx, hzx, hxy, hzy, dx, dy, dz, pa, pb;
+    int g;
+};
+
+template <typename R, bool MAT, bool FAST>
+__global__ void __launch_bounds__(256, 4) e3d_core_kernel(const __grid_constant__ EParams<float, R> p, const Div3 D3,
+                                                          const SplitBox s) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = s.yl + blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
+    if (ix >= nx || iy >= s.yr) return;
+    const int z0 = s.zl + blockIdx.z * s.zc;
+    const int z1 = min(z0 + s.zc, s.zr);
+    const int sy = p.L.px, sz = p.L.sz;
+    const int bxl = p.bc[MFD_XL], byl = p.bc[MFD_YL], bzl = p.bc[MFD_ZL];
+    const bool xl = ix == 0, yl = iy == 0;
+    const int ox = !xl ? -1 : (bxl == MFD_BC_PERIODIC ? nx - 1 : 0);
+    const int oy = !yl ? -sy : (byl == MFD_BC_PERIODIC ? (ny - 1) * sy : 0);
+    const bool zx = xl && bxl == MFD_BC_DIRICHLET, zy = yl && byl == MFD_BC_DIRICHLET;
+    const XCol X = xcol(p.lay[MFD_XL], p.lay[MFD_XR], ix, 0, 1);   // E uses psi pair (0, 1)
+    const int kstep = X.nb * ny;
+    int k = X.q + X.nb * (iy + ny * z0);
+    const float Md10 = p.Md10, Md20 = p.Md20, Me0 = p.Me0;
+    const float* __restrict__ Hx = p.Hx;
+    const float* __restrict__ Hy = p.Hy;
+    const float* __restrict__ Hz = p.Hz;
+    float* Dx = p.Dx;
+    float* Dy = p.Dy;
+    float* Dz = p.Dz;
+    float* Ex = p.Ex;
+    float* Ey = p.Ey;
+    float* Ez = p.Ez;
+    int c = ix + sy * iy + sz * z0;
+    float hx_zm, hy_zm;
+    if (z0 > 0) {
+        hx_zm = Hx[c - sz];
+        hy_zm = Hy[c - sz];
+    } else {
+        const int oz = bzl == MFD_BC_PERIODIC ? (nz - 1) * sz : 0;
+        hx_zm = bzl == MFD_BC_DIRICHLET ? 0.0f : Hx[c + oz];
+        hy_zm = bzl == MFD_BC_DIRICHLET ? 0.0f : Hy[c + oz];
+    }
+    auto load = [&](int cc, int kk) {
+        ECoreLoad v;
+        v.hx = Hx[cc];
+        v.hy = Hy[cc];
+        v.hz = Hz[cc];
+        v.hyx = Hy[cc + ox];
+        v.hzx = Hz[cc + ox];
+        v.hxy = Hx[cc + oy];
+        v.hzy = Hz[cc + oy];
+        v.dx = Dx[cc];
+        v.dy = Dy[cc];
+        v.dz = Dz[cc];
+        v.g = MAT ? (int)p.geom[cc] : 0;
+        v.pa = X.in ? X.pa[kk] : 0.0f;
+        v.pb = X.in ? X.pb[kk] : 0.0f;
+        return v;
+    };
+    ECoreLoad cur = load(c, k);
+    for (int iz = z0; iz < z1; ++iz, c += sz, k += kstep) {
+        ECoreLoad nxt;
+        if (iz + 1 < z1) nxt = load(c + sz, k + kstep);
+        const float hx = cur.hx, hy = cur.hy, hz = cur.hz;
+        const float hy_xm = zx ? 0.0f : cur.hyx, hz_xm = zx ? 0.0f : cur.hzx;
+        const float hx_ym = zy ? 0.0f : cur.hxy, hz_ym = zy ? 0.0f : cur.hzy;
+        const float num[6] = {hx - hx_ym, hx - hx_zm, hy - hy_xm, hy - hy_zm, hz - hz_xm, hz - hz_ym};
+        float q[6];
+        div6<FAST>(D3, num, q);
+        const float dHxy = q[0], dHxz = q[1], dHyz = q[3], dHzy = q[5];
+        float dHyx = q[2], dHzx = q[4];
+        float Md1 = Md10, Md2 = Md20, Me = Me0;
+        bool simple = true;
+        if (MAT && cur.g) {
+            const MatDev<float, R>& m = p.mats[cur.g - 1];
+            Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
+        }
+        float D0 = cur.dx, D1 = cur.dy, D2 = cur.dz;
+        if (X.in) {   // cpml_e<-1> of the column's x face
+            const float pa = X.B * cur.pa + X.A * dHyx;
+            const float pb = X.B * cur.pb + X.A * dHzx;
+            X.pa[k] = pa;
+            X.pb[k] = pb;
+            D1 -= Md2 * pb;
+            D2 += Md2 * pa;
+            dHyx = cdiv<FAST>(dHyx, X.K);
+            dHzx = cdiv<FAST>(dHzx, X.K);
+        }
+        D0 = Md1 * D0 + Md2 * (dHzy - dHyz);
+        D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
+        D2 = Md1 * D2 + Md2 * (dHyx - dHxy);
+        Dx[c] = D0;
+        Dy[c] = D1;
+        Dz[c] = D2;
+        if (simple) {
+            Ex[c] = D0 * Me;
+            Ey[c] = D1 * Me;
+            Ez[c] = D2 * Me;
+        }
+        hx_zm = hx;
+        hy_zm = hy;
+        cur = nxt;
+    }
+}
+
+template <typename R, bool MAT, bool FAST>
+__global__ void __launch_bounds__(128) e3d_slab_kernel(const __grid_constant__ EParams<float, R> p, const Div3 D3,
+                                                       const SplitBox s) {
+    const int ix = blockIdx.y * blockDim.x + threadIdx.x;
+    const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
+    if (ix >= nx) return;
+    int iy, iz;
+    slab_row(s, ny, (int)blockIdx.x, iy, iz);
+    const int sy = p.L.px, sz = p.L.sz;
+    const int bxl = p.bc[MFD_XL], byl = p.bc[MFD_YL], bzl = p.bc[MFD_ZL];
+    const bool xl = ix == 0, yl = iy == 0, zl = iz == 0;
+    const int ox = !xl ? -1 : (bxl == MFD_BC_PERIODIC ? nx - 1 : 0);
+    const int oy = !yl ? -sy : (byl == MFD_BC_PERIODIC ? (ny - 1) * sy : 0);
+    const int oz = !zl ? -sz : (bzl == MFD_BC_PERIODIC ? (nz - 1) * sz : 0);
+    const bool zx = xl && bxl == MFD_BC_DIRICHLET, zy = yl && byl == MFD_BC_DIRICHLET, zz = zl && bzl == MFD_BC_DIRICHLET;
+    const int c = ix + sy * iy + sz * iz;
+    const float hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
+    const float hy_xm = zx ? 0.0f : p.Hy[c + ox], hz_xm = zx ? 0.0f : p.Hz[c + ox];
+    const float hx_ym = zy ? 0.0f : p.Hx[c + oy], hz_ym = zy ? 0.0f : p.Hz[c + oy];
+    const float hx_zm = zz ? 0.0f : p.Hx[c + oz], hy_zm = zz ? 0.0f : p.Hy[c + oz];
+    const float num[6] = {hx - hx_ym, hx - hx_zm, hy - hy_xm, hy - hy_zm, hz - hz_xm, hz - hz_ym};
+    float q[6];
+    div6<FAST>(D3, num, q);
+    float dHxy = q[0], dHxz = q[1], dHyx = q[2], dHyz = q[3], dHzx = q[4], dHzy = q[5];
+    float Md1 = p.Md10, Md2 = p.Md20, Me = p.Me0;
+    bool simple = true;
+    if (MAT) {
+        const int g = p.geom[c];
+        if (g) {
+            const MatDev<float, R>& m = p.mats[g - 1];
+            Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
+        }
+    }
+    float D0 = p.Dx[c], D1 = p.Dy[c], D2 = p.Dz[c];
+    const LayerDev<float>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL], &lyr = p.lay[MFD_YR],
+                          &lzl = p.lay[MFD_ZL], &lzr = p.lay[MFD_ZR];
+    if (lxl.nb && ix < lxl.ib) cpml_e<-1, FAST>(lxl, ix, ix + lxl.nb * (iy + ny * iz), Md2, dHyx, dHzx, D1, D2);
+    if (lxr.nb && ix >= lxr.ib - 1) {
+        const int qq = ix - (lxr.ib - 1);
+        cpml_e<-1, FAST>(lxr, qq, qq + lxr.nb * (iy + ny * iz), Md2, dHyx, dHzx, D1, D2);
+    }
+    if (lyl.nb && iy < lyl.ib) cpml_e<+1, FAST>(lyl, iy, ix + sy * (iy + lyl.nb * iz), Md2, dHxy, dHzy, D0, D2);
+    if (lyr.nb && iy >= lyr.ib - 1) {
+        const int qq = iy - (lyr.ib - 1);
+        cpml_e<+1, FAST>(lyr, qq, ix + sy * (qq + lyr.nb * iz), Md2, dHxy, dHzy, D0, D2);
+    }
+    if (lzl.nb && iz < lzl.ib) cpml_e<-1, FAST>(lzl, iz, ix + sy * (iy + ny * iz), Md2, dHxz, dHyz, D0, D1);
+    if (lzr.nb && iz >= lzr.ib - 1) {
+        const int qq = iz - (lzr.ib - 1);
+        cpml_e<-1, FAST>(lzr, qq, ix + sy * (iy + ny * qq), Md2, dHxz, dHyz, D0, D1);
+    }
+    D0 = Md1 * D0 + Md2 * (dHzy - dHyz);
+    D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
+    D2 = Md1 * D2 + Md2 * (dHyx - dHxy);
+    p.Dx[c] = D0;
+    p.Dy[c] = D1;
+    p.Dz[c] = D2;
+    if (simple) {
+        p.Ex[c] = D0 * Me;
+        p.Ey[c] = D1 * Me;
+        p.Ez[c] = D2 * Me;
+    }
+}
+
+}  // namespace mfd

@@ -140,6 +140,35 @@ def model_sources(ndim, nsteps=50):
     return M.Model(g, [s1, s2, s3], tmax=(nsteps - 0.5) * dt, pml=100e-9)
 
 
+def model_wide_rows(bcx, nsteps=45):
+    """3-D rows longer than one warp's span of 4-cell groups and not a multiple of 4 cells
+    (137 x 5 x 6): sources on the first and the last x cell so the x boundary condition
+    matters, CPML on the left x face, materials straddling group and warp boundaries."""
+    g = grid3((137, 5, 6))
+    xe = 68 * 50e-9
+    src = M.SoftSource(geometry=lambda x, y, z: np.abs(x - xe) < 26e-9,
+                       waveform=lambda x, y, z, t: 1e3 * pulse(t), component="Ez")
+    s2 = M.SoftSource(geometry=(-xe, 0.0, 0.0), waveform=lambda x, y, z, t: 5e2 * pulse(t), component="Ey")
+    dt = 0.5 / C0 / np.sqrt(3 / (50e-9) ** 2)
+    m1 = M.Material(geometry=lambda x, y, z: x > 0.3e-6, eps=2.25, mu=1.3, sigma=2e4)
+    m2 = M.Material(geometry=lambda x, y, z: np.abs(x + 0.2e-6) < 130e-9, eps=3.0,
+                    chi=M.DrudeSusceptibility(wp=1.37e16, gamma=1.07e14))
+    return M.Model(g, [src, s2], tmax=(nsteps - 0.5) * dt, pml=(150e-9, 0, 0, 0, 0, 0),
+                   bc=(bcx, bcx, "periodic", "periodic", "neumann", "dirichlet"), material=[m1, m2])
+
+
+def model_layers(n, pml, nsteps=40):
+    """3-D grid of n cells with the given CPML thicknesses (faces xl, xr, yl, yr, zl, zr),
+    e.g. layers that overlap in a dimension or exist on one axis only."""
+    g = grid3(n)
+    src = M.SoftSource(geometry=(0.0, 0.0, 0.0), waveform=lambda x, y, z, t: 1e3 * pulse(t), component="Ez")
+    dt = 0.5 / C0 / np.sqrt(3 / (50e-9) ** 2)
+    m1 = M.Material(geometry=lambda x, y, z: x + y > 0, eps=2.25, mu=1.3, sigma=2e4)
+    cp = M.CPML(thickness=150e-9, kmax=3.0, alpha=0.05, R0=1e-8, m=3)
+    faces = tuple(cp if t else 0 for t in pml)
+    return M.Model(g, src, tmax=(nsteps - 0.5) * dt, pml=faces, material=m1)
+
+
 def monitors(ndim):
     pt = _geo_point(ndim, (0.0, 0.0, 100e-9))
     plane = _plane(ndim, 150e-9)

@@ -108,6 +108,49 @@ def test_parity_tfsf_record_replay(ndim, dtype, oracle_lib, gpu_lib):
     assert np.abs(got2["field/Ex"]).max() > 0
 
 
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("bcx", ["periodic", "dirichlet", "neumann"])
+def test_parity_wide_rows(bcx, dtype, oracle_lib, gpu_lib):
+    """Rows of 137 cells: several warps per row, a partial last 4-cell group, x neighbours
+    taken across lanes, warps and the boundary."""
+    model = C.model_wide_rows(bcx)
+    ref = C.run_all(model, oracle_lib, dtype)
+    got = C.run_all(model, gpu_lib, dtype)
+    _compare(ref, got, dtype, exact=True)
+    assert np.abs(got["field/Ez"]).max() > 0
+
+
+LAYER_CASES = {
+    "x_overlap": ((5, 7, 6), (1, 1, 1, 1, 1, 1)),
+    "y_overlap": ((20, 5, 9), (1, 1, 1, 1, 1, 1)),
+    "z_overlap": ((20, 9, 5), (1, 1, 1, 1, 1, 1)),
+    "y_only": ((20, 18, 16), (0, 0, 1, 1, 0, 0)),
+    "x_only": ((20, 18, 16), (1, 1, 0, 0, 0, 0)),
+    "y_z_right": ((20, 18, 16), (0, 0, 0, 1, 0, 1)),
+}
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("case", sorted(LAYER_CASES))
+def test_parity_layer_layouts(case, dtype, oracle_lib, gpu_lib):
+    """CPML layers that overlap in one dimension (the single-precision 3-D update is then not
+    split into core rows and layer slabs) or exist on some faces only."""
+    model = C.model_layers(*LAYER_CASES[case])
+    ref = C.run_all(model, oracle_lib, dtype)
+    got = C.run_all(model, gpu_lib, dtype)
+    _compare(ref, got, dtype, exact=True)
+
+
+@pytest.mark.parametrize("builder", ["bcs", "materials"])
+def test_parity_unsplit_3d(builder, monkeypatch, oracle_lib, gpu_lib):
+    """MFD_KERNEL3D=unsplit selects the single-kernel 3-D updates; they agree bit for bit."""
+    monkeypatch.setenv("MFD_KERNEL3D", "unsplit")
+    model = getattr(C, "model_" + builder)(3)
+    ref = C.run_all(model, oracle_lib, np.float32)
+    got = C.run_all(model, gpu_lib, np.float32)
+    _compare(ref, got, np.float32, exact=True)
+
+
 @pytest.mark.parametrize("ndim", [2, 3])
 def test_chunked_runs_equal_single_run(ndim, gpu_lib):
     """Splitting a run into several mfd_run calls changes nothing (the deferred Sa/E2
