@@ -224,6 +224,28 @@ MFD_API int mfd_write_field(mfd_handle* h, int32_t comp, const void* src);
  * rho*rho0) as nx*ny*nz double. */
 MFD_API int mfd_read_integral(mfd_handle* h, int32_t which, void* dst);
 
+/* mfd_read_integral without any device memory allocation.  No counterpart in the
+ * reference (its integral outputs are plain arrays of the model).
+ *
+ * For callers that cannot allocate device memory when they read results: a host program
+ * whose GPU memory is held by another allocator's pool (a framework's caching allocator
+ * that reserved most of HBM, so cudaMalloc fails), or a serving loop that must not call
+ * cudaMalloc/cudaFree between steps (they can synchronise the device and stall work on
+ * other streams).  mfd_read_integral allocates a grid-sized temporary for JE and rho_end;
+ * this entry point stages them through a fixed buffer inside the library instead -- a
+ * device array of MFD_NOALLOC_SCRATCH_BYTES (16 MiB) -- a few z-planes at a time.  Sa and
+ * E2 are copied straight from their arrays, as by mfd_read_integral.
+ *
+ * Limit: one z-plane (nx*ny elements; T for JE, double for rho_end) must fit in the
+ * buffer, else MFD_ERR_INVALID with both sizes in mfd_last_error().
+ * Nothing in the buffer has to start at zero: each call writes every element it copies out.
+ * The buffer is shared by all handles on a device: calls that overlap in time on the same
+ * device race on it, so serialise them.  The first call on a device performs the set-up
+ * (it looks up the buffer's device address, which makes the driver load the library's
+ * device globals): make that first call before any stream capture on that device. */
+#define MFD_NOALLOC_SCRATCH_BYTES (16u << 20)
+MFD_API int mfd_read_integral_noalloc(mfd_handle* h, int32_t which, void* dst);
+
 /* Monitor m, component comp.  Field monitor: T [nt][npts] ([nt] when sum).  Spectral
  * monitor: double complex [nw][npts] ([nw] when sum) as interleaved (re, im). */
 MFD_API int mfd_read_monitor(mfd_handle* h, int32_t m, int32_t comp, void* dst);

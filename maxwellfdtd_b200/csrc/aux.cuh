@@ -262,4 +262,25 @@ __global__ void __launch_bounds__(256) scatter_state_kernel(const MatDev<T, R>* 
     else ((double*)out)[c] = pl ? 0.0 + (double)(m->rho[bi] * m->rho0) : 0.0;
 }
 
+// The same values for the z-planes z0 .. z0 + gridDim.z - 1 only, written densely (x fastest,
+// then y, then z) from `out`, for the allocation-free read that stages a few planes at a time
+// through a fixed device buffer.
+template <typename T, typename R>
+__global__ void __launch_bounds__(256) scatter_state_planes_kernel(const MatDev<T, R>* __restrict__ mats,
+                                                                   const uint8_t* __restrict__ geom, Layout L,
+                                                                   void* out, int which, int z0) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y, iz = z0 + (int)blockIdx.z;
+    if (ix >= L.nx) return;
+    const long long c = ix + (long long)L.px * iy + L.sz * iz;
+    const long long o = ix + (long long)L.nx * (iy + (long long)L.ny * blockIdx.z);
+    const int g = geom[c];
+    const MatDev<T, R>* m = g ? mats + (g - 1) : nullptr;
+    const bool pl = m && m->plasma;
+    long long bi = 0;
+    if (pl) bi = (long long)(ix - m->bx0) + (long long)m->bnx * ((long long)(iy - m->by0) + (long long)m->bny * (iz - m->bz0));
+    if (which == MFD_INT_JE) ((T*)out)[o] = pl ? m->JE[bi] : T(0);
+    else ((double*)out)[o] = pl ? 0.0 + (double)(m->rho[bi] * m->rho0) : 0.0;
+}
+
 }  // namespace mfd

@@ -56,6 +56,7 @@ struct HandleBase {
     virtual int read_field(int comp, void* dst) = 0;
     virtual int write_field(int comp, const void* src) = 0;
     virtual int read_integral(int which, void* dst) = 0;
+    virtual int read_integral_noalloc(int which, void* dst) = 0;
     virtual int read_monitor(int m, int comp, void* dst) = 0;
     virtual int read_record(int k, void* dst) = 0;
     virtual int64_t record_size(int k) const = 0;
@@ -89,6 +90,28 @@ static void bounded_sync(cudaStream_t st) {
 }
 
 static long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
+
+// Staging buffer of mfd_read_integral_noalloc: a file-scope device array, so reading JE and
+// rho_end needs no device allocation at read time.  Shared by every handle on a device.
+static __device__ __align__(256) unsigned char g_read_scratch[MFD_NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_read_scratch on the current device, looked up once per device
+// (cudaGetSymbolAddress makes the driver load the module's device globals on first use).
+static void* read_scratch(int dev) {
+    static std::mutex mu;
+    static std::map<int, void*> addr;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = addr.find(dev);
+    if (it != addr.end()) return it->second;
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_read_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        throw Error(MFD_ERR_CUDA, std::string("cudaGetSymbolAddress of the read scratch buffer failed: ") + cudaGetErrorString(e));
+    }
+    addr[dev] = p;
+    return p;
+}
 
 // Exhaustive check of the constant-divisor fast path (see DivC in mfd_device.cuh): for every
 // significand x in [1, 2), the correction step must reproduce IEEE x/d bit for bit.
@@ -1229,6 +1252,40 @@ class Engine : public HandleBase {
         return MFD_ERR_INVALID;
     }
 
+    // JE / rho_end staged through g_read_scratch a few z-planes at a time (no device
+    // allocation); Sa and E2 are plain copies from their arrays.
+    bool noalloc_ready = false;
+    int read_integral_noalloc(int which, void* dst) override {
+        MFD_CK(cudaSetDevice(dev));
+        if (which == MFD_INT_SA || which == MFD_INT_E2) return read_integral(which, dst);
+        if (which != MFD_INT_JE && which != MFD_INT_RHO) { err = "bad integral"; return MFD_ERR_INVALID; }
+        const size_t es = which == MFD_INT_JE ? sizeof(T) : sizeof(double);
+        const size_t plane = (size_t)nx * ny * es;
+        if (plane > (size_t)MFD_NOALLOC_SCRATCH_BYTES) {
+            err = "mfd_read_integral_noalloc: one z-plane of this grid is " + std::to_string(plane) +
+                  " bytes, more than its " + std::to_string((size_t)MFD_NOALLOC_SCRATCH_BYTES) +
+                  "-byte scratch buffer; use mfd_read_integral";
+            return MFD_ERR_INVALID;
+        }
+        if (!any_plasma || !any_geom) { std::memset(dst, 0, (size_t)N * es); return MFD_OK; }
+        unsigned char* scratch = (unsigned char*)read_scratch(dev);
+        if (!noalloc_ready) {   // load the kernel now rather than at its first launch
+            cudaFuncAttributes fa;
+            MFD_CK(cudaFuncGetAttributes(&fa, scatter_state_planes_kernel<T, R>));
+            noalloc_ready = true;
+        }
+        const int per = (int)std::min<size_t>({(size_t)nz, (size_t)MFD_NOALLOC_SCRATCH_BYTES / plane, (size_t)65535});
+        for (int z0 = 0; z0 < nz; z0 += per) {
+            const int n = std::min(per, nz - z0);
+            dim3 grd((nx + 255) / 256, ny, n);
+            scatter_state_planes_kernel<T, R><<<grd, 256, 0, st>>>(mats_dev, geom, layout(), scratch, which, z0);
+            MFD_CK(cudaGetLastError());
+            MFD_CK(cudaMemcpyAsync((char*)dst + (size_t)z0 * plane, scratch, (size_t)n * plane, cudaMemcpyDeviceToHost, st));
+        }
+        bounded_sync(st);
+        return MFD_OK;
+    }
+
     int read_monitor(int m, int comp, void* dst) override {
         if (m < 0 || m >= (int)mons_host.size()) { err = "bad monitor"; return MFD_ERR_INVALID; }
         int k = -1;
@@ -1364,6 +1421,9 @@ int mfd_run(mfd_handle* h, int64_t a, int64_t b) { MFD_GUARD(h, h->impl->run(a, 
 int mfd_read_field(mfd_handle* h, int32_t comp, void* dst) { MFD_GUARD(h, h->impl->read_field(comp, dst)); }
 int mfd_write_field(mfd_handle* h, int32_t comp, const void* src) { MFD_GUARD(h, h->impl->write_field(comp, src)); }
 int mfd_read_integral(mfd_handle* h, int32_t which, void* dst) { MFD_GUARD(h, h->impl->read_integral(which, dst)); }
+int mfd_read_integral_noalloc(mfd_handle* h, int32_t which, void* dst) {
+    MFD_GUARD(h, h->impl->read_integral_noalloc(which, dst));
+}
 int mfd_read_monitor(mfd_handle* h, int32_t m, int32_t comp, void* dst) { MFD_GUARD(h, h->impl->read_monitor(m, comp, dst)); }
 int mfd_read_tfsf_record(mfd_handle* h, int32_t k, void* dst) { MFD_GUARD(h, h->impl->read_record(k, dst)); }
 
