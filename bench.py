@@ -181,6 +181,8 @@ def run_gpu(args):
     h_gbs = h_bytes / (h_ms * 1e-3) / 1e9
     per_kernel = {k: {"ms": round(kt1[k][0] - kt0[k][0], 4), "launches": int(kt1[k][1] - kt0[k][1])} for k in kt1}
 
+    plain = plain_stepper(lib, args, local) if rank == 0 and not args.no_plain else None
+
     # end to end through the public API with host buffers
     t0 = time.perf_counter()
     b2, meta2 = model.build_desc(dtype, mons, device=local)
@@ -232,6 +234,7 @@ def run_gpu(args):
                          "h_kernel": {"achieved": round(h_gbs, 1), "frac": round(h_gbs / peak, 4),
                                       "algorithmic_bytes_per_launch": h_bytes, "mean_launch_ms": round(h_ms, 5)}},
             "kernels": per_kernel,
+            "plain_stepper": plain,
             "gpu_launches": launches,
             "device_bytes": dev_bytes,
             "cpu_baseline": cpu,
@@ -242,6 +245,33 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def plain_stepper(lib, args, device, steps=20):
+    """The plain FP32 stepper at 256^3 (vacuum, 12-cell CPML, Sa sum): H and E update times
+    and their HBM roofline fractions, CUDA events per update."""
+    from maxwellfdtd_b200 import _abi, workloads
+    model, _ = workloads.plain_256(nt=steps + 5, n=args.n)
+    b, meta = model.build_desc(np.float32, None, device=device)
+    st = _abi.Stepper(lib, b, np.float32)
+    st.run(1, 3)
+    k0 = st.kernel_times()
+    st.set_profiling(True)
+    st.run(4, 3 + steps)
+    st.set_profiling(False)
+    k1 = st.kernel_times()
+    ms = st.last_run_ms()
+    st.close()
+    h_bytes, e_bytes = algorithmic_bytes(model, meta, np.float32)
+    peak, kind = peaks()
+    h_ms = (k1["H"][0] - k0["H"][0]) / steps
+    e_ms = (k1["E"][0] - k0["E"][0]) / steps
+    N = model.grid.Nx * model.grid.Ny * model.grid.Nz
+    return {"workload": f"plain_256: {args.n}^3 FP32 vacuum, 12-cell CPML, soft point source, Sa sum",
+            "value": round(N * steps / (ms * 1e-3) / 1e9, 3), "unit": "Gcell-updates/s", "steps": steps,
+            "h_update": {"ms": round(h_ms, 5), "bytes": h_bytes, "frac": round(h_bytes / (h_ms * 1e-3) / 1e9 / peak, 4)},
+            "e_update": {"ms": round(e_ms, 5), "bytes": e_bytes, "frac": round(e_bytes / (e_ms * 1e-3) / 1e9 / peak, 4)},
+            "peak_gbs": peak, "peak_kind": kind}
 
 
 def _oracle_lib():
@@ -311,6 +341,7 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-stepper roofline measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -78,13 +78,14 @@ __device__ __forceinline__ T tfsf_apply(const RectStmt& t, T v, T inc) {
 template <typename T>
 __global__ void __launch_bounds__(256) tfsf_kernel(const __grid_constant__ RectParams<T> p) {
     const RectStmt& s = p.s[blockIdx.y];
-    const long long local = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int local = blockIdx.x * blockDim.x + threadIdx.x;
     if (local >= s.len) return;
     const int nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
-    const int ix = s.x0 + (int)(local % nxr);
-    const long long rest = local / nxr;
-    const int iy = s.y0 + (int)(rest % nyr);
-    const int iz = s.z0 + (int)(rest / nyr);
+    const int rest = local / nxr;
+    const int ix = s.x0 + (local - rest * nxr);
+    const int iz0 = rest / nyr;
+    const int iy = s.y0 + (rest - iz0 * nyr);
+    const int iz = s.z0 + iz0;
     for (unsigned long long m = s.prev; m; m &= m - 1)
         if (rect_has(p.s[__ffsll((long long)m) - 1], ix, iy, iz)) return;
     T* F = p.F[s.comp];
@@ -100,13 +101,14 @@ __global__ void __launch_bounds__(256) tfsf_kernel(const __grid_constant__ RectP
 template <typename T>
 __global__ void __launch_bounds__(256) record_kernel(const __grid_constant__ RectParams<T> p) {
     const RectStmt& s = p.s[blockIdx.y];
-    const long long local = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int local = blockIdx.x * blockDim.x + threadIdx.x;
     if (local >= s.len) return;
     const int nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
-    const int ix = s.x0 + (int)(local % nxr);
-    const long long rest = local / nxr;
-    const int iy = s.y0 + (int)(rest % nyr);
-    const int iz = s.z0 + (int)(rest / nyr);
+    const int rest = local / nxr;
+    const int ix = s.x0 + (local - rest * nxr);
+    const int iz0 = rest / nyr;
+    const int iy = s.y0 + (rest - iz0 * nyr);
+    const int iz = s.z0 + iz0;
     const int c = ix + p.L.px * iy + p.L.sz * iz;
     p.arr[s.k][p.it0 * s.len + local] = p.F[s.comp][c];
 }
@@ -168,38 +170,64 @@ __global__ void __launch_bounds__(256) monitor_fieldsum_kernel(const MonDev<T>* 
 }
 
 // Spectral monitor, per point: S[k][w][j] += F * (2 e_w(t) dt) for each staged step in
-// order (dft.jl:560-566).  A thread owns MFD_DFT_W frequencies of one point.
+// order (dft.jl:560-566).  A block owns MFD_DFT_W frequencies of 2 * blockDim.x points; each
+// thread two points (j and j + blockDim.x, both coalesced).  The block's factors for all
+// staged steps are staged once in shared memory (the same for every point), so the inner
+// loop issues one ring load per point and broadcast shared loads per factor.
 #define MFD_DFT_W 8
+#define MFD_DFT_MAXSLOTS 64
 template <typename T>
 __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __restrict__ mon, int ncomp, int nslots,
                                                           long long it0_first) {
+    __shared__ double2 tw[MFD_DFT_MAXSLOTS * MFD_DFT_W];   // [slot][w]
     const MonDev<T>& M = *mon;
-    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
     const int w0 = blockIdx.z * MFD_DFT_W;
-    if (j >= M.npts) return;
     const int nw = M.nw;
     const int wn = min(MFD_DFT_W, nw - w0);
-    double sr[MFD_DFT_W], si[MFD_DFT_W];
-    double2* S = M.S + ((long long)k * nw + w0) * M.npts + j;
+    for (int i = threadIdx.x; i < nslots * MFD_DFT_W; i += blockDim.x) {
+        const int sl = i / MFD_DFT_W, w = i - sl * MFD_DFT_W;
+        tw[i] = w < wn ? M.phasor[(it0_first + sl) * nw + w0 + w] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const long long npts = M.npts;
+    const long long j0 = blockIdx.x * 2LL * blockDim.x + threadIdx.x;
+    const long long j1 = j0 + blockDim.x;
+    if (j0 >= npts) return;
+    const bool two = j1 < npts;
+    double ar[MFD_DFT_W], ai[MFD_DFT_W], br[MFD_DFT_W], bi[MFD_DFT_W];
+    double2* S = M.S + ((long long)k * nw + w0) * npts;
 #pragma unroll
-    for (int w = 0; w < MFD_DFT_W; ++w)
-        if (w < wn) { const double2 s = S[(long long)w * M.npts]; sr[w] = s.x; si[w] = s.y; }
-    for (int slot = 0; slot < nslots; ++slot) {
-        const double f = (double)M.ring[((long long)slot * ncomp + k) * M.npts + j];
-        const double2* e = M.phasor + (it0_first + slot) * nw + w0;   // 2 exp(...) dt, tabulated
+    for (int w = 0; w < MFD_DFT_W; ++w) {
+        ar[w] = ai[w] = br[w] = bi[w] = 0.0;
+        if (w < wn) {
+            const double2 a = S[(long long)w * npts + j0];
+            ar[w] = a.x; ai[w] = a.y;
+            if (two) { const double2 b = S[(long long)w * npts + j1]; br[w] = b.x; bi[w] = b.y; }
+        }
+    }
+    const T* ring = M.ring + (long long)k * npts;
+    const long long rstride = (long long)ncomp * npts;
+    for (int sl = 0; sl < nslots; ++sl) {
+        const double f = (double)ring[sl * rstride + j0];
+        const double g = two ? (double)ring[sl * rstride + j1] : 0.0;
+        const double2* e = tw + sl * MFD_DFT_W;
 #pragma unroll
         for (int w = 0; w < MFD_DFT_W; ++w) {
-            if (w < wn) {
-                const double2 tw = e[w];
-                sr[w] = sr[w] + f * tw.x;
-                si[w] = si[w] + f * tw.y;
-            }
+            const double2 t = e[w];
+            ar[w] = ar[w] + f * t.x;
+            ai[w] = ai[w] + f * t.y;
+            br[w] = br[w] + g * t.x;
+            bi[w] = bi[w] + g * t.y;
         }
     }
 #pragma unroll
-    for (int w = 0; w < MFD_DFT_W; ++w)
-        if (w < wn) S[(long long)w * M.npts] = make_double2(sr[w], si[w]);
+    for (int w = 0; w < MFD_DFT_W; ++w) {
+        if (w < wn) {
+            S[(long long)w * npts + j0] = make_double2(ar[w], ai[w]);
+            if (two) S[(long long)w * npts + j1] = make_double2(br[w], bi[w]);
+        }
+    }
 }
 
 // Spectral monitor with sum: S[k][w] += 2 * sum_j(F_j e_w(t)) * dt (dft.jl:556-559).

@@ -289,7 +289,7 @@ class Engine : public HandleBase {
     int32_t bad_kind = 0;
 
     // launch shapes
-    int bx3 = 32, by3 = 8, zc3 = 16;
+    int bx3 = 32, by3 = 4, zc3 = 8;   // 3-D z-march tiles: measured best of {32x8, 32x4} x {8, 16} planes at 256^3
     // single-precision 3-D updates split into core rows and CPML slabs (yee3d_split.cuh)
     bool use_split = false;
     SplitBox sbox{};
@@ -741,6 +741,7 @@ class Engine : public HandleBase {
                 if (j < i) p.s[i].prev |= 1ull << j; else p.s[i].next |= 1ull << j;
             }
             tfsf_maxlen = std::max(tfsf_maxlen, p.s[i].len);
+            if (p.s[i].len >= (1ll << 31)) throw Error(MFD_ERR_INVALID, "TFSF face larger than 2^31 cells");
         }
         for (int k = 0; k < narr; ++k)
             if (nonzero[k]) p.arr[k] = upload((const T*)d->tfsf.inc[k], (size_t)alen[k] * nt);
@@ -798,6 +799,7 @@ class Engine : public HandleBase {
             s.k = i;
             s.len = (long long)(s.x1 - s.x0 + 1) * (s.y1 - s.y0 + 1) * (s.z1 - s.z0 + 1);
             rec_maxlen = std::max(rec_maxlen, s.len);
+            if (s.len >= (1ll << 31)) throw Error(MFD_ERR_INVALID, "TFSF record face larger than 2^31 cells");
             p.arr[i] = dalloc<T>((size_t)s.len * nt);
         }
     }
@@ -819,7 +821,7 @@ class Engine : public HandleBase {
         if (need_ring) {
             // staging depth: up to 64 steps, at most ~512 MB of staged values
             long long cap = (512ll << 20) / ((long long)sizeof(T) * ring_vals);
-            ring_k = (int)std::max(1ll, std::min(64ll, cap));
+            ring_k = (int)std::max(1ll, std::min((long long)MFD_DFT_MAXSLOTS, cap));
         }
         for (int m = 0; m < d->nmon; ++m) {
             const mfd_monitor& a = d->mons[m];
@@ -955,8 +957,9 @@ class Engine : public HandleBase {
     void launch_H_f32(const HParams<float>& p) {
         if (use_split) {
             kcount = 0;
-            if (sbox.yr > sbox.yl && sbox.zr > sbox.zl) {
-                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (sbox.zr - sbox.zl + zc3 - 1) / zc3);
+            const int zn = sbox.zr - sbox.zl;
+            if (sbox.yr > sbox.yl && zn > 0) {
+                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
                 h3d_core_kernel<MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, sbox);
                 kcount++;
             }
@@ -982,8 +985,9 @@ class Engine : public HandleBase {
     void launch_E_f32(const EParams<float, R>& p) {
         if (use_split) {
             kcount = 0;
-            if (sbox.yr > sbox.yl && sbox.zr > sbox.zl) {
-                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (sbox.zr - sbox.zl + zc3 - 1) / zc3);
+            const int zn = sbox.zr - sbox.zl;
+            if (sbox.yr > sbox.yl && zn > 0) {
+                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
                 e3d_core_kernel<R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sbox);
                 kcount++;
             }
@@ -1113,7 +1117,7 @@ class Engine : public HandleBase {
                 });
             } else if (M.kind == MFD_MON_SPECTRAL && !M.sum) {
                 launch(KC_DFT, [&] {
-                    dim3 grd((unsigned)((M.npts + 255) / 256), ncomp_mon, (M.nw + MFD_DFT_W - 1) / MFD_DFT_W);
+                    dim3 grd((unsigned)((M.npts + 511) / 512), ncomp_mon, (M.nw + MFD_DFT_W - 1) / MFD_DFT_W);
                     monitor_dft_kernel<T><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first);
                 });
             } else if (M.kind == MFD_MON_SPECTRAL) {

@@ -7,6 +7,9 @@ plane wave along +z (600 nm, 3 fs), and DFT monitors on the six faces of a 160^3
 wavelengths 400-900 nm with double-precision sums.  The incident TFSF data are the
 analytic plane wave sampled at the Yee positions, standing in for a vacuum record run.
 
+plain_256: the plain FP32 stepper at 256^3 -- vacuum, dx = 2 nm, 12-cell CPML on all faces,
+one soft point source; only the H/E updates with CPML and the Sa running sum.
+
 dielectric_100: 100^3 grid, dx = 20 nm, 10-cell CPML, Float64, a dielectric sphere
 (radius 500 nm, eps = 2.25), a TFSF x-polarised Gaussian pulse (800 nm, 10 fs intensity
 FWHM) along +z, and one point monitor.
@@ -14,7 +17,7 @@ FWHM) along +z, and one point monitor.
 import numpy as np
 
 from . import (C0, EPS0, MU0, Grid, DrudeSusceptibility, FieldMonitor, LorentzSusceptibility, Material, Model,
-               SpectralMonitor, TFSFSource)
+               SoftSource, SpectralMonitor, TFSFSource)
 from .model import time_range, time_step
 from .sources import TFSF_NAMES_3D
 
@@ -99,6 +102,16 @@ def plasmonics_256(nt=4000, n=256, with_monitors=True):
         ]
         mons = [SpectralMonitor(fc, w=w) for fc in faces]
     return model, mons
+
+
+def plain_256(nt=40, n=256):
+    dx = 2e-9
+    L = (n - 1) * dx / 2
+    grid = Grid(xmin=-L, xmax=L, Nx=n, ymin=-L, ymax=L, Ny=n, zmin=-L, zmax=L, Nz=n)
+    dt = time_step(grid, 0.5)
+    w0 = 2 * np.pi * C0 / 600e-9
+    src = SoftSource(geometry=(0.0, 0.0, 0.0), waveform=lambda x, y, z, t: np.sin(w0 * t), component="Ex")
+    return Model(grid, src, tmax=(nt - 0.5) * dt, pml=12 * dx), None
 
 
 def dielectric_100(nt=1000, n=100):
