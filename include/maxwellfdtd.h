@@ -255,6 +255,35 @@ MFD_API int mfd_read_tfsf_record(mfd_handle* h, int32_t k, void* dst);
 /* Element count of TFSF array k for the record box (0 if k is unused). */
 MFD_API int64_t mfd_tfsf_record_size(const mfd_handle* h, int32_t k);
 
+/* ---- batches of 2-D models ------------------------------------------------------------
+ * No counterpart in the reference, which runs one model per solve! call.  A batch steps
+ * many independent 2-D single-precision models together: each half-step of all members is
+ * one persistent launch over a table of (member, tile) pairs, and a CUDA graph of several
+ * steps is replayed, so hundreds of small models of different sizes do not each pay a
+ * handful of launches per step.  A member is an ordinary handle (mfd_create, 2-D, MFD_F32,
+ * rho_fp64 = 1) with point sources and field monitors without sum; the batch runs its steps
+ * done+1 .. it_last exactly as mfd_run(h, done+1, it_last) would, with bit-identical results,
+ * and then retires it: mfd_status / mfd_read_* work on it again.  Until it retires, the
+ * caller must not run, read, write or destroy the handle (mfd_run returns MFD_ERR_INVALID).
+ * Members join at any time (mfd_batch_add between mfd_batch_run calls), each with its own
+ * step count; the persistent launches skip members whose window has ended. */
+typedef struct mfd_batch mfd_batch;
+MFD_API int mfd_batch_create(int32_t device, mfd_batch** out);
+MFD_API void mfd_batch_destroy(mfd_batch* b);
+MFD_API int mfd_batch_add(mfd_batch* b, mfd_handle* h, int64_t it_last);
+/* Advance every member by up to max_steps steps; members that reach their last step are
+ * retired.  n_active receives the number of members still running. */
+MFD_API int mfd_batch_run(mfd_batch* b, int64_t max_steps, int32_t* n_active);
+/* Tile shape of the persistent launches (tile_x a multiple of 32, tile_x*tile_z <= 512;
+ * 0, 0 = autotune: the first graph replays try candidate shapes and keep the cheapest per
+ * cell-update -- results do not depend on the shape) and steps per graph (0 = keep). */
+MFD_API int mfd_batch_config(mfd_batch* b, int32_t tile_x, int32_t tile_z, int32_t graph_steps);
+/* Current tile shape, device time of all mfd_batch_run calls (CUDA events), cell-updates and
+ * kernel launches (graph nodes included) so far. */
+MFD_API int mfd_batch_info(const mfd_batch* b, int32_t* tile_x, int32_t* tile_z, double* device_ms,
+                           int64_t* cell_updates, int64_t* launches);
+MFD_API const char* mfd_batch_last_error(const mfd_batch* b);
+
 /* Device-time measurement: when on, every kernel launch of mfd_run is bracketed by CUDA
  * events on the handle's stream and its duration is summed per kernel class. */
 MFD_API int mfd_set_profiling(mfd_handle* h, int32_t on);

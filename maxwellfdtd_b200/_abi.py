@@ -126,6 +126,18 @@ class Library:
             self.kernel_times = fn("kernel_times", C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int32])
             self.last_run_ms = fn("last_run_ms", C.c_int, [vp, C.POINTER(C.c_double)])
             self.device_bytes = fn("device_bytes", C.c_int64, [vp])
+        # batches of 2-D models (CUDA library only)
+        self.has_batch = hasattr(L, p + "batch_create")
+        if self.has_batch:
+            self.batch_create = fn("batch_create", C.c_int, [C.c_int32, C.POINTER(vp)])
+            self.batch_destroy = fn("batch_destroy", None, [vp])
+            self.batch_add = fn("batch_add", C.c_int, [vp, vp, C.c_int64])
+            self.batch_run = fn("batch_run", C.c_int, [vp, C.c_int64, C.POINTER(C.c_int32)])
+            self.batch_config = fn("batch_config", C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32])
+            self.batch_info = fn("batch_info", C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                                         C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                                         C.POINTER(C.c_int64)])
+            self.batch_last_error = fn("batch_last_error", C.c_char_p, [vp])
 
 
 class Stepper:
@@ -216,3 +228,58 @@ class Stepper:
         out = np.empty(n, dtype=self.dtype)
         self._check(self.lib.read_tfsf_record(self.h, int(k), out.ctypes.data_as(C.c_void_p)))
         return out
+
+
+class Batch:
+    """A batch of 2-D single-precision models stepped together (mfd_batch_*).  Members are
+    Steppers; each runs its steps done+1 .. it_last as one mfd_run call would and is then
+    retired (usable again)."""
+
+    def __init__(self, lib, device=0):
+        if not getattr(lib, "has_batch", False):
+            raise RuntimeError("this library has no batch entry points")
+        self.lib = lib
+        b = C.c_void_p()
+        st = lib.batch_create(int(device), C.byref(b))
+        if st != MFD_OK:
+            raise StepperError(st, f"batch create failed ({st}): {lib.create_error().decode()}")
+        self.b = b
+        self.members = []
+
+    def _check(self, st):
+        if st != MFD_OK:
+            raise StepperError(st, self.lib.batch_last_error(self.b).decode())
+
+    def add(self, stepper, it_last):
+        self._check(self.lib.batch_add(self.b, stepper.h, int(it_last)))
+        self.members.append(stepper)
+
+    def run(self, max_steps):
+        """Advance every member by up to max_steps steps; returns the number still running."""
+        n = C.c_int32()
+        self._check(self.lib.batch_run(self.b, int(max_steps), C.byref(n)))
+        return n.value
+
+    def run_all(self, chunk=1 << 20):
+        while self.run(chunk):
+            pass
+
+    def config(self, tile_x=0, tile_z=0, graph_steps=0):
+        self._check(self.lib.batch_config(self.b, int(tile_x), int(tile_z), int(graph_steps)))
+
+    def info(self):
+        tx, tz, ms, cu, nl = C.c_int32(), C.c_int32(), C.c_double(), C.c_int64(), C.c_int64()
+        self._check(self.lib.batch_info(self.b, C.byref(tx), C.byref(tz), C.byref(ms), C.byref(cu), C.byref(nl)))
+        return {"tile": (tx.value, tz.value), "device_ms": ms.value, "cell_updates": cu.value, "launches": nl.value}
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

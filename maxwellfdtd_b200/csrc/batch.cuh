@@ -1,0 +1,161 @@
+// batch.cuh -- many independent 2-D models stepped together (sm_100a).
+//
+// Each half-step of every member of a batch is one persistent launch: the grid is sized to
+// the GPU (SMs x resident blocks) and each block walks a table of tiles (member, tile
+// origin), so hundreds of small, unevenly sized models cost a handful of launches per step
+// instead of a handful per model.  Every per-member quantity that changes from step to step
+// (the step index, the running-sum flag, the polarisation ping-pong parity) lives in the
+// member's device state and is advanced on the device, so a CUDA graph of several steps can
+// be replayed unchanged.  The per-cell arithmetic is the single-model code (h2d_cell,
+// e2d_cell, material_cell, the point-source expression), so a member's results are
+// bit-identical to running it alone.
+#pragma once
+
+#include "aux.cuh"
+#include "yee.cuh"
+
+namespace mfd {
+
+enum { BF_MATH = 1, BF_MAT = 2, BF_FAST = 4 };
+
+// Per-member state (device).  Steps are 1-based; the member runs steps first..last.
+struct BMember {
+    const HParams<float>* hp;              // the member's update parameters (static fields)
+    const EParams<float, double>* ep;
+    const MonParams<float>* mp;            // field monitors (gathered every step)
+    long long it;                          // step being run; > last once the member is done
+    long long first, last;
+    int flags;                             // BF_*
+    int pad;
+};
+
+struct BTile {      // cells x0 .. x0+blockDim.x-1, z0 .. z0+blockDim.y-1 of member m
+    int m, x0, z0, pad;
+};
+
+struct BMatTile {   // one row segment of material g's bounding box: x0 .. x0+blockDim.x-1 at iz
+    int m, g, x0, iz;
+};
+
+struct BSrc {       // one point source of a member (sources.jl:122-131, 235-244)
+    float* F;
+    const long long* cells;
+    const double* wave;
+    const double* amp;
+    const double* gt;
+    long long npts;
+    int kind;
+    float coeff;
+};
+
+struct BPoint {     // point i of source s (entries of one source pass) or of monitor s
+    int m, s;
+    long long i;
+};
+
+__device__ __forceinline__ bool b_active(const BMember& M) { return M.it <= M.last; }
+
+template <bool MATH, bool FAST>
+__device__ __forceinline__ void b_h2d(const BMember& M, int ix, int iz) {
+    h2d_cell<float, MATH, FAST>(*M.hp, M.it > M.first ? 1 : 0, M.it - 1, ix, iz);
+}
+
+__global__ void __launch_bounds__(512) batch_h2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
+                                                        const int* __restrict__ ntiles) {
+    const int n = *ntiles;
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const BTile tl = tiles[t];
+        const BMember& M = mem[tl.m];
+        if (!b_active(M)) continue;
+        const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
+        if (ix >= M.hp->L.nx || iz >= M.hp->L.nz) continue;
+        switch (M.flags & (BF_MATH | BF_FAST)) {
+            case 0: b_h2d<false, false>(M, ix, iz); break;
+            case BF_MATH: b_h2d<true, false>(M, ix, iz); break;
+            case BF_FAST: b_h2d<false, true>(M, ix, iz); break;
+            default: b_h2d<true, true>(M, ix, iz); break;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(512) batch_e2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
+                                                        const int* __restrict__ ntiles) {
+    const int n = *ntiles;
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const BTile tl = tiles[t];
+        const BMember& M = mem[tl.m];
+        if (!b_active(M)) continue;
+        const EParams<float, double>& p = *M.ep;
+        const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
+        if (ix >= p.L.nx || iz >= p.L.nz) continue;
+        switch (M.flags & (BF_MAT | BF_FAST)) {
+            case 0: e2d_cell<float, double, false, false>(p, ix, iz); break;
+            case BF_MAT: e2d_cell<float, double, true, false>(p, ix, iz); break;
+            case BF_FAST: e2d_cell<float, double, false, true>(p, ix, iz); break;
+            default: e2d_cell<float, double, true, true>(p, ix, iz); break;
+        }
+    }
+}
+
+// ADE / Kerr / plasma response of material g's cells (material_kernel for 2-D members).
+__global__ void __launch_bounds__(128) batch_material2d_kernel(const BMember* __restrict__ mem,
+                                                               const BMatTile* __restrict__ tiles,
+                                                               const int* __restrict__ ntiles) {
+    const int n = *ntiles;
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const BMatTile tl = tiles[t];
+        const BMember& M = mem[tl.m];
+        if (!b_active(M)) continue;
+        const EParams<float, double>& p = *M.ep;
+        const MatDev<float, double>* m = p.mats + (tl.g - 1);
+        const int ix = tl.x0 + threadIdx.x;
+        if (ix >= m->bx0 + m->bnx) continue;
+        const int c = ix + p.L.sz * tl.iz;
+        if (p.geom[c] != tl.g) continue;
+        float Dv[2] = {p.Dx[c], p.Dz[c]};
+        float* Ep[2] = {p.Ex, p.Ez};
+        material_cell<float, double, 2>(m, ix, 0, tl.iz, Ep, c, Dv, (int)((M.it - 1) & 1), p.dt);
+    }
+}
+
+// One pass of point sources: entry i is a point of the k-th source of its member, so a
+// member's sources act in tuple order across passes (models.jl:128-130).
+__global__ void __launch_bounds__(256) batch_source_kernel(const BMember* __restrict__ mem, const BSrc* __restrict__ srcs,
+                                                           const BPoint* __restrict__ pts, const int* __restrict__ npts) {
+    const int n = *npts;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const BPoint e = pts[i];
+        const BMember& M = mem[e.m];
+        if (!b_active(M)) continue;
+        const BSrc& S = srcs[e.s];
+        const long long it0 = M.it - 1;
+        const double w = S.wave ? S.wave[it0 * S.npts + e.i] : S.amp[e.i] * S.gt[it0];
+        const long long c = S.cells[e.i];
+        if (S.kind == MFD_SRC_SOFT) S.F[c] = (float)((double)S.F[c] + (double)S.coeff * w);
+        else S.F[c] = (float)w;
+    }
+}
+
+// Field monitors without sum: hist[k][it-1][j] = F_k[cells[j]] (monitor_gather_kernel).
+__global__ void __launch_bounds__(256) batch_gather_kernel(const BMember* __restrict__ mem, const BPoint* __restrict__ pts,
+                                                           const int* __restrict__ npts) {
+    const int n = *npts;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const BPoint e = pts[i];
+        const BMember& M = mem[e.m];
+        if (!b_active(M)) continue;
+        const MonParams<float>& p = *M.mp;
+        const MonDev<float>& D = p.mons[e.s];
+        const long long it0 = M.it - 1;
+        const int cell = D.cells[e.i];
+        for (int k = 0; k < p.ncomp; ++k) D.hist[((long long)k * p.nt + it0) * D.npts + e.i] = p.comp[k][cell];
+    }
+}
+
+// End of a batch step: every active member moves to its next step.
+__global__ void batch_advance_kernel(BMember* __restrict__ mem, int n) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x)
+        if (mem[m].it <= mem[m].last) mem[m].it += 1;
+}
+
+}  // namespace mfd

@@ -28,6 +28,7 @@
 #include "yee.cuh"
 #include "yee3d_tma.cuh"
 #include "yee3d_split.cuh"
+#include "batch.cuh"
 
 namespace mfd {
 
@@ -1159,7 +1160,10 @@ class Engine : public HandleBase {
         });
     }
 
+    bool in_batch = false;     // stepped by a batch until it retires
+
     int run(int64_t a, int64_t b) override {
+        if (in_batch) { err = "the model is being stepped by a batch"; return MFD_ERR_INVALID; }
         if (bad_step) { err = "the model holds non-finite fields from step " + std::to_string(bad_step); return MFD_ERR_NONFINITE; }
         if (a != done + 1 || b < a - 1 || b > nt) { err = "steps must be consecutive and within 1..Nt"; return MFD_ERR_INVALID; }
         if (b < a) return MFD_OK;
@@ -1172,6 +1176,12 @@ class Engine : public HandleBase {
             launch_monitors(it);
             if (record) launch_record(it);
         }
+        return finish(a, b);
+    }
+
+    // End of a run of steps a..b (also of a batch member's window): staged monitors, the
+    // running sums of step b, and the per-step NaN/Inf flags.
+    int finish(int64_t a, int64_t b) {
         flush_monitors();
         launch_sums(b);
         MFD_CK(cudaEventRecord(run_ev[1], st));
@@ -1351,6 +1361,306 @@ struct mfd_handle {
     std::unique_ptr<HandleBase> impl;
 };
 
+// ------------------------------------------------------------------------------------------
+// Batch of 2-D single-precision models (batch.cuh): members are ordinary handles; the batch
+// runs each one's steps first..last with persistent batched launches replayed from a CUDA
+// graph of `gsteps` steps, then retires it with the same end-of-run work as mfd_run.
+// ------------------------------------------------------------------------------------------
+template <typename U>
+struct DevBuf {
+    U* p = nullptr;
+    size_t cap = 0;
+    void reserve(size_t n) {
+        if (n <= cap) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const size_t c = std::max<size_t>(n, 64);
+        if (cudaMalloc(&p, c * sizeof(U)) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(MFD_ERR_OOM, "batch table allocation failed");
+        }
+        cap = c;
+    }
+    void upload(const std::vector<U>& v, cudaStream_t st) {
+        reserve(v.size());
+        if (!v.empty()) MFD_CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(U), cudaMemcpyHostToDevice, st));
+    }
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+
+struct mfd_batch {
+    using E = Engine<float, double>;
+    struct Member {
+        mfd_handle* h;
+        E* e;
+        long long first, last, it;
+        int flags;
+        HParams<float>* hp = nullptr;
+        EParams<float, double>* ep = nullptr;
+        MonParams<float>* mp = nullptr;
+        long long cells;
+    };
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    std::string err;
+    std::vector<Member> mem;
+    // tables
+    DevBuf<BMember> d_mem;
+    DevBuf<BTile> d_tiles;
+    DevBuf<BMatTile> d_mtiles;
+    DevBuf<BSrc> d_srcs;
+    DevBuf<BPoint> d_mpts;
+    std::vector<std::unique_ptr<DevBuf<BPoint>>> d_spass;
+    DevBuf<int> d_counts;   // [0] tiles, [1] material tiles, [2] monitor points, [3 + k] points of source pass k
+    int ntiles = 0, nmtiles = 0, nmpts = 0;
+    std::vector<int> spass_n;
+    // graph
+    cudaGraphExec_t gexec = nullptr;
+    int gsteps = 16, built_steps = 0;
+    bool dirty = true;
+    // tiles and autotuning
+    int tx = 0, tz = 0;           // fixed shape, or 0 = autotune
+    int cur_tx = 32, cur_tz = 8;
+    std::vector<std::pair<int, int>> cands{{32, 4}, {32, 8}, {64, 4}, {128, 2}, {32, 16}, {64, 8}};
+    size_t tune_next = 0;
+    std::vector<double> tune_cost;
+    bool tuned = false;
+    // statistics
+    double dev_ms = 0;
+    long long cell_updates = 0, launches = 0;
+
+    ~mfd_batch() {
+        cudaSetDevice(dev);
+        if (st) cudaStreamSynchronize(st);
+        if (gexec) cudaGraphExecDestroy(gexec);
+        for (auto& m : mem) release(m);
+        for (auto e : ev) if (e) cudaEventDestroy(e);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    static void release(Member& m) {
+        if (m.hp) cudaFree(m.hp);
+        if (m.ep) cudaFree(m.ep);
+        if (m.mp) cudaFree(m.mp);
+        m.hp = nullptr; m.ep = nullptr; m.mp = nullptr;
+        if (m.e) m.e->in_batch = false;
+    }
+
+    template <typename U>
+    U* copy_struct(const U& v) {
+        U* d = nullptr;
+        if (cudaMalloc(&d, sizeof(U)) != cudaSuccess) { cudaGetLastError(); throw Error(MFD_ERR_OOM, "batch member allocation failed"); }
+        MFD_CK(cudaMemcpy(d, &v, sizeof(U), cudaMemcpyHostToDevice));
+        return d;
+    }
+
+    void init(int device) {
+        dev = device;
+        MFD_CK(cudaSetDevice(dev));
+        MFD_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        MFD_CK(cudaEventCreate(&ev[0]));
+        MFD_CK(cudaEventCreate(&ev[1]));
+        d_counts.reserve(64);
+    }
+
+    int add(mfd_handle* h, long long last) {
+        if (!h || !h->impl) { err = "null handle"; return MFD_ERR_INVALID; }
+        E* e = dynamic_cast<E*>(h->impl.get());
+        if (!e) { err = "batch members must be single precision with double-precision plasma density (the default)"; return MFD_ERR_INVALID; }
+        if (e->ndim != 2) { err = "batch members must be 2-D models"; return MFD_ERR_INVALID; }
+        if (e->dev != dev) { err = "batch member on another device"; return MFD_ERR_INVALID; }
+        if (e->in_batch) { err = "model already in a batch"; return MFD_ERR_INVALID; }
+        if (e->tfsf || e->record || e->need_ring) { err = "batch members support point sources and field monitors without sum (no TFSF, TFSF record, summed or spectral monitors)"; return MFD_ERR_INVALID; }
+        if (e->bad_step) { err = "the model holds non-finite fields"; return MFD_ERR_NONFINITE; }
+        if (last <= e->done || last > e->nt) { err = "the last step must be after the model's current step and within 1..Nt"; return MFD_ERR_INVALID; }
+        MFD_CK(cudaSetDevice(dev));
+        Member m{};
+        m.h = h; m.e = e; m.first = e->done + 1; m.last = last; m.it = m.first;
+        m.flags = (e->math_needed ? BF_MATH : 0) | (e->any_geom ? BF_MAT : 0) | (e->fastdiv ? BF_FAST : 0);
+        m.cells = (long long)e->nx * e->nz;
+        try {
+            m.hp = copy_struct(e->hparams(0, 0));
+            m.ep = copy_struct(e->eparams());
+            m.mp = copy_struct(e->mon_p);
+        } catch (...) {
+            release(m);
+            throw;
+        }
+        MFD_CK(cudaStreamSynchronize(e->st));          // the member's own work is complete
+        MFD_CK(cudaEventRecord(e->run_ev[0], e->st));
+        e->in_batch = true;
+        mem.push_back(m);
+        dirty = true;
+        return MFD_OK;
+    }
+
+    // Tables of the current members and tile shape, then the graph of gsteps steps.
+    void rebuild() {
+        std::vector<BMember> hm;
+        std::vector<BTile> tiles;
+        std::vector<BMatTile> mt;
+        std::vector<BSrc> srcs;
+        std::vector<std::vector<BPoint>> passes;
+        std::vector<BPoint> mpts;
+        for (size_t i = 0; i < mem.size(); ++i) {
+            const Member& m = mem[i];
+            E* e = m.e;
+            hm.push_back(BMember{m.hp, m.ep, m.mp, m.it, m.first, m.last, m.flags, 0});
+            const int mi = (int)i;
+            for (int z = 0; z < e->nz; z += cur_tz)
+                for (int x = 0; x < e->nx; x += cur_tx) tiles.push_back(BTile{mi, x, z, 0});
+            for (int g : e->response_mats) {
+                const MatDev<float, double>& md = e->mats_host[g - 1];
+                for (int z = md.bz0; z < md.bz0 + md.bnz; ++z)
+                    for (int x = md.bx0; x < md.bx0 + md.bnx; x += 128) mt.push_back(BMatTile{mi, g, x, z});
+            }
+            for (size_t k = 0; k < e->srcs.size(); ++k) {
+                const auto& S = e->srcs[k];
+                if (passes.size() <= k) passes.emplace_back();
+                const int si = (int)srcs.size();
+                srcs.push_back(BSrc{e->F[S.comp], S.cells, S.wave, S.amp, S.gt, S.npts, S.kind, S.coeff});
+                for (long long j = 0; j < S.npts; ++j) passes[k].push_back(BPoint{mi, si, j});
+            }
+            for (size_t k = 0; k < e->mons_host.size(); ++k)
+                for (long long j = 0; j < e->mons_host[k].npts; ++j) mpts.push_back(BPoint{mi, (int)k, j});
+        }
+        d_mem.upload(hm, st);
+        d_tiles.upload(tiles, st);
+        d_mtiles.upload(mt, st);
+        d_srcs.upload(srcs, st);
+        d_mpts.upload(mpts, st);
+        while (d_spass.size() < passes.size()) d_spass.emplace_back(new DevBuf<BPoint>());
+        spass_n.assign(passes.size(), 0);
+        for (size_t k = 0; k < passes.size(); ++k) {
+            d_spass[k]->upload(passes[k], st);
+            spass_n[k] = (int)passes[k].size();
+        }
+        if (passes.size() + 3 > 64) throw Error(MFD_ERR_INVALID, "batch members have at most 61 sources");
+        std::vector<int> counts(3 + passes.size());
+        ntiles = counts[0] = (int)tiles.size();
+        nmtiles = counts[1] = (int)mt.size();
+        nmpts = counts[2] = (int)mpts.size();
+        for (size_t k = 0; k < passes.size(); ++k) counts[3 + k] = spass_n[k];
+        d_counts.upload(counts, st);
+        MFD_CK(cudaStreamSynchronize(st));
+        build_graph();
+        dirty = false;
+    }
+
+    int grid_for(const void* fn, int threads, int work) {
+        int per_sm = 0, sms = 0;
+        MFD_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0));
+        MFD_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        return std::max(1, std::min(std::max(1, per_sm) * sms, work));
+    }
+
+    int kernels_per_step() const {
+        int k = 3 + (nmtiles ? 1 : 0) + (nmpts ? 1 : 0);
+        for (int n : spass_n) k += n ? 1 : 0;
+        return k;
+    }
+
+    void launch_step() {
+        const dim3 blk(cur_tx, cur_tz);
+        const int gt = grid_for((const void*)batch_h2d_kernel, cur_tx * cur_tz, ntiles);
+        batch_h2d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+        batch_e2d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+        if (nmtiles) {
+            const int g = grid_for((const void*)batch_material2d_kernel, 128, nmtiles);
+            batch_material2d_kernel<<<g, 128, 0, st>>>(d_mem.p, d_mtiles.p, d_counts.p + 1);
+        }
+        for (size_t k = 0; k < spass_n.size(); ++k) {
+            if (!spass_n[k]) continue;
+            batch_source_kernel<<<(spass_n[k] + 255) / 256, 256, 0, st>>>(d_mem.p, d_srcs.p, d_spass[k]->p, d_counts.p + 3 + k);
+        }
+        if (nmpts) batch_gather_kernel<<<(nmpts + 255) / 256, 256, 0, st>>>(d_mem.p, d_mpts.p, d_counts.p + 2);
+        batch_advance_kernel<<<((int)mem.size() + 255) / 256, 256, 0, st>>>(d_mem.p, (int)mem.size());
+    }
+
+    void build_graph() {
+        if (gexec) { MFD_CK(cudaGraphExecDestroy(gexec)); gexec = nullptr; }
+        cudaGraph_t g = nullptr;
+        MFD_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < gsteps; ++i) launch_step();
+        const cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (ce != cudaSuccess) { cudaGetLastError(); throw Error(MFD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)); }
+        const cudaError_t ie = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) { cudaGetLastError(); throw Error(MFD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie)); }
+        built_steps = gsteps;
+    }
+
+    // Retire members whose window is done: the end-of-run work of mfd_run on their streams.
+    void retire() {
+        std::vector<Member> keep;
+        for (auto& m : mem) {
+            if (m.it <= m.last) { keep.push_back(m); continue; }
+            m.e->in_batch = false;
+            m.e->finish(m.first, m.last);   // its status (NaN/Inf step) is kept by the handle
+            release(m);
+            dirty = true;
+        }
+        mem.swap(keep);
+    }
+
+    int run(long long max_steps, int* n_active) {
+        MFD_CK(cudaSetDevice(dev));
+        long long done_steps = 0;
+        while (done_steps < max_steps && !mem.empty()) {
+            // autotune: one graph chunk per candidate tile shape, then the cheapest per cell-update
+            if (!tuned) {
+                if (tx > 0) { cur_tx = tx; cur_tz = tz; tuned = true; dirty = true; }
+                else if (tune_next < cands.size()) {
+                    if (cur_tx != cands[tune_next].first || cur_tz != cands[tune_next].second || !gexec) {
+                        cur_tx = cands[tune_next].first; cur_tz = cands[tune_next].second; dirty = true;
+                    }
+                }
+            }
+            if (dirty || built_steps != gsteps) rebuild();
+            long long active_cells = 0;
+            for (auto& m : mem) active_cells += m.cells * std::min<long long>(gsteps, m.last - m.it + 1);
+            const bool chunk = max_steps - done_steps >= gsteps;
+            const int n = chunk ? gsteps : (int)(max_steps - done_steps);
+            MFD_CK(cudaEventRecord(ev[0], st));
+            if (chunk) MFD_CK(cudaGraphLaunch(gexec, st));
+            else for (int i = 0; i < n; ++i) launch_step();
+            MFD_CK(cudaEventRecord(ev[1], st));
+            MFD_CK(cudaGetLastError());
+            bounded_sync(st);
+            float ms = 0;
+            MFD_CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            long long cu = 0;
+            for (auto& m : mem) {
+                const long long adv = std::min<long long>(n, m.last - m.it + 1);
+                cu += m.cells * adv;
+                m.it += adv;
+            }
+            dev_ms += ms;
+            cell_updates += cu;
+            launches += (long long)n * kernels_per_step();
+            if (!tuned && tx == 0 && chunk) {
+                tune_cost.push_back(active_cells > 0 ? ms / (double)active_cells : 1e30);
+                if (++tune_next >= cands.size()) {
+                    size_t best = 0;
+                    for (size_t i = 1; i < tune_cost.size(); ++i) if (tune_cost[i] < tune_cost[best]) best = i;
+                    cur_tx = cands[best].first; cur_tz = cands[best].second;
+                    tuned = true;
+                    dirty = true;
+                }
+            }
+            // the device advanced every member; members that finished leave the tables
+            bool any_done = false;
+            for (auto& m : mem) any_done = any_done || m.it > m.last;
+            if (any_done) retire();
+            done_steps += n;
+        }
+        if (n_active) *n_active = (int)mem.size();
+        return MFD_OK;
+    }
+};
+
 static int validate_desc(const mfd_desc* d) {
     if (!d) { g_create_error = "null descriptor"; return MFD_ERR_INVALID; }
     if (d->abi_version != MFD_ABI_VERSION) { g_create_error = "ABI version mismatch"; return MFD_ERR_INVALID; }
@@ -1422,6 +1732,70 @@ void mfd_destroy(mfd_handle* h) { delete h; }
     } while (0)
 
 int mfd_run(mfd_handle* h, int64_t a, int64_t b) { MFD_GUARD(h, h->impl->run(a, b)); }
+
+#define MFD_BGUARD(b, expr)                                  \
+    do {                                                     \
+        if (!(b)) return MFD_ERR_INVALID;                    \
+        try {                                                \
+            return (expr);                                   \
+        } catch (const Error& e) {                           \
+            (b)->err = e.what();                             \
+            return e.code;                                   \
+        } catch (const std::bad_alloc&) {                    \
+            (b)->err = "out of host memory";                 \
+            return MFD_ERR_OOM;                              \
+        }                                                    \
+    } while (0)
+
+int mfd_batch_create(int32_t device, mfd_batch** out) {
+    if (!out) return MFD_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); g_create_error = "no CUDA device"; return MFD_ERR_NODEVICE; }
+    if (device < 0 || device >= ndev) { g_create_error = "bad device ordinal"; return MFD_ERR_INVALID; }
+    std::unique_ptr<mfd_batch> b(new mfd_batch);
+    try {
+        b->init(device);
+    } catch (const Error& e) {
+        g_create_error = e.what();
+        return e.code;
+    }
+    *out = b.release();
+    return MFD_OK;
+}
+
+void mfd_batch_destroy(mfd_batch* b) { delete b; }
+
+int mfd_batch_add(mfd_batch* b, mfd_handle* h, int64_t it_last) { MFD_BGUARD(b, b->add(h, it_last)); }
+
+int mfd_batch_run(mfd_batch* b, int64_t max_steps, int32_t* n_active) { MFD_BGUARD(b, b->run(max_steps, n_active)); }
+
+int mfd_batch_config(mfd_batch* b, int32_t tile_x, int32_t tile_z, int32_t graph_steps) {
+    if (!b) return MFD_ERR_INVALID;
+    if (tile_x < 0 || tile_z < 0 || (tile_x > 0) != (tile_z > 0) || tile_x * tile_z > 512 || (tile_x && tile_x % 32) ||
+        graph_steps < 0 || graph_steps > 4096) {
+        b->err = "tile_x must be a multiple of 32 with tile_x * tile_z <= 512 (0, 0 = autotune); graph_steps in 1..4096 (0 = keep)";
+        return MFD_ERR_INVALID;
+    }
+    b->tx = tile_x; b->tz = tile_z;
+    b->tuned = false; b->tune_next = 0; b->tune_cost.clear();
+    if (graph_steps) b->gsteps = graph_steps;
+    b->dirty = true;
+    return MFD_OK;
+}
+
+int mfd_batch_info(const mfd_batch* b, int32_t* tile_x, int32_t* tile_z, double* device_ms, int64_t* cell_updates,
+                   int64_t* launches) {
+    if (!b) return MFD_ERR_INVALID;
+    if (tile_x) *tile_x = b->cur_tx;
+    if (tile_z) *tile_z = b->cur_tz;
+    if (device_ms) *device_ms = b->dev_ms;
+    if (cell_updates) *cell_updates = b->cell_updates;
+    if (launches) *launches = b->launches;
+    return MFD_OK;
+}
+
+const char* mfd_batch_last_error(const mfd_batch* b) { return b ? b->err.c_str() : "null batch"; }
 int mfd_read_field(mfd_handle* h, int32_t comp, void* dst) { MFD_GUARD(h, h->impl->read_field(comp, dst)); }
 int mfd_write_field(mfd_handle* h, int32_t comp, const void* src) { MFD_GUARD(h, h->impl->write_field(comp, src)); }
 int mfd_read_integral(mfd_handle* h, int32_t which, void* dst) { MFD_GUARD(h, h->impl->read_integral(which, dst)); }

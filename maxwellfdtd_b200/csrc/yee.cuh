@@ -63,6 +63,13 @@ __device__ __forceinline__ void guard(const HParams<T>& p, T ex) {
     if (bad) atomicOr(p.flags + (p.prev_step - 1), bad);
 }
 
+// The same for an explicit step (batched launches keep the step per member on the device).
+template <typename T>
+__device__ __forceinline__ void guard_at(int* flags, long long prev_step, T ex) {
+    const int bad = (isnan(ex) ? 1 : 0) | (isinf(ex) ? 2 : 0);
+    if (bad) atomicOr(flags + (prev_step - 1), bad);
+}
+
 template <typename T>
 __device__ __forceinline__ bool in_layers(const LayerDev<T>& lo, const LayerDev<T>& hi, int i) {
     return (lo.nb && i < lo.ib) || (hi.nb && i >= hi.ib - 1);
@@ -527,12 +534,11 @@ __global__ void __launch_bounds__(256, 4) e3d_f32_kernel(const __grid_constant__
 // ------------------------------------------------------------------------------------------
 // 2-D (x-z plane): one thread per cell
 // ------------------------------------------------------------------------------------------
+// One cell of the 2-D H update; `accum` and `prev_step` are the step's running-sum flag and
+// the previous step (p.accum / p.prev_step for a single model, per-member state in a batch).
 template <typename T, bool MATH, bool FAST>
-__global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParams<T> p) {
-    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void h2d_cell(const HParams<T>& p, int accum, long long prev_step, int ix, int iz) {
     const int nx = p.L.nx, nz = p.L.nz;
-    if (ix >= nx || iz >= nz) return;
     const int sz = p.L.sz;
     const int c = ix + sz * iz;
     const T ex = p.Ex[c], ez = p.Ez[c];
@@ -542,11 +548,11 @@ __global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParam
     if (iz < nz - 1) ex_zp = p.Ex[c + sz];
     else { const int b = p.bc[MFD_ZR]; ex_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ex[c - (nz - 1) * sz] : T(0), ex); }
     T hy = p.Hy[c];
-    if (p.accum) {
+    if (accum) {
         const T a = -ez * hy, b = ex * hy;
         p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b) * p.dt;
         if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ez * ez) * p.dt;
-        guard(p, ex);
+        guard_at(p.flags, prev_step, ex);
     }
     T Mh = p.Mh0;
     if (MATH) { const int g = p.geom[c]; if (g) Mh = p.matMh[g - 1]; }
@@ -596,12 +602,18 @@ __global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParam
     p.Hy[c] = hy;
 }
 
-template <typename T, typename R, bool MAT, bool FAST>
-__global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParams<T, R> p) {
+template <typename T, bool MATH, bool FAST>
+__global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParams<T> p) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= p.L.nx || iz >= p.L.nz) return;
+    h2d_cell<T, MATH, FAST>(p, p.accum, p.prev_step, ix, iz);
+}
+
+// One cell of the 2-D E update (D with CPML; E of cells without a response material).
+template <typename T, typename R, bool MAT, bool FAST>
+__device__ __forceinline__ void e2d_cell(const EParams<T, R>& p, int ix, int iz) {
     const int nx = p.L.nx, nz = p.L.nz;
-    if (ix >= nx || iz >= nz) return;
     const int sz = p.L.sz;
     const int c = ix + sz * iz;
     const T hy = p.Hy[c];
@@ -670,6 +682,14 @@ __global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParam
         p.Ex[c] = D0 * Me;
         p.Ez[c] = D2 * Me;
     }
+}
+
+template <typename T, typename R, bool MAT, bool FAST>
+__global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParams<T, R> p) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= p.L.nx || iz >= p.L.nz) return;
+    e2d_cell<T, R, MAT, FAST>(p, ix, iz);
 }
 
 // ------------------------------------------------------------------------------------------
