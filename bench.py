@@ -73,29 +73,37 @@ def algorithmic_bytes(model, meta, dtype):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 20 ms from before the warm-up;
+    summary() keeps the samples taken inside the marked (timed) window, or the nearest ones
+    when the window is shorter than the sampling interval."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.window = None
         self.path = os.path.join("/tmp", f"mfd_clocks_{os.getpid()}.csv")
 
-    def __enter__(self):
+    def start(self):
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)   # let the sampler start before the measured work
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
 
-    def __exit__(self, *a):
+    def mark(self, t0, t1):
+        self.window = (t0, t1)
+
+    def stop(self):
         if self.proc is not None:
+            time.sleep(0.05)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -104,6 +112,14 @@ class ClockSampler:
         if hasattr(self, "fh"):
             self.fh.close()
 
+    @staticmethod
+    def _t(stamp):
+        import datetime
+        try:
+            return datetime.datetime.strptime(stamp.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
     def summary(self):
         if self.proc is None or not os.path.exists(self.path):
             return None
@@ -111,16 +127,25 @@ class ClockSampler:
         with open(self.path) as f:
             for line in f:
                 p = [x.strip() for x in line.split(",")]
-                if len(p) >= 9:
+                if len(p) >= 10 and p[2].replace(".", "").isdigit():
                     rows.append(p)
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        inside = rows
+        if self.window is not None:
+            t0, t1 = self.window
+            stamped = [(self._t(r[0]), r) for r in rows]
+            stamped = [(t, r) for t, r in stamped if t is not None]
+            inside = [r for t, r in stamped if t0 <= t <= t1]
+            if not inside and stamped:    # window shorter than the interval: the nearest samples
+                mid = 0.5 * (t0 + t1)
+                inside = [r for _, r in sorted(stamped, key=lambda tr: abs(tr[0] - mid))[:2]]
+        sm = [float(r[2]) for r in inside]
+        mx = [float(r[3]) for r in inside if r[3].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        reasons = sorted({names[i] for r in inside for i in range(4) if r[6 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(inside)}
 
 
 def dist_setup():
@@ -151,6 +176,7 @@ def run_gpu(args):
     b, meta = model.build_desc(dtype, mons, device=local)
     st = _abi.Stepper(lib, b, dtype)
     N = model.grid.Nx * model.grid.Ny * model.grid.Nz
+    clk = ClockSampler(local).start()
     # warm-up
     st.run(1, W)
     kt0 = st.kernel_times()
@@ -158,8 +184,10 @@ def run_gpu(args):
         dist.barrier()
         torch.cuda.synchronize()
     st.set_profiling(True)
-    with ClockSampler(local) as clk:
-        st.run(W + 1, W + K)        # timed: K steps, CUDA events on the library's stream
+    t_w0 = time.time()
+    st.run(W + 1, W + K)        # timed: K steps, CUDA events on the library's stream
+    clk.mark(t_w0, time.time())
+    clk.stop()
     st.set_profiling(False)
     ms = st.last_run_ms()
     kt1 = st.kernel_times()
@@ -244,6 +272,122 @@ def run_gpu(args):
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
+    return out
+
+
+def bytes_2d(model):
+    """Algorithmic HBM bytes of one 2-D cell-update (FP32): H reads Ex, Ez, Hy and writes Hy,
+    with the Sa (and E2 with materials) running sums read and written; E reads Hy, Dx, Dz and
+    writes Dx, Dz, Ex, Ez; the material map once per half-step; CPML psi pairs on layer cells;
+    Debye/Drude/Lorentz poles on material cells (P^n, P^{n-1} read, P^{n+1} written, E^n read)."""
+    g = model.grid
+    N = g.Nx * g.Nz
+    geo = np.count_nonzero(model.geometry)
+    h = N * (4 * 4 + 8 + (8 if geo else 0) + (1 if geo else 0))
+    e = N * (4 + 8 + 8 + 8 + (1 if geo else 0))
+    for f, L in enumerate(model.pml):
+        if L.nb and f // 2 != 1:
+            n_axis = g.Nx if f // 2 == 0 else g.Nz
+            h += N // n_axis * L.nb * 8
+            e += N // n_axis * L.nb * 8
+    for imat, m in enumerate(model.materials, start=1):
+        if m.nq:
+            cells = int(np.count_nonzero(model.geometry == imat))
+            e += cells * (2 * 4 + m.nq * 2 * 3 * 4)
+    return h + e
+
+
+def run_batch2d(args):
+    """Batched 2-D configuration: all models in one batch (persistent launches, CUDA graph,
+    autotuned tiles) against the same models run as sequential plain solves."""
+    import maxwellfdtd_b200 as M
+    from maxwellfdtd_b200 import _abi, workloads
+    ws, rank, local = dist_setup()
+    lib = M.load_library()
+    models = workloads.batch2d(n=args.sims, seed=args.seed, steps_scale=args.steps_scale)
+    cu_total = sum(m.grid.Nx * m.grid.Nz * m.Nt for m, _ in models)
+    bytes_total = sum(bytes_2d(m) * m.Nt for m, _ in models)
+    clk = ClockSampler(local).start()
+    # warm-up: a small batch of the first members for a few steps (loads the kernels)
+    wb = _abi.Batch(lib, local)
+    warm = []
+    for m, mo in models[:8]:
+        b, meta = m.build_desc(np.float32, mo, device=local)
+        st = _abi.Stepper(lib, b, np.float32)
+        wb.add(st, min(m.Nt, 3 * 16))
+        warm.append(st)
+    wb.run_all()
+    wb.close()
+    for st in warm:
+        st.close()
+    # batched, end to end: upload every member, run all, read every member's fields and monitors
+    t0 = time.time()
+    batch = _abi.Batch(lib, local)
+    held = []
+    h2d = 0
+    for m, mo in models:
+        b, meta = m.build_desc(np.float32, mo, device=local)
+        h2d += sum(a.nbytes for a in b.keep if isinstance(a, np.ndarray))
+        st = _abi.Stepper(lib, b, np.float32)
+        batch.add(st, m.Nt)
+        held.append((st, meta, m))
+    t_up = time.time()
+    batch.run_all()
+    t_run = time.time()
+    clk.mark(t_up, t_run)
+    clk.stop()
+    d2h = 0
+    for st, meta, m in held:
+        for c in (1, 6, 8):
+            d2h += st.read_field(c).nbytes
+        for k, mm in enumerate(meta["monitors"]):
+            for c in (1, 6, 8):
+                d2h += st.read_monitor(k, c, (m.Nt, len(mm["cells"])), False).nbytes
+    t_end = time.time()
+    info = batch.info()
+    batch.close()
+    for st, _, _ in held:
+        st.close()
+    dev_ms = info["device_ms"]
+    value = cu_total / (dev_ms * 1e-3) / 1e9
+    # sequential plain solves of a seeded subset (device time of each mfd_run call)
+    seq = [models[i] for i in np.random.default_rng(args.seed + 1).choice(len(models), min(args.seq_sims, len(models)), replace=False)]
+    seq_ms, seq_cu = 0.0, 0
+    for m, mo in seq:
+        b, meta = m.build_desc(np.float32, mo, device=local)
+        st = _abi.Stepper(lib, b, np.float32)
+        st.run(1, m.Nt)
+        seq_ms += st.last_run_ms()
+        seq_cu += m.grid.Nx * m.grid.Nz * m.Nt
+        st.close()
+    seq_value = seq_cu / (seq_ms * 1e-3) / 1e9
+    peak, kind = peaks()
+    achieved = bytes_total / (dev_ms * 1e-3) / 1e9
+    out = {
+        "metric": "Gcell-updates/s", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": 1,
+        "steps": int(sum(m.Nt for m, _ in models)), "warmup": 3, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"batch2d: {len(models)} 2-D models, Nx,Nz in [128,1024], dx=20nm, 10-cell CPML, "
+                               f"1-20 ellipses eps in [1,12] (half Debye), Ricker point source, 4 point monitors, "
+                               f"steps 2000-6000 x {args.steps_scale}",
+                   "cells": int(sum(m.grid.Nx * m.grid.Nz for m, _ in models)), "cell_updates": int(cu_total),
+                   "seed": args.seed, "parallelism": "one batch, persistent launches, CUDA graph",
+                   "l2": "inputs larger than L2", "tile": list(info["tile"])},
+        "e2e": {"value": round(cu_total / (t_end - t0) / 1e9, 3), "unit": "Gcell-updates/s",
+                "h2d_bytes_per_step": int(h2d / max(1, max(m.Nt for m, _ in models))),
+                "d2h_bytes_per_step": int(d2h / max(1, max(m.Nt for m, _ in models))),
+                "includes": "descriptor upload of every member + batched run + read-back of fields and monitors",
+                "wall_s": round(t_end - t0, 3)},
+        "roofline": {"bound": "hbm", "kernel": "batched 2-D step (batch_h2d + batch_e2d + material/sources/monitors)",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": None, "algorithmic_bytes": int(bytes_total), "peak_kind": kind},
+        "sequential": {"value": round(seq_value, 3), "unit": "Gcell-updates/s", "sims": len(seq),
+                       "note": "the same kind of models run one at a time with mfd_run (device time per run)"},
+        "batched_vs_sequential": round(value / seq_value, 2),
+        "gpu_launches": int(info["launches"]),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out), flush=True)
     return out
 
 
@@ -342,6 +486,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-stepper roofline measurement")
+    ap.add_argument("--workload", default="plasmonics", choices=["plasmonics", "batch2d"])
+    ap.add_argument("--sims", type=int, default=256, help="batch2d: number of models")
+    ap.add_argument("--steps-scale", type=float, default=0.25, help="batch2d: scale of the 2000-6000 step counts")
+    ap.add_argument("--seq-sims", type=int, default=16, help="batch2d: models timed as sequential solves")
+    ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -349,6 +498,8 @@ def main():
         if args.steps > 20:
             args.steps = 20   # each reference step is a full 256^3 step on the CPU
         run_reference(args)
+    elif args.workload == "batch2d":
+        run_batch2d(args)
     else:
         run_gpu(args)
 

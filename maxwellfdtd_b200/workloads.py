@@ -10,14 +10,20 @@ analytic plane wave sampled at the Yee positions, standing in for a vacuum recor
 plain_256: the plain FP32 stepper at 256^3 -- vacuum, dx = 2 nm, 12-cell CPML on all faces,
 one soft point source; only the H/E updates with CPML and the Sa running sum.
 
+batch2d: many independent 2-D models of seeded, uneven sizes -- Nx, Nz uniform in
+[128, 1024], dx = 20 nm, 10-cell CPML, 2000-6000 steps (scaled by steps_scale), 1-20 random
+ellipses per domain with eps uniform in [1, 12] and, for half of them, a Debye pole
+(deps uniform in [1, 5], tau log-uniform in [1e-15, 1e-13] s), a soft Ricker point source
+(lambda0 uniform in 400-1600 nm) and 4 point field monitors.
+
 dielectric_100: 100^3 grid, dx = 20 nm, 10-cell CPML, Float64, a dielectric sphere
 (radius 500 nm, eps = 2.25), a TFSF x-polarised Gaussian pulse (800 nm, 10 fs intensity
 FWHM) along +z, and one point monitor.
 """
 import numpy as np
 
-from . import (C0, EPS0, MU0, Grid, DrudeSusceptibility, FieldMonitor, LorentzSusceptibility, Material, Model,
-               SoftSource, SpectralMonitor, TFSFSource)
+from . import (C0, EPS0, MU0, Grid, DebyeSusceptibility, DrudeSusceptibility, FieldMonitor, LorentzSusceptibility,
+               Material, Model, SoftSource, SpectralMonitor, TFSFSource)
 from .model import time_range, time_step
 from .sources import TFSF_NAMES_3D
 
@@ -131,3 +137,46 @@ def dielectric_100(nt=1000, n=100):
     data = _plane_wave_tfsf(grid, i1, i2, t, f, grid.z[i1[2] - 1], dt)
     model = Model(grid, TFSFSource(data=data), tmax=(nt - 0.5) * dt, pml=10 * dx, material=mat)
     return model, [FieldMonitor((0.0, 0.0, 0.0))]
+
+
+def ricker(lam0):
+    """Ricker wavelet of centre frequency c/lam0, delayed by 1.5 periods."""
+    f0 = C0 / lam0
+    t0 = 1.5 / f0
+
+    def w(x, z, t):
+        a = (np.pi * f0 * (t - t0)) ** 2
+        return (1 - 2 * a) * np.exp(-a)
+    return w
+
+
+def batch2d(n=256, seed=0, steps_scale=1.0, nmin=128, nmax=1024):
+    """List of (model, monitors) for the batched 2-D configuration."""
+    rng = np.random.default_rng(seed)
+    dx = 20e-9
+    out = []
+    for i in range(n):
+        nx, nz = int(rng.integers(nmin, nmax + 1)), int(rng.integers(nmin, nmax + 1))
+        nsteps = max(2, int(round(int(rng.integers(2000, 6001)) * steps_scale)))
+        Lx, Lz = (nx - 1) * dx / 2, (nz - 1) * dx / 2
+        grid = Grid(xmin=-Lx, xmax=Lx, Nx=nx, zmin=-Lz, zmax=Lz, Nz=nz)
+        dt = time_step(grid, 0.5)
+        mats = []
+        for k in range(int(rng.integers(1, 21))):
+            cx, cz = rng.uniform(-0.8, 0.8) * Lx, rng.uniform(-0.8, 0.8) * Lz
+            a, b = rng.uniform(0.02, 0.25) * Lx, rng.uniform(0.02, 0.25) * Lz
+            geo = (lambda cx, cz, a, b: (lambda x, z: ((x - cx) / a) ** 2 + ((z - cz) / b) ** 2 <= 1))(cx, cz, a, b)
+            eps = float(rng.uniform(1, 12))
+            if rng.uniform() < 0.5:
+                chi = DebyeSusceptibility(deps=float(rng.uniform(1, 5)), tau=float(10 ** rng.uniform(-15, -13)))
+                mats.append(Material(geometry=geo, eps=eps, chi=chi))
+            else:
+                mats.append(Material(geometry=geo, eps=eps))
+        lam0 = float(rng.uniform(400e-9, 1600e-9))
+        sx, sz = rng.uniform(-0.5, 0.5) * Lx, rng.uniform(-0.5, 0.5) * Lz
+        src = SoftSource(geometry=(sx, sz), waveform=ricker(lam0), component="Ez")
+        mons = [FieldMonitor((float(rng.uniform(-0.7, 0.7) * Lx), float(rng.uniform(-0.7, 0.7) * Lz))) for _ in range(4)]
+        model = Model(grid, src, tmax=(nsteps - 0.5) * dt, pml=10 * dx, material=mats)
+        out.append((model, mons))
+    return out
+
