@@ -391,6 +391,66 @@ def run_batch2d(args):
     return out
 
 
+def run_serve(args):
+    """Served mixed stream: Poisson arrivals of 2-D and 3-D solves through the serving loop
+    (admission by device memory, continuous batching of 2-D requests, solo lanes for 3-D),
+    against the same requests solved one at a time."""
+    import maxwellfdtd_b200 as M
+    from maxwellfdtd_b200 import serve, workloads
+    ws, rank, local = dist_setup()
+    lib = M.load_library()
+    stream = workloads.served(n=args.requests, rate=args.rate, seed=args.seed, steps_scale=args.steps_scale)
+    reqs = [serve.Request(i, m, mo, a) for i, (a, m, mo) in enumerate(stream)]   # client-side descriptors
+    # warm-up: two small requests alone (loads the kernels)
+    for _, m, mo in workloads.served(n=2, seed=args.seed + 7, steps_scale=0.01, n2=(64, 96), n3=(24, 32)):
+        serve.solve_alone(lib, serve.Request(-1, m, mo, 0.0))
+    clk = ClockSampler(local).start()
+    srv = serve.Server(lib, device=local, budget_bytes=args.budget_gb * 1e9, max_active=args.slots,
+                       max_solo=args.solo_lanes, chunk=64)
+    t0 = time.time()
+    stats = srv.run(reqs)
+    clk.mark(t0, time.time())
+    clk.stop()
+    h2d = sum(sum(a.nbytes for a in r.builder.keep if isinstance(a, np.ndarray)) for r in reqs)
+    d2h = sum(sum(v.nbytes for v in r.out.values()) for r in reqs if r.out)
+    # the same kind of requests as sequential plain solves (a seeded subset, end to end each)
+    pick = np.random.default_rng(args.seed + 1).choice(len(reqs), min(args.seq_sims, len(reqs)), replace=False)
+    seq_t, seq_cu = 0.0, 0
+    for i in pick:
+        _, _, wall = serve.solve_alone(lib, reqs[i], fields=False)
+        seq_t += wall
+        seq_cu += reqs[i].cell_updates
+    seq_value = seq_cu / seq_t / 1e9
+    value = stats["gcell_updates_per_s"]
+    out = {
+        "metric": "Gcell-updates/s", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": 1,
+        "steps": int(sum(r.model.Nt for r in reqs)), "warmup": 2, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"served: {len(reqs)} requests, Poisson {args.rate}/s, 2-D sides 256-2048 / 3-D sides "
+                               f"64-256 (dx=10nm), 500-5000 steps x {args.steps_scale}, dielectric/Drude/Lorentz, "
+                               f"TFSF or soft plane source, spectral monitor 8-32 freq FP64",
+                   "budget_gb": args.budget_gb, "slots": args.slots, "solo_lanes": args.solo_lanes, "seed": args.seed,
+                   "parallelism": "one GPU: continuous batch of 2-D requests + concurrent solo lanes"},
+        "latency": {"p50_s": round(stats["latency_p50_s"], 4), "p99_s": round(stats["latency_p99_s"], 4),
+                    "queue_wait_p50_s": round(stats["queue_wait_p50_s"], 4),
+                    "queue_wait_p99_s": round(stats["queue_wait_p99_s"], 4)},
+        "e2e": {"value": round(value, 3), "unit": "Gcell-updates/s",
+                "h2d_bytes_per_step": int(h2d / max(1, sum(r.model.Nt for r in reqs))),
+                "d2h_bytes_per_step": int(d2h / max(1, sum(r.model.Nt for r in reqs))),
+                "includes": "every request from arrival: admission, upload, steps, read-back of its monitors (spectra)"},
+        "requests": {"batched": stats["batched"], "solo": stats["solo"], "errors": stats["errors"],
+                     "phase_sum_s": {k: round(v, 3) for k, v in stats["phase_sum_s"].items()},
+                     "makespan_s": round(stats["makespan_s"], 3), "cell_updates": stats["cell_updates"],
+                     "peak_device_gb": round(srv.peak_used / 1e9, 2), "peak_active": srv.peak_active},
+        "sequential": {"value": round(seq_value, 3), "unit": "Gcell-updates/s", "requests": len(pick),
+                       "note": "the same kind of requests solved one at a time, end to end (create, run, read-back of monitors)"},
+        "served_vs_sequential": round(value / seq_value, 2),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def plain_stepper(lib, args, device, steps=20):
     """The plain FP32 stepper at 256^3 (vacuum, 12-cell CPML, Sa sum): H and E update times
     and their HBM roofline fractions, CUDA events per update."""
@@ -486,10 +546,16 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-stepper roofline measurement")
-    ap.add_argument("--workload", default="plasmonics", choices=["plasmonics", "batch2d"])
+    ap.add_argument("--workload", default="plasmonics", choices=["plasmonics", "batch2d", "serve"])
+    ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate (1/s)")
+    ap.add_argument("--budget-gb", type=float, default=160.0, help="serve: device-memory admission budget")
+    ap.add_argument("--slots", type=int, default=64, help="serve: requests resident at once")
+    ap.add_argument("--solo-lanes", type=int, default=16, help="serve: concurrent solo lanes")
     ap.add_argument("--sims", type=int, default=256, help="batch2d: number of models")
-    ap.add_argument("--steps-scale", type=float, default=0.25, help="batch2d: scale of the 2000-6000 step counts")
-    ap.add_argument("--seq-sims", type=int, default=16, help="batch2d: models timed as sequential solves")
+    ap.add_argument("--steps-scale", type=float, default=None,
+                    help="batch2d / serve: scale of the step counts (default 0.25 / 0.25)")
+    ap.add_argument("--seq-sims", type=int, default=16, help="batch2d / serve: models timed as sequential solves")
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
@@ -499,7 +565,11 @@ def main():
             args.steps = 20   # each reference step is a full 256^3 step on the CPU
         run_reference(args)
     elif args.workload == "batch2d":
+        args.steps_scale = 0.25 if args.steps_scale is None else args.steps_scale
         run_batch2d(args)
+    elif args.workload == "serve":
+        args.steps_scale = 0.25 if args.steps_scale is None else args.steps_scale
+        run_serve(args)
     else:
         run_gpu(args)
 

@@ -12,6 +12,7 @@ MFD_OK, MFD_ERR_INVALID, MFD_ERR_OOM, MFD_ERR_CUDA, MFD_ERR_NONFINITE, MFD_ERR_T
 MFD_F32, MFD_F64 = 0, 1
 MFD_INT_SA, MFD_INT_E2, MFD_INT_JE, MFD_INT_RHO = range(4)
 MFD_RATE_NONE, MFD_RATE_POWER, MFD_RATE_TABLE = range(3)
+MFD_MON_FIELD, MFD_MON_SPECTRAL = range(2)
 
 _dp = C.POINTER(C.c_double)
 

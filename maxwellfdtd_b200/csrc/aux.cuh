@@ -75,10 +75,10 @@ __device__ __forceinline__ T tfsf_apply(const RectStmt& t, T v, T inc) {
 // Grid row blockIdx.y = statement.  A cell reached by several statements of the same
 // component (edges of the 3-D TFSF box) is updated by the thread of its first statement,
 // which applies all of them in statement order -- the order of the reference's broadcasts.
+// Point `local` of statement si at step it0 (0-based).
 template <typename T>
-__global__ void __launch_bounds__(256) tfsf_kernel(const __grid_constant__ RectParams<T> p) {
-    const RectStmt& s = p.s[blockIdx.y];
-    const int local = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void tfsf_point(const RectParams<T>& p, int si, int local, long long it0) {
+    const RectStmt& s = p.s[si];
     if (local >= s.len) return;
     const int nxr = s.x1 - s.x0 + 1, nyr = s.y1 - s.y0 + 1;
     const int rest = local / nxr;
@@ -90,12 +90,17 @@ __global__ void __launch_bounds__(256) tfsf_kernel(const __grid_constant__ RectP
         if (rect_has(p.s[__ffsll((long long)m) - 1], ix, iy, iz)) return;
     T* F = p.F[s.comp];
     const int c = ix + p.L.px * iy + p.L.sz * iz;
-    T v = tfsf_apply(s, F[c], p.arr[s.k][p.it0 * s.len + local]);
+    T v = tfsf_apply(s, F[c], p.arr[s.k][it0 * s.len + local]);
     for (unsigned long long m = s.next; m; m &= m - 1) {
         const RectStmt& t = p.s[__ffsll((long long)m) - 1];
-        if (rect_has(t, ix, iy, iz)) v = tfsf_apply(t, v, p.arr[t.k][p.it0 * t.len + rect_local(t, ix, iy, iz)]);
+        if (rect_has(t, ix, iy, iz)) v = tfsf_apply(t, v, p.arr[t.k][it0 * t.len + rect_local(t, ix, iy, iz)]);
     }
     F[c] = v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) tfsf_kernel(const __grid_constant__ RectParams<T> p) {
+    tfsf_point(p, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x, p.it0);
 }
 
 template <typename T>

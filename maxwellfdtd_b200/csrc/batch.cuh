@@ -22,9 +22,11 @@ enum { BF_MATH = 1, BF_MAT = 2, BF_FAST = 4 };
 struct BMember {
     const HParams<float>* hp;              // the member's update parameters (static fields)
     const EParams<float, double>* ep;
-    const MonParams<float>* mp;            // field monitors (gathered every step)
+    const MonParams<float>* mp;            // monitors (gathered every step)
+    const RectParams<float>* rp;           // TFSF statements (null: none)
     long long it;                          // step being run; > last once the member is done
     long long first, last;
+    long long ring_first;                  // 0-based step staged in ring slot 0
     int flags;                             // BF_*
     int pad;
 };
@@ -51,6 +53,10 @@ struct BSrc {       // one point source of a member (sources.jl:122-131, 235-244
 struct BPoint {     // point i of source s (entries of one source pass) or of monitor s
     int m, s;
     long long i;
+};
+
+struct BRow {       // TFSF statement s of member m (grid rows of one TFSF pass)
+    int m, s;
 };
 
 __device__ __forceinline__ bool b_active(const BMember& M) { return M.it <= M.last; }
@@ -136,7 +142,17 @@ __global__ void __launch_bounds__(256) batch_source_kernel(const BMember* __rest
     }
 }
 
-// Field monitors without sum: hist[k][it-1][j] = F_k[cells[j]] (monitor_gather_kernel).
+// TFSF injection of the members whose TFSF acts in this source pass: grid row = (member,
+// statement), as tfsf_kernel.
+__global__ void __launch_bounds__(256) batch_tfsf_kernel(const BMember* __restrict__ mem, const BRow* __restrict__ rows) {
+    const BRow r = rows[blockIdx.y];
+    const BMember& M = mem[r.m];
+    if (!b_active(M)) return;
+    tfsf_point(*M.rp, r.s, blockIdx.x * blockDim.x + threadIdx.x, M.it - 1);
+}
+
+// Monitor gather (monitor_gather_kernel): field monitors without sum to their history,
+// the others to the member's staging ring, slot = steps since ring_first.
 __global__ void __launch_bounds__(256) batch_gather_kernel(const BMember* __restrict__ mem, const BPoint* __restrict__ pts,
                                                            const int* __restrict__ npts) {
     const int n = *npts;
@@ -148,7 +164,12 @@ __global__ void __launch_bounds__(256) batch_gather_kernel(const BMember* __rest
         const MonDev<float>& D = p.mons[e.s];
         const long long it0 = M.it - 1;
         const int cell = D.cells[e.i];
-        for (int k = 0; k < p.ncomp; ++k) D.hist[((long long)k * p.nt + it0) * D.npts + e.i] = p.comp[k][cell];
+        if (D.kind == MFD_MON_FIELD && !D.sum) {
+            for (int k = 0; k < p.ncomp; ++k) D.hist[((long long)k * p.nt + it0) * D.npts + e.i] = p.comp[k][cell];
+        } else {
+            const long long slot = it0 - M.ring_first;
+            for (int k = 0; k < p.ncomp; ++k) D.ring[(slot * p.ncomp + k) * D.npts + e.i] = p.comp[k][cell];
+        }
     }
 }
 

@@ -92,6 +92,24 @@ static void bounded_sync(cudaStream_t st) {
 
 static long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
 
+// Device memory comes from the device's stream-ordered pool (cudaMallocAsync / cudaFreeAsync
+// on the owning stream): creating or destroying a model then never synchronises the whole
+// device, so models created and destroyed while others run (a serving loop) do not stall
+// them.  The pool keeps freed memory for reuse instead of returning it at each sync.
+static void retain_pool(int dev) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    done.push_back(dev);
+}
+
 // Staging buffer of mfd_read_integral_noalloc: a file-scope device array, so reading JE and
 // rho_end needs no device allocation at read time.  Shared by every handle on a device.
 static __device__ __align__(256) unsigned char g_read_scratch[MFD_NOALLOC_SCRATCH_BYTES];
@@ -153,9 +171,9 @@ class DivisorCache {
             const int n = (int)todo_d.size();
             float *dd = nullptr, *dr = nullptr;
             int* df = nullptr;
-            MFD_CK(cudaMalloc(&dd, n * sizeof(float)));
-            MFD_CK(cudaMalloc(&dr, n * sizeof(float)));
-            MFD_CK(cudaMalloc(&df, n * sizeof(int)));
+            MFD_CK(cudaMallocAsync(&dd, n * sizeof(float), st));
+            MFD_CK(cudaMallocAsync(&dr, n * sizeof(float), st));
+            MFD_CK(cudaMallocAsync(&df, n * sizeof(int), st));
             MFD_CK(cudaMemcpyAsync(dd, todo_d.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
             MFD_CK(cudaMemcpyAsync(dr, todo_r.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
             MFD_CK(cudaMemsetAsync(df, 0, n * sizeof(int), st));
@@ -163,10 +181,10 @@ class DivisorCache {
             MFD_CK(cudaGetLastError());
             std::vector<int> fails(n);
             MFD_CK(cudaMemcpyAsync(fails.data(), df, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+            cudaFreeAsync(dd, st);
+            cudaFreeAsync(dr, st);
+            cudaFreeAsync(df, st);
             MFD_CK(cudaStreamSynchronize(st));
-            cudaFree(dd);
-            cudaFree(dr);
-            cudaFree(df);
             for (int j = 0; j < n; ++j) {
                 uint32_t key;
                 std::memcpy(&key, &todo_d[j], 4);
@@ -284,7 +302,9 @@ class Engine : public HandleBase {
     bool need_ring = false;
 
     int* d_flags = nullptr;     // [nt] per-step NaN/Inf flags of Ex
-    int* h_flags = nullptr;     // pinned copy
+    int* h_flags = nullptr;     // host copy
+    std::vector<int> h_flags_v;
+    int h_timeout_v = 0;
 
     int64_t done = 0, bad_step = 0;
     int32_t bad_kind = 0;
@@ -315,14 +335,14 @@ class Engine : public HandleBase {
 
     ~Engine() override {
         cudaSetDevice(dev);
-        if (st) cudaStreamSynchronize(st);
-        for (void* p : allocs) cudaFree(p);
+        if (st) {
+            for (void* p : allocs) cudaFreeAsync(p, st);
+            cudaStreamSynchronize(st);
+        }
         for (auto e : ev_pool) cudaEventDestroy(e);
         for (auto& pe : pend) { cudaEventDestroy(pe.second.first); cudaEventDestroy(pe.second.second); }
         if (run_ev[0]) cudaEventDestroy(run_ev[0]);
         if (run_ev[1]) cudaEventDestroy(run_ev[1]);
-        if (h_flags) cudaFreeHost(h_flags);
-        if (h_timeout) cudaFreeHost(h_timeout);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -330,10 +350,10 @@ class Engine : public HandleBase {
     U* dalloc(size_t n) {
         if (n == 0) n = 1;
         void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, n * sizeof(U));
+        cudaError_t e = cudaMallocAsync(&p, n * sizeof(U), st);
         if (e != cudaSuccess) {
             cudaGetLastError();
-            throw Error(MFD_ERR_OOM, "cudaMalloc of " + std::to_string(n * sizeof(U)) + " bytes failed: " + cudaGetErrorString(e));
+            throw Error(MFD_ERR_OOM, "device allocation of " + std::to_string(n * sizeof(U)) + " bytes failed: " + cudaGetErrorString(e));
         }
         allocs.push_back(p);
         bytes += (int64_t)(n * sizeof(U));
@@ -376,6 +396,7 @@ class Engine : public HandleBase {
     void init(const mfd_desc* d) {
         dev = d->device;
         MFD_CK(cudaSetDevice(dev));
+        retain_pool(dev);
         MFD_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         MFD_CK(cudaEventCreate(&run_ev[0]));
         MFD_CK(cudaEventCreate(&run_ev[1]));
@@ -537,7 +558,8 @@ class Engine : public HandleBase {
         if (d->tfsf_record) init_record(d);
         init_monitors(d);
         d_flags = dalloc<int>((size_t)nt);
-        MFD_CK(cudaHostAlloc(&h_flags, (size_t)nt * sizeof(int), cudaHostAllocDefault));
+        h_flags_v.assign((size_t)nt, 0);
+        h_flags = h_flags_v.data();
         MFD_CK(cudaStreamSynchronize(st));
         const char* tune = std::getenv("MFD_TILE3D");
         if (tune) {
@@ -548,7 +570,7 @@ class Engine : public HandleBase {
         }
         init_split();
         d_timeout = dalloc<int>(1);
-        MFD_CK(cudaHostAlloc(&h_timeout, sizeof(int), cudaHostAllocDefault));
+        h_timeout = &h_timeout_v;
         init_tma();
     }
 
@@ -1367,26 +1389,33 @@ struct mfd_handle {
 // graph of `gsteps` steps, then retires it with the same end-of-run work as mfd_run.
 // ------------------------------------------------------------------------------------------
 template <typename U>
-struct DevBuf {
+struct DevBuf {   // a device table that grows; stream-ordered pool memory of the batch's stream
     U* p = nullptr;
     size_t cap = 0;
-    void reserve(size_t n) {
+    cudaStream_t st = nullptr;
+    void reserve(size_t n, cudaStream_t s) {
+        st = s;
         if (n <= cap) return;
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, st);
         p = nullptr;
         cap = 0;
         const size_t c = std::max<size_t>(n, 64);
-        if (cudaMalloc(&p, c * sizeof(U)) != cudaSuccess) {
+        if (cudaMallocAsync(&p, c * sizeof(U), st) != cudaSuccess) {
             cudaGetLastError();
             throw Error(MFD_ERR_OOM, "batch table allocation failed");
         }
         cap = c;
     }
-    void upload(const std::vector<U>& v, cudaStream_t st) {
-        reserve(v.size());
+    void upload(const std::vector<U>& v, cudaStream_t s) {
+        reserve(v.size(), s);
         if (!v.empty()) MFD_CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(U), cudaMemcpyHostToDevice, st));
     }
-    ~DevBuf() { if (p) cudaFree(p); }
+    void release() {
+        if (p && st) cudaFreeAsync(p, st);
+        p = nullptr;
+        cap = 0;
+    }
+    ~DevBuf() { release(); }
 };
 
 struct mfd_batch {
@@ -1399,6 +1428,7 @@ struct mfd_batch {
         HParams<float>* hp = nullptr;
         EParams<float, double>* ep = nullptr;
         MonParams<float>* mp = nullptr;
+        RectParams<float>* rp = nullptr;
         long long cells;
     };
     int dev = 0;
@@ -1413,6 +1443,8 @@ struct mfd_batch {
     DevBuf<BSrc> d_srcs;
     DevBuf<BPoint> d_mpts;
     std::vector<std::unique_ptr<DevBuf<BPoint>>> d_spass;
+    std::vector<std::unique_ptr<DevBuf<BRow>>> d_tpass;   // TFSF rows of source pass k
+    std::vector<int> tpass_n, tpass_len;
     DevBuf<int> d_counts;   // [0] tiles, [1] material tiles, [2] monitor points, [3 + k] points of source pass k
     int ntiles = 0, nmtiles = 0, nmpts = 0;
     std::vector<int> spass_n;
@@ -1436,23 +1468,29 @@ struct mfd_batch {
         if (st) cudaStreamSynchronize(st);
         if (gexec) cudaGraphExecDestroy(gexec);
         for (auto& m : mem) release(m);
+        d_mem.release(); d_tiles.release(); d_mtiles.release(); d_srcs.release(); d_mpts.release(); d_counts.release();
+        d_spass.clear();
+        d_tpass.clear();
+        if (st) cudaStreamSynchronize(st);
         for (auto e : ev) if (e) cudaEventDestroy(e);
         if (st) cudaStreamDestroy(st);
     }
 
-    static void release(Member& m) {
-        if (m.hp) cudaFree(m.hp);
-        if (m.ep) cudaFree(m.ep);
-        if (m.mp) cudaFree(m.mp);
-        m.hp = nullptr; m.ep = nullptr; m.mp = nullptr;
+    void release(Member& m) {
+        if (m.hp) cudaFreeAsync(m.hp, st);
+        if (m.ep) cudaFreeAsync(m.ep, st);
+        if (m.mp) cudaFreeAsync(m.mp, st);
+        if (m.rp) cudaFreeAsync(m.rp, st);
+        m.hp = nullptr; m.ep = nullptr; m.mp = nullptr; m.rp = nullptr;
         if (m.e) m.e->in_batch = false;
     }
 
     template <typename U>
     U* copy_struct(const U& v) {
         U* d = nullptr;
-        if (cudaMalloc(&d, sizeof(U)) != cudaSuccess) { cudaGetLastError(); throw Error(MFD_ERR_OOM, "batch member allocation failed"); }
-        MFD_CK(cudaMemcpy(d, &v, sizeof(U), cudaMemcpyHostToDevice));
+        if (cudaMallocAsync(&d, sizeof(U), st) != cudaSuccess) { cudaGetLastError(); throw Error(MFD_ERR_OOM, "batch member allocation failed"); }
+        MFD_CK(cudaMemcpyAsync(d, &v, sizeof(U), cudaMemcpyHostToDevice, st));
+        MFD_CK(cudaStreamSynchronize(st));   // the host copy is a temporary
         return d;
     }
 
@@ -1462,7 +1500,8 @@ struct mfd_batch {
         MFD_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         MFD_CK(cudaEventCreate(&ev[0]));
         MFD_CK(cudaEventCreate(&ev[1]));
-        d_counts.reserve(64);
+        retain_pool(dev);
+        d_counts.reserve(64, st);
     }
 
     int add(mfd_handle* h, long long last) {
@@ -1472,7 +1511,7 @@ struct mfd_batch {
         if (e->ndim != 2) { err = "batch members must be 2-D models"; return MFD_ERR_INVALID; }
         if (e->dev != dev) { err = "batch member on another device"; return MFD_ERR_INVALID; }
         if (e->in_batch) { err = "model already in a batch"; return MFD_ERR_INVALID; }
-        if (e->tfsf || e->record || e->need_ring) { err = "batch members support point sources and field monitors without sum (no TFSF, TFSF record, summed or spectral monitors)"; return MFD_ERR_INVALID; }
+        if (e->record) { err = "batch members cannot record TFSF data"; return MFD_ERR_INVALID; }
         if (e->bad_step) { err = "the model holds non-finite fields"; return MFD_ERR_NONFINITE; }
         if (last <= e->done || last > e->nt) { err = "the last step must be after the model's current step and within 1..Nt"; return MFD_ERR_INVALID; }
         MFD_CK(cudaSetDevice(dev));
@@ -1484,6 +1523,7 @@ struct mfd_batch {
             m.hp = copy_struct(e->hparams(0, 0));
             m.ep = copy_struct(e->eparams());
             m.mp = copy_struct(e->mon_p);
+            if (e->tfsf) m.rp = copy_struct(e->tfsf_p);
         } catch (...) {
             release(m);
             throw;
@@ -1503,11 +1543,13 @@ struct mfd_batch {
         std::vector<BMatTile> mt;
         std::vector<BSrc> srcs;
         std::vector<std::vector<BPoint>> passes;
+        std::vector<std::vector<BRow>> tpasses;
+        std::vector<int> tlen;
         std::vector<BPoint> mpts;
         for (size_t i = 0; i < mem.size(); ++i) {
             const Member& m = mem[i];
             E* e = m.e;
-            hm.push_back(BMember{m.hp, m.ep, m.mp, m.it, m.first, m.last, m.flags, 0});
+            hm.push_back(BMember{m.hp, m.ep, m.mp, m.rp, m.it, m.first, m.last, e->ring_first, m.flags, 0});
             const int mi = (int)i;
             for (int z = 0; z < e->nz; z += cur_tz)
                 for (int x = 0; x < e->nx; x += cur_tx) tiles.push_back(BTile{mi, x, z, 0});
@@ -1515,6 +1557,12 @@ struct mfd_batch {
                 const MatDev<float, double>& md = e->mats_host[g - 1];
                 for (int z = md.bz0; z < md.bz0 + md.bnz; ++z)
                     for (int x = md.bx0; x < md.bx0 + md.bnx; x += 128) mt.push_back(BMatTile{mi, g, x, z});
+            }
+            if (e->tfsf) {   // TFSF acts in source pass tfsf_order, before point source tfsf_order
+                const size_t k = (size_t)e->tfsf_order;
+                if (tpasses.size() <= k) { tpasses.resize(k + 1); tlen.resize(k + 1, 0); }
+                for (int q = 0; q < e->tfsf_p.n; ++q) tpasses[k].push_back(BRow{mi, q});
+                tlen[k] = std::max(tlen[k], (int)e->tfsf_maxlen);
             }
             for (size_t k = 0; k < e->srcs.size(); ++k) {
                 const auto& S = e->srcs[k];
@@ -1531,12 +1579,25 @@ struct mfd_batch {
         d_mtiles.upload(mt, st);
         d_srcs.upload(srcs, st);
         d_mpts.upload(mpts, st);
+        if (tpasses.size() > passes.size()) passes.resize(tpasses.size());
+        tpasses.resize(passes.size());
+        tlen.resize(passes.size(), 0);
         while (d_spass.size() < passes.size()) d_spass.emplace_back(new DevBuf<BPoint>());
+        while (d_tpass.size() < passes.size()) d_tpass.emplace_back(new DevBuf<BRow>());
         spass_n.assign(passes.size(), 0);
+        tpass_n.assign(passes.size(), 0);
+        tpass_len = tlen;
         for (size_t k = 0; k < passes.size(); ++k) {
             d_spass[k]->upload(passes[k], st);
             spass_n[k] = (int)passes[k].size();
+            d_tpass[k]->upload(tpasses[k], st);
+            tpass_n[k] = (int)tpasses[k].size();
+            if (tpass_n[k] > 65535) throw Error(MFD_ERR_INVALID, "too many TFSF statements in one batch pass");
         }
+        // graph length: at most the smallest staging ring of any member (rings are flushed between replays)
+        ring_cap = gsteps;
+        for (auto& m : mem)
+            if (m.e->need_ring) ring_cap = std::min(ring_cap, m.e->ring_k);
         if (passes.size() + 3 > 64) throw Error(MFD_ERR_INVALID, "batch members have at most 61 sources");
         std::vector<int> counts(3 + passes.size());
         ntiles = counts[0] = (int)tiles.size();
@@ -1556,9 +1617,12 @@ struct mfd_batch {
         return std::max(1, std::min(std::max(1, per_sm) * sms, work));
     }
 
+    int ring_cap = 16;          // steps per graph replay (gsteps, or less when a member's ring is shorter)
+
     int kernels_per_step() const {
         int k = 3 + (nmtiles ? 1 : 0) + (nmpts ? 1 : 0);
         for (int n : spass_n) k += n ? 1 : 0;
+        for (int n : tpass_n) k += n ? 1 : 0;
         return k;
     }
 
@@ -1572,8 +1636,10 @@ struct mfd_batch {
             batch_material2d_kernel<<<g, 128, 0, st>>>(d_mem.p, d_mtiles.p, d_counts.p + 1);
         }
         for (size_t k = 0; k < spass_n.size(); ++k) {
-            if (!spass_n[k]) continue;
-            batch_source_kernel<<<(spass_n[k] + 255) / 256, 256, 0, st>>>(d_mem.p, d_srcs.p, d_spass[k]->p, d_counts.p + 3 + k);
+            if (tpass_n[k])
+                batch_tfsf_kernel<<<dim3((unsigned)((tpass_len[k] + 255) / 256), tpass_n[k]), 256, 0, st>>>(d_mem.p, d_tpass[k]->p);
+            if (spass_n[k])
+                batch_source_kernel<<<(spass_n[k] + 255) / 256, 256, 0, st>>>(d_mem.p, d_srcs.p, d_spass[k]->p, d_counts.p + 3 + k);
         }
         if (nmpts) batch_gather_kernel<<<(nmpts + 255) / 256, 256, 0, st>>>(d_mem.p, d_mpts.p, d_counts.p + 2);
         batch_advance_kernel<<<((int)mem.size() + 255) / 256, 256, 0, st>>>(d_mem.p, (int)mem.size());
@@ -1583,13 +1649,31 @@ struct mfd_batch {
         if (gexec) { MFD_CK(cudaGraphExecDestroy(gexec)); gexec = nullptr; }
         cudaGraph_t g = nullptr;
         MFD_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        for (int i = 0; i < gsteps; ++i) launch_step();
+        for (int i = 0; i < ring_cap; ++i) launch_step();
         const cudaError_t ce = cudaStreamEndCapture(st, &g);
         if (ce != cudaSuccess) { cudaGetLastError(); throw Error(MFD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)); }
         const cudaError_t ie = cudaGraphInstantiate(&gexec, g, 0);
         cudaGraphDestroy(g);
         if (ie != cudaSuccess) { cudaGetLastError(); throw Error(MFD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie)); }
-        built_steps = gsteps;
+        built_steps = ring_cap;
+    }
+
+    // Before a replay of n steps: flush members whose staging ring cannot take n more steps,
+    // and start a new ring window where one is empty (its first slot is this step).
+    void prepare_rings(int n) {
+        for (size_t i = 0; i < mem.size(); ++i) {
+            Member& m = mem[i];
+            E* e = m.e;
+            if (!e->need_ring || m.it > m.last) continue;
+            if (e->ring_used > 0 && e->ring_used + n > e->ring_k) {
+                e->flush_monitors();
+                bounded_sync(e->st);
+            }
+            if (e->ring_used == 0 && e->ring_first != m.it - 1) {
+                e->ring_first = m.it - 1;
+                MFD_CK(cudaMemcpyAsync(&d_mem.p[i].ring_first, &e->ring_first, sizeof(long long), cudaMemcpyHostToDevice, st));
+            }
+        }
     }
 
     // Retire members whose window is done: the end-of-run work of mfd_run on their streams.
@@ -1618,11 +1702,13 @@ struct mfd_batch {
                     }
                 }
             }
-            if (dirty || built_steps != gsteps) rebuild();
+            if (dirty) rebuild();
+            const int gs = built_steps;
             long long active_cells = 0;
-            for (auto& m : mem) active_cells += m.cells * std::min<long long>(gsteps, m.last - m.it + 1);
-            const bool chunk = max_steps - done_steps >= gsteps;
-            const int n = chunk ? gsteps : (int)(max_steps - done_steps);
+            for (auto& m : mem) active_cells += m.cells * std::min<long long>(gs, m.last - m.it + 1);
+            const bool chunk = max_steps - done_steps >= gs;
+            const int n = chunk ? gs : (int)(max_steps - done_steps);
+            prepare_rings(n);
             MFD_CK(cudaEventRecord(ev[0], st));
             if (chunk) MFD_CK(cudaGraphLaunch(gexec, st));
             else for (int i = 0; i < n; ++i) launch_step();
@@ -1633,9 +1719,10 @@ struct mfd_batch {
             MFD_CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
             long long cu = 0;
             for (auto& m : mem) {
-                const long long adv = std::min<long long>(n, m.last - m.it + 1);
+                const long long adv = std::max<long long>(0, std::min<long long>(n, m.last - m.it + 1));
                 cu += m.cells * adv;
                 m.it += adv;
+                if (m.e->need_ring) m.e->ring_used += (int)adv;
             }
             dev_ms += ms;
             cell_updates += cu;

@@ -16,6 +16,12 @@ ellipses per domain with eps uniform in [1, 12] and, for half of them, a Debye p
 (deps uniform in [1, 5], tau log-uniform in [1e-15, 1e-13] s), a soft Ricker point source
 (lambda0 uniform in 400-1600 nm) and 4 point field monitors.
 
+served: a stream of solves of mixed kind for the serving loop -- Poisson arrivals; 2-D
+(sides uniform in [256, 2048]) or 3-D (sides uniform in [64, 256]) grids, 500-5000 steps
+(scaled by steps_scale); a random mix of dielectric, Drude and Lorentz spheres/discs; an
+x-polarised plane-wave TFSF source (2-D) or a soft plane source; spectral monitors at 8-32
+frequencies with FP64 sums on a line (2-D) or plane (3-D).
+
 dielectric_100: 100^3 grid, dx = 20 nm, 10-cell CPML, Float64, a dielectric sphere
 (radius 500 nm, eps = 2.25), a TFSF x-polarised Gaussian pulse (800 nm, 10 fs intensity
 FWHM) along +z, and one point monitor.
@@ -23,7 +29,7 @@ FWHM) along +z, and one point monitor.
 import numpy as np
 
 from . import (C0, EPS0, MU0, Grid, DebyeSusceptibility, DrudeSusceptibility, FieldMonitor, LorentzSusceptibility,
-               Material, Model, SoftSource, SpectralMonitor, TFSFSource)
+               Material, Model, SeparableWaveform, SoftSource, SpectralMonitor, TFSFSource)
 from .model import time_range, time_step
 from .sources import TFSF_NAMES_3D
 
@@ -108,6 +114,107 @@ def plasmonics_256(nt=4000, n=256, with_monitors=True):
         ]
         mons = [SpectralMonitor(fc, w=w) for fc in faces]
     return model, mons
+
+
+def _plane_wave_tfsf_2d(grid, i1, i2, t, f, zs, dt):
+    """2-D TFSF record data of an x-polarised plane wave along +z (the layout a record run
+    writes: knots x, z and per face [nt][knots])."""
+    eta0 = np.sqrt(MU0 / EPS0)
+    ix1, iz1 = i1[0], i1[2]
+    ix2, iz2 = i2[0], i2[2]
+    z, dz = grid.z, grid.dz
+    te = t + dt
+    th = t + dt / 2
+    Ex = lambda zv: f(te[:, None] - (np.asarray(zv)[None, :] - zs) / C0)
+    Hy = lambda zv: f(th[:, None] - (np.asarray(zv)[None, :] + dz / 2 - zs) / C0) / eta0
+    xk = grid.x[ix1 - 1:ix2]
+    zk = z[iz1 - 1:iz2]
+    nt = len(t)
+    d = {"t": np.asarray(t), "box": np.array([grid.x[ix1 - 1], grid.x[ix2 - 1], z[iz1 - 1], z[iz2 - 1]]),
+         "x": xk, "z": zk}
+    d["incHy_1z"] = Hy(zk).astype(np.float32)
+    d["incEz_1z"] = np.zeros((nt, len(zk)), np.float32)
+    d["incHy_2z"] = d["incHy_1z"]
+    d["incEz_2z"] = d["incEz_1z"]
+    d["incHy_x1"] = np.repeat(Hy(z[iz1 - 2:iz1 - 1]), len(xk), axis=1).astype(np.float32)
+    d["incEx_x1"] = np.repeat(Ex(z[iz1 - 1:iz1]), len(xk), axis=1).astype(np.float32)
+    d["incHy_x2"] = np.repeat(Hy(z[iz2 - 1:iz2]), len(xk), axis=1).astype(np.float32)
+    d["incEx_x2"] = np.repeat(Ex(z[iz2 - 1:iz2]), len(xk), axis=1).astype(np.float32)
+    return d
+
+
+def served(n=64, rate=200.0, seed=0, steps_scale=1.0, frac3d=0.5, n2=(256, 2048), n3=(64, 256)):
+    """List of (arrival_s, model, monitors) for the serving loop, arrivals in order."""
+    rng = np.random.default_rng(seed)
+    t_arr = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    out = []
+    for i in range(n):
+        three = rng.uniform() < frac3d
+        nsteps = max(2, int(round(int(rng.integers(500, 5001)) * steps_scale)))
+        nw = int(rng.integers(8, 33))
+        lam = np.linspace(400e-9, 900e-9, nw)
+        w = 2 * np.pi * C0 / lam
+        kinds = rng.integers(0, 3, size=int(rng.integers(1, 4)))
+        if three:
+            nn = [int(rng.integers(n3[0], n3[1] + 1)) for _ in range(3)]
+            dx = 10e-9
+            L = [(k - 1) * dx / 2 for k in nn]
+            grid = Grid(xmin=-L[0], xmax=L[0], Nx=nn[0], ymin=-L[1], ymax=L[1], Ny=nn[1], zmin=-L[2], zmax=L[2], Nz=nn[2])
+            rmax = 0.25 * min(L)
+            pos = lambda: [float(rng.uniform(-0.3, 0.3) * l) for l in L]
+        else:
+            nn = [int(rng.integers(n2[0], n2[1] + 1)) for _ in range(2)]
+            dx = 10e-9
+            L = [(k - 1) * dx / 2 for k in nn]
+            grid = Grid(xmin=-L[0], xmax=L[0], Nx=nn[0], zmin=-L[1], zmax=L[1], Nz=nn[1])
+            rmax = 0.25 * min(L)
+            pos = lambda: [float(rng.uniform(-0.3, 0.3) * l) for l in L]
+        dt = time_step(grid, 0.5)
+        mats = []
+        for k in kinds:
+            c = pos()
+            r = float(rng.uniform(0.2, 1.0) * rmax)
+            if three:
+                geo = (lambda c, r: (lambda x, y, z: (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 <= r * r))(c, r)
+            else:
+                geo = (lambda c, r: (lambda x, z: (x - c[0]) ** 2 + (z - c[1]) ** 2 <= r * r))(c, r)
+            if k == 0:
+                mats.append(Material(geometry=geo, eps=float(rng.uniform(1.5, 12))))
+            elif k == 1:
+                mats.append(Material(geometry=geo, eps=float(rng.uniform(1, 9)),
+                                     chi=DrudeSusceptibility(wp=float(rng.uniform(0.5e16, 1.5e16)), gamma=1.07e14)))
+            else:
+                mats.append(Material(geometry=geo, eps=float(rng.uniform(1, 4)),
+                                     chi=LorentzSusceptibility(deps=float(rng.uniform(0.5, 3)), w0=float(rng.uniform(2e15, 6e15)),
+                                                               delta=5e14)))
+        lam0 = float(rng.uniform(500e-9, 800e-9))
+        w0 = 2 * np.pi * C0 / lam0
+        tau = 5e-15
+        f = lambda s, w0=w0, tau=tau: np.exp(-2 * np.log(2) * (s - 3 * tau) ** 2 / tau ** 2) * np.cos(w0 * (s - 3 * tau))
+        pml = 10 * dx
+        m_in = 14
+        if not three and rng.uniform() < 0.5:
+            t = time_range(dt, (nsteps - 0.5) * dt)
+            i1 = (m_in, 1, m_in)
+            i2 = (nn[0] + 1 - m_in, 1, nn[1] + 1 - m_in)
+            data = _plane_wave_tfsf_2d(grid, i1, i2, t, f, grid.z[i1[2] - 1], dt)
+            src = TFSFSource(data=data)
+        else:
+            z0 = -L[-1] + (m_in + 2) * dx
+            if three:
+                src = SoftSource(geometry=lambda x, y, z, z0=z0: np.abs(z - z0) < dx / 2,
+                                 waveform=SeparableWaveform(lambda x, y, z: np.ones_like(x), f), component="Ex")
+            else:
+                src = SoftSource(geometry=lambda x, z, z0=z0: np.abs(z - z0) < dx / 2,
+                                 waveform=SeparableWaveform(lambda x, z: np.ones_like(x), f), component="Ex")
+        zm = L[-1] - (m_in + 2) * dx
+        if three:
+            mon = SpectralMonitor(lambda x, y, z, zm=zm: np.abs(z - zm) < dx / 2, w=w)
+        else:
+            mon = SpectralMonitor(lambda x, z, zm=zm: np.abs(z - zm) < dx / 2, w=w)
+        model = Model(grid, src, tmax=(nsteps - 0.5) * dt, pml=pml, material=mats)
+        out.append((float(t_arr[i]), model, [mon]))
+    return out
 
 
 def plain_256(nt=40, n=256):

@@ -191,3 +191,70 @@ def test_batch_rejects_and_guards(gpu_lib):
     batch.close()
     st.close()
     st3.close()
+
+
+def rich_member(seed):
+    """2-D member with a plane-wave TFSF source (at a seeded position among its point
+    sources), spectral monitors (per point and summed) and a summed field monitor."""
+    from maxwellfdtd_b200 import workloads
+    from maxwellfdtd_b200.model import time_range
+    rng = np.random.default_rng(100 + seed)
+    nx, nz = int(rng.integers(40, 160)), int(rng.integers(40, 160))
+    nsteps = int(rng.integers(20, 150))
+    g = C.grid2((nx, nz))
+    dt = 0.5 / C.C0 / np.sqrt(2 / (50e-9) ** 2)
+    t = time_range(dt, (nsteps - 0.5) * dt)
+    m_in = 6
+    i1, i2 = (m_in, 1, m_in), (nx + 1 - m_in, 1, nz + 1 - m_in)
+    f = lambda s: C.pulse(s)
+    data = workloads._plane_wave_tfsf_2d(g, i1, i2, t, f, g.z[i1[2] - 1], dt)
+    srcs = [M.TFSFSource(data=data)]
+    if seed % 2:
+        srcs.insert(0, M.SoftSource(geometry=(0.0, 0.0), waveform=lambda x, z, t: 10 * C.pulse(t), component="Ez"))
+    mat = M.Material(geometry=lambda x, z: x ** 2 + z ** 2 <= (300e-9) ** 2, eps=2.0,
+                     chi=M.LorentzSusceptibility(deps=1.1, w0=4.2e15, delta=5e14))
+    model = M.Model(g, srcs, tmax=(nsteps - 0.5) * dt, pml=100e-9, material=mat)
+    line = lambda x, z: np.abs(z - 200e-9) < 26e-9
+    mons = [M.SpectralMonitor(line, w=np.linspace(1e15, 4e15, int(rng.integers(8, 33)))),
+            M.SpectralMonitor(line, sum=True),
+            M.FieldMonitor(line, sum=True), M.FieldMonitor((0.0, 100e-9))]
+    return model, mons
+
+
+def outputs_rich(st, model, meta):
+    out = {f"field/{c}": st.read_field(comp_index(c)) for c in field_components(2)}
+    out["Sa"] = st.read_integral(_abi.MFD_INT_SA)
+    for k, mm in enumerate(meta["monitors"]):
+        spectral = mm["kind"] == 1
+        for c in ("Hy", "Ex", "Ez"):
+            if spectral:
+                shape = (mm["dft"].Nw,) if mm["sum"] else (mm["dft"].Nw, len(mm["cells"]))
+            else:
+                shape = (model.Nt,) if mm["sum"] else (model.Nt, len(mm["cells"]))
+            out[f"mon/{k}/{c}"] = st.read_monitor(k, comp_index(c), shape, spectral)
+    out["status"] = np.array(st.status())
+    return out
+
+
+@pytest.mark.parametrize("graph", [16, 64, 3])
+def test_batch_tfsf_and_staged_monitors_match_alone(graph, gpu_lib):
+    models = [rich_member(s) for s in range(6)] + [member_model(s) for s in range(3)]
+    ref = []
+    for m, mo in models:
+        st, b, meta = make(m, mo, gpu_lib)
+        st.run(1, m.Nt)
+        ref.append(outputs_rich(st, m, meta))
+        st.close()
+    batch = _abi.Batch(gpu_lib)
+    batch.config(0, 0, graph)
+    held = []
+    for m, mo in models:
+        st, b, meta = make(m, mo, gpu_lib)
+        batch.add(st, m.Nt)
+        held.append((st, b, meta, m))
+    batch.run_all(chunk=100)
+    for (st, b, meta, m), r in zip(held, ref):
+        same(r, outputs_rich(st, m, meta))
+    batch.close()
+    for st, *_ in held:
+        st.close()

@@ -1,0 +1,49 @@
+"""The serving loop on the GPU: each request's results in the mix (batched 2-D members and
+solo 3-D lanes, admitted as memory frees up) equal its results alone, bit for bit; the
+admission footprint bounds what mfd_create allocates."""
+import numpy as np
+import pytest
+
+import cases as C
+import maxwellfdtd_b200 as M
+from maxwellfdtd_b200 import _abi, serve, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def footprint_models():
+    out = [(C.model_materials(3), C.monitors(3)), (C.model_materials(2), C.monitors(2)),
+           (C.model_plasma(3, "table"), None), (C.model_bcs(1), C.monitors(1))]
+    out += [(m, mo) for _, m, mo in workloads.served(n=6, steps_scale=0.02, n2=(64, 160), n3=(24, 48), seed=7)]
+    out += workloads.batch2d(n=3, steps_scale=0.01, nmin=64, nmax=128)
+    return out
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_footprint_bounds_device_bytes(dtype, gpu_lib):
+    for model, mons in footprint_models():
+        b, meta = model.build_desc(dtype, mons)
+        est = serve.footprint(b, model, dtype)
+        st = _abi.Stepper(gpu_lib, b, dtype)
+        got = st.device_bytes()
+        st.close()
+        assert got <= est <= 1.1 * got + (1 << 20), (model.grid.ndim, got, est)
+
+
+def test_serve_mix_matches_alone(gpu_lib):
+    reqs = [serve.Request(i, m, mo, a) for i, (a, m, mo) in
+            enumerate(workloads.served(n=10, steps_scale=0.02, n2=(64, 160), n3=(24, 48), seed=3))]
+    k = len(reqs)
+    for j, (m, mo) in enumerate(workloads.batch2d(n=6, steps_scale=0.01, nmin=64, nmax=160, seed=4)):
+        reqs.append(serve.Request(k + j, m, mo, 0.004 * j))
+    assert any(r.batchable for r in reqs) and any(not r.batchable for r in reqs)
+    budget = 3 * max(r.bytes for r in reqs)
+    srv = serve.Server(gpu_lib, budget_bytes=budget, max_active=6, max_solo=3, chunk=16, read_fields=True)
+    st = srv.run(reqs)
+    assert st["errors"] == 0 and st["requests"] == len(reqs)
+    assert srv.peak_used <= budget
+    for r in reqs:
+        ref, status, _ = serve.solve_alone(gpu_lib, r)
+        assert tuple(r.status) == tuple(status)
+        bad = [key for key in ref if not np.array_equal(ref[key], r.out[key], equal_nan=True)]
+        assert not bad, (r.id, r.batchable, bad)
