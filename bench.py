@@ -31,6 +31,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# DRAM traffic of one E and one H update (core + slab kernels) of the 256^3 workload, from one
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum of the launches of one step)
+NCU_TRAFFIC_256 = {"E": 805_242_112, "H": 862_623_744}
+
 WORKLOAD = "plasmonics_256: 256^3 FP32, Drude+Lorentz sphere r=60nm, 12-cell CPML, TFSF 600nm/3fs, 6x DFT faces x 64 freq FP64"
 
 
@@ -256,10 +260,12 @@ def run_gpu(args):
                     "d2h_bytes_per_step": int(d2h / K), "includes": "mfd_create upload + K steps + read-back",
                     "host_setup_s_excluded": round(t_desc, 3)},
             "roofline": {"bound": "hbm", "kernel": "E update (e3d_core_kernel + e3d_slab_kernel)", "achieved": round(e_gbs, 1),
-                         "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4), "traffic": None,
+                         "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4),
+                         "traffic": NCU_TRAFFIC_256["E"] if args.n == 256 else None,
                          "algorithmic_bytes_per_launch": e_bytes, "mean_launch_ms": round(e_ms, 5),
                          "peak_kind": peak_kind,
                          "h_kernel": {"achieved": round(h_gbs, 1), "frac": round(h_gbs / peak, 4),
+                                      "traffic": NCU_TRAFFIC_256["H"] if args.n == 256 else None,
                                       "algorithmic_bytes_per_launch": h_bytes, "mean_launch_ms": round(h_ms, 5)}},
             "kernels": per_kernel,
             "plain_stepper": plain,
