@@ -13,7 +13,8 @@ TFSF injection, monitor gather; the DFT accumulation runs every 64 staged steps)
             spectra, wall-clock with the device synchronised.
   roofline: the dominant kernel pair (the E update: core rows + CPML slabs; the H update
             alongside), algorithmic bytes per update / its mean time from CUDA events around
-            each update in the timed region, against the measured HBM copy bandwidth.
+            each update, measured over the K steps after the timed ones (the timed steps
+            themselves carry no per-launch events), against the measured HBM copy bandwidth.
 
 Multi-GPU: replicas (the path does not shard); each rank runs the same workload on its own
 GPU, scaling "weak".  ``--impl reference`` times the CPU oracle (the restatement of the
@@ -173,7 +174,7 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     W, K = args.warmup, args.steps
-    nt = W + K + 2
+    nt = W + 2 * K + 2
     model, mons = workloads.plasmonics_256(nt=nt, n=args.n)
     dtype = np.float32
     lib = M.load_library()
@@ -187,14 +188,19 @@ def run_gpu(args):
     if ws > 1:
         dist.barrier()
         torch.cuda.synchronize()
-    st.set_profiling(True)
     t_w0 = time.time()
-    st.run(W + 1, W + K)        # timed: K steps, CUDA events on the library's stream
+    st.run(W + 1, W + K)        # timed: K steps in one call, CUDA events around it on the library's stream
     clk.mark(t_w0, time.time())
     clk.stop()
-    st.set_profiling(False)
     ms = st.last_run_ms()
     kt1 = st.kernel_times()
+    launches = int(sum(kt1[k][1] - kt0[k][1] for k in kt1))
+    # the next K steps again with an event pair around every launch: per-kernel device times
+    st.set_profiling(True)
+    st.run(W + K + 1, W + 2 * K)
+    st.set_profiling(False)
+    kt2 = st.kernel_times()
+    kt0, kt1 = kt1, kt2
     dev_bytes = st.device_bytes()
     st.close()
     ms_max = ms
@@ -203,7 +209,6 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_max = float(t.item())
     value = N * K * ws / (ms_max * 1e-3) / 1e9
-    launches = int(sum(kt1[k][1] - kt0[k][1] for k in kt1))
     h_bytes, e_bytes = algorithmic_bytes(model, meta, dtype)
     # one E update and one H update per step, each a core-rows kernel plus a CPML-slab kernel
     e_ms = (kt1["E"][0] - kt0["E"][0]) / K
@@ -457,6 +462,137 @@ def run_serve(args):
     return out
 
 
+def _rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    den = max(np.linalg.norm(a), np.linalg.norm(b))
+    return 0.0 if den == 0 else float(np.linalg.norm(a - b) / den)
+
+
+def _fields(st, ndim):
+    from maxwellfdtd_b200.sources import comp_index, field_components
+    return {c: st.read_field(comp_index(c)) for c in field_components(ndim) if not c.startswith("D")}
+
+
+def _timed_solve(lib, model, mons, dtype, W, K, local, profile_steps=0):
+    """Warm-up W steps, then steps W+1..W+K in one timed call, then profile_steps more with
+    per-launch events; returns (stepper, ms, meta, per-kernel ms per step)."""
+    from maxwellfdtd_b200 import _abi
+    b, meta = model.build_desc(dtype, mons, device=local)
+    st = _abi.Stepper(lib, b, dtype)
+    st.run(1, W)
+    st.run(W + 1, W + K)
+    ms = st.last_run_ms()
+    per = None
+    if profile_steps:
+        k0 = st.kernel_times()
+        st.set_profiling(True)
+        st.run(W + K + 1, W + K + profile_steps)
+        st.set_profiling(False)
+        k1 = st.kernel_times()
+        per = {k: round((k1[k][0] - k0[k][0]) / profile_steps * 1e3, 2) for k in k1 if k1[k][1] > k0[k][1]}
+    return st, ms, meta, per
+
+
+def run_config(args):
+    """The reference-style configurations other than the headline: `dielectric100` (100^3
+    FP64 dielectric sphere, TFSF data from a vacuum record run, 1000 steps) and `nonlinear`
+    (192 x 192 x 1024 FP32 glass with 3 Lorentz poles, Kerr and FP64 plasma).  Device
+    throughput and the error against the FP64 CPU oracle (the full configuration for
+    dielectric100; a 48 x 48 x 256 grid of the same medium, spacing and source for nonlinear)."""
+    import tempfile
+    import maxwellfdtd_b200 as M
+    from maxwellfdtd_b200 import _abi, workloads
+    ws, rank, local = dist_setup()
+    lib = M.load_library()
+    peak, kind = peaks()
+    oracle = _oracle_lib()
+    threads = oracle.lib.oracle_set_threads(0)
+    if args.workload == "dielectric100":
+        dtype = np.float64
+        rec_model, box, scatter = workloads.dielectric_100_record(nt=1000)
+        with tempfile.TemporaryDirectory() as tmp:
+            sol = M.solve(rec_model, backend=M.B200(dtype), tfsf_record=True, tfsf_box=box,
+                          tfsf_fname=os.path.join(tmp, "rec.npz"))
+        model, mons = scatter(sol.out["tfsf_record"])
+        W = args.warmup
+        K = model.Nt - W - 20
+        clk = ClockSampler(local).start()
+        t0 = time.time()
+        st, ms, meta, per = _timed_solve(lib, model, mons, dtype, W, K, local, profile_steps=20)
+        clk.mark(t0, time.time())
+        clk.stop()
+        gpu = _fields(st, 3)
+        gpu_mon = st.read_monitor(0, 6, (model.Nt, 1), False)
+        st.close()
+        # the FP64 oracle on the same descriptor, all steps
+        b, meta = model.build_desc(dtype, mons)
+        so = _abi.Stepper(oracle, b, dtype)
+        t = time.perf_counter()
+        so.run(1, model.Nt)
+        cpu_s = time.perf_counter() - t
+        ref = _fields(so, 3)
+        ref_mon = so.read_monitor(0, 6, (model.Nt, 1), False)
+        so.close()
+        err = {c: _rel_l2(gpu[c], ref[c]) for c in gpu}
+        err["monitor_Ex"] = _rel_l2(gpu_mon, ref_mon)
+        err_note = "full configuration, all 1000 steps, FP64 GPU vs FP64 oracle"
+        wl = "dielectric100: 100^3 FP64, dx=20nm, 10-cell CPML, sphere r=500nm eps=2.25, TFSF 800nm/10fs from a vacuum record run, 1000 steps"
+        cpu = {"value": round(model.grid.Nx * model.grid.Ny * model.grid.Nz * model.Nt / cpu_s / 1e9, 5),
+               "unit": "Gcell-updates/s", "cores": int(threads), "kind": "port", "sample": f"all {model.Nt} steps ({cpu_s:.1f} s)"}
+    else:
+        dtype = np.float32
+        W, K = args.warmup, args.steps
+        model, mons = workloads.nonlinear_192(nt=W + K + 22)
+        clk = ClockSampler(local).start()
+        t0 = time.time()
+        st, ms, meta, per = _timed_solve(lib, model, mons, dtype, W, K, local, profile_steps=20)
+        clk.mark(t0, time.time())
+        clk.stop()
+        st.close()
+        # error: the same medium, spacing and source on a 48 x 48 x 256 grid, GPU FP32 vs oracle FP64
+        n_small, steps_small = (48, 48, 256), args.err_steps
+        small, _ = workloads.nonlinear_192(nt=steps_small, n=n_small)
+        out = {}
+        cpu_s = None
+        for tag, lib_, dt_ in (("gpu", lib, np.float32), ("fp64", oracle, np.float64), ("fp32", oracle, np.float32)):
+            b, meta = small.build_desc(dt_, None)
+            sx = _abi.Stepper(lib_, b, dt_)
+            t = time.perf_counter()
+            sx.run(1, small.Nt)
+            if tag == "fp64":
+                cpu_s = time.perf_counter() - t
+            out[tag] = {**_fields(sx, 3), "rho_end": sx.read_integral(_abi.MFD_INT_RHO)}
+            sx.close()
+        vec = lambda o, cs: np.concatenate([np.asarray(o[c], np.float64).ravel() for c in cs])
+        groups = {"E": ("Ex", "Ey", "Ez"), "H": ("Hx", "Hy", "Hz"), "rho_end": ("rho_end",)}
+        err = {g: _rel_l2(vec(out["gpu"], cs), vec(out["fp64"], cs)) for g, cs in groups.items()}
+        err["oracle_fp32_vs_fp64"] = {g: _rel_l2(vec(out["fp32"], cs), vec(out["fp64"], cs)) for g, cs in groups.items()}
+        err["gpu_vs_fp32_oracle"] = {g: _rel_l2(vec(out["gpu"], cs), vec(out["fp32"], cs)) for g, cs in groups.items()}
+        err_note = f"{n_small[0]}x{n_small[1]}x{n_small[2]} grid of the same configuration, {steps_small} steps, FP32 GPU (rho FP64) vs FP64 oracle"
+        wl = ("nonlinear: 192x192x1024 FP32, dx=dy=100nm dz=20nm, 16-cell CPML, glass: 3 Sellmeier Lorentz poles + Kerr "
+              "n2=2.5e-20 + 8-photon plasma (rho FP64), Gaussian beam w0=3um 800nm 30fs 5e17 W/m^2")
+        Ns = n_small[0] * n_small[1] * n_small[2]
+        cpu = {"value": round(Ns * steps_small / cpu_s / 1e9, 5), "unit": "Gcell-updates/s", "cores": int(threads),
+               "kind": "port", "sample": f"FP64 oracle, {steps_small} steps of the {n_small} grid ({cpu_s:.1f} s)"}
+    N = model.grid.Nx * model.grid.Ny * model.grid.Nz
+    value = N * K / (ms * 1e-3) / 1e9
+    h_bytes, e_bytes = algorithmic_bytes(model, meta, dtype)
+    achieved = (h_bytes + e_bytes) / (ms * 1e-3 / K) / 1e9
+    out = {"metric": "Gcell-updates/s", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": 1, "steps": K,
+           "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if dtype == np.float64 else "f32", "data": "synthetic",
+           "config": {"workload": wl, "grid": [model.grid.Nx, model.grid.Ny, model.grid.Nz], "cells": N},
+           "roofline": {"bound": "hbm", "kernel": "whole step (H + E updates, material response, sources, monitors)",
+                        "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                        "traffic": None, "algorithmic_bytes_per_step": int(h_bytes + e_bytes), "peak_kind": kind},
+           "kernels_us_per_step": per,
+           "error_vs_fp64_oracle": {"rel_l2": err, "how": err_note},
+           "cpu_baseline": cpu, "clocks": clk.summary()}
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def plain_stepper(lib, args, device, steps=20):
     """The plain FP32 stepper at 256^3 (vacuum, 12-cell CPML, Sa sum): H and E update times
     and their HBM roofline fractions, CUDA events per update."""
@@ -552,7 +688,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-stepper roofline measurement")
-    ap.add_argument("--workload", default="plasmonics", choices=["plasmonics", "batch2d", "serve"])
+    ap.add_argument("--workload", default="plasmonics", choices=["plasmonics", "batch2d", "serve", "dielectric100", "nonlinear"])
+    ap.add_argument("--err-steps", type=int, default=300, help="nonlinear: steps of the oracle comparison")
     ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--budget-gb", type=float, default=160.0, help="serve: device-memory admission budget")
@@ -573,6 +710,8 @@ def main():
     elif args.workload == "batch2d":
         args.steps_scale = 0.25 if args.steps_scale is None else args.steps_scale
         run_batch2d(args)
+    elif args.workload in ("dielectric100", "nonlinear"):
+        run_config(args)
     elif args.workload == "serve":
         args.steps_scale = 0.25 if args.steps_scale is None else args.steps_scale
         run_serve(args)

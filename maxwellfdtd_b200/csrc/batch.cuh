@@ -120,7 +120,15 @@ __global__ void __launch_bounds__(128) batch_material2d_kernel(const BMember* __
         if (p.geom[c] != tl.g) continue;
         float Dv[2] = {p.Dx[c], p.Dz[c]};
         float* Ep[2] = {p.Ex, p.Ez};
-        material_cell<float, double, 2>(m, ix, 0, tl.iz, Ep, c, Dv, (int)((M.it - 1) & 1), p.dt);
+        const int cur = (int)((M.it - 1) & 1);
+        const long long bi = (long long)(ix - m->bx0) + (long long)m->bnx * (tl.iz - m->bz0);
+        switch (m->nq) {
+            case 0: material_cell_n<float, double, 2, 0>(m, bi, Ep, c, Dv, cur, p.dt); break;
+            case 1: material_cell_n<float, double, 2, 1>(m, bi, Ep, c, Dv, cur, p.dt); break;
+            case 2: material_cell_n<float, double, 2, 2>(m, bi, Ep, c, Dv, cur, p.dt); break;
+            case 3: material_cell_n<float, double, 2, 3>(m, bi, Ep, c, Dv, cur, p.dt); break;
+            default: material_cell<float, double, 2>(m, ix, 0, tl.iz, Ep, c, Dv, cur, p.dt); break;
+        }
     }
 }
 

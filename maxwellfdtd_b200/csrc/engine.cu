@@ -1090,10 +1090,16 @@ class Engine : public HandleBase {
                 if (any_geom) { if (fastdiv) launch_E_t<true, true>(p); else launch_E_t<true, false>(p); }
                 else { if (fastdiv) launch_E_t<false, true>(p); else launch_E_t<false, false>(p); }
             });
-        // E of dispersive / plasma / Kerr cells (material_kernel)
+        // E of dispersive / plasma / Kerr cells: material_flat_kernel for up to 3 poles,
+        // material_kernel (poles in a runtime loop) beyond
         for (int g : response_mats) {
             const MatDev<T, R>& m = mats_host[g - 1];
             launch(KC_MAT, [&] {
+                if (m.nq <= 3 && ndim >= 2) {
+                    if (ndim == 3) launch_mat_flat<3>(g, m, cur);
+                    else launch_mat_flat<2>(g, m, cur);
+                    return;
+                }
                 dim3 grd((m.bnx + 127) / 128, m.bny, m.bnz);
                 if (ndim == 3)
                     material_kernel<T, R, 3><<<grd, 128, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], F[MFD_DY], F[MFD_DZ],
@@ -1105,6 +1111,19 @@ class Engine : public HandleBase {
                     material_kernel<T, R, 1><<<grd, 128, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], nullptr, nullptr,
                                                                   F[MFD_EX], nullptr, nullptr, cur, dt);
             });
+        }
+    }
+
+    template <int NC>
+    void launch_mat_flat(int g, const MatDev<T, R>& m, int cur) {
+        const unsigned blocks = (unsigned)((m.bsize + 255) / 256);
+        T* Dy = NC == 3 ? F[MFD_DY] : nullptr;
+        T* Ey = NC == 3 ? F[MFD_EY] : nullptr;
+        switch (m.nq) {
+            case 0: material_flat_kernel<T, R, NC, 0><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], Dy, F[MFD_DZ], F[MFD_EX], Ey, F[MFD_EZ], cur, dt); break;
+            case 1: material_flat_kernel<T, R, NC, 1><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], Dy, F[MFD_DZ], F[MFD_EX], Ey, F[MFD_EZ], cur, dt); break;
+            case 2: material_flat_kernel<T, R, NC, 2><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], Dy, F[MFD_DZ], F[MFD_EX], Ey, F[MFD_EZ], cur, dt); break;
+            default: material_flat_kernel<T, R, NC, 3><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], Dy, F[MFD_DZ], F[MFD_EX], Ey, F[MFD_EZ], cur, dt); break;
         }
     }
 

@@ -298,4 +298,108 @@ __device__ __forceinline__ void material_cell(const MatDev<T, R>* __restrict__ m
     }
 }
 
+// material_cell with the number of poles NQ known at compile time: every load of the cell
+// (E^n, both polarisation buffers of every pole, the plasma state) is issued before any
+// store, so the poles do not become dependent round trips to memory.  The arithmetic is
+// material_cell's, expression for expression.  bi is the cell's index in the material's box.
+template <typename T, typename R, int NC, int NQ>
+__device__ __forceinline__ void material_cell_n(const MatDev<T, R>* __restrict__ m, long long bi,
+                                                T* const* E, long long c, const T* Dv, int cur, T dt) {
+    const T Me = m->Me;
+    const bool plasma = m->plasma != 0;
+    const long long bs = m->bsize;
+    T sumP[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) sumP[k] = T(0);
+    T En[NC];
+    if (NQ > 0 || plasma) {
+#pragma unroll
+        for (int k = 0; k < NC; ++k) En[k] = E[k][c];
+    }
+    constexpr int NQ1 = NQ > 0 ? NQ : 1;
+    T pn[NQ1][NC], pm[NQ1][NC];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            pn[q][k] = m->P[((long long)(cur * NQ + q) * NC + k) * bs + bi];
+            pm[q][k] = m->P[((long long)((1 - cur) * NQ + q) * NC + k) * bs + bi];
+        }
+    R rho = R(0), drho = R(0);
+    T Ppn[NC], Ppm[NC], Pav[NC], JEv = T(0);
+    if (plasma) {
+        rho = m->rho[bi];
+        drho = m->drho[bi];
+        JEv = m->JE[bi];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            Ppn[k] = m->Pp[((long long)cur * NC + k) * bs + bi];
+            Ppm[k] = m->Pp[((long long)(1 - cur) * NC + k) * bs + bi];
+            Pav[k] = m->Pa[(long long)k * bs + bi];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        const T Aq = m->Aq[q], Bq = m->Bq[q], Cq = m->Cq[q];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            const T pnew = Aq * pn[q][k] + Bq * pm[q][k] + Cq * En[k];
+            m->P[((long long)((1 - cur) * NQ + q) * NC + k) * bs + bi] = pnew;
+            sumP[k] += pnew;
+        }
+    }
+    if (plasma) {
+        T E2 = En[0] * En[0];
+#pragma unroll
+        for (int k = 1; k < NC; ++k) E2 = E2 + En[k] * En[k];
+        T II = m->ksi * E2;
+        T Ppnew[NC];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            Ppnew[k] = m->Ap * Ppn[k] + m->Bp * Ppm[k] + m->Cp * rho * m->rho0 * En[k];
+            m->Pp[((long long)(1 - cur) * NC + k) * bs + bi] = Ppnew[k];
+        }
+#pragma unroll
+        for (int k = 0; k < NC; ++k) sumP[k] += Ppnew[k];
+        T invE2 = (E2 >= Eps<T>::v()) ? T(1) / E2 : T(0);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            T v = Pav[k] + m->Ma * drho * m->rho0 * En[k] * invE2;
+            m->Pa[(long long)k * bs + bi] = v;
+            sumP[k] += v;
+        }
+        if (m->rate_kind == MFD_RATE_TABLE) {
+            T R1 = rate_table<T>(m->rate_x, m->rate_y, m->rate_n, II);
+            plasma_density<T, R, T>(rho, drho, R1, m->Rava * E2, dt);
+        } else if (m->rate_kind == MFD_RATE_POWER) {
+            T lg = log10(II);
+            T a = m->rate_order * lg;
+            double R1 = pow(10.0, (double)a + m->rate_log10c);
+            plasma_density<T, R, double>(rho, drho, R1, m->Rava * E2, dt);
+        } else {
+            plasma_density<T, R, T>(rho, drho, T(0), m->Rava * E2, dt);
+        }
+        m->rho[bi] = rho;
+        m->drho[bi] = drho;
+        T acc = (Ppnew[0] - Ppm[0]) / (2 * dt) * En[0];
+#pragma unroll
+        for (int k = 1; k < NC; ++k) acc = acc + (Ppnew[k] - Ppm[k]) / (2 * dt) * En[k];
+        m->JE[bi] = JEv + acc * dt;
+    }
+    if (m->kerr) {
+        const T Mk2 = m->Mk2, Mk3 = m->Mk3;
+        const T Me2 = Me * Me, Me3 = Me * Me * Me;
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            T X = Dv[k] - sumP[k];
+            T X2 = X * X;
+            E[k][c] = (1 + 1 * Mk2 * Me2 * X + 2 * Mk3 * Me3 * X2) /
+                      (1 + 2 * Mk2 * Me2 * X + 3 * Mk3 * Me3 * X2) * X * Me;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NC; ++k) E[k][c] = (Dv[k] - sumP[k]) * Me;
+    }
+}
+
 }  // namespace mfd

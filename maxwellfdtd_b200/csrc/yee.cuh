@@ -815,6 +815,39 @@ __global__ void __launch_bounds__(128) material_kernel(const MatDev<T, R>* __res
     material_cell<T, R, NC>(m, ix, iy, iz, Ep, c, Dv, cur, dt);
 }
 
+// The same with the box flattened (one thread per box cell, full warps whatever the box's
+// width) and the number of poles NQ known at compile time (material_cell_n).
+template <typename T, typename R, int NC, int NQ>
+__global__ void __launch_bounds__(256) material_flat_kernel(const MatDev<T, R>* __restrict__ mats, int g,
+                                                           const uint8_t* __restrict__ geom, Layout L,
+                                                           const T* D0, const T* D1, const T* D2, T* E0, T* E1, T* E2,
+                                                           int cur, T dt) {
+    const MatDev<T, R>* m = mats + (g - 1);
+    const long long bi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (bi >= m->bsize) return;
+    const int bnx = m->bnx, bny = m->bny;
+    const long long row = bi / bnx;
+    const int bx = (int)(bi - row * bnx);
+    const long long bz = row / bny;
+    const int by = (int)(row - bz * bny);
+    const int ix = m->bx0 + bx, iy = m->by0 + by, iz = m->bz0 + (int)bz;
+    const int c = ix + L.px * iy + L.sz * iz;
+    if (geom[c] != g) return;
+    T Dv[NC];
+    T* Ep[NC];
+    if (NC == 3) {
+        Dv[0] = D0[c]; Dv[1 % NC] = D1[c]; Dv[2 % NC] = D2[c];
+        Ep[0] = E0; Ep[1 % NC] = E1; Ep[2 % NC] = E2;
+    } else if (NC == 2) {
+        Dv[0] = D0[c]; Dv[1 % NC] = D2[c];
+        Ep[0] = E0; Ep[1 % NC] = E2;
+    } else {
+        Dv[0] = D0[c];
+        Ep[0] = E0;
+    }
+    material_cell_n<T, R, NC, NQ>(m, bi, Ep, c, Dv, cur, dt);
+}
+
 // Running sums and NaN/Inf guard for the last step of a run (the H kernel of the next step
 // does this for every other step).
 template <typename T>

@@ -16,6 +16,14 @@ ellipses per domain with eps uniform in [1, 12] and, for half of them, a Debye p
 (deps uniform in [1, 5], tau log-uniform in [1e-15, 1e-13] s), a soft Ricker point source
 (lambda0 uniform in 400-1600 nm) and 4 point field monitors.
 
+nonlinear_192: 192 x 192 x 1024 grid, dx = dy = 100 nm, dz = 20 nm, 16-cell CPML, FP32 with the
+plasma density in FP64; the whole domain is a fused-silica-like glass: eps_inf = 1 and three
+Lorentz poles from Malitson's Sellmeier fit (deps = B_i, w0 = 2 pi c / sqrt(C_i), small
+damping), Kerr n2 = 2.5e-20 m^2/W (chi3 = 4/3 n0^2 eps0 c n2), an 8-photon ionisation
+plasma (rate sigma8 I^8 with sigma8 = 1e-130, rho0 = 2.1e28 m^-3, collision time 1 fs,
+Ui = 9 eV); a soft Gaussian-beam source (w0 = 3 um, 800 nm, 30 fs, 5e17 W/m^2) on a plane
+near the low-z face.
+
 served: a stream of solves of mixed kind for the serving loop -- Poisson arrivals; 2-D
 (sides uniform in [256, 2048]) or 3-D (sides uniform in [64, 256]) grids, 500-5000 steps
 (scaled by steps_scale); a random mix of dielectric, Drude and Lorentz spheres/discs; an
@@ -215,6 +223,62 @@ def served(n=64, rate=200.0, seed=0, steps_scale=1.0, frac3d=0.5, n2=(256, 2048)
         model = Model(grid, src, tmax=(nsteps - 0.5) * dt, pml=pml, material=mats)
         out.append((float(t_arr[i]), model, [mon]))
     return out
+
+
+def nonlinear_192(nt=12000, n=(192, 192, 1024)):
+    from .materials import Plasma, PowerLawRate
+    nx, ny, nz = n
+    dx, dz = 100e-9, 20e-9
+    Lx, Ly, Lz = (nx - 1) * dx / 2, (ny - 1) * dx / 2, (nz - 1) * dz / 2
+    grid = Grid(xmin=-Lx, xmax=Lx, Nx=nx, ymin=-Ly, ymax=Ly, Ny=ny, zmin=-Lz, zmax=Lz, Nz=nz)
+    dt = time_step(grid, 0.5)
+    sellmeier = ((0.6961663, 0.0684043e-6), (0.4079426, 0.1162414e-6), (0.8974794, 9.896161e-6))
+    chi = [LorentzSusceptibility(deps=B, w0=2 * np.pi * C0 / lam, delta=1e12) for B, lam in sellmeier]
+    n0 = 1.45
+    chi3 = 4 / 3 * n0 ** 2 * EPS0 * C0 * 2.5e-20
+    lam0 = 800e-9
+    w0 = 2 * np.pi * C0 / lam0
+    plasma = Plasma(ionrate=PowerLawRate(order=8, sigma=1e-130), rho0=2.1e28, nuc=1 / 1e-15, frequency=w0, Uiev=9.0,
+                    mr=0.64)
+    glass = Material(geometry=lambda x, y, z: np.ones_like(x, dtype=bool), eps=1.0, chi=chi, chi3=chi3, plasma=plasma)
+    I0, tau, wb = 5e17, 30e-15, 3e-6
+    E0 = np.sqrt(2 * I0 / (n0 * EPS0 * C0))
+    t0 = 2 * tau
+    pulse = lambda t: np.exp(-2 * np.log(2) * (t - t0) ** 2 / tau ** 2) * np.cos(w0 * (t - t0))
+    zs = -Lz + (16 + 4) * dz
+    src = SoftSource(geometry=lambda x, y, z: np.abs(z - zs) < dz / 2,
+                     waveform=SeparableWaveform(lambda x, y, z: E0 * np.exp(-(x ** 2 + y ** 2) / wb ** 2), pulse),
+                     component="Ex")
+    pml = (16 * dx, 16 * dx, 16 * dx, 16 * dx, 16 * dz, 16 * dz)
+    return Model(grid, src, tmax=(nt - 0.5) * dt, pml=pml, material=glass), None
+
+
+def dielectric_100_record(nt=1000, n=100):
+    """The dielectric_100 configuration with its TFSF data made the reference's way: a
+    vacuum run with a soft Ex plane source, periodic in x and y, absorbing in z, records the
+    incident fields on the box (returns the record model and a function that builds the
+    scattering model from the recorded data)."""
+    dx = 20e-9
+    L = (n - 1) * dx / 2
+    grid = Grid(xmin=-L, xmax=L, Nx=n, ymin=-L, ymax=L, Ny=n, zmin=-L, zmax=L, Nz=n)
+    dt = time_step(grid, 0.5)
+    fwhm = 10e-15
+    t0 = 3 * fwhm
+    w0 = 2 * np.pi * C0 / 800e-9
+    f = lambda s: np.exp(-2 * np.log(2) * (s - t0) ** 2 / fwhm ** 2) * np.cos(w0 * (s - t0))
+    zs = -L + 12 * dx
+    src = SoftSource(geometry=lambda x, y, z: np.abs(z - zs) < dx / 2,
+                     waveform=SeparableWaveform(lambda x, y, z: np.ones_like(x), f), component="Ex")
+    record = Model(grid, src, tmax=(nt - 0.5) * dt, pml=(0, 0, 0, 0, 10 * dx, 10 * dx))
+    m = 11
+    box = (grid.x[m - 1], grid.x[n - m], grid.y[m - 1], grid.y[n - m], grid.z[m - 1], grid.z[n - m])
+
+    def scatter(data):
+        r = 500e-9
+        mat = Material(geometry=lambda x, y, z: x * x + y * y + z * z <= r * r, eps=2.25)
+        return Model(grid, TFSFSource(data=data), tmax=(nt - 0.5) * dt, pml=10 * dx, material=mat), \
+            [FieldMonitor((0.0, 0.0, 0.0))]
+    return record, box, scatter
 
 
 def plain_256(nt=40, n=256):

@@ -169,6 +169,22 @@ def model_layers(n, pml, nsteps=40):
     return M.Model(g, src, tmax=(nsteps - 0.5) * dt, pml=faces, material=m1)
 
 
+def model_poles(ndim, npoles, kerr=False, nsteps=50):
+    """A ball with npoles dispersion poles (Lorentz/Drude/Debye in turn), optionally Kerr,
+    overlapping a slab with one pole: the material kernels by pole count."""
+    g = _grid(ndim)
+    src = M.SoftSource(geometry=_plane(ndim, -250e-9), waveform=_src_wave(ndim, 3e8), component="Ex")
+    dt = 0.5 / C0 / np.sqrt(ndim / (50e-9) ** 2)
+    kinds = [lambda i: M.LorentzSusceptibility(deps=0.5 + 0.2 * i, w0=(3 + i) * 1e15, delta=(1 + i) * 1e14),
+             lambda i: M.DrudeSusceptibility(wp=(1 + 0.1 * i) * 1e16, gamma=1.07e14),
+             lambda i: M.DebyeSusceptibility(deps=1.0 + i, tau=(1 + i) * 1e-14)]
+    chi = [kinds[i % 3](i) for i in range(npoles)]
+    m1 = M.Material(geometry=_ball(ndim, 200e-9), eps=2.0, chi=chi, chi3=1e-19 if kerr else None)
+    slab = (lambda x, y, z: z >= 200e-9) if ndim == 3 else ((lambda x, z: z >= 200e-9) if ndim == 2 else (lambda z: z >= 300e-9))
+    m2 = M.Material(geometry=slab, eps=1.5, chi=M.LorentzSusceptibility(deps=0.7, w0=5e15, delta=2e14))
+    return M.Model(g, src, tmax=(nsteps - 0.5) * dt, pml=150e-9, material=[m1, m2])
+
+
 def monitors(ndim):
     pt = _geo_point(ndim, (0.0, 0.0, 100e-9))
     plane = _plane(ndim, 150e-9)

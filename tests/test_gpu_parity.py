@@ -151,6 +151,17 @@ def test_parity_unsplit_3d(builder, monkeypatch, oracle_lib, gpu_lib):
     _compare(ref, got, np.float32, exact=True)
 
 
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("ndim", [1, 2, 3])
+@pytest.mark.parametrize("npoles,kerr", [(3, True), (3, False), (5, True)])
+def test_parity_pole_counts(npoles, kerr, ndim, dtype, oracle_lib, gpu_lib):
+    """Three poles (the compile-time pole-count kernels) and five (the runtime loop)."""
+    model = C.model_poles(ndim, npoles, kerr)
+    ref = C.run_all(model, oracle_lib, dtype)
+    got = C.run_all(model, gpu_lib, dtype)
+    _compare(ref, got, dtype, exact=True)
+
+
 @pytest.mark.parametrize("ndim", [2, 3])
 def test_chunked_runs_equal_single_run(ndim, gpu_lib):
     """Splitting a run into several mfd_run calls changes nothing (the deferred Sa/E2
