@@ -153,6 +153,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(inside)}
 
 
+def max_over_ranks(value, ws):
+    """The largest of `value` over the ranks (the job's time is its slowest rank's)."""
+    if ws <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -175,7 +187,7 @@ def run_gpu(args):
                                 device_id=torch.device("cuda", local))
     W, K = args.warmup, args.steps
     nt = W + 2 * K + 2
-    model, mons = workloads.plasmonics_256(nt=nt, n=args.n)
+    model, mons = workloads.plasmonics_256(nt=nt, n=args.size)
     dtype = np.float32
     lib = M.load_library()
     b, meta = model.build_desc(dtype, mons, device=local)
@@ -203,11 +215,7 @@ def run_gpu(args):
     kt0, kt1 = kt1, kt2
     dev_bytes = st.device_bytes()
     st.close()
-    ms_max = ms
-    if ws > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, ws)
     value = N * K * ws / (ms_max * 1e-3) / 1e9
     h_bytes, e_bytes = algorithmic_bytes(model, meta, dtype)
     # one E update and one H update per step, each a core-rows kernel plus a CPML-slab kernel
@@ -237,10 +245,7 @@ def run_gpu(args):
             d2h += st2.read_monitor(m, c, (ms_["dft"].Nw, len(ms_["cells"])), True).nbytes
     t_e2e = time.perf_counter() - t0
     st2.close()
-    if ws > 1:
-        t = torch.tensor([t_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = max_over_ranks(t_e2e, ws)
     e2e = N * K * ws / t_e2e / 1e9
 
     out = None
@@ -259,18 +264,18 @@ def run_gpu(args):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "cells": N, "steps_per_sim": 4000,
+            "config": {"workload": WORKLOAD, "grid": [args.size] * 3, "cells": N, "steps_per_sim": 4000,
                        "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (fields 604 MB)"},
             "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d / K),
                     "d2h_bytes_per_step": int(d2h / K), "includes": "mfd_create upload + K steps + read-back",
                     "host_setup_s_excluded": round(t_desc, 3)},
             "roofline": {"bound": "hbm", "kernel": "E update (e3d_core_kernel + e3d_slab_kernel)", "achieved": round(e_gbs, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4),
-                         "traffic": NCU_TRAFFIC_256["E"] if args.n == 256 else None,
+                         "traffic": NCU_TRAFFIC_256["E"] if args.size == 256 else None,
                          "algorithmic_bytes_per_launch": e_bytes, "mean_launch_ms": round(e_ms, 5),
                          "peak_kind": peak_kind,
                          "h_kernel": {"achieved": round(h_gbs, 1), "frac": round(h_gbs / peak, 4),
-                                      "traffic": NCU_TRAFFIC_256["H"] if args.n == 256 else None,
+                                      "traffic": NCU_TRAFFIC_256["H"] if args.size == 256 else None,
                                       "algorithmic_bytes_per_launch": h_bytes, "mean_launch_ms": round(h_ms, 5)}},
             "kernels": per_kernel,
             "plain_stepper": plain,
@@ -597,7 +602,7 @@ def plain_stepper(lib, args, device, steps=20):
     """The plain FP32 stepper at 256^3 (vacuum, 12-cell CPML, Sa sum): H and E update times
     and their HBM roofline fractions, CUDA events per update."""
     from maxwellfdtd_b200 import _abi, workloads
-    model, _ = workloads.plain_256(nt=steps + 5, n=args.n)
+    model, _ = workloads.plain_256(nt=steps + 5, n=args.size)
     b, meta = model.build_desc(np.float32, None, device=device)
     st = _abi.Stepper(lib, b, np.float32)
     st.run(1, 3)
@@ -613,7 +618,7 @@ def plain_stepper(lib, args, device, steps=20):
     h_ms = (k1["H"][0] - k0["H"][0]) / steps
     e_ms = (k1["E"][0] - k0["E"][0]) / steps
     N = model.grid.Nx * model.grid.Ny * model.grid.Nz
-    return {"workload": f"plain_256: {args.n}^3 FP32 vacuum, 12-cell CPML, soft point source, Sa sum",
+    return {"workload": f"plain_256: {args.size}^3 FP32 vacuum, 12-cell CPML, soft point source, Sa sum",
             "value": round(N * steps / (ms * 1e-3) / 1e9, 3), "unit": "Gcell-updates/s", "steps": steps,
             "h_update": {"ms": round(h_ms, 5), "bytes": h_bytes, "frac": round(h_bytes / (h_ms * 1e-3) / 1e9 / peak, 4)},
             "e_update": {"ms": round(e_ms, 5), "bytes": e_bytes, "frac": round(e_bytes / (e_ms * 1e-3) / 1e9 / peak, 4)},
@@ -644,7 +649,7 @@ def cpu_baseline(args, model, mons, steps=None):
     st.close()
     N = model.grid.Nx * model.grid.Ny * model.grid.Nz
     return {"value": round(N * steps / dt / 1e9, 5), "unit": "Gcell-updates/s", "cores": int(threads),
-            "kind": "port", "sample": f"{steps} full steps of the {args.n}^3 workload ({dt:.1f} s)"}
+            "kind": "port", "sample": f"{steps} full steps of the {args.size}^3 workload ({dt:.1f} s)"}
 
 
 def run_reference(args):
@@ -655,7 +660,7 @@ def run_reference(args):
     W, K = args.warmup, args.steps
     # each step a bounded sample: full 256^3 steps on the host cores
     nt = W + K + 2
-    model, mons = workloads.plasmonics_256(nt=nt, n=args.n)
+    model, mons = workloads.plasmonics_256(nt=nt, n=args.size)
     lib = _oracle_lib()
     threads = lib.lib.oracle_set_threads(0)
     b, meta = model.build_desc(np.float32, mons)
@@ -670,9 +675,9 @@ def run_reference(args):
     out = {"impl": "reference", "metric": "Gcell-updates/s", "value": round(v, 5), "unit": "Gcell-updates/s",
            "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": round(dt * 1e3 / K, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "cells": N, "parallelism": "host cores"},
+           "config": {"workload": WORKLOAD, "grid": [args.size] * 3, "cells": N, "parallelism": "host cores"},
            "cpu_baseline": {"value": round(v, 5), "unit": "Gcell-updates/s", "cores": int(threads), "kind": "port",
-                            "sample": f"{K} full steps of the {args.n}^3 workload after {W} warm-up steps"},
+                            "sample": f"{K} full steps of the {args.size}^3 workload after {W} warm-up steps"},
            "e2e": {"value": round(v, 5), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return out
@@ -684,7 +689,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--size", type=int, default=256, help="grid side of the headline workload")
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-stepper roofline measurement")

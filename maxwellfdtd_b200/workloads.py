@@ -101,13 +101,13 @@ def plasmonics_256(nt=4000, n=256, with_monitors=True):
     t0 = 3 * tau
     w0 = 2 * np.pi * C0 / 600e-9
     f = lambda s: np.exp(-2 * np.log(2) * (s - t0) ** 2 / tau ** 2) * np.cos(w0 * (s - t0))
-    m = 20                                   # TFSF box faces 20 cells in from the edges
+    m = max(4, round(20 * n / 256))          # TFSF box faces 20 cells in from the edges at 256^3
     i1, i2 = (m, m, m), (n + 1 - m, n + 1 - m, n + 1 - m)
     data = _plane_wave_tfsf(grid, i1, i2, t, f, grid.z[i1[2] - 1], dt)
     model = Model(grid, TFSFSource(data=data), tmax=(nt - 0.5) * dt, pml=12 * dx, material=gold)
     mons = None
     if with_monitors:
-        h = 80 * dx + dx / 2                # faces on grid planes (coordinates are odd multiples of dx/2)
+        h = round(80 * n / 256) * dx + dx / 2   # faces on grid planes (coordinates are odd multiples of dx/2)
         lam = np.linspace(400e-9, 900e-9, 64)
         w = 2 * np.pi * C0 / lam
         eps = dx / 2
