@@ -592,7 +592,7 @@ class Engine : public HandleBase {
     // The split needs layers that do not overlap in any dimension; MFD_KERNEL3D=unsplit
     // keeps the single-kernel updates (for comparison).
     void init_split() {
-        if (ndim != 3 || sizeof(T) != 4) return;
+        if (ndim != 3) return;
         if (const char* k = std::getenv("MFD_KERNEL3D"))
             if (!std::strcmp(k, "unsplit")) return;
         const int xl = lay[MFD_XL].nb ? lay[MFD_XL].ib : 0, xr = lay[MFD_XR].nb ? lay[MFD_XR].ib - 1 : nx;
@@ -976,23 +976,49 @@ class Engine : public HandleBase {
         e3d_tma_kernel<R, MAT, FAST><<<grd, blk, TMA_STAGES * EStage::BYTES, st>>>(etma, tma_zc);
     }
 
+    // 3-D updates split into core rows and CPML slabs (yee3d_split.cuh), either element type
+    template <bool MATH, bool FAST, bool ACC, bool E2S>
+    void launch_H_split(const HParams<T>& p) {
+        kcount = 0;
+        const int zn = sbox.zr - sbox.zl;
+        if (sbox.yr > sbox.yl && zn > 0) {
+            dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
+            h3d_core_kernel<T, MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, sbox);
+            kcount++;
+        }
+        if (slab_rows) {
+            dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
+            h3d_slab_kernel<T, MATH, FAST, ACC, E2S><<<grd, 128, 0, st>>>(p, d3, sbox);
+            kcount++;
+        }
+    }
+
+    template <bool MATH, bool FAST>
+    void launch_H_split_acc(const HParams<T>& p) {
+        if (!p.accum) launch_H_split<MATH, FAST, false, false>(p);
+        else if (p.sum_e2) launch_H_split<MATH, FAST, true, true>(p);
+        else launch_H_split<MATH, FAST, true, false>(p);
+    }
+
+    template <bool MAT, bool FAST>
+    void launch_E_split(const EParams<T, R>& p) {
+        kcount = 0;
+        const int zn = sbox.zr - sbox.zl;
+        if (sbox.yr > sbox.yl && zn > 0) {
+            dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
+            e3d_core_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sbox);
+            kcount++;
+        }
+        if (slab_rows) {
+            dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
+            e3d_slab_kernel<T, R, MAT, FAST><<<grd, 128, 0, st>>>(p, d3, sbox);
+            kcount++;
+        }
+    }
+
+    // single-kernel single-precision 3-D updates (CPML layers that overlap in a dimension)
     template <bool MATH, bool FAST, bool ACC, bool E2S>
     void launch_H_f32(const HParams<float>& p) {
-        if (use_split) {
-            kcount = 0;
-            const int zn = sbox.zr - sbox.zl;
-            if (sbox.yr > sbox.yl && zn > 0) {
-                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
-                h3d_core_kernel<MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, sbox);
-                kcount++;
-            }
-            if (slab_rows) {
-                dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
-                h3d_slab_kernel<MATH, FAST, ACC, E2S><<<grd, 128, 0, st>>>(p, d3, sbox);
-                kcount++;
-            }
-            return;
-        }
         dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
         h3d_f32_kernel<MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, zc3);
     }
@@ -1006,27 +1032,19 @@ class Engine : public HandleBase {
 
     template <bool MAT, bool FAST>
     void launch_E_f32(const EParams<float, R>& p) {
-        if (use_split) {
-            kcount = 0;
-            const int zn = sbox.zr - sbox.zl;
-            if (sbox.yr > sbox.yl && zn > 0) {
-                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
-                e3d_core_kernel<R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sbox);
-                kcount++;
-            }
-            if (slab_rows) {
-                dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
-                e3d_slab_kernel<R, MAT, FAST><<<grd, 128, 0, st>>>(p, d3, sbox);
-                kcount++;
-            }
-            return;
-        }
         dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
         e3d_f32_kernel<R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, zc3);
     }
 
     void launch_H(int accum, long long prev_step) {
         HParams<T> p = hparams(accum, prev_step);
+        if (ndim == 3 && use_split && !use_tma) {
+            launch(KC_H, [&] {
+                if (math_needed) { if (fastdiv) launch_H_split_acc<true, true>(p); else launch_H_split_acc<true, false>(p); }
+                else { if (fastdiv) launch_H_split_acc<false, true>(p); else launch_H_split_acc<false, false>(p); }
+            });
+            return;
+        }
         if constexpr (sizeof(T) == 4) {
             if (ndim == 3 && !use_tma) {
                 const HParams<float>& pf = reinterpret_cast<const HParams<float>&>(p);
@@ -1068,15 +1086,22 @@ class Engine : public HandleBase {
     void launch_E(int cur) {
         EParams<T, R> p = eparams();
         bool done_tma = false;
+        if (ndim == 3 && use_split && !use_tma) {
+            launch(KC_E, [&] {
+                if (any_geom) { if (fastdiv) launch_E_split<true, true>(p); else launch_E_split<true, false>(p); }
+                else { if (fastdiv) launch_E_split<false, true>(p); else launch_E_split<false, false>(p); }
+            });
+            done_tma = true;
+        }
         if constexpr (sizeof(T) == 4) {
-            if (ndim == 3 && !use_tma) {
+            if (ndim == 3 && !use_tma && !done_tma) {
                 const EParams<float, R>& pf = reinterpret_cast<const EParams<float, R>&>(p);
                 launch(KC_E, [&] {
                     if (any_geom) { if (fastdiv) launch_E_f32<true, true>(pf); else launch_E_f32<true, false>(pf); }
                     else { if (fastdiv) launch_E_f32<false, true>(pf); else launch_E_f32<false, false>(pf); }
                 });
                 done_tma = true;
-            } else if (use_tma) {
+            } else if (use_tma && !done_tma) {
                 std::memcpy(&etma.p, &p, sizeof(p));
                 launch(KC_E, [&] {
                     if (any_geom) { if (fastdiv) launch_E_tma<true, true>(); else launch_E_tma<true, false>(); }

@@ -1,4 +1,4 @@
-// yee3d_split.cuh -- single-precision 3-D updates split by CPML region (sm_100a).
+// yee3d_split.cuh -- 3-D updates (single and double precision) split by CPML region (sm_100a).
 //
 // A 3-D grid with CPML layers on the y and z faces is cut into
 //   core  : rows outside the y and z layers (all x), marched along z by h3d_core_kernel /
@@ -8,8 +8,9 @@
 //           prefetched with the fields: a layer cell costs its psi traffic and a few flops;
 //   slab  : every cell of the y and z layers (h3d_slab_kernel / e3d_slab_kernel), one cell
 //           per thread with all of its loads issued together, general CPML (any faces).
-// The per-cell arithmetic is that of h3d_f32_kernel / e3d_f32_kernel (yee.cuh), operation
-// for operation and with the faces in the same order, so results are bit-identical.  The
+// The per-cell arithmetic is that of h3d_f32_kernel / e3d_f32_kernel (single precision) and
+// h3d_kernel / e3d_kernel (double precision) in yee.cuh, operation for operation and with
+// the faces in the same order, so results are bit-identical.  The
 // split needs layers that do not overlap in any dimension (checked on the host, which
 // otherwise launches the unsplit kernels).
 #pragma once
@@ -42,18 +43,39 @@ __device__ __forceinline__ void slab_row(const SplitBox& s, int ny, int r, int& 
     }
 }
 
+// The six curl derivatives of a cell, q = num / (dy, dz, dx, dz, dx, dy): for single precision
+// the verified branch-free division (div6), for double precision IEEE division.
+template <typename T, bool FAST>
+__device__ __forceinline__ void curl_div(const Div3& D3, const DivC<T>& ddx, const DivC<T>& ddy, const DivC<T>& ddz,
+                                         const T (&num)[6], T (&q)[6]) {
+    if constexpr (sizeof(T) == 4) {
+        div6<FAST>(D3, num, q);
+    } else {
+        q[0] = num[0] / ddy.d; q[1] = num[1] / ddz.d; q[2] = num[2] / ddx.d;
+        q[3] = num[3] / ddz.d; q[4] = num[4] / ddx.d; q[5] = num[5] / ddy.d;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ bool maybe_nonfinite(T x) {
+    if constexpr (sizeof(T) == 4) return !(fabsf(x) <= FLT_MAX);
+    else return !(fabs(x) <= DBL_MAX);
+}
+
 // x-layer state of one column: which face (none / left / right), its coefficients and psi.
+template <typename T>
 struct XCol {
     bool in;
     int q, nb;
-    float A, B;
-    DivC<float> K;
-    float* pa;
-    float* pb;
+    T A, B;
+    DivC<T> K;
+    T* pa;
+    T* pb;
 };
 
-__device__ __forceinline__ XCol xcol(const LayerDev<float>& lxl, const LayerDev<float>& lxr, int ix, int ia, int ib) {
-    XCol x;
+template <typename T>
+__device__ __forceinline__ XCol<T> xcol(const LayerDev<T>& lxl, const LayerDev<T>& lxr, int ix, int ia, int ib) {
+    XCol<T> x;
     const bool l = lxl.nb && ix < lxl.ib;
     const bool r = lxr.nb && ix >= lxr.ib - 1;
     x.in = l || r;
@@ -62,25 +84,26 @@ __device__ __forceinline__ XCol xcol(const LayerDev<float>& lxl, const LayerDev<
     x.pa = l ? lxl.psi[ia] : lxr.psi[ia];
     x.pb = l ? lxl.psi[ib] : lxr.psi[ib];
     if (x.in) {
-        const LayerDev<float>& lx = l ? lxl : lxr;
+        const LayerDev<T>& lx = l ? lxl : lxr;
         x.A = lx.A[x.q];
         x.B = lx.B[x.q];
         x.K = lx.K[x.q];
     } else {
-        x.A = x.B = 0.0f;
-        x.K = DivC<float>{};
+        x.A = x.B = T(0);
+        x.K = DivC<T>{};
     }
     return x;
 }
 
+template <typename T>
 struct HCoreLoad {
-    float ez, eyx, ezx, exy, ezy, exz, eyz, hx, hy, hz, sa, e2, pa, pb;
+    T ez, eyx, ezx, exy, ezy, exz, eyz, hx, hy, hz, sa, e2, pa, pb;
     int g;
 };
 
-template <bool MATH, bool FAST, bool ACC, bool E2S>
-__global__ void __launch_bounds__(256, 4) h3d_core_kernel(const __grid_constant__ HParams<float> p, const Div3 D3,
-                                                          const SplitBox s) {
+template <typename T, bool MATH, bool FAST, bool ACC, bool E2S>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) h3d_core_kernel(const __grid_constant__ HParams<T> p,
+                                                                               const Div3 D3, const SplitBox s) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = s.yl + blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -95,22 +118,22 @@ __global__ void __launch_bounds__(256, 4) h3d_core_kernel(const __grid_constant_
     const int ozw = bzr == MFD_BC_PERIODIC ? -(nz - 1) * sz : 0;
     const int zlast_zero = bzr == MFD_BC_DIRICHLET ? nz - 1 : -1;
     const bool zx = xr && bxr == MFD_BC_DIRICHLET, zy = yr && byr == MFD_BC_DIRICHLET;
-    const XCol X = xcol(p.lay[MFD_XL], p.lay[MFD_XR], ix, 2, 3);   // H uses psi pair (2, 3)
+    const XCol<T> X = xcol<T>(p.lay[MFD_XL], p.lay[MFD_XR], ix, 2, 3);   // H uses psi pair (2, 3)
     const int kstep = X.nb * ny;
     int k = X.q + X.nb * (iy + ny * z0);
-    const float dt = p.dt, Mh0 = p.Mh0;
-    const float* __restrict__ Ex = p.Ex;
-    const float* __restrict__ Ey = p.Ey;
-    const float* __restrict__ Ez = p.Ez;
-    float* Hx = p.Hx;
-    float* Hy = p.Hy;
-    float* Hz = p.Hz;
-    float* Sa = p.Sa;
-    float* E2 = p.E2;
+    const T dt = p.dt, Mh0 = p.Mh0;
+    const T* __restrict__ Ex = p.Ex;
+    const T* __restrict__ Ey = p.Ey;
+    const T* __restrict__ Ez = p.Ez;
+    T* Hx = p.Hx;
+    T* Hy = p.Hy;
+    T* Hz = p.Hz;
+    T* Sa = p.Sa;
+    T* E2 = p.E2;
     int c = ix + sy * iy + sz * z0;
-    float ex = Ex[c], ey = Ey[c];
+    T ex = Ex[c], ey = Ey[c];
     auto load = [&](int cc, int iz, int kk) {
-        HCoreLoad v;
+        HCoreLoad<T> v;
         const int oz = iz < nz - 1 ? sz : ozw;
         v.ez = Ez[cc];
         v.eyx = Ey[cc + ox];
@@ -122,39 +145,39 @@ __global__ void __launch_bounds__(256, 4) h3d_core_kernel(const __grid_constant_
         v.hx = Hx[cc];
         v.hy = Hy[cc];
         v.hz = Hz[cc];
-        v.sa = ACC ? Sa[cc] : 0.0f;
-        v.e2 = (ACC && E2S) ? E2[cc] : 0.0f;
+        v.sa = ACC ? Sa[cc] : T(0);
+        v.e2 = (ACC && E2S) ? E2[cc] : T(0);
         v.g = MATH ? (int)p.geom[cc] : 0;
-        v.pa = X.in ? X.pa[kk] : 0.0f;
-        v.pb = X.in ? X.pb[kk] : 0.0f;
+        v.pa = X.in ? X.pa[kk] : T(0);
+        v.pb = X.in ? X.pb[kk] : T(0);
         return v;
     };
-    HCoreLoad cur = load(c, z0, k);
+    HCoreLoad<T> cur = load(c, z0, k);
     for (int iz = z0; iz < z1; ++iz, c += sz, k += kstep) {
-        HCoreLoad nxt;
+        HCoreLoad<T> nxt;
         if (iz + 1 < z1) nxt = load(c + sz, iz + 1, k + kstep);
-        const float ez = cur.ez;
-        const float ey_xp = zx ? 0.0f : cur.eyx, ez_xp = zx ? 0.0f : cur.ezx;
-        const float ex_yp = zy ? 0.0f : cur.exy, ez_yp = zy ? 0.0f : cur.ezy;
+        const T ez = cur.ez;
+        const T ey_xp = zx ? T(0) : cur.eyx, ez_xp = zx ? T(0) : cur.ezx;
+        const T ex_yp = zy ? T(0) : cur.exy, ez_yp = zy ? T(0) : cur.ezy;
         const bool zz = iz == zlast_zero;
-        const float ex_zp = zz ? 0.0f : cur.exz, ey_zp = zz ? 0.0f : cur.eyz;
-        float hx = cur.hx, hy = cur.hy, hz = cur.hz;
+        const T ex_zp = zz ? T(0) : cur.exz, ey_zp = zz ? T(0) : cur.eyz;
+        T hx = cur.hx, hy = cur.hy, hz = cur.hz;
         if (ACC) {
-            const float a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
+            const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
             Sa[c] = cur.sa + sqrt0(a * a + b * b + d * d) * dt;
             if (E2S) E2[c] = cur.e2 + (ex * ex + ey * ey + ez * ez) * dt;
-            if (!(fabsf(ex) <= FLT_MAX)) guard(p, ex);
+            if (maybe_nonfinite(ex)) guard(p, ex);
         }
-        float Mh = Mh0;
+        T Mh = Mh0;
         if (MATH && cur.g) Mh = p.matMh[cur.g - 1];
-        const float num[6] = {ex_yp - ex, ex_zp - ex, ey_xp - ey, ey_zp - ey, ez_xp - ez, ez_yp - ez};
-        float q[6];
-        div6<FAST>(D3, num, q);
-        const float dExy = q[0], dExz = q[1], dEyz = q[3], dEzy = q[5];
-        float dEyx = q[2], dEzx = q[4];
+        const T num[6] = {ex_yp - ex, ex_zp - ex, ey_xp - ey, ey_zp - ey, ez_xp - ez, ez_yp - ez};
+        T q[6];
+        curl_div<T, FAST>(D3, p.ddx, p.ddy, p.ddz, num, q);
+        const T dExy = q[0], dExz = q[1], dEyz = q[3], dEzy = q[5];
+        T dEyx = q[2], dEzx = q[4];
         if (X.in) {   // cpml_h<+1> of the column's x face
-            const float pa = X.B * cur.pa + X.A * dEyx;
-            const float pb = X.B * cur.pb + X.A * dEzx;
+            const T pa = X.B * cur.pa + X.A * dEyx;
+            const T pb = X.B * cur.pb + X.A * dEzx;
             X.pa[k] = pa;
             X.pb[k] = pb;
             hy += Mh * pb;
@@ -174,8 +197,8 @@ __global__ void __launch_bounds__(256, 4) h3d_core_kernel(const __grid_constant_
     }
 }
 
-template <bool MATH, bool FAST, bool ACC, bool E2S>
-__global__ void __launch_bounds__(128) h3d_slab_kernel(const __grid_constant__ HParams<float> p, const Div3 D3,
+template <typename T, bool MATH, bool FAST, bool ACC, bool E2S>
+__global__ void __launch_bounds__(128) h3d_slab_kernel(const __grid_constant__ HParams<T> p, const Div3 D3,
                                                        const SplitBox s) {
     const int ix = blockIdx.y * blockDim.x + threadIdx.x;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -190,27 +213,27 @@ __global__ void __launch_bounds__(128) h3d_slab_kernel(const __grid_constant__ H
     const int oz = !zr ? sz : (bzr == MFD_BC_PERIODIC ? -(nz - 1) * sz : 0);
     const bool zx = xr && bxr == MFD_BC_DIRICHLET, zy = yr && byr == MFD_BC_DIRICHLET, zz = zr && bzr == MFD_BC_DIRICHLET;
     const int c = ix + sy * iy + sz * iz;
-    const float ex = p.Ex[c], ey = p.Ey[c], ez = p.Ez[c];
-    const float ey_xp = zx ? 0.0f : p.Ey[c + ox], ez_xp = zx ? 0.0f : p.Ez[c + ox];
-    const float ex_yp = zy ? 0.0f : p.Ex[c + oy], ez_yp = zy ? 0.0f : p.Ez[c + oy];
-    const float ex_zp = zz ? 0.0f : p.Ex[c + oz], ey_zp = zz ? 0.0f : p.Ey[c + oz];
-    float hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
+    const T ex = p.Ex[c], ey = p.Ey[c], ez = p.Ez[c];
+    const T ey_xp = zx ? T(0) : p.Ey[c + ox], ez_xp = zx ? T(0) : p.Ez[c + ox];
+    const T ex_yp = zy ? T(0) : p.Ex[c + oy], ez_yp = zy ? T(0) : p.Ez[c + oy];
+    const T ex_zp = zz ? T(0) : p.Ex[c + oz], ey_zp = zz ? T(0) : p.Ey[c + oz];
+    T hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
     if (ACC) {
-        const float a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
+        const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
         p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b + d * d) * p.dt;
         if (E2S) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
-        if (!(fabsf(ex) <= FLT_MAX)) guard(p, ex);
+        if (maybe_nonfinite(ex)) guard(p, ex);
     }
-    float Mh = p.Mh0;
+    T Mh = p.Mh0;
     if (MATH) {
         const int g = p.geom[c];
         if (g) Mh = p.matMh[g - 1];
     }
-    const float num[6] = {ex_yp - ex, ex_zp - ex, ey_xp - ey, ey_zp - ey, ez_xp - ez, ez_yp - ez};
-    float q[6];
-    div6<FAST>(D3, num, q);
-    float dExy = q[0], dExz = q[1], dEyx = q[2], dEyz = q[3], dEzx = q[4], dEzy = q[5];
-    const LayerDev<float>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL], &lyr = p.lay[MFD_YR],
+    const T num[6] = {ex_yp - ex, ex_zp - ex, ey_xp - ey, ey_zp - ey, ez_xp - ez, ez_yp - ez};
+    T q[6];
+    curl_div<T, FAST>(D3, p.ddx, p.ddy, p.ddz, num, q);
+    T dExy = q[0], dExz = q[1], dEyx = q[2], dEyz = q[3], dEzx = q[4], dEzy = q[5];
+    const LayerDev<T>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL], &lyr = p.lay[MFD_YR],
                           &lzl = p.lay[MFD_ZL], &lzr = p.lay[MFD_ZR];
     if (lxl.nb && ix < lxl.ib) cpml_h<+1, FAST>(lxl, ix, ix + lxl.nb * (iy + ny * iz), Mh, dEyx, dEzx, hy, hz);
     if (lxr.nb && ix >= lxr.ib - 1) {
@@ -235,14 +258,15 @@ __global__ void __launch_bounds__(128) h3d_slab_kernel(const __grid_constant__ H
     p.Hz[c] = hz;
 }
 
+template <typename T>
 struct ECoreLoad {
-    float hx, hy, hz, hyx, hzx, hxy, hzy, dx, dy, dz, pa, pb;
+    T hx, hy, hz, hyx, hzx, hxy, hzy, dx, dy, dz, pa, pb;
     int g;
 };
 
-template <typename R, bool MAT, bool FAST>
-__global__ void __launch_bounds__(256, 4) e3d_core_kernel(const __grid_constant__ EParams<float, R> p, const Div3 D3,
-                                                          const SplitBox s) {
+template <typename T, typename R, bool MAT, bool FAST>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) e3d_core_kernel(const __grid_constant__ EParams<T, R> p,
+                                                                               const Div3 D3, const SplitBox s) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = s.yl + blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -255,31 +279,31 @@ __global__ void __launch_bounds__(256, 4) e3d_core_kernel(const __grid_constant_
     const int ox = !xl ? -1 : (bxl == MFD_BC_PERIODIC ? nx - 1 : 0);
     const int oy = !yl ? -sy : (byl == MFD_BC_PERIODIC ? (ny - 1) * sy : 0);
     const bool zx = xl && bxl == MFD_BC_DIRICHLET, zy = yl && byl == MFD_BC_DIRICHLET;
-    const XCol X = xcol(p.lay[MFD_XL], p.lay[MFD_XR], ix, 0, 1);   // E uses psi pair (0, 1)
+    const XCol<T> X = xcol<T>(p.lay[MFD_XL], p.lay[MFD_XR], ix, 0, 1);   // E uses psi pair (0, 1)
     const int kstep = X.nb * ny;
     int k = X.q + X.nb * (iy + ny * z0);
-    const float Md10 = p.Md10, Md20 = p.Md20, Me0 = p.Me0;
-    const float* __restrict__ Hx = p.Hx;
-    const float* __restrict__ Hy = p.Hy;
-    const float* __restrict__ Hz = p.Hz;
-    float* Dx = p.Dx;
-    float* Dy = p.Dy;
-    float* Dz = p.Dz;
-    float* Ex = p.Ex;
-    float* Ey = p.Ey;
-    float* Ez = p.Ez;
+    const T Md10 = p.Md10, Md20 = p.Md20, Me0 = p.Me0;
+    const T* __restrict__ Hx = p.Hx;
+    const T* __restrict__ Hy = p.Hy;
+    const T* __restrict__ Hz = p.Hz;
+    T* Dx = p.Dx;
+    T* Dy = p.Dy;
+    T* Dz = p.Dz;
+    T* Ex = p.Ex;
+    T* Ey = p.Ey;
+    T* Ez = p.Ez;
     int c = ix + sy * iy + sz * z0;
-    float hx_zm, hy_zm;
+    T hx_zm, hy_zm;
     if (z0 > 0) {
         hx_zm = Hx[c - sz];
         hy_zm = Hy[c - sz];
     } else {
         const int oz = bzl == MFD_BC_PERIODIC ? (nz - 1) * sz : 0;
-        hx_zm = bzl == MFD_BC_DIRICHLET ? 0.0f : Hx[c + oz];
-        hy_zm = bzl == MFD_BC_DIRICHLET ? 0.0f : Hy[c + oz];
+        hx_zm = bzl == MFD_BC_DIRICHLET ? T(0) : Hx[c + oz];
+        hy_zm = bzl == MFD_BC_DIRICHLET ? T(0) : Hy[c + oz];
     }
     auto load = [&](int cc, int kk) {
-        ECoreLoad v;
+        ECoreLoad<T> v;
         v.hx = Hx[cc];
         v.hy = Hy[cc];
         v.hz = Hz[cc];
@@ -291,32 +315,32 @@ __global__ void __launch_bounds__(256, 4) e3d_core_kernel(const __grid_constant_
         v.dy = Dy[cc];
         v.dz = Dz[cc];
         v.g = MAT ? (int)p.geom[cc] : 0;
-        v.pa = X.in ? X.pa[kk] : 0.0f;
-        v.pb = X.in ? X.pb[kk] : 0.0f;
+        v.pa = X.in ? X.pa[kk] : T(0);
+        v.pb = X.in ? X.pb[kk] : T(0);
         return v;
     };
-    ECoreLoad cur = load(c, k);
+    ECoreLoad<T> cur = load(c, k);
     for (int iz = z0; iz < z1; ++iz, c += sz, k += kstep) {
-        ECoreLoad nxt;
+        ECoreLoad<T> nxt;
         if (iz + 1 < z1) nxt = load(c + sz, k + kstep);
-        const float hx = cur.hx, hy = cur.hy, hz = cur.hz;
-        const float hy_xm = zx ? 0.0f : cur.hyx, hz_xm = zx ? 0.0f : cur.hzx;
-        const float hx_ym = zy ? 0.0f : cur.hxy, hz_ym = zy ? 0.0f : cur.hzy;
-        const float num[6] = {hx - hx_ym, hx - hx_zm, hy - hy_xm, hy - hy_zm, hz - hz_xm, hz - hz_ym};
-        float q[6];
-        div6<FAST>(D3, num, q);
-        const float dHxy = q[0], dHxz = q[1], dHyz = q[3], dHzy = q[5];
-        float dHyx = q[2], dHzx = q[4];
-        float Md1 = Md10, Md2 = Md20, Me = Me0;
+        const T hx = cur.hx, hy = cur.hy, hz = cur.hz;
+        const T hy_xm = zx ? T(0) : cur.hyx, hz_xm = zx ? T(0) : cur.hzx;
+        const T hx_ym = zy ? T(0) : cur.hxy, hz_ym = zy ? T(0) : cur.hzy;
+        const T num[6] = {hx - hx_ym, hx - hx_zm, hy - hy_xm, hy - hy_zm, hz - hz_xm, hz - hz_ym};
+        T q[6];
+        curl_div<T, FAST>(D3, p.ddx, p.ddy, p.ddz, num, q);
+        const T dHxy = q[0], dHxz = q[1], dHyz = q[3], dHzy = q[5];
+        T dHyx = q[2], dHzx = q[4];
+        T Md1 = Md10, Md2 = Md20, Me = Me0;
         bool simple = true;
         if (MAT && cur.g) {
-            const MatDev<float, R>& m = p.mats[cur.g - 1];
+            const MatDev<T, R>& m = p.mats[cur.g - 1];
             Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
         }
-        float D0 = cur.dx, D1 = cur.dy, D2 = cur.dz;
+        T D0 = cur.dx, D1 = cur.dy, D2 = cur.dz;
         if (X.in) {   // cpml_e<-1> of the column's x face
-            const float pa = X.B * cur.pa + X.A * dHyx;
-            const float pb = X.B * cur.pb + X.A * dHzx;
+            const T pa = X.B * cur.pa + X.A * dHyx;
+            const T pb = X.B * cur.pb + X.A * dHzx;
             X.pa[k] = pa;
             X.pb[k] = pb;
             D1 -= Md2 * pb;
@@ -341,8 +365,8 @@ __global__ void __launch_bounds__(256, 4) e3d_core_kernel(const __grid_constant_
     }
 }
 
-template <typename R, bool MAT, bool FAST>
-__global__ void __launch_bounds__(128) e3d_slab_kernel(const __grid_constant__ EParams<float, R> p, const Div3 D3,
+template <typename T, typename R, bool MAT, bool FAST>
+__global__ void __launch_bounds__(128) e3d_slab_kernel(const __grid_constant__ EParams<T, R> p, const Div3 D3,
                                                        const SplitBox s) {
     const int ix = blockIdx.y * blockDim.x + threadIdx.x;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -357,25 +381,25 @@ __global__ void __launch_bounds__(128) e3d_slab_kernel(const __grid_constant__ E
     const int oz = !zl ? -sz : (bzl == MFD_BC_PERIODIC ? (nz - 1) * sz : 0);
     const bool zx = xl && bxl == MFD_BC_DIRICHLET, zy = yl && byl == MFD_BC_DIRICHLET, zz = zl && bzl == MFD_BC_DIRICHLET;
     const int c = ix + sy * iy + sz * iz;
-    const float hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
-    const float hy_xm = zx ? 0.0f : p.Hy[c + ox], hz_xm = zx ? 0.0f : p.Hz[c + ox];
-    const float hx_ym = zy ? 0.0f : p.Hx[c + oy], hz_ym = zy ? 0.0f : p.Hz[c + oy];
-    const float hx_zm = zz ? 0.0f : p.Hx[c + oz], hy_zm = zz ? 0.0f : p.Hy[c + oz];
-    const float num[6] = {hx - hx_ym, hx - hx_zm, hy - hy_xm, hy - hy_zm, hz - hz_xm, hz - hz_ym};
-    float q[6];
-    div6<FAST>(D3, num, q);
-    float dHxy = q[0], dHxz = q[1], dHyx = q[2], dHyz = q[3], dHzx = q[4], dHzy = q[5];
-    float Md1 = p.Md10, Md2 = p.Md20, Me = p.Me0;
+    const T hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
+    const T hy_xm = zx ? T(0) : p.Hy[c + ox], hz_xm = zx ? T(0) : p.Hz[c + ox];
+    const T hx_ym = zy ? T(0) : p.Hx[c + oy], hz_ym = zy ? T(0) : p.Hz[c + oy];
+    const T hx_zm = zz ? T(0) : p.Hx[c + oz], hy_zm = zz ? T(0) : p.Hy[c + oz];
+    const T num[6] = {hx - hx_ym, hx - hx_zm, hy - hy_xm, hy - hy_zm, hz - hz_xm, hz - hz_ym};
+    T q[6];
+    curl_div<T, FAST>(D3, p.ddx, p.ddy, p.ddz, num, q);
+    T dHxy = q[0], dHxz = q[1], dHyx = q[2], dHyz = q[3], dHzx = q[4], dHzy = q[5];
+    T Md1 = p.Md10, Md2 = p.Md20, Me = p.Me0;
     bool simple = true;
     if (MAT) {
         const int g = p.geom[c];
         if (g) {
-            const MatDev<float, R>& m = p.mats[g - 1];
+            const MatDev<T, R>& m = p.mats[g - 1];
             Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
         }
     }
-    float D0 = p.Dx[c], D1 = p.Dy[c], D2 = p.Dz[c];
-    const LayerDev<float>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL], &lyr = p.lay[MFD_YR],
+    T D0 = p.Dx[c], D1 = p.Dy[c], D2 = p.Dz[c];
+    const LayerDev<T>&lxl = p.lay[MFD_XL], &lxr = p.lay[MFD_XR], &lyl = p.lay[MFD_YL], &lyr = p.lay[MFD_YR],
                           &lzl = p.lay[MFD_ZL], &lzr = p.lay[MFD_ZR];
     if (lxl.nb && ix < lxl.ib) cpml_e<-1, FAST>(lxl, ix, ix + lxl.nb * (iy + ny * iz), Md2, dHyx, dHzx, D1, D2);
     if (lxr.nb && ix >= lxr.ib - 1) {
