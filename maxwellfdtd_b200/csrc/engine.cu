@@ -310,7 +310,7 @@ class Engine : public HandleBase {
     int32_t bad_kind = 0;
 
     // launch shapes
-    int bx3 = 32, by3 = 4, zc3 = 8;   // 3-D z-march tiles: measured best of {32x8, 32x4} x {8, 16} planes at 256^3
+    int bx3 = 32, by3 = 4, zc3 = 4;   // 3-D z-march tiles: 32x4 columns, 4 planes (best at 100^3, neutral at 256^3)
     // single-precision 3-D updates split into core rows and CPML slabs (yee3d_split.cuh)
     bool use_split = false;
     SplitBox sbox{};
