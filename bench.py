@@ -228,7 +228,9 @@ def run_gpu(args):
 
     plain = plain_stepper(lib, args, local) if rank == 0 and not args.no_plain else None
 
-    # end to end through the public API with host buffers
+    # end to end through the public API with host buffers: results land in page-locked
+    # buffers the caller owns (allocated once, before the timed region)
+    pinned = _pinned_outputs(model, meta, dtype)
     t0 = time.perf_counter()
     b2, meta2 = model.build_desc(dtype, mons, device=local)
     t_desc = time.perf_counter() - t0
@@ -238,11 +240,12 @@ def run_gpu(args):
     st2.run(1, K)
     d2h = 0
     for c in (6, 7, 8, 0, 1, 2):
-        d2h += st2.read_field(c).nbytes
-    d2h += st2.read_integral(_abi.MFD_INT_SA).nbytes + st2.read_integral(_abi.MFD_INT_E2).nbytes
+        d2h += st2.read_field(c, out=pinned[("f", c)]).nbytes
+    d2h += st2.read_integral(_abi.MFD_INT_SA, out=pinned["Sa"]).nbytes
+    d2h += st2.read_integral(_abi.MFD_INT_E2, out=pinned["E2"]).nbytes
     for m, ms_ in enumerate(meta2["monitors"]):
         for c in (0, 1, 2, 6, 7, 8):
-            d2h += st2.read_monitor(m, c, (ms_["dft"].Nw, len(ms_["cells"])), True).nbytes
+            d2h += st2.read_monitor(m, c, (ms_["dft"].Nw, len(ms_["cells"])), True, out=pinned[("m", m, c)]).nbytes
     t_e2e = time.perf_counter() - t0
     st2.close()
     t_e2e = max_over_ranks(t_e2e, ws)
@@ -251,6 +254,7 @@ def run_gpu(args):
     out = None
     if rank == 0:
         cpu = None if (args.no_cpu or ws > 1) else cpu_baseline(args, model, mons)
+        err = None if (args.no_cpu or ws > 1) else headline_error(lib, local)
         out = {
             "metric": "Gcell-updates/s",
             "value": round(value, 3),
@@ -267,7 +271,8 @@ def run_gpu(args):
             "config": {"workload": WORKLOAD, "grid": [args.size] * 3, "cells": N, "steps_per_sim": 4000,
                        "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (fields 604 MB)"},
             "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d / K),
-                    "d2h_bytes_per_step": int(d2h / K), "includes": "mfd_create upload + K steps + read-back",
+                    "d2h_bytes_per_step": int(d2h / K),
+                "includes": "mfd_create upload + K steps + read-back of fields, Sa/E2, spectra into caller-owned page-locked buffers",
                     "host_setup_s_excluded": round(t_desc, 3)},
             "roofline": {"bound": "hbm", "kernel": "E update (e3d_core_kernel + e3d_slab_kernel)", "achieved": round(e_gbs, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4),
@@ -282,6 +287,7 @@ def run_gpu(args):
             "gpu_launches": launches,
             "device_bytes": dev_bytes,
             "cpu_baseline": cpu,
+            "error_vs_fp64_oracle": err,
             "clocks": clk.summary(),
         }
         print(json.dumps(out), flush=True)
@@ -625,6 +631,61 @@ def plain_stepper(lib, args, device, steps=20):
             "peak_gbs": peak, "peak_kind": kind}
 
 
+def _pinned_outputs(model, meta, dtype):
+    """Page-locked host arrays for the read-back of the e2e measurement (torch's pinned
+    allocator), or ordinary arrays when no CUDA is present."""
+    import torch
+    g = model.grid
+    N = g.Nx * g.Ny * g.Nz
+
+    def arr(n, dt):
+        tdt = {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64,
+               np.dtype(np.complex128): torch.complex128}[np.dtype(dt)]
+        t = torch.empty(int(n), dtype=tdt, pin_memory=torch.cuda.is_available())
+        return t.numpy()
+    out = {("f", c): arr(N, dtype) for c in (6, 7, 8, 0, 1, 2)}
+    out["Sa"] = arr(N, dtype)
+    out["E2"] = arr(N, dtype)
+    for m, ms_ in enumerate(meta["monitors"]):
+        for c in (0, 1, 2, 6, 7, 8):
+            out[("m", m, c)] = arr(ms_["dft"].Nw * len(ms_["cells"]), np.complex128).reshape(ms_["dft"].Nw, len(ms_["cells"]))
+    return out
+
+
+def headline_error(lib, device, n=96, steps=60):
+    """Relative L2 error of the single-precision GPU result against the FP64 oracle on an
+    n^3 version of the headline configuration (same spacing, sphere, TFSF and monitors
+    scaled with the grid): the E and H vectors, Sa, and the DFT spectra; and the distance to
+    the oracle run in single precision (the parity measure, 0 when bit-identical)."""
+    from maxwellfdtd_b200 import _abi, workloads
+    from maxwellfdtd_b200.sources import comp_index
+    oracle = _oracle_lib()
+    oracle.lib.oracle_set_threads(0)
+    model, mons = workloads.plasmonics_256(nt=steps, n=n)
+    res = {}
+    for tag, lb, dt in (("gpu", lib, np.float32), ("fp64", oracle, np.float64), ("fp32", oracle, np.float32)):
+        b, meta = model.build_desc(dt, mons, device=device if lb is lib else 0)
+        st = _abi.Stepper(lb, b, dt)
+        st.run(1, model.Nt)
+        o = {c: st.read_field(comp_index(c)) for c in ("Hx", "Hy", "Hz", "Ex", "Ey", "Ez")}
+        o["Sa"] = st.read_integral(_abi.MFD_INT_SA)
+        o["dft"] = np.concatenate([st.read_monitor(k, comp_index(c), (mm["dft"].Nw, len(mm["cells"])), True).ravel()
+                                   for k, mm in enumerate(meta["monitors"]) for c in ("Hx", "Hy", "Hz", "Ex", "Ey", "Ez")])
+        st.close()
+        res[tag] = o
+    vec = lambda o, cs: np.concatenate([np.asarray(o[c]).ravel() for c in cs])
+    groups = {"E": ("Ex", "Ey", "Ez"), "H": ("Hx", "Hy", "Hz"), "Sa": ("Sa",), "dft": ("dft",)}
+
+    def rel(a, b):
+        a = np.concatenate([a.real.ravel(), a.imag.ravel()]) if np.iscomplexobj(a) else a.astype(np.float64)
+        b = np.concatenate([b.real.ravel(), b.imag.ravel()]) if np.iscomplexobj(b) else b.astype(np.float64)
+        den = max(np.linalg.norm(a), np.linalg.norm(b))
+        return 0.0 if den == 0 else float(np.linalg.norm(a - b) / den)
+    return {"rel_l2": {g: rel(vec(res["gpu"], cs), vec(res["fp64"], cs)) for g, cs in groups.items()},
+            "gpu_vs_fp32_oracle": {g: rel(vec(res["gpu"], cs), vec(res["fp32"], cs)) for g, cs in groups.items()},
+            "how": f"{n}^3 version of the workload (dx=2nm, same sphere, TFSF and DFT faces scaled), {steps} steps"}
+
+
 def _oracle_lib():
     from maxwellfdtd_b200 import _abi
     so = os.path.join(ROOT, "oracle", "libmfd_oracle.so")
@@ -690,7 +751,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=256, help="grid side of the headline workload")
-    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--cpu-steps", type=int, default=40, help="steps of the CPU-baseline sample (about 10 s on 16 cores)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-stepper roofline measurement")
     ap.add_argument("--workload", default="plasmonics", choices=["plasmonics", "batch2d", "serve", "dielectric100", "nonlinear"])

@@ -180,8 +180,19 @@ class Stepper:
         self.lib.status(self.h, C.byref(d), C.byref(b), C.byref(k))
         return d.value, b.value, k.value
 
-    def read_field(self, comp):
-        out = np.empty(self.N, dtype=self.dtype)
+    @staticmethod
+    def _dest(out, n, dtype, shape=None):
+        """The caller's buffer (e.g. page-locked memory, which the copy reaches at full DMA
+        speed) when given and of the right size and type, else a new array."""
+        if out is None:
+            return np.empty(shape if shape is not None else n, dtype=dtype)
+        if out.dtype != np.dtype(dtype) or out.size != (int(np.prod(shape)) if shape is not None else n) \
+                or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("output buffer of the wrong size, type or layout")
+        return out
+
+    def read_field(self, comp, out=None):
+        out = self._dest(out, self.N, self.dtype)
         self._check(self.lib.read_field(self.h, int(comp), out.ctypes.data_as(C.c_void_p)))
         return out
 
@@ -190,17 +201,14 @@ class Stepper:
         assert v.size == self.N
         self._check(self.lib.write_field(self.h, int(comp), v.ctypes.data_as(C.c_void_p)))
 
-    def read_integral(self, which):
+    def read_integral(self, which, out=None):
         dt = np.float64 if which == MFD_INT_RHO else self.dtype
-        out = np.empty(self.N, dtype=dt)
+        out = self._dest(out, self.N, dt)
         self._check(self.lib.read_integral(self.h, int(which), out.ctypes.data_as(C.c_void_p)))
         return out
 
-    def read_monitor(self, m, comp, shape, spectral):
-        if spectral:
-            out = np.empty(shape, dtype=np.complex128)
-        else:
-            out = np.empty(shape, dtype=self.dtype)
+    def read_monitor(self, m, comp, shape, spectral, out=None):
+        out = self._dest(out, None, np.complex128 if spectral else self.dtype, shape)
         self._check(self.lib.read_monitor(self.h, int(m), int(comp), out.ctypes.data_as(C.c_void_p)))
         return out
 

@@ -126,3 +126,27 @@ def test_oracle_rejects_bad_descriptors(oracle_lib):
     b.desc.tfsf.i1[2], b.desc.tfsf.i2[2] = 1, 5
     assert oracle_lib.create(C.byref(b.desc), C.byref(h)) == _abi.MFD_ERR_INVALID
     assert "TFSF box" in oracle_lib.create_error().decode()
+
+
+def test_readers_fill_caller_buffers(oracle_lib):
+    """read_field / read_integral / read_monitor write into a buffer the caller owns (for
+    example page-locked memory) and refuse one of the wrong size or type."""
+    import cases as C
+    model = C.model_vacuum(2)
+    mons = C.monitors(2)
+    b, meta = model.build_desc(np.float32, mons)
+    st = _abi.Stepper(oracle_lib, b, np.float32)
+    st.run(1, model.Nt)
+    buf = np.full(st.N, np.nan, np.float32)
+    assert st.read_field(6, out=buf) is buf and np.array_equal(buf, st.read_field(6))
+    sa = np.empty(st.N, np.float32)
+    assert np.array_equal(st.read_integral(_abi.MFD_INT_SA, out=sa), st.read_integral(_abi.MFD_INT_SA))
+    mm = meta["monitors"][3]
+    shape = (mm["dft"].Nw, len(mm["cells"]))
+    spec = np.empty(shape, np.complex128)
+    assert np.array_equal(st.read_monitor(3, 6, shape, True, out=spec), st.read_monitor(3, 6, shape, True))
+    with pytest.raises(ValueError):
+        st.read_field(6, out=np.empty(st.N - 1, np.float32))
+    with pytest.raises(ValueError):
+        st.read_field(6, out=np.empty(st.N, np.float64))
+    st.close()
