@@ -143,16 +143,25 @@ struct MonParams {
     const MonDev<T>* mons;
 };
 
-// Grid row blockIdx.y = monitor * ncomp + component.
+// Grid row blockIdx.y = monitor; a thread gathers every component of one point (one cell
+// index load, the component loads independent of each other).
 template <typename T>
 __global__ void __launch_bounds__(256) monitor_gather_kernel(const __grid_constant__ MonParams<T> p, long long it0, int slot) {
-    const int m = blockIdx.y / p.ncomp, k = blockIdx.y - m * p.ncomp;
-    const MonDev<T>& M = p.mons[m];
+    const MonDev<T>& M = p.mons[blockIdx.y];
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (j >= M.npts) return;
-    const T v = p.comp[k][M.cells[j]];
-    if (M.kind == MFD_MON_FIELD && !M.sum) M.hist[((long long)k * p.nt + it0) * M.npts + j] = v;
-    else M.ring[((long long)slot * p.ncomp + k) * M.npts + j] = v;
+    const int cell = M.cells[j];
+    T v[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        if (k < p.ncomp) v[k] = p.comp[k][cell];
+    const bool hist = M.kind == MFD_MON_FIELD && !M.sum;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        if (k >= p.ncomp) break;
+        if (hist) M.hist[((long long)k * p.nt + it0) * M.npts + j] = v[k];
+        else M.ring[((long long)slot * p.ncomp + k) * M.npts + j] = v[k];
+    }
 }
 
 // Summed field monitor: hist[k][it] = sum over points (block reduction in T).

@@ -1202,7 +1202,7 @@ class Engine : public HandleBase {
         const int slot = ring_used;
         launch(KC_MON, [&] {
             const long long nb = (mon_maxpts + 255) / 256;
-            monitor_gather_kernel<T><<<dim3((unsigned)nb, mon_p.nmon * ncomp_mon), 256, 0, st>>>(mon_p, it - 1, slot);
+            monitor_gather_kernel<T><<<dim3((unsigned)nb, mon_p.nmon), 256, 0, st>>>(mon_p, it - 1, slot);
         });
         if (need_ring) {
             ring_used++;
