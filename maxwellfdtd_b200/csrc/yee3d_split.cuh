@@ -17,6 +17,13 @@
 
 #include "yee.cuh"
 
+#ifndef MFD_CORE_MINB
+#define MFD_CORE_MINB 4   // single-precision core kernels: blocks of 256 threads' worth per SM (64 registers)
+#endif
+#ifndef MFD_SLAB_MINB
+#define MFD_SLAB_MINB 16  // single-precision slab kernels: 16 blocks of 128 threads per SM (32 registers; measured faster than 40)
+#endif
+
 namespace mfd {
 
 // Rows of the core box and the slab region.  Cells with iz < zl or iz >= zr are in a z layer,
@@ -102,7 +109,7 @@ struct HCoreLoad {
 };
 
 template <typename T, bool MATH, bool FAST, bool ACC, bool E2S>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) h3d_core_kernel(const __grid_constant__ HParams<T> p,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) h3d_core_kernel(const __grid_constant__ HParams<T> p,
                                                                                const Div3 D3, const SplitBox s) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = s.yl + blockIdx.y * blockDim.y + threadIdx.y;
@@ -198,7 +205,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) h3d_core_kernel(c
 }
 
 template <typename T, bool MATH, bool FAST, bool ACC, bool E2S>
-__global__ void __launch_bounds__(128) h3d_slab_kernel(const __grid_constant__ HParams<T> p, const Div3 D3,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) h3d_slab_kernel(const __grid_constant__ HParams<T> p, const Div3 D3,
                                                        const SplitBox s) {
     const int ix = blockIdx.y * blockDim.x + threadIdx.x;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -265,7 +272,7 @@ struct ECoreLoad {
 };
 
 template <typename T, typename R, bool MAT, bool FAST>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) e3d_core_kernel(const __grid_constant__ EParams<T, R> p,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) e3d_core_kernel(const __grid_constant__ EParams<T, R> p,
                                                                                const Div3 D3, const SplitBox s) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = s.yl + blockIdx.y * blockDim.y + threadIdx.y;
@@ -366,7 +373,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) e3d_core_kernel(c
 }
 
 template <typename T, typename R, bool MAT, bool FAST>
-__global__ void __launch_bounds__(128) e3d_slab_kernel(const __grid_constant__ EParams<T, R> p, const Div3 D3,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) e3d_slab_kernel(const __grid_constant__ EParams<T, R> p, const Div3 D3,
                                                        const SplitBox s) {
     const int ix = blockIdx.y * blockDim.x + threadIdx.x;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
