@@ -246,6 +246,18 @@ MFD_API int mfd_read_integral(mfd_handle* h, int32_t which, void* dst);
 #define MFD_NOALLOC_SCRATCH_BYTES (16u << 20)
 MFD_API int mfd_read_integral_noalloc(mfd_handle* h, int32_t which, void* dst);
 
+/* Field snapshots taken during mfd_run (the frames write_fields saves at the output steps,
+ * src/outputs.jl:156-179).  After each of the nsteps listed steps (1-based, increasing, after
+ * the model's current step) the ncomp listed components (MFD_HX..MFD_EZ) are copied on the
+ * device into a staging slot and from there to dst on a copy stream, while the following
+ * steps run.  dst holds nsteps x ncomp x (nx*ny*nz) elements of T, frame f component k at
+ * element (f*ncomp + k)*nx*ny*nz, each dense with x fastest; page-locked memory reaches full
+ * DMA speed.  A frame is complete when the mfd_run call that ran its step returns.  Two
+ * staging slots of ncomp fields are allocated on the device at the first call.  nsteps = 0
+ * clears the list. */
+MFD_API int mfd_set_snapshots(mfd_handle* h, int32_t ncomp, const int32_t* comps, int64_t nsteps,
+                              const int64_t* steps, void* dst);
+
 /* Monitor m, component comp.  Field monitor: T [nt][npts] ([nt] when sum).  Spectral
  * monitor: double complex [nw][npts] ([nw] when sum) as interleaved (re, im). */
 MFD_API int mfd_read_monitor(mfd_handle* h, int32_t m, int32_t comp, void* dst);

@@ -127,6 +127,11 @@ class Library:
             self.kernel_times = fn("kernel_times", C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int32])
             self.last_run_ms = fn("last_run_ms", C.c_int, [vp, C.POINTER(C.c_double)])
             self.device_bytes = fn("device_bytes", C.c_int64, [vp])
+        # field snapshots during a run (CUDA library only)
+        self.has_snapshots = hasattr(L, p + "set_snapshots")
+        if self.has_snapshots:
+            self.set_snapshots = fn("set_snapshots", C.c_int, [vp, C.c_int32, C.POINTER(C.c_int32), C.c_int64,
+                                                              C.POINTER(C.c_int64), vp])
         # batches of 2-D models (CUDA library only)
         self.has_batch = hasattr(L, p + "batch_create")
         if self.has_batch:
@@ -211,6 +216,17 @@ class Stepper:
         out = self._dest(out, None, np.complex128 if spectral else self.dtype, shape)
         self._check(self.lib.read_monitor(self.h, int(m), int(comp), out.ctypes.data_as(C.c_void_p)))
         return out
+
+    def set_snapshots(self, comps, steps, dst):
+        """Frames of the listed components after each listed step, copied into dst
+        (len(steps) x len(comps) x N elements of the model's type) while the run goes on."""
+        comps = np.ascontiguousarray(comps, dtype=np.int32)
+        steps = np.ascontiguousarray(steps, dtype=np.int64)
+        if dst.dtype != self.dtype or dst.size != len(steps) * len(comps) * self.N or not dst.flags["C_CONTIGUOUS"]:
+            raise ValueError("snapshot buffer of the wrong size, type or layout")
+        self._snap = (comps, steps, dst)   # kept alive while the library writes into dst
+        self._check(self.lib.set_snapshots(self.h, len(comps), comps.ctypes.data_as(C.POINTER(C.c_int32)), len(steps),
+                                           steps.ctypes.data_as(C.POINTER(C.c_int64)), dst.ctypes.data_as(C.c_void_p)))
 
     KERNEL_CLASSES = ("H", "E", "sources", "tfsf", "monitors", "dft", "sums", "material")
 

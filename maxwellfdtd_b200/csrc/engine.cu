@@ -58,6 +58,7 @@ struct HandleBase {
     virtual int write_field(int comp, const void* src) = 0;
     virtual int read_integral(int which, void* dst) = 0;
     virtual int read_integral_noalloc(int which, void* dst) = 0;
+    virtual int set_snapshots(int ncomp, const int32_t* comps, int64_t nsteps, const int64_t* steps, void* dst) = 0;
     virtual int read_monitor(int m, int comp, void* dst) = 0;
     virtual int read_record(int k, void* dst) = 0;
     virtual int64_t record_size(int k) const = 0;
@@ -287,6 +288,19 @@ class Engine : public HandleBase {
     RectParams<T> tfsf_p{};
     long long tfsf_maxlen = 0, rec_maxlen = 0;
     bool record = false;
+
+    // Field snapshots (mfd_set_snapshots): after each listed step the listed components are
+    // copied on the device into one of two staging slots (the compute stream), and from the
+    // slot to the caller's host buffer on a copy stream while the steps go on.
+    std::vector<int> snap_comps;
+    std::vector<int64_t> snap_steps;
+    size_t snap_next = 0;
+    char* snap_dst = nullptr;
+    T* snap_stage = nullptr;            // [2][ncomp][Np]
+    int snap_cap = 0;                   // components the staging slots hold
+    bool snap_busy[2] = {false, false};
+    cudaStream_t st3 = nullptr;
+    cudaEvent_t ev_snap_ready[2] = {nullptr, nullptr}, ev_snap_free[2] = {nullptr, nullptr};
     RectParams<T> rec_p{};
     int rec_narr = 0;
 
@@ -335,6 +349,7 @@ class Engine : public HandleBase {
 
     ~Engine() override {
         cudaSetDevice(dev);
+        if (st3) cudaStreamSynchronize(st3);
         if (st) {
             for (void* p : allocs) cudaFreeAsync(p, st);
             cudaStreamSynchronize(st);
@@ -343,6 +358,9 @@ class Engine : public HandleBase {
         for (auto& pe : pend) { cudaEventDestroy(pe.second.first); cudaEventDestroy(pe.second.second); }
         if (run_ev[0]) cudaEventDestroy(run_ev[0]);
         if (run_ev[1]) cudaEventDestroy(run_ev[1]);
+        for (auto e : ev_snap_ready) if (e) cudaEventDestroy(e);
+        for (auto e : ev_snap_free) if (e) cudaEventDestroy(e);
+        if (st3) cudaStreamDestroy(st3);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -1241,8 +1259,64 @@ class Engine : public HandleBase {
             launch_sources(it);
             launch_monitors(it);
             if (record) launch_record(it);
+            if (snap_next < snap_steps.size() && snap_steps[snap_next] == it) snapshot();
         }
         return finish(a, b);
+    }
+
+    // Frame snap_next: device copies into a free staging slot, then the host copies on st3.
+    void snapshot() {
+        const int slot = (int)(snap_next & 1);
+        if (snap_busy[slot]) MFD_CK(cudaStreamWaitEvent(st, ev_snap_free[slot], 0));
+        const int nc = (int)snap_comps.size();
+        for (int k = 0; k < nc; ++k)
+            MFD_CK(cudaMemcpyAsync(snap_stage + ((size_t)slot * nc + k) * Np, F[snap_comps[k]], (size_t)Np * sizeof(T),
+                                   cudaMemcpyDeviceToDevice, st));
+        MFD_CK(cudaEventRecord(ev_snap_ready[slot], st));
+        MFD_CK(cudaStreamWaitEvent(st3, ev_snap_ready[slot], 0));
+        for (int k = 0; k < nc; ++k) {
+            char* h = snap_dst + ((size_t)snap_next * nc + k) * (size_t)N * sizeof(T);
+            MFD_CK(cudaMemcpy2DAsync(h, (size_t)nx * sizeof(T), snap_stage + ((size_t)slot * nc + k) * Np, (size_t)px * sizeof(T),
+                                     (size_t)nx * sizeof(T), (size_t)ny * nz, cudaMemcpyDeviceToHost, st3));
+        }
+        MFD_CK(cudaEventRecord(ev_snap_free[slot], st3));
+        snap_busy[slot] = true;
+        snap_next++;
+    }
+
+    int set_snapshots(int ncomp, const int32_t* comps, int64_t nsteps, const int64_t* steps, void* dst) override {
+        if (in_batch) { err = "the model is being stepped by a batch"; return MFD_ERR_INVALID; }
+        if (ncomp < 1 || ncomp > 9 || nsteps < 0 || (nsteps > 0 && (!comps || !steps || !dst))) {
+            err = "snapshots need 1..9 components, the steps and a destination";
+            return MFD_ERR_INVALID;
+        }
+        for (int k = 0; k < ncomp; ++k)
+            if (comps[k] < 0 || comps[k] > 8 || !F[comps[k]]) { err = "snapshot component not in this field"; return MFD_ERR_INVALID; }
+        for (int64_t i = 0; i < nsteps; ++i)
+            if (steps[i] <= done || steps[i] > nt || (i && steps[i] <= steps[i - 1])) {
+                err = "snapshot steps must increase and lie after the model's current step, within 1..Nt";
+                return MFD_ERR_INVALID;
+            }
+        MFD_CK(cudaSetDevice(dev));
+        if (st3) MFD_CK(cudaStreamSynchronize(st3));
+        if (!st3) {
+            MFD_CK(cudaStreamCreateWithFlags(&st3, cudaStreamNonBlocking));
+            for (int i = 0; i < 2; ++i) {
+                MFD_CK(cudaEventCreateWithFlags(&ev_snap_ready[i], cudaEventDisableTiming));
+                MFD_CK(cudaEventCreateWithFlags(&ev_snap_free[i], cudaEventDisableTiming));
+            }
+        }
+        if (nsteps > 0 && ncomp > snap_cap) {
+            snap_stage = dalloc<T>((size_t)2 * ncomp * Np);   // kept until the handle is destroyed
+            snap_cap = ncomp;
+            MFD_CK(cudaStreamSynchronize(st));
+        }
+        snap_comps.assign(comps, comps + ncomp);
+        snap_steps.assign(steps, steps + nsteps);
+        snap_next = 0;
+        snap_dst = (char*)dst;
+        snap_busy[0] = snap_busy[1] = false;
+        return MFD_OK;
     }
 
     // End of a run of steps a..b (also of a batch member's window): staged monitors, the
@@ -1250,6 +1324,7 @@ class Engine : public HandleBase {
     int finish(int64_t a, int64_t b) {
         flush_monitors();
         launch_sums(b);
+        if (st3 && (snap_busy[0] || snap_busy[1])) bounded_sync(st3);   // frames of steps <= b are on the host
         MFD_CK(cudaEventRecord(run_ev[1], st));
         MFD_CK(cudaMemcpyAsync(h_flags + (a - 1), d_flags + (a - 1), (size_t)(b - a + 1) * sizeof(int),
                                cudaMemcpyDeviceToHost, st));
@@ -1556,6 +1631,7 @@ struct mfd_batch {
         if (e->dev != dev) { err = "batch member on another device"; return MFD_ERR_INVALID; }
         if (e->in_batch) { err = "model already in a batch"; return MFD_ERR_INVALID; }
         if (e->record) { err = "batch members cannot record TFSF data"; return MFD_ERR_INVALID; }
+        if (e->snap_next < e->snap_steps.size()) { err = "batch members cannot take field snapshots"; return MFD_ERR_INVALID; }
         if (e->bad_step) { err = "the model holds non-finite fields"; return MFD_ERR_NONFINITE; }
         if (last <= e->done || last > e->nt) { err = "the last step must be after the model's current step and within 1..Nt"; return MFD_ERR_INVALID; }
         MFD_CK(cudaSetDevice(dev));
@@ -1932,6 +2008,9 @@ int mfd_write_field(mfd_handle* h, int32_t comp, const void* src) { MFD_GUARD(h,
 int mfd_read_integral(mfd_handle* h, int32_t which, void* dst) { MFD_GUARD(h, h->impl->read_integral(which, dst)); }
 int mfd_read_integral_noalloc(mfd_handle* h, int32_t which, void* dst) {
     MFD_GUARD(h, h->impl->read_integral_noalloc(which, dst));
+}
+int mfd_set_snapshots(mfd_handle* h, int32_t ncomp, const int32_t* comps, int64_t nsteps, const int64_t* steps, void* dst) {
+    MFD_GUARD(h, h->impl->set_snapshots(ncomp, comps, nsteps, steps, dst));
 }
 int mfd_read_monitor(mfd_handle* h, int32_t m, int32_t comp, void* dst) { MFD_GUARD(h, h->impl->read_monitor(m, comp, dst)); }
 int mfd_read_tfsf_record(mfd_handle* h, int32_t k, void* dst) { MFD_GUARD(h, h->impl->read_record(k, dst)); }

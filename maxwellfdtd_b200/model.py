@@ -367,7 +367,18 @@ def _run(model, st, meta, dtype, fname, nframes, nstride, dtout, components, mon
     snaps = {c: [] for c in components}
     if isfields and model.isplasma:
         snaps["rho"] = []
-    stops = sorted(set(out_steps) | {Nt})
+    # frames on a copy stream while the run goes on, when the library takes snapshots (rho
+    # of plasma models is read at the output steps)
+    device_frames = isfields and getattr(st.lib, "has_snapshots", False) and "rho" not in snaps
+    if device_frames:
+        # an ordinary host array: page-locking one for a single solve costs more than the
+        # faster copies save (a caller of mfd_set_snapshots that reuses page-locked memory
+        # gets the frames fully hidden behind the steps)
+        buf = np.empty(len(out_steps) * len(components) * st.N, dtype=dtype)
+        st.set_snapshots([comp_index(c) for c in components], out_steps, buf)
+        stops = [Nt]
+    else:
+        stops = sorted(set(out_steps) | {Nt})
     a = 1
     for stop in stops:
         while a <= stop:
@@ -379,11 +390,16 @@ def _run(model, st, meta, dtype, fname, nframes, nstride, dtout, components, mon
                     raise RuntimeError(str(e)) from None
                 raise
             a = b + 1
-        if stop in out_steps:
+        if stop in out_steps and not device_frames:
             for c in components:
                 snaps[c].append(st.read_field(comp_index(c)).reshape(shape, order="F"))
             if "rho" in snaps:
                 snaps["rho"].append(st.read_integral(_abi.MFD_INT_RHO).reshape(shape, order="F").astype(dtype))
+    if device_frames:
+        frames = buf.reshape(len(out_steps), len(components), st.N)
+        for k, c in enumerate(components):
+            snaps[c] = [frames[f, k].reshape(shape, order="F").copy() for f in range(len(out_steps))]
+        st.set_snapshots([comp_index(components[0])], [], np.empty(0, dtype))
     if isfields:
         out["fields/t"] = np.asarray(t_T)[np.array(out_steps) - 1]
         for c, v in snaps.items():

@@ -190,3 +190,43 @@ def test_nonfinite_guard_matches_oracle(oracle_lib, gpu_lib):
         st.close()
     assert results[0] == results[1], results
     assert results[0][0] > 1
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_snapshot_frames(ndim, dtype, oracle_lib, gpu_lib, monkeypatch):
+    """Field frames at the output steps (solve with nstride): taken on the device during the
+    run and copied on a side stream, they equal the oracle's frames and the frames read by
+    stopping the run at each output step."""
+    model = C.model_materials(ndim)
+    kw = dict(nstride=9)
+
+    def frames(lib):
+        sol = M.solve(model, backend=M.B200(dtype, library=lib), **kw)
+        return {k: v for k, v in sol.out.items() if k.startswith("fields/")}
+    ref = frames(oracle_lib)
+    assert gpu_lib.has_snapshots and not getattr(oracle_lib, "has_snapshots", False)
+    got = frames(gpu_lib)
+    monkeypatch.setattr(gpu_lib, "has_snapshots", False)
+    stop = frames(gpu_lib)
+    assert set(ref) == set(got) == set(stop) and len(ref) > 2
+    for k in ref:
+        assert np.array_equal(ref[k], got[k]) and np.array_equal(got[k], stop[k]), k
+
+
+def test_snapshot_errors(gpu_lib):
+    model = C.model_vacuum(3)
+    b, _ = model.build_desc(np.float32, None)
+    st = _abi.Stepper(gpu_lib, b, np.float32)
+    buf = np.empty(2 * st.N, np.float32)
+    with pytest.raises(_abi.StepperError):
+        st.set_snapshots([6, 7], [model.Nt + 1], buf)          # beyond Nt
+    with pytest.raises(_abi.StepperError):
+        st.set_snapshots([6], [5, 5], buf)                     # not increasing
+    st.run(1, 10)
+    with pytest.raises(_abi.StepperError):
+        st.set_snapshots([6], [3, 12], buf)                    # before the current step
+    st.set_snapshots([6], [11, 12], buf)
+    st.run(11, 12)
+    assert np.array_equal(buf[st.N:], st.read_field(6))
+    st.close()
