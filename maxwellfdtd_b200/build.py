@@ -9,7 +9,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = [os.path.join(HERE, "csrc", "engine.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("yee.cuh", "aux.cuh", "mfd_device.cuh", "tma.cuh", "yee3d_tma.cuh", "yee3d_split.cuh")] + \
+DEPS = SRC + sorted(os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc")) if f.endswith(".cuh")) + \
     [os.path.join(os.path.dirname(HERE), "include", "maxwellfdtd.h")]
 OUT = os.path.join(HERE, "libmaxwellfdtd_b200.so")
 

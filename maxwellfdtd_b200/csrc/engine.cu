@@ -27,6 +27,7 @@
 #include "aux.cuh"
 #include "yee.cuh"
 #include "yee3d_tma.cuh"
+#include "yee3d_async.cuh"
 #include "yee3d_split.cuh"
 #include "batch.cuh"
 
@@ -114,6 +115,12 @@ static void retain_pool(int dev) {
 // Staging buffer of mfd_read_integral_noalloc: a file-scope device array, so reading JE and
 // rho_end needs no device allocation at read time.  Shared by every handle on a device.
 static __device__ __align__(256) unsigned char g_read_scratch[MFD_NOALLOC_SCRATCH_BYTES];
+
+// Kernels that stage planes in static shared memory ask for the largest shared-memory
+// carveout, so that as many blocks as their registers allow are resident per SM.
+static void prefer_shared(const void* f) {
+    cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+}
 
 // Device address of g_read_scratch on the current device, looked up once per device
 // (cudaGetSymbolAddress makes the driver load the module's device globals on first use).
@@ -324,6 +331,8 @@ class Engine : public HandleBase {
     int32_t bad_kind = 0;
 
     // launch shapes
+    bool core_async = true;    // single-precision core rows staged by cp.async (MFD_CORE_ASYNC=0: register z-march)
+    int async_zc = 8;          // planes per block of the staged core kernels (MFD_ASYNC_ZC)
     int bx3 = 32, by3 = 4, zc3 = 4;   // 3-D z-march tiles: 32x4 columns, 4 planes (best at 100^3, neutral at 256^3)
     // single-precision 3-D updates split into core rows and CPML slabs (yee3d_split.cuh)
     bool use_split = false;
@@ -620,6 +629,9 @@ class Engine : public HandleBase {
         sbox = SplitBox{yl, yr, zl, zr, zc3, (zl + nz - zr) * ny};
         slab_rows = (long long)sbox.nzr + (long long)(zr - zl) * (yl + ny - yr);
         use_split = true;
+        if (const char* a = std::getenv("MFD_CORE_ASYNC")) core_async = std::atoi(a) != 0;
+        if (const char* z = std::getenv("MFD_ASYNC_ZC")) async_zc = std::max(1, std::atoi(z));
+
     }
 
     void init_tma() {
@@ -1000,9 +1012,21 @@ class Engine : public HandleBase {
         kcount = 0;
         const int zn = sbox.zr - sbox.zl;
         if (sbox.yr > sbox.yl && zn > 0) {
-            dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
-            h3d_core_kernel<T, MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, sbox);
-            kcount++;
+            if constexpr (sizeof(T) == 4) {
+                if (core_async) {
+                    prefer_shared((const void*)h3d_core_async_kernel<MATH, FAST, ACC, E2S>);
+                    SplitBox sa = sbox;
+                    sa.zc = async_zc;
+                    dim3 blk(AS_TX, AS_TY), grd((nx + AS_TX - 1) / AS_TX, (sbox.yr - sbox.yl + AS_TY - 1) / AS_TY, (zn + async_zc - 1) / async_zc);
+                    h3d_core_async_kernel<MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, sa);
+                    kcount++;
+                }
+            }
+            if (!(sizeof(T) == 4 && core_async)) {
+                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
+                h3d_core_kernel<T, MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, sbox);
+                kcount++;
+            }
         }
         if (slab_rows) {
             dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
@@ -1023,9 +1047,26 @@ class Engine : public HandleBase {
         kcount = 0;
         const int zn = sbox.zr - sbox.zl;
         if (sbox.yr > sbox.yl && zn > 0) {
-            dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
-            e3d_core_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sbox);
-            kcount++;
+            // The staged E kernel is used without material cells only: with the material
+            // index it measured slower than e3d_core_kernel (0.239 vs 0.218 ms per E update
+            // at 256^3 with a dispersive sphere), without it faster (0.736 vs 0.720 of the
+            // copy bandwidth, vacuum 256^3).
+            constexpr bool staged = sizeof(T) == 4 && !MAT;
+            if constexpr (staged) {
+                if (core_async) {
+                    prefer_shared((const void*)e3d_core_async_kernel<R, MAT, FAST>);
+                    SplitBox sa = sbox;
+                    sa.zc = async_zc;
+                    dim3 blk(AS_TX, AS_TY), grd((nx + AS_TX - 1) / AS_TX, (sbox.yr - sbox.yl + AS_TY - 1) / AS_TY, (zn + async_zc - 1) / async_zc);
+                    e3d_core_async_kernel<R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sa);
+                    kcount++;
+                }
+            }
+            if (!(staged && core_async)) {
+                dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
+                e3d_core_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sbox);
+                kcount++;
+            }
         }
         if (slab_rows) {
             dim3 grd((unsigned)slab_rows, (nx + 127) / 128);

@@ -151,6 +151,25 @@ def test_parity_unsplit_3d(builder, monkeypatch, oracle_lib, gpu_lib):
     _compare(ref, got, np.float32, exact=True)
 
 
+@pytest.mark.parametrize("mode", [("1", "1"), ("1", "3"), ("1", "8"), ("0", "8")])
+@pytest.mark.parametrize("builder", ["bcs", "materials", "wide_periodic", "wide_neumann", "wide_dirichlet", "y_z_right", "x_only"])
+def test_parity_core_kernels(builder, mode, monkeypatch, oracle_lib, gpu_lib):
+    """The single-precision core rows run staged in shared memory by asynchronous copies
+    (the default, at several z-chunk lengths) or as the register z-march (MFD_CORE_ASYNC=0);
+    both agree with the oracle bit for bit."""
+    monkeypatch.setenv("MFD_CORE_ASYNC", mode[0])
+    monkeypatch.setenv("MFD_ASYNC_ZC", mode[1])
+    if builder.startswith("wide_"):
+        model = C.model_wide_rows(builder[5:])
+    elif builder in LAYER_CASES:
+        model = C.model_layers(*LAYER_CASES[builder])
+    else:
+        model = getattr(C, "model_" + builder)(3)
+    ref = C.run_all(model, oracle_lib, np.float32)
+    got = C.run_all(model, gpu_lib, np.float32)
+    _compare(ref, got, np.float32, exact=True)
+
+
 @pytest.mark.parametrize("dtype", DTYPES)
 @pytest.mark.parametrize("ndim", [1, 2, 3])
 @pytest.mark.parametrize("npoles,kerr", [(3, True), (3, False), (5, True)])
