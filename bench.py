@@ -232,12 +232,14 @@ def run_gpu(args):
     # buffers the caller owns (allocated once, before the timed region)
     pinned = _pinned_outputs(model, meta, dtype)
     t0 = time.perf_counter()
-    b2, meta2 = model.build_desc(dtype, mons, device=local)
+    b2, meta2 = model.build_desc(dtype, mons, device=local, host_alloc=_pinned_array)
     t_desc = time.perf_counter() - t0
     h2d = sum(a.nbytes for a in b2.keep if isinstance(a, np.ndarray))
     t0 = time.perf_counter()
     st2 = _abi.Stepper(lib, b2, dtype)
+    t_create = time.perf_counter() - t0
     st2.run(1, K)
+    t_run = time.perf_counter() - t0 - t_create
     d2h = 0
     for c in (6, 7, 8, 0, 1, 2):
         d2h += st2.read_field(c, out=pinned[("f", c)]).nbytes
@@ -247,6 +249,7 @@ def run_gpu(args):
         for c in (0, 1, 2, 6, 7, 8):
             d2h += st2.read_monitor(m, c, (ms_["dft"].Nw, len(ms_["cells"])), True, out=pinned[("m", m, c)]).nbytes
     t_e2e = time.perf_counter() - t0
+    t_read = t_e2e - t_create - t_run
     st2.close()
     t_e2e = max_over_ranks(t_e2e, ws)
     e2e = N * K * ws / t_e2e / 1e9
@@ -272,8 +275,9 @@ def run_gpu(args):
                        "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (fields 604 MB)"},
             "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d / K),
                     "d2h_bytes_per_step": int(d2h / K),
-                "includes": "mfd_create upload + K steps + read-back of fields, Sa/E2, spectra into caller-owned page-locked buffers",
-                    "host_setup_s_excluded": round(t_desc, 3)},
+                "includes": "mfd_create upload from page-locked inputs + K steps + read-back of fields, Sa/E2, spectra into caller-owned page-locked buffers",
+                    "host_setup_s_excluded": round(t_desc, 3),
+                    "split_s": {"create": round(t_create, 4), "run": round(t_run, 4), "read_back": round(t_read, 4)}},
             "roofline": {"bound": "hbm", "kernel": "E update (e3d_core_kernel + e3d_slab_kernel)", "achieved": round(e_gbs, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4),
                          "traffic": NCU_TRAFFIC_256["E"] if args.size == 256 else None,
@@ -319,16 +323,25 @@ def bytes_2d(model):
     return h + e
 
 
-def run_batch2d(args):
-    """Batched 2-D configuration: all models in one batch (persistent launches, CUDA graph,
-    autotuned tiles) against the same models run as sequential plain solves."""
+def run_batch2d(args, three=False):
+    """Batched configuration (2-D models, or with three=True small 3-D ones): all models in one
+    batch (persistent launches, CUDA graph, autotuned tiles) against the same models run as
+    sequential plain solves."""
     import maxwellfdtd_b200 as M
     from maxwellfdtd_b200 import _abi, workloads
     ws, rank, local = dist_setup()
     lib = M.load_library()
-    models = workloads.batch2d(n=args.sims, seed=args.seed, steps_scale=args.steps_scale)
-    cu_total = sum(m.grid.Nx * m.grid.Nz * m.Nt for m, _ in models)
-    bytes_total = sum(bytes_2d(m) * m.Nt for m, _ in models)
+    if three:
+        models = workloads.batch3d(n=args.sims, seed=args.seed, steps_scale=args.steps_scale)
+        comps = (0, 1, 2, 6, 7, 8)
+        bytes_of = lambda m: sum(algorithmic_bytes(m, None, np.float32))
+    else:
+        models = workloads.batch2d(n=args.sims, seed=args.seed, steps_scale=args.steps_scale)
+        comps = (1, 6, 8)
+        bytes_of = bytes_2d
+    ncell = lambda m: m.grid.Nx * m.grid.Ny * m.grid.Nz
+    cu_total = sum(ncell(m) * m.Nt for m, _ in models)
+    bytes_total = sum(bytes_of(m) * m.Nt for m, _ in models)
     clk = ClockSampler(local).start()
     # warm-up: a small batch of the first members for a few steps (loads the kernels)
     wb = _abi.Batch(lib, local)
@@ -360,10 +373,10 @@ def run_batch2d(args):
     clk.stop()
     d2h = 0
     for st, meta, m in held:
-        for c in (1, 6, 8):
+        for c in comps:
             d2h += st.read_field(c).nbytes
         for k, mm in enumerate(meta["monitors"]):
-            for c in (1, 6, 8):
+            for c in comps:
                 d2h += st.read_monitor(k, c, (m.Nt, len(mm["cells"])), False).nbytes
     t_end = time.time()
     info = batch.info()
@@ -380,7 +393,7 @@ def run_batch2d(args):
         st = _abi.Stepper(lib, b, np.float32)
         st.run(1, m.Nt)
         seq_ms += st.last_run_ms()
-        seq_cu += m.grid.Nx * m.grid.Nz * m.Nt
+        seq_cu += ncell(m) * m.Nt
         st.close()
     seq_value = seq_cu / (seq_ms * 1e-3) / 1e9
     peak, kind = peaks()
@@ -389,10 +402,13 @@ def run_batch2d(args):
         "metric": "Gcell-updates/s", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": 1,
         "steps": int(sum(m.Nt for m, _ in models)), "warmup": 3, "ms_per_step": None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"batch2d: {len(models)} 2-D models, Nx,Nz in [128,1024], dx=20nm, 10-cell CPML, "
-                               f"1-20 ellipses eps in [1,12] (half Debye), Ricker point source, 4 point monitors, "
-                               f"steps 2000-6000 x {args.steps_scale}",
-                   "cells": int(sum(m.grid.Nx * m.grid.Nz for m, _ in models)), "cell_updates": int(cu_total),
+        "config": {"workload": (f"batch3d: {len(models)} 3-D models, Nx,Ny,Nz in [48,128], dx=20nm, 8-cell CPML, "
+                                f"1-5 spheres eps in [1,12] (half Debye), Ricker point source, 4 point monitors, "
+                                f"steps 500-2000 x {args.steps_scale}") if three else
+                               (f"batch2d: {len(models)} 2-D models, Nx,Nz in [128,1024], dx=20nm, 10-cell CPML, "
+                                f"1-20 ellipses eps in [1,12] (half Debye), Ricker point source, 4 point monitors, "
+                                f"steps 2000-6000 x {args.steps_scale}"),
+                   "cells": int(sum(ncell(m) for m, _ in models)), "cell_updates": int(cu_total),
                    "seed": args.seed, "parallelism": "one batch, persistent launches, CUDA graph",
                    "l2": "inputs larger than L2", "tile": list(info["tile"])},
         "e2e": {"value": round(cu_total / (t_end - t0) / 1e9, 3), "unit": "Gcell-updates/s",
@@ -400,7 +416,8 @@ def run_batch2d(args):
                 "d2h_bytes_per_step": int(d2h / max(1, max(m.Nt for m, _ in models))),
                 "includes": "descriptor upload of every member + batched run + read-back of fields and monitors",
                 "wall_s": round(t_end - t0, 3)},
-        "roofline": {"bound": "hbm", "kernel": "batched 2-D step (batch_h2d + batch_e2d + material/sources/monitors)",
+        "roofline": {"bound": "hbm", "kernel": ("batched 3-D step (batch_h3d + batch_e3d + material/sources/monitors)" if three
+                                                else "batched 2-D step (batch_h2d + batch_e2d + material/sources/monitors)"),
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": None, "algorithmic_bytes": int(bytes_total), "peak_kind": kind},
         "sequential": {"value": round(seq_value, 3), "unit": "Gcell-updates/s", "sims": len(seq),
@@ -631,6 +648,14 @@ def plain_stepper(lib, args, device, steps=20):
             "peak_gbs": peak, "peak_kind": kind}
 
 
+def _pinned_array(n, dtype):
+    """A page-locked 1-D host array (torch's pinned allocator), or an ordinary one without CUDA."""
+    import torch
+    tdt = {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64, np.dtype(np.uint8): torch.uint8,
+           np.dtype(np.int64): torch.int64, np.dtype(np.complex128): torch.complex128}[np.dtype(dtype)]
+    return torch.empty(int(n), dtype=tdt, pin_memory=torch.cuda.is_available()).numpy()
+
+
 def _pinned_outputs(model, meta, dtype):
     """Page-locked host arrays for the read-back of the e2e measurement (torch's pinned
     allocator), or ordinary arrays when no CUDA is present."""
@@ -639,10 +664,7 @@ def _pinned_outputs(model, meta, dtype):
     N = g.Nx * g.Ny * g.Nz
 
     def arr(n, dt):
-        tdt = {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64,
-               np.dtype(np.complex128): torch.complex128}[np.dtype(dt)]
-        t = torch.empty(int(n), dtype=tdt, pin_memory=torch.cuda.is_available())
-        return t.numpy()
+        return _pinned_array(n, dt)
     out = {("f", c): arr(N, dtype) for c in (6, 7, 8, 0, 1, 2)}
     out["Sa"] = arr(N, dtype)
     out["E2"] = arr(N, dtype)
@@ -754,7 +776,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=40, help="steps of the CPU-baseline sample (about 10 s on 16 cores)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-stepper roofline measurement")
-    ap.add_argument("--workload", default="plasmonics", choices=["plasmonics", "batch2d", "serve", "dielectric100", "nonlinear"])
+    ap.add_argument("--workload", default="plasmonics", choices=["plasmonics", "batch2d", "batch3d", "serve", "dielectric100", "nonlinear"])
     ap.add_argument("--err-steps", type=int, default=300, help="nonlinear: steps of the oracle comparison")
     ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate (1/s)")
@@ -773,9 +795,9 @@ def main():
         if args.steps > 20:
             args.steps = 20   # each reference step is a full 256^3 step on the CPU
         run_reference(args)
-    elif args.workload == "batch2d":
+    elif args.workload in ("batch2d", "batch3d"):
         args.steps_scale = 0.25 if args.steps_scale is None else args.steps_scale
-        run_batch2d(args)
+        run_batch2d(args, three=args.workload == "batch3d")
     elif args.workload in ("dielectric100", "nonlinear"):
         run_config(args)
     elif args.workload == "serve":

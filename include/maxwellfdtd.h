@@ -267,13 +267,15 @@ MFD_API int mfd_read_tfsf_record(mfd_handle* h, int32_t k, void* dst);
 /* Element count of TFSF array k for the record box (0 if k is unused). */
 MFD_API int64_t mfd_tfsf_record_size(const mfd_handle* h, int32_t k);
 
-/* ---- batches of 2-D models ------------------------------------------------------------
+/* ---- batches of 2-D and 3-D models -----------------------------------------------------
  * No counterpart in the reference, which runs one model per solve! call.  A batch steps
- * many independent 2-D single-precision models together: each half-step of all members is
- * one persistent launch over a table of (member, tile) pairs, and a CUDA graph of several
- * steps is replayed, so hundreds of small models of different sizes do not each pay a
- * handful of launches per step.  A member is an ordinary handle (mfd_create, 2-D, MFD_F32,
- * rho_fp64 = 1) with point sources and field monitors without sum; the batch runs its steps
+ * many independent 2-D and 3-D single-precision models together: each half-step of all
+ * members is a persistent launch over a table of (member, tile) pairs (one for the 2-D and
+ * one for the 3-D members), and a CUDA graph of several steps is replayed, so hundreds of
+ * small models of different sizes do not each pay a handful of launches per step.  A member
+ * is an ordinary handle (mfd_create, 2-D or 3-D, MFD_F32, rho_fp64 = 1) with any sources
+ * (point, TFSF replay) and monitors, but no TFSF recording and no field snapshots; the batch
+ * runs its steps
  * done+1 .. it_last exactly as mfd_run(h, done+1, it_last) would, with bit-identical results,
  * and then retires it: mfd_status / mfd_read_* work on it again.  Until it retires, the
  * caller must not run, read, write or destroy the handle (mfd_run returns MFD_ERR_INVALID).

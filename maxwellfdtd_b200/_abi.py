@@ -74,14 +74,22 @@ def dptr(a):
 
 
 class DescBuilder:
-    """Owns every array the descriptor points to (keep it alive while the library reads it)."""
+    """Owns every array the descriptor points to (keep it alive while the library reads it).
 
-    def __init__(self):
+    host_alloc(n, dtype) -> 1-D array, when given, provides the storage of arrays of at least
+    1 MiB (e.g. page-locked memory, which mfd_create uploads at full DMA speed)."""
+
+    def __init__(self, host_alloc=None):
         self.keep = []
         self.desc = Desc()
+        self.host_alloc = host_alloc
 
     def arr(self, a, dtype):
         a = np.ascontiguousarray(a, dtype=dtype)
+        if self.host_alloc is not None and a.nbytes >= (1 << 20):
+            dst = self.host_alloc(a.size, np.dtype(dtype))
+            dst[...] = a.reshape(-1)
+            a = dst.reshape(a.shape)
         self.keep.append(a)
         return a
 

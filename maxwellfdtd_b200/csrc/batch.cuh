@@ -1,4 +1,4 @@
-// batch.cuh -- many independent 2-D models stepped together (sm_100a).
+// batch.cuh -- many independent 2-D and 3-D models stepped together (sm_100a).
 //
 // Each half-step of every member of a batch is one persistent launch: the grid is sized to
 // the GPU (SMs x resident blocks) and each block walks a table of tiles (member, tile
@@ -6,17 +6,20 @@
 // instead of a handful per model.  Every per-member quantity that changes from step to step
 // (the step index, the running-sum flag, the polarisation ping-pong parity) lives in the
 // member's device state and is advanced on the device, so a CUDA graph of several steps can
-// be replayed unchanged.  The per-cell arithmetic is the single-model code (h2d_cell,
-// e2d_cell, material_cell, the point-source expression), so a member's results are
-// bit-identical to running it alone.
+// be replayed unchanged.  The per-cell arithmetic is the single-model code (h2d_cell /
+// e2d_cell, the 3-D h3d_cell / e3d_cell of the CPML slabs, material_cell, the point-source
+// expression), so a member's results are bit-identical to running it alone.  2-D and 3-D
+// members have their own tile tables and kernels (the 3-D cell code needs more registers);
+// a 3-D tile covers x cells by (y, z) rows numbered y + ny z.
 #pragma once
 
 #include "aux.cuh"
 #include "yee.cuh"
+#include "yee3d_split.cuh"
 
 namespace mfd {
 
-enum { BF_MATH = 1, BF_MAT = 2, BF_FAST = 4 };
+enum { BF_MATH = 1, BF_MAT = 2, BF_FAST = 4, BF_3D = 8 };
 
 // Per-member state (device).  Steps are 1-based; the member runs steps first..last.
 struct BMember {
@@ -29,14 +32,15 @@ struct BMember {
     long long ring_first;                  // 0-based step staged in ring slot 0
     int flags;                             // BF_*
     int pad;
+    Div3 d3;                               // grid-spacing divisors of a 3-D member (div6)
 };
 
-struct BTile {      // cells x0 .. x0+blockDim.x-1, z0 .. z0+blockDim.y-1 of member m
+struct BTile {      // cells x0 .. x0+blockDim.x-1 of rows z0 .. z0+blockDim.y-1 of member m
     int m, x0, z0, pad;
 };
 
-struct BMatTile {   // one row segment of material g's bounding box: x0 .. x0+blockDim.x-1 at iz
-    int m, g, x0, iz;
+struct BMatTile {   // one row segment of material g's bounding box: x0 .. x0+blockDim.x-1 at (iy, iz)
+    int m, g, x0, iy, iz;
 };
 
 struct BSrc {       // one point source of a member (sources.jl:122-131, 235-244)
@@ -128,6 +132,92 @@ __global__ void __launch_bounds__(128) batch_material2d_kernel(const BMember* __
             case 2: material_cell_n<float, double, 2, 2>(m, bi, Ep, c, Dv, cur, p.dt); break;
             case 3: material_cell_n<float, double, 2, 3>(m, bi, Ep, c, Dv, cur, p.dt); break;
             default: material_cell<float, double, 2>(m, ix, 0, tl.iz, Ep, c, Dv, cur, p.dt); break;
+        }
+    }
+}
+
+// 3-D members: the running sums of the previous step are added from a member's second step
+// on; tile rows are (y, z) rows numbered y + ny z.
+template <bool MATH, bool FAST>
+__device__ __forceinline__ void b_h3d(const BMember& M, int ix, int iy, int iz) {
+    const HParams<float>& p = *M.hp;
+    if (M.it == M.first) h3d_cell<float, MATH, FAST, false, false>(p, M.d3, M.it - 1, ix, iy, iz);
+    else if (p.sum_e2) h3d_cell<float, MATH, FAST, true, true>(p, M.d3, M.it - 1, ix, iy, iz);
+    else h3d_cell<float, MATH, FAST, true, false>(p, M.d3, M.it - 1, ix, iy, iz);
+}
+
+__device__ __forceinline__ bool b_row3(const Layout& L, int r, int& iy, int& iz) {
+    if (r >= L.ny * L.nz) return false;
+    iz = r / L.ny;
+    iy = r - iz * L.ny;
+    return true;
+}
+
+__global__ void __launch_bounds__(512) batch_h3d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
+                                                        const int* __restrict__ ntiles) {
+    const int n = *ntiles;
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const BTile tl = tiles[t];
+        const BMember& M = mem[tl.m];
+        if (!b_active(M)) continue;
+        const Layout& L = M.hp->L;
+        const int ix = tl.x0 + threadIdx.x;
+        int iy, iz;
+        if (ix >= L.nx || !b_row3(L, tl.z0 + threadIdx.y, iy, iz)) continue;
+        switch (M.flags & (BF_MATH | BF_FAST)) {
+            case 0: b_h3d<false, false>(M, ix, iy, iz); break;
+            case BF_MATH: b_h3d<true, false>(M, ix, iy, iz); break;
+            case BF_FAST: b_h3d<false, true>(M, ix, iy, iz); break;
+            default: b_h3d<true, true>(M, ix, iy, iz); break;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(512) batch_e3d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
+                                                        const int* __restrict__ ntiles) {
+    const int n = *ntiles;
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const BTile tl = tiles[t];
+        const BMember& M = mem[tl.m];
+        if (!b_active(M)) continue;
+        const EParams<float, double>& p = *M.ep;
+        const int ix = tl.x0 + threadIdx.x;
+        int iy, iz;
+        if (ix >= p.L.nx || !b_row3(p.L, tl.z0 + threadIdx.y, iy, iz)) continue;
+        switch (M.flags & (BF_MAT | BF_FAST)) {
+            case 0: e3d_cell<float, double, false, false>(p, M.d3, ix, iy, iz); break;
+            case BF_MAT: e3d_cell<float, double, true, false>(p, M.d3, ix, iy, iz); break;
+            case BF_FAST: e3d_cell<float, double, false, true>(p, M.d3, ix, iy, iz); break;
+            default: e3d_cell<float, double, true, true>(p, M.d3, ix, iy, iz); break;
+        }
+    }
+}
+
+// ADE / Kerr / plasma response of material g's cells of 3-D members.
+__global__ void __launch_bounds__(128) batch_material3d_kernel(const BMember* __restrict__ mem,
+                                                               const BMatTile* __restrict__ tiles,
+                                                               const int* __restrict__ ntiles) {
+    const int n = *ntiles;
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const BMatTile tl = tiles[t];
+        const BMember& M = mem[tl.m];
+        if (!b_active(M)) continue;
+        const EParams<float, double>& p = *M.ep;
+        const MatDev<float, double>* m = p.mats + (tl.g - 1);
+        const int ix = tl.x0 + threadIdx.x;
+        if (ix >= m->bx0 + m->bnx) continue;
+        const int c = ix + p.L.px * tl.iy + p.L.sz * tl.iz;
+        if (p.geom[c] != tl.g) continue;
+        float Dv[3] = {p.Dx[c], p.Dy[c], p.Dz[c]};
+        float* Ep[3] = {p.Ex, p.Ey, p.Ez};
+        const int cur = (int)((M.it - 1) & 1);
+        const long long bi = (long long)(ix - m->bx0) + (long long)m->bnx * ((tl.iy - m->by0) + (long long)m->bny * (tl.iz - m->bz0));
+        switch (m->nq) {
+            case 0: material_cell_n<float, double, 3, 0>(m, bi, Ep, c, Dv, cur, p.dt); break;
+            case 1: material_cell_n<float, double, 3, 1>(m, bi, Ep, c, Dv, cur, p.dt); break;
+            case 2: material_cell_n<float, double, 3, 2>(m, bi, Ep, c, Dv, cur, p.dt); break;
+            case 3: material_cell_n<float, double, 3, 3>(m, bi, Ep, c, Dv, cur, p.dt); break;
+            default: material_cell<float, double, 3>(m, ix, tl.iy, tl.iz, Ep, c, Dv, cur, p.dt); break;
         }
     }
 }

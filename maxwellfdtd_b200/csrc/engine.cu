@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -93,6 +94,49 @@ static void bounded_sync(cudaStream_t st) {
 }
 
 static long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
+
+// Runs fn(lo, hi) over [0, n) split into contiguous ranges on up to 16 host threads (one
+// range, on the calling thread, below min_per_thread items per thread).
+template <typename Fn>
+static void parallel_ranges(long long n, long long min_per_thread, Fn&& fn) {
+    const long long hw = std::max(1u, std::thread::hardware_concurrency());
+    const long long nth = std::max(1LL, std::min({16LL, hw, n / std::max(1LL, min_per_thread)}));
+    if (nth == 1) {
+        fn(0LL, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const long long chunk = (n + nth - 1) / nth;
+    for (long long t = 0; t < nth; ++t) {
+        const long long lo = t * chunk, hi = std::min(n, lo + chunk);
+        if (lo < hi) th.emplace_back([&fn, lo, hi] { fn(lo, hi); });
+    }
+    for (auto& t : th) t.join();
+}
+
+// True when any byte of [p, p + bytes) is not zero.  A float array that holds only +0.0 is
+// all zero; one holding -0.0 counts as not zero, which only keeps work that changes nothing.
+static bool any_nonzero_bytes(const void* p, size_t bytes) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    std::atomic<bool> found{false};
+    parallel_ranges((long long)bytes, 4LL << 20, [&](long long lo, long long hi) {
+        constexpr long long BLK = 1 << 16;
+        for (long long a = lo; a < hi && !found.load(std::memory_order_relaxed); a += BLK) {
+            const long long e = std::min(hi, a + BLK);
+            uint64_t acc = 0;
+            long long i = a;
+            for (; i < e && (i & 7); ++i) acc |= b[i];
+            for (; i + 8 <= e; i += 8) {
+                uint64_t w;
+                std::memcpy(&w, b + i, 8);
+                acc |= w;
+            }
+            for (; i < e; ++i) acc |= b[i];
+            if (acc) found.store(true, std::memory_order_relaxed);
+        }
+    });
+    return found.load();
+}
 
 // Device memory comes from the device's stream-ordered pool (cudaMallocAsync / cudaFreeAsync
 // on the owning stream): creating or destroying a model then never synchronises the whole
@@ -460,23 +504,43 @@ class Engine : public HandleBase {
         std::vector<int> bx0(nmat + 1, INT32_MAX), bx1(nmat + 1, -1), by0(nmat + 1, INT32_MAX), by1(nmat + 1, -1),
             bz0(nmat + 1, INT32_MAX), bz1(nmat + 1, -1);
         if (d->geometry) {
+            // padded copy of the map and each material's bounding box, z-planes split over
+            // host threads (per-thread boxes merged after)
             gpad.assign((size_t)Np, 0);
-            for (int iz = 0; iz < nz; ++iz)
-                for (int iy = 0; iy < ny; ++iy) {
-                    const uint8_t* row = d->geometry + (size_t)nx * (iy + (size_t)ny * iz);
-                    uint8_t* prow = gpad.data() + (size_t)px * iy + (size_t)sz * iz;
-                    for (int ix = 0; ix < nx; ++ix) {
-                        int g = row[ix];
-                        if (g > nmat) throw Error(MFD_ERR_INVALID, "geometry index beyond nmat");
-                        prow[ix] = (uint8_t)g;
-                        if (g) {
-                            any_geom = true;
-                            bx0[g] = std::min(bx0[g], ix); bx1[g] = std::max(bx1[g], ix);
-                            by0[g] = std::min(by0[g], iy); by1[g] = std::max(by1[g], iy);
-                            bz0[g] = std::min(bz0[g], iz); bz1[g] = std::max(bz1[g], iz);
+            std::mutex mu;
+            bool bad = false;
+            parallel_ranges(nz, 4, [&](long long z0, long long z1) {
+                std::vector<int> a0(nmat + 1, INT32_MAX), a1(nmat + 1, -1), b0(nmat + 1, INT32_MAX), b1(nmat + 1, -1),
+                    c0(nmat + 1, INT32_MAX), c1(nmat + 1, -1);
+                bool any = false, over = false;
+                for (int iz = (int)z0; iz < (int)z1; ++iz)
+                    for (int iy = 0; iy < ny; ++iy) {
+                        const uint8_t* row = d->geometry + (size_t)nx * (iy + (size_t)ny * iz);
+                        uint8_t* prow = gpad.data() + (size_t)px * iy + (size_t)sz * iz;
+                        std::memcpy(prow, row, (size_t)nx);
+                        uint8_t orv = 0;
+                        for (int ix = 0; ix < nx; ++ix) orv |= row[ix];
+                        if (!orv) continue;
+                        for (int ix = 0; ix < nx; ++ix) {
+                            const int g = row[ix];
+                            if (!g) continue;
+                            if (g > nmat) { over = true; continue; }
+                            any = true;
+                            a0[g] = std::min(a0[g], ix); a1[g] = std::max(a1[g], ix);
+                            b0[g] = std::min(b0[g], iy); b1[g] = std::max(b1[g], iy);
+                            c0[g] = std::min(c0[g], iz); c1[g] = std::max(c1[g], iz);
                         }
                     }
+                std::lock_guard<std::mutex> lk(mu);
+                bad = bad || over;
+                any_geom = any_geom || any;
+                for (int g = 1; g <= nmat; ++g) {
+                    bx0[g] = std::min(bx0[g], a0[g]); bx1[g] = std::max(bx1[g], a1[g]);
+                    by0[g] = std::min(by0[g], b0[g]); by1[g] = std::max(by1[g], b1[g]);
+                    bz0[g] = std::min(bz0[g], c0[g]); bz1[g] = std::max(bz1[g], c1[g]);
                 }
+            });
+            if (bad) throw Error(MFD_ERR_INVALID, "geometry index beyond nmat");
         }
         if (any_geom) {
             geom = upload(gpad.data(), gpad.size());
@@ -766,9 +830,7 @@ class Engine : public HandleBase {
         std::vector<bool> nonzero(24, false);
         for (int k = 0; k < narr; ++k) {
             if (!d->tfsf.inc[k]) throw Error(MFD_ERR_INVALID, "missing TFSF incident array");
-            const T* a = (const T*)d->tfsf.inc[k];
-            const size_t n = (size_t)alen[k] * nt;
-            for (size_t i = 0; i < n && !nonzero[k]; ++i) nonzero[k] = a[i] != T(0);
+            nonzero[k] = any_nonzero_bytes(d->tfsf.inc[k], (size_t)alen[k] * nt * sizeof(T));
         }
         RectParams<T>& p = tfsf_p;
         std::memset(&p, 0, sizeof(p));
@@ -1544,7 +1606,7 @@ struct mfd_handle {
 };
 
 // ------------------------------------------------------------------------------------------
-// Batch of 2-D single-precision models (batch.cuh): members are ordinary handles; the batch
+// Batch of 2-D and 3-D single-precision models (batch.cuh): members are ordinary handles; the batch
 // runs each one's steps first..last with persistent batched launches replayed from a CUDA
 // graph of `gsteps` steps, then retires it with the same end-of-run work as mfd_run.
 // ------------------------------------------------------------------------------------------
@@ -1598,15 +1660,17 @@ struct mfd_batch {
     std::vector<Member> mem;
     // tables
     DevBuf<BMember> d_mem;
-    DevBuf<BTile> d_tiles;
-    DevBuf<BMatTile> d_mtiles;
+    DevBuf<BTile> d_tiles, d_tiles3;       // tiles of 2-D / 3-D members
+    DevBuf<BMatTile> d_mtiles, d_mtiles3;
     DevBuf<BSrc> d_srcs;
     DevBuf<BPoint> d_mpts;
     std::vector<std::unique_ptr<DevBuf<BPoint>>> d_spass;
     std::vector<std::unique_ptr<DevBuf<BRow>>> d_tpass;   // TFSF rows of source pass k
     std::vector<int> tpass_n, tpass_len;
-    DevBuf<int> d_counts;   // [0] tiles, [1] material tiles, [2] monitor points, [3 + k] points of source pass k
-    int ntiles = 0, nmtiles = 0, nmpts = 0;
+    // [0] 2-D tiles, [1] 2-D material tiles, [2] monitor points, [3] 3-D tiles, [4] 3-D material
+    // tiles, [5 + k] points of source pass k
+    DevBuf<int> d_counts;
+    int ntiles = 0, nmtiles = 0, nmpts = 0, ntiles3 = 0, nmtiles3 = 0;
     std::vector<int> spass_n;
     // graph
     cudaGraphExec_t gexec = nullptr;
@@ -1628,7 +1692,8 @@ struct mfd_batch {
         if (st) cudaStreamSynchronize(st);
         if (gexec) cudaGraphExecDestroy(gexec);
         for (auto& m : mem) release(m);
-        d_mem.release(); d_tiles.release(); d_mtiles.release(); d_srcs.release(); d_mpts.release(); d_counts.release();
+        d_mem.release(); d_tiles.release(); d_mtiles.release(); d_tiles3.release(); d_mtiles3.release();
+        d_srcs.release(); d_mpts.release(); d_counts.release();
         d_spass.clear();
         d_tpass.clear();
         if (st) cudaStreamSynchronize(st);
@@ -1668,7 +1733,7 @@ struct mfd_batch {
         if (!h || !h->impl) { err = "null handle"; return MFD_ERR_INVALID; }
         E* e = dynamic_cast<E*>(h->impl.get());
         if (!e) { err = "batch members must be single precision with double-precision plasma density (the default)"; return MFD_ERR_INVALID; }
-        if (e->ndim != 2) { err = "batch members must be 2-D models"; return MFD_ERR_INVALID; }
+        if (e->ndim < 2) { err = "batch members must be 2-D or 3-D models"; return MFD_ERR_INVALID; }
         if (e->dev != dev) { err = "batch member on another device"; return MFD_ERR_INVALID; }
         if (e->in_batch) { err = "model already in a batch"; return MFD_ERR_INVALID; }
         if (e->record) { err = "batch members cannot record TFSF data"; return MFD_ERR_INVALID; }
@@ -1678,8 +1743,8 @@ struct mfd_batch {
         MFD_CK(cudaSetDevice(dev));
         Member m{};
         m.h = h; m.e = e; m.first = e->done + 1; m.last = last; m.it = m.first;
-        m.flags = (e->math_needed ? BF_MATH : 0) | (e->any_geom ? BF_MAT : 0) | (e->fastdiv ? BF_FAST : 0);
-        m.cells = (long long)e->nx * e->nz;
+        m.flags = (e->math_needed ? BF_MATH : 0) | (e->any_geom ? BF_MAT : 0) | (e->fastdiv ? BF_FAST : 0) | (e->ndim == 3 ? BF_3D : 0);
+        m.cells = (long long)e->nx * e->ny * e->nz;
         try {
             m.hp = copy_struct(e->hparams(0, 0));
             m.ep = copy_struct(e->eparams());
@@ -1700,8 +1765,8 @@ struct mfd_batch {
     // Tables of the current members and tile shape, then the graph of gsteps steps.
     void rebuild() {
         std::vector<BMember> hm;
-        std::vector<BTile> tiles;
-        std::vector<BMatTile> mt;
+        std::vector<BTile> tiles, tiles3;
+        std::vector<BMatTile> mt, mt3;
         std::vector<BSrc> srcs;
         std::vector<std::vector<BPoint>> passes;
         std::vector<std::vector<BRow>> tpasses;
@@ -1710,14 +1775,18 @@ struct mfd_batch {
         for (size_t i = 0; i < mem.size(); ++i) {
             const Member& m = mem[i];
             E* e = m.e;
-            hm.push_back(BMember{m.hp, m.ep, m.mp, m.rp, m.it, m.first, m.last, e->ring_first, m.flags, 0});
+            hm.push_back(BMember{m.hp, m.ep, m.mp, m.rp, m.it, m.first, m.last, e->ring_first, m.flags, 0, e->d3});
             const int mi = (int)i;
-            for (int z = 0; z < e->nz; z += cur_tz)
-                for (int x = 0; x < e->nx; x += cur_tx) tiles.push_back(BTile{mi, x, z, 0});
+            const bool d3 = e->ndim == 3;
+            const int rows = d3 ? e->ny * e->nz : e->nz;   // 3-D: rows y + ny z
+            for (int z = 0; z < rows; z += cur_tz)
+                for (int x = 0; x < e->nx; x += cur_tx) (d3 ? tiles3 : tiles).push_back(BTile{mi, x, z, 0});
             for (int g : e->response_mats) {
                 const MatDev<float, double>& md = e->mats_host[g - 1];
+                const int y0 = d3 ? md.by0 : 0, y1 = d3 ? md.by0 + md.bny : 1;
                 for (int z = md.bz0; z < md.bz0 + md.bnz; ++z)
-                    for (int x = md.bx0; x < md.bx0 + md.bnx; x += 128) mt.push_back(BMatTile{mi, g, x, z});
+                    for (int y = y0; y < y1; ++y)
+                        for (int x = md.bx0; x < md.bx0 + md.bnx; x += 128) (d3 ? mt3 : mt).push_back(BMatTile{mi, g, x, y, z});
             }
             if (e->tfsf) {   // TFSF acts in source pass tfsf_order, before point source tfsf_order
                 const size_t k = (size_t)e->tfsf_order;
@@ -1738,6 +1807,8 @@ struct mfd_batch {
         d_mem.upload(hm, st);
         d_tiles.upload(tiles, st);
         d_mtiles.upload(mt, st);
+        d_tiles3.upload(tiles3, st);
+        d_mtiles3.upload(mt3, st);
         d_srcs.upload(srcs, st);
         d_mpts.upload(mpts, st);
         if (tpasses.size() > passes.size()) passes.resize(tpasses.size());
@@ -1759,12 +1830,14 @@ struct mfd_batch {
         ring_cap = gsteps;
         for (auto& m : mem)
             if (m.e->need_ring) ring_cap = std::min(ring_cap, m.e->ring_k);
-        if (passes.size() + 3 > 64) throw Error(MFD_ERR_INVALID, "batch members have at most 61 sources");
-        std::vector<int> counts(3 + passes.size());
+        if (passes.size() + 5 > 64) throw Error(MFD_ERR_INVALID, "batch members have at most 59 sources");
+        std::vector<int> counts(5 + passes.size());
         ntiles = counts[0] = (int)tiles.size();
         nmtiles = counts[1] = (int)mt.size();
         nmpts = counts[2] = (int)mpts.size();
-        for (size_t k = 0; k < passes.size(); ++k) counts[3 + k] = spass_n[k];
+        ntiles3 = counts[3] = (int)tiles3.size();
+        nmtiles3 = counts[4] = (int)mt3.size();
+        for (size_t k = 0; k < passes.size(); ++k) counts[5 + k] = spass_n[k];
         d_counts.upload(counts, st);
         MFD_CK(cudaStreamSynchronize(st));
         build_graph();
@@ -1781,7 +1854,7 @@ struct mfd_batch {
     int ring_cap = 16;          // steps per graph replay (gsteps, or less when a member's ring is shorter)
 
     int kernels_per_step() const {
-        int k = 3 + (nmtiles ? 1 : 0) + (nmpts ? 1 : 0);
+        int k = 1 + (ntiles ? 2 : 0) + (ntiles3 ? 2 : 0) + (nmtiles ? 1 : 0) + (nmtiles3 ? 1 : 0) + (nmpts ? 1 : 0);
         for (int n : spass_n) k += n ? 1 : 0;
         for (int n : tpass_n) k += n ? 1 : 0;
         return k;
@@ -1789,18 +1862,35 @@ struct mfd_batch {
 
     void launch_step() {
         const dim3 blk(cur_tx, cur_tz);
-        const int gt = grid_for((const void*)batch_h2d_kernel, cur_tx * cur_tz, ntiles);
-        batch_h2d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
-        batch_e2d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+        if (ntiles) {
+            const int gt = grid_for((const void*)batch_h2d_kernel, cur_tx * cur_tz, ntiles);
+            batch_h2d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+        }
+        if (ntiles3) {
+            const int gt = grid_for((const void*)batch_h3d_kernel, cur_tx * cur_tz, ntiles3);
+            batch_h3d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles3.p, d_counts.p + 3);
+        }
+        if (ntiles) {
+            const int gt = grid_for((const void*)batch_e2d_kernel, cur_tx * cur_tz, ntiles);
+            batch_e2d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+        }
+        if (ntiles3) {
+            const int gt = grid_for((const void*)batch_e3d_kernel, cur_tx * cur_tz, ntiles3);
+            batch_e3d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles3.p, d_counts.p + 3);
+        }
         if (nmtiles) {
             const int g = grid_for((const void*)batch_material2d_kernel, 128, nmtiles);
             batch_material2d_kernel<<<g, 128, 0, st>>>(d_mem.p, d_mtiles.p, d_counts.p + 1);
+        }
+        if (nmtiles3) {
+            const int g = grid_for((const void*)batch_material3d_kernel, 128, nmtiles3);
+            batch_material3d_kernel<<<g, 128, 0, st>>>(d_mem.p, d_mtiles3.p, d_counts.p + 4);
         }
         for (size_t k = 0; k < spass_n.size(); ++k) {
             if (tpass_n[k])
                 batch_tfsf_kernel<<<dim3((unsigned)((tpass_len[k] + 255) / 256), tpass_n[k]), 256, 0, st>>>(d_mem.p, d_tpass[k]->p);
             if (spass_n[k])
-                batch_source_kernel<<<(spass_n[k] + 255) / 256, 256, 0, st>>>(d_mem.p, d_srcs.p, d_spass[k]->p, d_counts.p + 3 + k);
+                batch_source_kernel<<<(spass_n[k] + 255) / 256, 256, 0, st>>>(d_mem.p, d_srcs.p, d_spass[k]->p, d_counts.p + 5 + k);
         }
         if (nmpts) batch_gather_kernel<<<(nmpts + 255) / 256, 256, 0, st>>>(d_mem.p, d_mpts.p, d_counts.p + 2);
         batch_advance_kernel<<<((int)mem.size() + 255) / 256, 256, 0, st>>>(d_mem.p, (int)mem.size());

@@ -204,14 +204,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) h3d_c
     }
 }
 
+// One cell of the 3-D H update with every CPML face it lies in (one thread per cell; also the
+// cell code of batched 3-D models).  prev_step indexes the NaN/Inf flags of the running sums.
 template <typename T, bool MATH, bool FAST, bool ACC, bool E2S>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) h3d_slab_kernel(const __grid_constant__ HParams<T> p, const Div3 D3,
-                                                       const SplitBox s) {
-    const int ix = blockIdx.y * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void h3d_cell(const HParams<T>& p, const Div3& D3, long long prev_step, int ix, int iy, int iz) {
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
-    if (ix >= nx) return;
-    int iy, iz;
-    slab_row(s, ny, (int)blockIdx.x, iy, iz);
     const int sy = p.L.px, sz = p.L.sz;
     const int bxr = p.bc[MFD_XR], byr = p.bc[MFD_YR], bzr = p.bc[MFD_ZR];
     const bool xr = ix == nx - 1, yr = iy == ny - 1, zr = iz == nz - 1;
@@ -229,7 +226,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) h3d_s
         const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
         p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b + d * d) * p.dt;
         if (E2S) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
-        if (maybe_nonfinite(ex)) guard(p, ex);
+        if (maybe_nonfinite(ex)) guard_at(p.flags, prev_step, ex);
     }
     T Mh = p.Mh0;
     if (MATH) {
@@ -263,6 +260,16 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) h3d_s
     p.Hx[c] = hx;
     p.Hy[c] = hy;
     p.Hz[c] = hz;
+}
+
+template <typename T, bool MATH, bool FAST, bool ACC, bool E2S>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) h3d_slab_kernel(const __grid_constant__ HParams<T> p, const Div3 D3,
+                                                       const SplitBox s) {
+    const int ix = blockIdx.y * blockDim.x + threadIdx.x;
+    if (ix >= p.L.nx) return;
+    int iy, iz;
+    slab_row(s, p.L.ny, (int)blockIdx.x, iy, iz);
+    h3d_cell<T, MATH, FAST, ACC, E2S>(p, D3, p.prev_step, ix, iy, iz);
 }
 
 template <typename T>
@@ -372,14 +379,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) e3d_c
     }
 }
 
+// One cell of the 3-D E update with every CPML face it lies in (also the cell code of batched
+// 3-D models).
 template <typename T, typename R, bool MAT, bool FAST>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) e3d_slab_kernel(const __grid_constant__ EParams<T, R> p, const Div3 D3,
-                                                       const SplitBox s) {
-    const int ix = blockIdx.y * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void e3d_cell(const EParams<T, R>& p, const Div3& D3, int ix, int iy, int iz) {
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
-    if (ix >= nx) return;
-    int iy, iz;
-    slab_row(s, ny, (int)blockIdx.x, iy, iz);
     const int sy = p.L.px, sz = p.L.sz;
     const int bxl = p.bc[MFD_XL], byl = p.bc[MFD_YL], bzl = p.bc[MFD_ZL];
     const bool xl = ix == 0, yl = iy == 0, zl = iz == 0;
@@ -434,6 +438,16 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) e3d_s
         p.Ey[c] = D1 * Me;
         p.Ez[c] = D2 * Me;
     }
+}
+
+template <typename T, typename R, bool MAT, bool FAST>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) e3d_slab_kernel(const __grid_constant__ EParams<T, R> p, const Div3 D3,
+                                                       const SplitBox s) {
+    const int ix = blockIdx.y * blockDim.x + threadIdx.x;
+    if (ix >= p.L.nx) return;
+    int iy, iz;
+    slab_row(s, p.L.ny, (int)blockIdx.x, iy, iz);
+    e3d_cell<T, R, MAT, FAST>(p, D3, ix, iy, iz);
 }
 
 }  // namespace mfd

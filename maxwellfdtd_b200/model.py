@@ -125,11 +125,13 @@ class Model:
             return (adapt_range(g.x, dtype), adapt_range(g.z, dtype))
         return (adapt_range(g.x, dtype), adapt_range(g.y, dtype), adapt_range(g.z, dtype))
 
-    def build_desc(self, dtype, monitors=(), tfsf_box=None, rho_fp64=True, device=0):
-        """C descriptor for this model in element type ``dtype`` plus host-side metadata."""
+    def build_desc(self, dtype, monitors=(), tfsf_box=None, rho_fp64=True, device=0, host_alloc=None):
+        """C descriptor for this model in element type ``dtype`` plus host-side metadata.
+        ``host_alloc(n, dtype)`` provides the storage of the large input arrays (e.g.
+        page-locked memory)."""
         dtype = np.dtype(dtype)
         g = self.grid
-        b = _abi.DescBuilder()
+        b = _abi.DescBuilder(host_alloc)
         d = b.desc
         d.abi_version = _abi.ABI_VERSION
         d.ndim = g.ndim

@@ -5,12 +5,14 @@ time; each is admitted when its device-memory footprint fits the budget and a sl
 free, in arrival order.  Its state then stays resident on the device until it completes.
 Admitted work overlaps on the device while earlier requests are still running:
 
-- 2-D single-precision requests join the running batch (mfd_batch_*: persistent launches
-  over all members, CUDA-graph replay), which admits them between its graph replays:
-  continuous batching;
-- every other request (3-D, double precision) runs as a solo lane: its own handle and CUDA
-  stream, stepped from a worker thread (the ctypes calls release the GIL), so several
-  lanes and the batch keep the GPU busy together.
+- 2-D and small 3-D (at most BATCH_3D_MAX_CELLS cells) single-precision requests join the
+  running batch (mfd_batch_*: persistent launches over all members, CUDA-graph replay),
+  which admits them between its graph replays: continuous batching;
+- every other request (larger 3-D, double precision) runs as a solo lane: its own handle
+  and CUDA stream, stepped from a worker thread (the ctypes calls release the GIL), so
+  several lanes and the batch keep the GPU busy together.  A large 3-D grid runs faster on
+  its own: its core rows use the staged z-march kernels, while a batch updates one cell per
+  thread.
 
 Every request computes exactly what it computes alone (a batch member is bit-identical to
 its solo run; a solo lane is a solo run), which the tests check.  The loop records arrival,
@@ -24,6 +26,8 @@ from collections import deque
 import numpy as np
 
 from . import _abi
+
+BATCH_3D_MAX_CELLS = 1 << 20   # 3-D requests up to this many cells join the batch
 
 _NCOMP = {1: 3, 2: 5, 3: 9}
 _NCOMP_E = {1: 1, 2: 2, 3: 3}
@@ -114,7 +118,8 @@ class Request:
         self.cells = g.Nx * g.Ny * g.Nz
         self.cell_updates = self.cells * model.Nt
         d = self.builder.desc
-        self.batchable = g.ndim == 2 and self.dtype == np.float32 and bool(d.rho_fp64) and not d.tfsf_record
+        small = g.ndim == 2 or (g.ndim == 3 and self.cells <= BATCH_3D_MAX_CELLS)
+        self.batchable = small and self.dtype == np.float32 and bool(d.rho_fp64) and not d.tfsf_record
         self.t_submit = self.t_admit = self.t_done = None
         self.t_created = self.t_ran = None       # upload finished, last step finished
         self.stepper = None
@@ -145,8 +150,8 @@ def read_results(st, req, fields=True):
 
 
 class Server:
-    """Admission by device-memory footprint, continuous batching of 2-D requests, solo
-    lanes for the rest; see the module docstring."""
+    """Admission by device-memory footprint, continuous batching of 2-D and small 3-D
+    requests, solo lanes for the rest; see the module docstring."""
 
     def __init__(self, lib, device=0, budget_bytes=160e9, max_active=64, max_solo=16, chunk=64,
                  use_batch=True, keep_results=True, read_fields=False):

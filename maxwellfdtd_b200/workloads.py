@@ -310,15 +310,51 @@ def dielectric_100(nt=1000, n=100):
     return model, [FieldMonitor((0.0, 0.0, 0.0))]
 
 
-def ricker(lam0):
-    """Ricker wavelet of centre frequency c/lam0, delayed by 1.5 periods."""
+def ricker(lam0, ndim=2):
+    """Ricker wavelet of centre frequency c/lam0, delayed by 1.5 periods (a waveform of the
+    coordinates of an ndim-dimensional grid and t)."""
     f0 = C0 / lam0
     t0 = 1.5 / f0
 
-    def w(x, z, t):
+    def r(t):
         a = (np.pi * f0 * (t - t0)) ** 2
         return (1 - 2 * a) * np.exp(-a)
-    return w
+    if ndim == 3:
+        return lambda x, y, z, t: r(t)
+    return lambda x, z, t: r(t)
+
+
+def batch3d(n=64, seed=0, steps_scale=1.0, nmin=48, nmax=128):
+    """List of (model, monitors) of small uneven 3-D models for a batch: sides uniform in
+    [nmin, nmax] (independently per axis), dx = 20 nm, 8-cell CPML, 1-5 spheres with eps in
+    [1, 12] (half of them Debye), a Ricker soft point source, 4 point monitors, 500-2000 steps."""
+    rng = np.random.default_rng(seed)
+    dx = 20e-9
+    out = []
+    for i in range(n):
+        nn = [int(rng.integers(nmin, nmax + 1)) for _ in range(3)]
+        nsteps = max(2, int(round(int(rng.integers(500, 2001)) * steps_scale)))
+        L = [(k - 1) * dx / 2 for k in nn]
+        grid = Grid(xmin=-L[0], xmax=L[0], Nx=nn[0], ymin=-L[1], ymax=L[1], Ny=nn[1], zmin=-L[2], zmax=L[2], Nz=nn[2])
+        dt = time_step(grid, 0.5)
+        mats = []
+        for k in range(int(rng.integers(1, 6))):
+            c = [float(rng.uniform(-0.6, 0.6) * l) for l in L]
+            r = float(rng.uniform(0.05, 0.3) * min(L))
+            geo = (lambda c, r: (lambda x, y, z: (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 <= r * r))(c, r)
+            eps = float(rng.uniform(1, 12))
+            if rng.uniform() < 0.5:
+                chi = DebyeSusceptibility(deps=float(rng.uniform(1, 5)), tau=float(10 ** rng.uniform(-15, -13)))
+                mats.append(Material(geometry=geo, eps=eps, chi=chi))
+            else:
+                mats.append(Material(geometry=geo, eps=eps))
+        lam0 = float(rng.uniform(400e-9, 1600e-9))
+        sp = tuple(float(rng.uniform(-0.4, 0.4) * l) for l in L)
+        src = SoftSource(geometry=sp, waveform=ricker(lam0, ndim=3), component="Ez")
+        mons = [FieldMonitor(tuple(float(rng.uniform(-0.6, 0.6) * l) for l in L)) for _ in range(4)]
+        model = Model(grid, src, tmax=(nsteps - 0.5) * dt, pml=8 * dx, material=mats)
+        out.append((model, mons))
+    return out
 
 
 def batch2d(n=256, seed=0, steps_scale=1.0, nmin=128, nmax=1024):

@@ -1,6 +1,6 @@
-"""Batches of 2-D models (mfd_batch_*): every member's results are bit-identical to running
-it alone with mfd_run, whatever the tile shape, the graph length, the join time or the mix
-of sizes, step counts, materials and sources in the batch."""
+"""Batches of 2-D and 3-D models (mfd_batch_*): every member's results are bit-identical to
+running it alone with mfd_run, whatever the tile shape, the graph length, the join time or
+the mix of sizes, dimensions, step counts, materials and sources in the batch."""
 import numpy as np
 import pytest
 
@@ -172,11 +172,11 @@ def test_batch_nonfinite_member_reports_like_alone(gpu_lib):
 
 def test_batch_rejects_and_guards(gpu_lib):
     batch = _abi.Batch(gpu_lib)
-    m3 = C.model_vacuum(3)
+    m3 = C.model_vacuum(1)
     st3, _, _ = make(m3, None, gpu_lib)
     with pytest.raises(_abi.StepperError) as ei:
         batch.add(st3, m3.Nt)
-    assert ei.value.code == _abi.MFD_ERR_INVALID and "2-D" in str(ei.value)
+    assert ei.value.code == _abi.MFD_ERR_INVALID and "2-D or 3-D" in str(ei.value)
     m, mo = member_model(1)
     st, b, meta = make(m, mo, gpu_lib)
     with pytest.raises(_abi.StepperError):
@@ -258,3 +258,84 @@ def test_batch_tfsf_and_staged_monitors_match_alone(graph, gpu_lib):
     batch.close()
     for st, *_ in held:
         st.close()
+
+
+def outputs_nd(st, model, meta):
+    """Every output of a 2-D or 3-D member: fields, Sa, E2, each monitor's components, status."""
+    nd = model.grid.ndim
+    out = {f"field/{c}": st.read_field(comp_index(c)) for c in field_components(nd)}
+    out["Sa"] = st.read_integral(_abi.MFD_INT_SA)
+    out["E2"] = st.read_integral(_abi.MFD_INT_E2)
+    for k, mm in enumerate(meta["monitors"]):
+        spectral = mm["kind"] == 1
+        for c in field_components(nd):
+            if c.startswith("D"):
+                continue
+            if spectral:
+                shape = (mm["dft"].Nw,) if mm["sum"] else (mm["dft"].Nw, len(mm["cells"]))
+            else:
+                shape = (model.Nt,) if mm["sum"] else (model.Nt, len(mm["cells"]))
+            out[f"mon/{k}/{c}"] = st.read_monitor(k, comp_index(c), shape, spectral)
+    out["status"] = np.array(st.status())
+    return out
+
+
+def members_3d(lib):
+    """3-D members: mixed boundary conditions with CPML kmax != 1 on some faces, conductive and
+    magnetic materials with Debye/Drude/Lorentz/Kerr, three and five poles, plasma, CPML
+    layers that overlap, a TFSF replay (of a record run on lib), and every kind of monitor."""
+    rec = C.run_all(C.model_tfsf_record(3), lib, np.float32, tfsf_box_=C.tfsf_box(3))
+    record = {k[4:]: v for k, v in rec.items() if k.startswith("rec/")}
+    return [(C.model_bcs(3), C.monitors(3)), (C.model_materials(3), C.monitors(3)),
+            (C.model_poles(3, 3, True), None), (C.model_poles(3, 5, False), C.monitors(3)),
+            (C.model_plasma(3), None), (C.model_layers((20, 9, 5), (1, 1, 1, 1, 1, 1)), None),
+            (C.model_tfsf_replay(3, record), C.monitors(3))]
+
+
+@pytest.mark.parametrize("tile,graph", [((0, 0), 16), ((32, 4), 7), ((64, 8), 64)])
+def test_batch_3d_members_match_alone(tile, graph, gpu_lib):
+    """3-D members mixed with 2-D members equal their solo runs bit for bit."""
+    models = members_3d(gpu_lib) + [member_model(s) for s in range(4)] + [rich_member(s) for s in range(2)]
+    ref = []
+    for m, mo in models:
+        st, b, meta = make(m, mo, gpu_lib)
+        st.run(1, m.Nt)
+        ref.append(outputs_nd(st, m, meta))
+        st.close()
+    batch = _abi.Batch(gpu_lib)
+    batch.config(*tile, graph)
+    held = []
+    for m, mo in models:
+        st, b, meta = make(m, mo, gpu_lib)
+        batch.add(st, m.Nt)
+        held.append((st, b, meta, m))
+    batch.run_all(chunk=23)
+    for (st, b, meta, m), r in zip(held, ref):
+        same(r, outputs_nd(st, m, meta))
+    info = batch.info()
+    assert info["cell_updates"] == sum(m.grid.Nx * m.grid.Ny * m.grid.Nz * m.Nt for m, _ in models)
+    batch.close()
+    for st, *_ in held:
+        st.close()
+
+
+def test_batch_3d_member_matches_oracle(oracle_lib, gpu_lib):
+    """A batched 3-D member (materials, monitors) against the CPU oracle: bit for bit, the
+    summed monitors (another summation order) within 1e-5."""
+    m, mo = C.model_materials(3), C.monitors(3)
+    st0, b0, meta0 = make(m, mo, oracle_lib)
+    st0.run(1, m.Nt)
+    ref = outputs_nd(st0, m, meta0)
+    st0.close()
+    batch = _abi.Batch(gpu_lib)
+    st, b, meta = make(m, mo, gpu_lib)
+    batch.add(st, m.Nt)
+    batch.run_all()
+    got = outputs_nd(st, m, meta)
+    for k in ref:
+        if k.startswith("mon/1/") or k.startswith("mon/4/"):
+            np.testing.assert_allclose(got[k], ref[k], rtol=1e-5, atol=1e-30)
+        else:
+            assert np.array_equal(got[k], ref[k], equal_nan=True), k
+    batch.close()
+    st.close()

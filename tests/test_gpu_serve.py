@@ -1,5 +1,5 @@
-"""The serving loop on the GPU: each request's results in the mix (batched 2-D members and
-solo 3-D lanes, admitted as memory frees up) equal its results alone, bit for bit; the
+"""The serving loop on the GPU: each request's results in the mix (batched 2-D and small 3-D
+members, solo lanes, admitted as memory frees up) equal its results alone, bit for bit; the
 admission footprint bounds what mfd_create allocates."""
 import numpy as np
 import pytest
@@ -36,7 +36,10 @@ def test_serve_mix_matches_alone(gpu_lib):
     k = len(reqs)
     for j, (m, mo) in enumerate(workloads.batch2d(n=6, steps_scale=0.01, nmin=64, nmax=160, seed=4)):
         reqs.append(serve.Request(k + j, m, mo, 0.004 * j))
-    assert any(r.batchable for r in reqs) and any(not r.batchable for r in reqs)
+    k = len(reqs)
+    reqs.append(serve.Request(k, C.model_materials(3), C.monitors(3), 0.01, dtype=np.float64))   # a solo lane
+    assert any(r.batchable and r.model.grid.ndim == 3 for r in reqs)
+    assert any(r.batchable and r.model.grid.ndim == 2 for r in reqs) and any(not r.batchable for r in reqs)
     budget = 3 * max(r.bytes for r in reqs)
     srv = serve.Server(gpu_lib, budget_bytes=budget, max_active=6, max_solo=3, chunk=16, read_fields=True)
     st = srv.run(reqs)
