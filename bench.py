@@ -432,7 +432,8 @@ def run_batch2d(args, three=False):
 
 def run_serve(args):
     """Served mixed stream: Poisson arrivals of 2-D and 3-D solves through the serving loop
-    (admission by device memory, continuous batching of 2-D requests, solo lanes for 3-D),
+    (admission by device memory, continuous batching of 2-D and small 3-D requests, solo
+    lanes for the rest),
     against the same requests solved one at a time."""
     import maxwellfdtd_b200 as M
     from maxwellfdtd_b200 import serve, workloads
