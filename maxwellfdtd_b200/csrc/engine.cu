@@ -381,6 +381,8 @@ class Engine : public HandleBase {
     // single-precision 3-D updates split into core rows and CPML slabs (yee3d_split.cuh)
     bool use_split = false;
     SplitBox sbox{};
+    SplitBox mat_rows{};   // core rows/planes holding material cells, aligned to the staged E tiles
+    int mbox[6] = {0, -1, 0, -1, 0, -1};   // bounding box of the material cells (x0, x1, y0, y1, z0, z1; empty: none)
     long long slab_rows = 0;
     int kcount = 1;             // kernels issued by the current launch() call
     // TMA-fed 3-D kernels (single precision)
@@ -541,6 +543,13 @@ class Engine : public HandleBase {
                 }
             });
             if (bad) throw Error(MFD_ERR_INVALID, "geometry index beyond nmat");
+            for (int g = 1; g <= nmat; ++g) {
+                if (bx1[g] < 0) continue;
+                const bool first = mbox[1] < mbox[0];
+                mbox[0] = first ? bx0[g] : std::min(mbox[0], bx0[g]); mbox[1] = std::max(mbox[1], bx1[g]);
+                mbox[2] = first ? by0[g] : std::min(mbox[2], by0[g]); mbox[3] = std::max(mbox[3], by1[g]);
+                mbox[4] = first ? bz0[g] : std::min(mbox[4], bz0[g]); mbox[5] = std::max(mbox[5], bz1[g]);
+            }
         }
         if (any_geom) {
             geom = upload(gpad.data(), gpad.size());
@@ -695,6 +704,19 @@ class Engine : public HandleBase {
         use_split = true;
         if (const char* a = std::getenv("MFD_CORE_ASYNC")) core_async = std::atoi(a) != 0;
         if (const char* z = std::getenv("MFD_ASYNC_ZC")) async_zc = std::max(1, std::atoi(z));
+        // rows and planes of the core box that hold material cells, widened to the staged
+        // E kernel's tiles (AS_TY rows, async_zc planes from the core box's corner)
+        mat_rows = SplitBox{0, 0, 0, 0, async_zc, 0};
+        if (mbox[1] >= mbox[0]) {
+            const int y0 = std::max(mbox[2], yl), y1 = std::min(mbox[3] + 1, yr);
+            const int z0 = std::max(mbox[4], zl), z1 = std::min(mbox[5] + 1, zr);
+            if (y0 < y1 && z0 < z1) {
+                mat_rows.yl = yl + (y0 - yl) / AS_TY * AS_TY;
+                mat_rows.yr = std::min(yr, yl + (y1 - yl + AS_TY - 1) / AS_TY * AS_TY);
+                mat_rows.zl = zl + (z0 - zl) / async_zc * async_zc;
+                mat_rows.zr = std::min(zr, zl + (z1 - zl + async_zc - 1) / async_zc * async_zc);
+            }
+        }
 
     }
 
@@ -1109,22 +1131,34 @@ class Engine : public HandleBase {
         kcount = 0;
         const int zn = sbox.zr - sbox.zl;
         if (sbox.yr > sbox.yl && zn > 0) {
-            // The staged E kernel is used without material cells only: with the material
-            // index it measured slower than e3d_core_kernel (0.239 vs 0.218 ms per E update
-            // at 256^3 with a dispersive sphere), without it faster (0.736 vs 0.720 of the
-            // copy bandwidth, vacuum 256^3).
-            constexpr bool staged = sizeof(T) == 4 && !MAT;
-            if constexpr (staged) {
+            // The staged E kernel has no material-map variant (compiled with the map it
+            // measured slower than e3d_core_kernel: 0.239 vs 0.218 ms per E update at 256^3
+            // with a dispersive sphere).  With a map, the staged kernel without it updates
+            // every tile outside the rows and planes of the materials' bounding box, and the
+            // register march with the map updates those (mat_rows, aligned to the tiles).
+            if constexpr (sizeof(T) == 4) {
                 if (core_async) {
-                    prefer_shared((const void*)e3d_core_async_kernel<R, MAT, FAST>);
+                    prefer_shared((const void*)e3d_core_async_kernel<R, false, FAST>);
                     SplitBox sa = sbox;
                     sa.zc = async_zc;
+                    const int4 skip = MAT ? make_int4(mat_rows.yl, mat_rows.yr, mat_rows.zl, mat_rows.zr) : make_int4(0, 0, 0, 0);
+                    const bool all_mat = MAT && mat_rows.yl == sbox.yl && mat_rows.yr == sbox.yr && mat_rows.zl == sbox.zl &&
+                                         mat_rows.zr == sbox.zr;   // nothing left for the staged kernel
                     dim3 blk(AS_TX, AS_TY), grd((nx + AS_TX - 1) / AS_TX, (sbox.yr - sbox.yl + AS_TY - 1) / AS_TY, (zn + async_zc - 1) / async_zc);
-                    e3d_core_async_kernel<R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sa);
-                    kcount++;
+                    if (!all_mat) {
+                        e3d_core_async_kernel<R, false, FAST><<<grd, blk, 0, st>>>(p, d3, sa, skip);
+                        kcount++;
+                    }
+                    if (MAT && mat_rows.yr > mat_rows.yl && mat_rows.zr > mat_rows.zl) {
+                        SplitBox sm = mat_rows;
+                        sm.zc = zc3;
+                        dim3 blk2(bx3, by3), grd2((nx + bx3 - 1) / bx3, (sm.yr - sm.yl + by3 - 1) / by3, (sm.zr - sm.zl + zc3 - 1) / zc3);
+                        e3d_core_kernel<T, R, MAT, FAST><<<grd2, blk2, 0, st>>>(p, d3, sm);
+                        kcount++;
+                    }
                 }
             }
-            if (!(staged && core_async)) {
+            if (!(sizeof(T) == 4 && core_async)) {
                 dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
                 e3d_core_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sbox);
                 kcount++;

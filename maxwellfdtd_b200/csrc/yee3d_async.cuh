@@ -241,9 +241,11 @@ constexpr int EA_NST = 5, EA_AHEAD = EA_NST - 3;   // the copy issued at plane i
 #define MFD_EASYNC_MINB 8   // blocks of 128 threads per SM e3d_core_async_kernel is compiled for
 #endif
 
+// skip (rows y0 .. y1-1, planes z0 .. z1-1, aligned to the tiles; empty when y0 == y1): the
+// blocks there are left to another kernel (the register march with the material map).
 template <typename R, bool MAT, bool FAST>
 __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_EASYNC_MINB) e3d_core_async_kernel(const __grid_constant__ EParams<float, R> p,
-                                                                        const Div3 D3, const SplitBox s) {
+                                                                        const Div3 D3, const SplitBox s, const int4 skip) {
     __shared__ __align__(16) EAStage S[EA_NST];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AS_TX * ty;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -251,6 +253,7 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_EASYNC_MINB) e3d_core_async
     const int x0 = blockIdx.x * AS_TX;
     const int y0 = s.yl + blockIdx.y * AS_TY;
     const int z0 = s.zl + blockIdx.z * s.zc;
+    if (y0 >= skip.x && y0 < skip.y && z0 >= skip.z && z0 < skip.w) return;   // block-uniform
     const int z1 = min(z0 + s.zc, s.zr);
     const int ix = x0 + tx, iy = y0 + ty;
     const bool act = ix < nx && iy < s.yr;
