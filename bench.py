@@ -34,7 +34,7 @@ sys.path.insert(0, ROOT)
 
 # DRAM traffic of one E and one H update (core + slab kernels) of the 256^3 workload, from one
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum of the launches of one step)
-NCU_TRAFFIC_256 = {"E": 805_242_112, "H": 862_623_744}
+NCU_TRAFFIC_256 = {"E": 760_243_968, "H": 857_313_280}
 
 WORKLOAD = "plasmonics_256: 256^3 FP32, Drude+Lorentz sphere r=60nm, 12-cell CPML, TFSF 600nm/3fs, 6x DFT faces x 64 freq FP64"
 
@@ -278,7 +278,7 @@ def run_gpu(args):
                 "includes": "mfd_create upload from page-locked inputs + K steps + read-back of fields, Sa/E2, spectra into caller-owned page-locked buffers",
                     "host_setup_s_excluded": round(t_desc, 3),
                     "split_s": {"create": round(t_create, 4), "run": round(t_run, 4), "read_back": round(t_read, 4)}},
-            "roofline": {"bound": "hbm", "kernel": "E update (e3d_core_kernel + e3d_slab_kernel)", "achieved": round(e_gbs, 1),
+            "roofline": {"bound": "hbm", "kernel": "E update (e3d_core_async_kernel + e3d_core_kernel on the material rows + e3d_slab_kernel)", "achieved": round(e_gbs, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4),
                          "traffic": NCU_TRAFFIC_256["E"] if args.size == 256 else None,
                          "algorithmic_bytes_per_launch": e_bytes, "mean_launch_ms": round(e_ms, 5),
