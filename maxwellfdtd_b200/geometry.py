@@ -61,7 +61,18 @@ def geometry2indices(geometry, grid, coords=None):
         idx = [int(np.argmin(np.abs(np.asarray(c, dtype=np.float64) - g))) for c, g in zip(cs, geometry)]
         return np.array([linear_index(grid, idx)], dtype=np.int64)
     mask = geometry2bool(geometry, grid, cs)
-    return np.flatnonzero(mask.ravel(order="F")).astype(np.int64)
+    # the linear indices (x fastest) of the set cells, sorted: the row-major positions of the
+    # set cells are converted, rather than making a column-major copy of the whole mask
+    shape = tuple(grid.shape)
+    pos = np.flatnonzero(np.ascontiguousarray(mask))
+    idx = np.unravel_index(pos, shape)
+    lin = np.zeros(len(pos), dtype=np.int64)
+    stride = 1
+    for k, n in enumerate(shape):
+        lin += idx[k].astype(np.int64) * stride
+        stride *= n
+    lin.sort()
+    return lin
 
 
 def cell_coords(grid, cells, coords=None):
