@@ -188,7 +188,9 @@ __global__ void __launch_bounds__(256) monitor_fieldsum_kernel(const MonDev<T>* 
 // thread two points (j and j + blockDim.x, both coalesced).  The block's factors for all
 // staged steps are staged once in shared memory (the same for every point), so the inner
 // loop issues one ring load per point and broadcast shared loads per factor.
+#ifndef MFD_DFT_W
 #define MFD_DFT_W 4   // frequencies per thread (4 measured faster than 8: fewer registers, more warps)
+#endif
 #define MFD_DFT_MAXSLOTS 64
 template <typename T>
 __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __restrict__ mon, int ncomp, int nslots,
