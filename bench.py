@@ -19,6 +19,11 @@ TFSF injection, monitor gather; the DFT accumulation runs every 64 staged steps)
 Multi-GPU: replicas (the path does not shard); each rank runs the same workload on its own
 GPU, scaling "weak".  ``--impl reference`` times the CPU oracle (the restatement of the
 reference's CPU path) on the host cores instead.
+
+Other workloads (``--workload``): ``dielectric100`` (100^3 FP64), ``nonlinear`` (192x192x1024
+FP32 glass with Kerr and plasma), ``batch2d`` (256 uneven 2-D models in one batch),
+``batch3d`` (small uneven 3-D models in one batch), ``serve`` (a Poisson stream of 2-D and
+3-D solves through the serving loop); each prints one JSON line with the same keys.
 """
 import argparse
 import json
