@@ -150,3 +150,47 @@ def test_readers_fill_caller_buffers(oracle_lib):
     with pytest.raises(ValueError):
         st.read_field(6, out=np.empty(st.N, np.float64))
     st.close()
+
+
+def test_geometry_indices_follow_a_column_major_scan():
+    """Monitor and source cell lists are the set cells' linear indices (x fastest), sorted:
+    the same as a column-major scan of the mask, for 1-D, 2-D and 3-D masks."""
+    from maxwellfdtd_b200 import geometry
+
+    class Shape:
+        def __init__(self, shape):
+            self.shape, self.ndim = shape, len(shape)
+
+    rng = np.random.default_rng(1)
+    for shape in [(40,), (13, 1, 7), (9, 5, 4), (1, 6, 11)]:
+        for frac in (0.0, 0.05, 0.5, 1.0):
+            mask = rng.uniform(size=shape) < frac
+            got = geometry.geometry2indices(mask, Shape(shape), coords=[np.arange(n) for n in shape])
+            assert got.dtype == np.int64
+            assert np.array_equal(got, np.flatnonzero(mask.ravel(order="F")))
+
+
+def test_descriptor_inputs_in_caller_storage(oracle_lib):
+    """Model.build_desc(host_alloc=...) puts the large input arrays in storage the caller
+    provides (e.g. page-locked memory); the oracle's results are unchanged."""
+    import cases
+    g = cases.grid3((128, 128, 64))   # a material map of 1 MiB
+    src = M.SoftSource(geometry=(0.0, 0.0, 0.0), waveform=lambda x, y, z, t: 1e3 * cases.pulse(t), component="Ez")
+    ball = M.Material(geometry=lambda x, y, z: x * x + y * y + z * z <= (400e-9) ** 2, eps=2.25)
+    model = M.Model(g, src, tmax=1e-15, pml=0, material=ball)
+    got_alloc = []
+
+    def alloc(n, dtype):
+        a = np.empty(n, dtype)
+        got_alloc.append(a)
+        return a
+
+    outs = []
+    for host_alloc in (None, alloc):
+        b, meta = model.build_desc(np.float32, None, host_alloc=host_alloc)
+        st = _abi.Stepper(oracle_lib, b, np.float32)
+        st.run(1, 5)
+        outs.append(st.read_field(8))
+        st.close()
+    assert got_alloc, "no array went to the caller's storage"
+    assert np.array_equal(outs[0], outs[1])
