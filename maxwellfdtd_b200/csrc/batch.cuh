@@ -157,42 +157,90 @@ __device__ __forceinline__ bool b_row3(const Layout& L, int r, int& iy, int& iz)
     return true;
 }
 
+#ifndef MFD_B3D_SMEM
+#define MFD_B3D_SMEM 1   // a block copies the member's update parameters to shared memory per tile
+#endif
+
+// Copies the member's parameter block (8-byte words) into shared memory; every thread of the
+// block takes part (call it where the whole block is).
+template <typename P>
+__device__ __forceinline__ void b_stage(P* dst, const P* src) {
+    static_assert(sizeof(P) % 8 == 0, "parameter blocks are whole 8-byte words");
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y, nth = blockDim.x * blockDim.y;
+    const long long* s = reinterpret_cast<const long long*>(src);
+    long long* d = reinterpret_cast<long long*>(dst);
+    for (int i = tid; i < (int)(sizeof(P) / 8); i += nth) d[i] = s[i];
+}
+
+template <bool MATH, bool FAST>
+__device__ __forceinline__ void b_h3d_p(const HParams<float>& p, const Div3& d3, long long it, long long first, int ix, int iy,
+                                        int iz) {
+    if (it == first) h3d_cell<float, MATH, FAST, false, false>(p, d3, it - 1, ix, iy, iz);
+    else if (p.sum_e2) h3d_cell<float, MATH, FAST, true, true>(p, d3, it - 1, ix, iy, iz);
+    else h3d_cell<float, MATH, FAST, true, false>(p, d3, it - 1, ix, iy, iz);
+}
+
 __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_h3d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
+    __shared__ __align__(16) HParams<float> sp;
+    __shared__ Div3 sd3;
     const int n = *ntiles;
+    int cur = -1;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
-        if (!b_active(M)) continue;
-        const Layout& L = M.hp->L;
+        if (!b_active(M)) continue;   // the same for the whole block
+        const long long it = M.it, first = M.first;
+        const int flags = M.flags;
+        if (MFD_B3D_SMEM && tl.m != cur) {
+            __syncthreads();          // the previous member's parameters are no longer read
+            b_stage(&sp, M.hp);
+            if (threadIdx.x == 0 && threadIdx.y == 0) sd3 = M.d3;
+            __syncthreads();
+            cur = tl.m;
+        }
+        const HParams<float>& p = MFD_B3D_SMEM ? sp : *M.hp;
+        const Div3& d3 = MFD_B3D_SMEM ? sd3 : M.d3;
         const int ix = tl.x0 + threadIdx.x;
         int iy, iz;
-        if (ix >= L.nx || !b_row3(L, tl.z0 + threadIdx.y, iy, iz)) continue;
-        switch (M.flags & (BF_MATH | BF_FAST)) {
-            case 0: b_h3d<false, false>(M, ix, iy, iz); break;
-            case BF_MATH: b_h3d<true, false>(M, ix, iy, iz); break;
-            case BF_FAST: b_h3d<false, true>(M, ix, iy, iz); break;
-            default: b_h3d<true, true>(M, ix, iy, iz); break;
+        if (ix >= p.L.nx || !b_row3(p.L, tl.z0 + threadIdx.y, iy, iz)) continue;
+        switch (flags & (BF_MATH | BF_FAST)) {
+            case 0: b_h3d_p<false, false>(p, d3, it, first, ix, iy, iz); break;
+            case BF_MATH: b_h3d_p<true, false>(p, d3, it, first, ix, iy, iz); break;
+            case BF_FAST: b_h3d_p<false, true>(p, d3, it, first, ix, iy, iz); break;
+            default: b_h3d_p<true, true>(p, d3, it, first, ix, iy, iz); break;
         }
     }
 }
 
 __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_e3d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
+    __shared__ __align__(16) EParams<float, double> sp;
+    __shared__ Div3 sd3;
     const int n = *ntiles;
+    int cur = -1;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
-        if (!b_active(M)) continue;
-        const EParams<float, double>& p = *M.ep;
+        if (!b_active(M)) continue;   // the same for the whole block
+        const int flags = M.flags;
+        if (MFD_B3D_SMEM && tl.m != cur) {
+            __syncthreads();
+            b_stage(&sp, M.ep);
+            if (threadIdx.x == 0 && threadIdx.y == 0) sd3 = M.d3;
+            __syncthreads();
+            cur = tl.m;
+        }
+        const EParams<float, double>& p = MFD_B3D_SMEM ? sp : *M.ep;
+        const Div3& d3 = MFD_B3D_SMEM ? sd3 : M.d3;
         const int ix = tl.x0 + threadIdx.x;
         int iy, iz;
         if (ix >= p.L.nx || !b_row3(p.L, tl.z0 + threadIdx.y, iy, iz)) continue;
-        switch (M.flags & (BF_MAT | BF_FAST)) {
-            case 0: e3d_cell<float, double, false, false>(p, M.d3, ix, iy, iz); break;
-            case BF_MAT: e3d_cell<float, double, true, false>(p, M.d3, ix, iy, iz); break;
-            case BF_FAST: e3d_cell<float, double, false, true>(p, M.d3, ix, iy, iz); break;
-            default: e3d_cell<float, double, true, true>(p, M.d3, ix, iy, iz); break;
+        switch (flags & (BF_MAT | BF_FAST)) {
+            case 0: e3d_cell<float, double, false, false>(p, d3, ix, iy, iz); break;
+            case BF_MAT: e3d_cell<float, double, true, false>(p, d3, ix, iy, iz); break;
+            case BF_FAST: e3d_cell<float, double, false, true>(p, d3, ix, iy, iz); break;
+            default: e3d_cell<float, double, true, true>(p, d3, ix, iy, iz); break;
         }
     }
 }
