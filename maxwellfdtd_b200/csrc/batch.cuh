@@ -65,40 +65,72 @@ struct BRow {       // TFSF statement s of member m (grid rows of one TFSF pass)
 
 __device__ __forceinline__ bool b_active(const BMember& M) { return M.it <= M.last; }
 
-template <bool MATH, bool FAST>
-__device__ __forceinline__ void b_h2d(const BMember& M, int ix, int iz) {
-    h2d_cell<float, MATH, FAST>(*M.hp, M.it > M.first ? 1 : 0, M.it - 1, ix, iz);
+// Copies the member's parameter block (8-byte words) into shared memory; every thread of the
+// block takes part (call it where the whole block is).
+template <typename P>
+__device__ __forceinline__ void b_stage(P* dst, const P* src) {
+    static_assert(sizeof(P) % 8 == 0, "parameter blocks are whole 8-byte words");
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y, nth = blockDim.x * blockDim.y;
+    const long long* s = reinterpret_cast<const long long*>(src);
+    long long* d = reinterpret_cast<long long*>(dst);
+    for (int i = tid; i < (int)(sizeof(P) / 8); i += nth) d[i] = s[i];
 }
+
+
+#ifndef MFD_B2D_SMEM
+#define MFD_B2D_SMEM 1   // 2-D blocks copy the member's parameters to shared memory per tile (42.1 vs 40.8 Gcell/s)
+#endif
 
 __global__ void __launch_bounds__(512) batch_h2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
+    __shared__ __align__(16) HParams<float> sp;
     const int n = *ntiles;
+    int cur = -1;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
-        if (!b_active(M)) continue;
+        if (!b_active(M)) continue;   // the same for the whole block
+        const int acc = M.it > M.first ? 1 : 0;
+        const long long prev = M.it - 1;
+        const int flags = M.flags;
+        if (MFD_B2D_SMEM && tl.m != cur) {
+            __syncthreads();          // the previous member's parameters are no longer read
+            b_stage(&sp, M.hp);
+            __syncthreads();
+            cur = tl.m;
+        }
+        const HParams<float>& p = MFD_B2D_SMEM ? sp : *M.hp;
         const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
-        if (ix >= M.hp->L.nx || iz >= M.hp->L.nz) continue;
-        switch (M.flags & (BF_MATH | BF_FAST)) {
-            case 0: b_h2d<false, false>(M, ix, iz); break;
-            case BF_MATH: b_h2d<true, false>(M, ix, iz); break;
-            case BF_FAST: b_h2d<false, true>(M, ix, iz); break;
-            default: b_h2d<true, true>(M, ix, iz); break;
+        if (ix >= p.L.nx || iz >= p.L.nz) continue;
+        switch (flags & (BF_MATH | BF_FAST)) {
+            case 0: h2d_cell<float, false, false>(p, acc, prev, ix, iz); break;
+            case BF_MATH: h2d_cell<float, true, false>(p, acc, prev, ix, iz); break;
+            case BF_FAST: h2d_cell<float, false, true>(p, acc, prev, ix, iz); break;
+            default: h2d_cell<float, true, true>(p, acc, prev, ix, iz); break;
         }
     }
 }
 
 __global__ void __launch_bounds__(512) batch_e2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
+    __shared__ __align__(16) EParams<float, double> sp;
     const int n = *ntiles;
+    int cur = -1;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
-        if (!b_active(M)) continue;
-        const EParams<float, double>& p = *M.ep;
+        if (!b_active(M)) continue;   // the same for the whole block
+        const int flags = M.flags;
+        if (MFD_B2D_SMEM && tl.m != cur) {
+            __syncthreads();
+            b_stage(&sp, M.ep);
+            __syncthreads();
+            cur = tl.m;
+        }
+        const EParams<float, double>& p = MFD_B2D_SMEM ? sp : *M.ep;
         const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
         if (ix >= p.L.nx || iz >= p.L.nz) continue;
-        switch (M.flags & (BF_MAT | BF_FAST)) {
+        switch (flags & (BF_MAT | BF_FAST)) {
             case 0: e2d_cell<float, double, false, false>(p, ix, iz); break;
             case BF_MAT: e2d_cell<float, double, true, false>(p, ix, iz); break;
             case BF_FAST: e2d_cell<float, double, false, true>(p, ix, iz); break;
@@ -160,17 +192,6 @@ __device__ __forceinline__ bool b_row3(const Layout& L, int r, int& iy, int& iz)
 #ifndef MFD_B3D_SMEM
 #define MFD_B3D_SMEM 1   // a block copies the member's update parameters to shared memory per tile
 #endif
-
-// Copies the member's parameter block (8-byte words) into shared memory; every thread of the
-// block takes part (call it where the whole block is).
-template <typename P>
-__device__ __forceinline__ void b_stage(P* dst, const P* src) {
-    static_assert(sizeof(P) % 8 == 0, "parameter blocks are whole 8-byte words");
-    const int tid = threadIdx.x + blockDim.x * threadIdx.y, nth = blockDim.x * blockDim.y;
-    const long long* s = reinterpret_cast<const long long*>(src);
-    long long* d = reinterpret_cast<long long*>(dst);
-    for (int i = tid; i < (int)(sizeof(P) / 8); i += nth) d[i] = s[i];
-}
 
 template <bool MATH, bool FAST>
 __device__ __forceinline__ void b_h3d_p(const HParams<float>& p, const Div3& d3, long long it, long long first, int ix, int iy,
