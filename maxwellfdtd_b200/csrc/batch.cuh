@@ -10,7 +10,9 @@
 // e2d_cell, the 3-D h3d_cell / e3d_cell of the CPML slabs, material_cell, the point-source
 // expression), so a member's results are bit-identical to running it alone.  2-D and 3-D
 // members have their own tile tables and kernels (the 3-D cell code needs more registers);
-// a 3-D tile covers x cells by (y, z) rows numbered y + ny z.
+// a 3-D tile covers x cells by (y, z) rows numbered y + ny z.  A block copies its tile's
+// member parameter block into shared memory whenever the member changes, so the cells read
+// the layout, pointers and coefficients from there rather than through dependent global loads.
 #pragma once
 
 #include "aux.cuh"
@@ -172,16 +174,7 @@ __global__ void __launch_bounds__(128) batch_material2d_kernel(const BMember* __
 #define MFD_B3D_MINB 3   // batched 3-D updates held to 40 registers (measured 16.0 against 15.0 Gcell/s at 58)
 #endif
 
-// 3-D members: the running sums of the previous step are added from a member's second step
-// on; tile rows are (y, z) rows numbered y + ny z.
-template <bool MATH, bool FAST>
-__device__ __forceinline__ void b_h3d(const BMember& M, int ix, int iy, int iz) {
-    const HParams<float>& p = *M.hp;
-    if (M.it == M.first) h3d_cell<float, MATH, FAST, false, false>(p, M.d3, M.it - 1, ix, iy, iz);
-    else if (p.sum_e2) h3d_cell<float, MATH, FAST, true, true>(p, M.d3, M.it - 1, ix, iy, iz);
-    else h3d_cell<float, MATH, FAST, true, false>(p, M.d3, M.it - 1, ix, iy, iz);
-}
-
+// 3-D members: tile rows are (y, z) rows numbered y + ny z.
 __device__ __forceinline__ bool b_row3(const Layout& L, int r, int& iy, int& iz) {
     if (r >= L.ny * L.nz) return false;
     iz = r / L.ny;
@@ -193,6 +186,7 @@ __device__ __forceinline__ bool b_row3(const Layout& L, int r, int& iy, int& iz)
 #define MFD_B3D_SMEM 1   // a block copies the member's update parameters to shared memory per tile
 #endif
 
+// The running sums of the previous step are added from a member's second step on.
 template <bool MATH, bool FAST>
 __device__ __forceinline__ void b_h3d_p(const HParams<float>& p, const Div3& d3, long long it, long long first, int ix, int iy,
                                         int iz) {
