@@ -27,7 +27,10 @@
 
 namespace mfd {
 
-constexpr int AS_TX = 32, AS_TY = 4, AS_NST = 5, AS_AHEAD = 3;
+#ifndef MFD_AS_TY
+#define MFD_AS_TY 4   // rows of a staged tile (a block is 32 x MFD_AS_TY threads)
+#endif
+constexpr int AS_TX = 32, AS_TY = MFD_AS_TY, AS_NST = 5, AS_AHEAD = 3;
 constexpr int AS_EW = AS_TX + 4;   // E rows: the tile's 32 columns and the 16-byte chunk holding x+1
 static_assert(AS_NST - AS_AHEAD == 2, "one barrier per plane needs two stages of slack");
 
@@ -49,7 +52,7 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 #ifndef MFD_HASYNC_MINB
-#define MFD_HASYNC_MINB 8   // blocks of 128 threads per SM h3d_core_async_kernel is compiled for
+#define MFD_HASYNC_MINB (1024 / (32 * MFD_AS_TY))   // 1024 resident threads per SM (64 registers)
 #endif
 
 template <bool MATH, bool FAST, bool ACC, bool E2S>
@@ -238,7 +241,7 @@ constexpr int EA_SLOTS = (AS_NE + EA_NO + AS_TX * AS_TY - 1) / (AS_TX * AS_TY);
 constexpr int EA_NST = 5, EA_AHEAD = EA_NST - 3;   // the copy issued at plane iz lands in the stage last read at iz - 2
 
 #ifndef MFD_EASYNC_MINB
-#define MFD_EASYNC_MINB 8   // blocks of 128 threads per SM e3d_core_async_kernel is compiled for
+#define MFD_EASYNC_MINB (1024 / (32 * MFD_AS_TY))   // 1024 resident threads per SM (64 registers)
 #endif
 
 // skip (rows y0 .. y1-1, planes z0 .. z1-1, aligned to the tiles; empty when y0 == y1): the
