@@ -185,13 +185,19 @@ static void* read_scratch(int dev) {
 }
 
 // Exhaustive check of the constant-divisor fast path (see DivC in mfd_device.cuh): for every
-// significand x in [1, 2), the correction step must reproduce IEEE x/d bit for bit.
-__global__ void verify_div_kernel(const float* __restrict__ ds, const float* __restrict__ rs, int* fails) {
+// significand x of the binade [1, 2) and of the band's lowest and highest binades (the
+// values of those binades inside [lo, hi]), the correction step must reproduce IEEE x/d bit
+// for bit.  blockIdx.z selects the binade.
+__global__ void verify_div_kernel(const float* __restrict__ ds, const float* __restrict__ rs, const float* __restrict__ los,
+                                  const float* __restrict__ his, int* fails) {
     const int j = blockIdx.y;
-    const float d = ds[j], r = rs[j];
+    const float d = ds[j], r = rs[j], lo = los[j], hi = his[j];
+    const unsigned eb = blockIdx.z == 0 ? 0x3f800000u
+                      : blockIdx.z == 1 ? (__float_as_uint(lo) & 0x7f800000u) : (__float_as_uint(hi) & 0x7f800000u);
     int bad = 0;
     for (unsigned m = blockIdx.x * blockDim.x + threadIdx.x; m < (1u << 23); m += gridDim.x * blockDim.x) {
-        const float x = __int_as_float(0x3f800000u | m);
+        const float x = __uint_as_float(eb | m);
+        if (x < lo || x > hi) continue;
         const float q0 = __fmul_rn(x, r);
         const float e = __fmaf_rn(-q0, d, x);
         const float q = __fmaf_rn(e, r, q0);
@@ -210,31 +216,39 @@ class DivisorCache {
     // Fills ok for each float divisor; runs the device check for values not seen yet.
     void verify(std::vector<DivC<float>>& dv, cudaStream_t st) {
         std::lock_guard<std::mutex> lk(mu_);
-        std::vector<float> todo_d, todo_r;
+        std::vector<float> todo_d, todo_r, todo_lo, todo_hi;
         for (auto& D : dv) {
             uint32_t key;
             std::memcpy(&key, &D.d, 4);
             if (!known_.count(key) && std::find(todo_d.begin(), todo_d.end(), D.d) == todo_d.end()) {
                 todo_d.push_back(D.d);
                 todo_r.push_back(D.r);
+                todo_lo.push_back(D.lo);
+                todo_hi.push_back(D.hi);
             }
         }
         if (!todo_d.empty()) {
             const int n = (int)todo_d.size();
-            float *dd = nullptr, *dr = nullptr;
+            float *dd = nullptr, *dr = nullptr, *dlo = nullptr, *dhi = nullptr;
             int* df = nullptr;
             MFD_CK(cudaMallocAsync(&dd, n * sizeof(float), st));
             MFD_CK(cudaMallocAsync(&dr, n * sizeof(float), st));
+            MFD_CK(cudaMallocAsync(&dlo, n * sizeof(float), st));
+            MFD_CK(cudaMallocAsync(&dhi, n * sizeof(float), st));
             MFD_CK(cudaMallocAsync(&df, n * sizeof(int), st));
             MFD_CK(cudaMemcpyAsync(dd, todo_d.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
             MFD_CK(cudaMemcpyAsync(dr, todo_r.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+            MFD_CK(cudaMemcpyAsync(dlo, todo_lo.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+            MFD_CK(cudaMemcpyAsync(dhi, todo_hi.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
             MFD_CK(cudaMemsetAsync(df, 0, n * sizeof(int), st));
-            verify_div_kernel<<<dim3(128, n), 256, 0, st>>>(dd, dr, df);
+            verify_div_kernel<<<dim3(128, n, 3), 256, 0, st>>>(dd, dr, dlo, dhi, df);
             MFD_CK(cudaGetLastError());
             std::vector<int> fails(n);
             MFD_CK(cudaMemcpyAsync(fails.data(), df, n * sizeof(int), cudaMemcpyDeviceToHost, st));
             cudaFreeAsync(dd, st);
             cudaFreeAsync(dr, st);
+            cudaFreeAsync(dlo, st);
+            cudaFreeAsync(dhi, st);
             cudaFreeAsync(df, st);
             MFD_CK(cudaStreamSynchronize(st));
             for (int j = 0; j < n; ++j) {
@@ -274,6 +288,13 @@ static EncodeTiledFn encode_tiled() {
     return fn;
 }
 
+// Lowest |x| of the fast path: 2^-100 keeps x - q0 d an exact float (its quantum stays at or
+// above the subnormal one) with two binades of margin; the device check covers the band's
+// lowest binade as well.
+#ifndef MFD_DIV_LO_EXP
+#define MFD_DIV_LO_EXP -100
+#endif
+
 template <typename T>
 static DivC<T> make_div(T d) {
     DivC<T> D{};
@@ -282,7 +303,7 @@ static DivC<T> make_div(T d) {
     D.ok = 0;
     if (sizeof(T) == 4 && d > T(0) && std::isnormal((double)d)) {
         const double r = (double)D.r;
-        D.lo = (T)std::max(std::ldexp(1.0, -76), std::ldexp(1.0, -100) / r);
+        D.lo = (T)std::max(std::ldexp(1.0, MFD_DIV_LO_EXP), std::ldexp(1.0, -100) / r);
         D.hi = (T)std::min(std::ldexp(1.0, 100), std::ldexp(1.0, 100) / r);
         D.ok = (D.lo <= T(1) && D.hi >= T(2)) ? 1 : 0;   // the checked binade lies in the band
         const float lo = (float)D.lo, hi = (float)D.hi;

@@ -47,9 +47,9 @@ struct Layout {
 // Scaling x by 2^k scales q0, e and q by 2^k exactly while all of them stay normal, so the
 // result equals RN(x/d) for every x in the band [lo, hi] (where they do) as soon as it does
 // for every significand of one binade.  The engine checks exactly that on the device, for
-// each divisor, against IEEE division over all 2^23 significands in [1, 2) before the first
-// step; a divisor that fails (or any double-precision divisor) keeps IEEE division
-// (ok = 0), as do numerators outside the band.
+// each divisor, against IEEE division over all 2^23 significands in [1, 2), and over the
+// band's lowest and highest binades, before the first step; a divisor that fails (or any
+// double-precision divisor) keeps IEEE division (ok = 0), as do numerators outside the band.
 // Kernels take FAST = true only when every divisor of the model passed the check; the
 // band test is one unsigned compare on the bit pattern (lob = bits(lo), span = bits(hi) -
 // bits(lo)).  A zero numerator returns x (0/d keeps the sign of x since d > 0).
