@@ -66,6 +66,8 @@ __device__ __forceinline__ T cdiv(T x, const DivC<T>& D) {
     return x / D.d;
 }
 
+__device__ __forceinline__ float qscaled(float x, float d, float r, unsigned lob1, unsigned hib);
+
 template <>
 __device__ __forceinline__ float cdiv<true, float>(float x, const DivC<float>& D) {
     const unsigned ax = __float_as_uint(x) & 0x7fffffffu;
@@ -75,7 +77,7 @@ __device__ __forceinline__ float cdiv<true, float>(float x, const DivC<float>& D
         return __fmaf_rn(e, D.r, q0);
     }
     if (ax == 0u) return x;
-    return __fdiv_rn(x, D.d);
+    return qscaled(x, D.d, D.r, D.lob - 1u, D.lob + D.span);
 }
 
 // The six curl derivatives of a cell divide by the three grid constants.  Div3 holds the
@@ -97,6 +99,23 @@ __device__ __forceinline__ float qcorr(float x, float d, float r) {
 
 // q[i] = RN(x[i] / d[i]) for the six derivatives, d = (dy, dz, dx, dz, dx, dy) in the order
 // (x-y, x-z, y-x, y-z, z-x, z-y) of the curl.
+// RN(x/d) for a numerator outside the band.  A normal x below the band is scaled by 2^32
+// into it (exact), divided by the correction step, and scaled back (exact while the
+// quotient stays normal, |q| >= 2^-126); anything else takes the IEEE division.  lob1 and
+// hib bound the band's bit patterns as in Div3.
+__device__ __forceinline__ float qscaled(float x, float d, float r, unsigned lob1, unsigned hib) {
+    const unsigned ax = __float_as_uint(x) & 0x7fffffffu;
+    if (ax >= 0x00800000u && ax - 1u < lob1) {
+        const float xs = x * 0x1p32f;
+        const unsigned axs = __float_as_uint(xs) & 0x7fffffffu;
+        if (axs - 1u >= lob1 && axs <= hib) {
+            const float qs = qcorr(xs, d, r);
+            if (fabsf(qs) >= 0x1p-94f) return qs * 0x1p-32f;
+        }
+    }
+    return __fdiv_rn(x, d);
+}
+
 template <bool FAST>
 __device__ __forceinline__ void div6(const Div3& D, const float (&x)[6], float (&q)[6]) {
     const float d[6] = {D.dy, D.dz, D.dx, D.dz, D.dx, D.dy};
@@ -114,7 +133,7 @@ __device__ __forceinline__ void div6(const Div3& D, const float (&x)[6], float (
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
             const unsigned ax = __float_as_uint(x[i]) & 0x7fffffffu;
-            if (ax != 0u && (ax - 1u < D.lob1 || ax > D.hib)) q[i] = __fdiv_rn(x[i], d[i]);
+            if (ax != 0u && (ax - 1u < D.lob1 || ax > D.hib)) q[i] = qscaled(x[i], d[i], r[i], D.lob1, D.hib);
         }
     } else {
 #pragma unroll
