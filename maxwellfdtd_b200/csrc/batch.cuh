@@ -37,7 +37,7 @@ struct BMember {
     Div3 d3;                               // grid-spacing divisors of a 3-D member (div6)
 };
 
-struct BTile {      // cells x0 .. x0+blockDim.x-1 of rows z0 .. z0+blockDim.y-1 of member m
+struct BTile {      // cells x0 .. x0+blockDim.x-1 of rows z0 .. z0+blockDim.y-1 of member m (3-D linear tiles: x0 = first cell)
     int m, x0, z0, pad;
 };
 
@@ -174,12 +174,30 @@ __global__ void __launch_bounds__(128) batch_material2d_kernel(const BMember* __
 #define MFD_B3D_MINB 3   // batched 3-D updates held to 40 registers (measured 16.0 against 15.0 Gcell/s at 58)
 #endif
 
+#ifndef MFD_B3D_LINEAR
+#define MFD_B3D_LINEAR 1   // 3-D tiles are runs of cells in x-fastest order (no idle lanes at short rows)
+#endif
+
 // 3-D members: tile rows are (y, z) rows numbered y + ny z.
 __device__ __forceinline__ bool b_row3(const Layout& L, int r, int& iy, int& iz) {
     if (r >= L.ny * L.nz) return false;
     iz = r / L.ny;
     iy = r - iz * L.ny;
     return true;
+}
+
+// The cell of a 3-D tile's thread: with linear tiles x0 is the tile's first cell in
+// x-fastest order and the block's threads take the next blockDim.x * blockDim.y cells;
+// otherwise the tile is x cells x0.. of rows z0...
+__device__ __forceinline__ bool b_cell3(const Layout& L, const BTile& tl, int& ix, int& iy, int& iz) {
+    if (MFD_B3D_LINEAR) {
+        const int l = tl.x0 + (int)(threadIdx.y * blockDim.x + threadIdx.x);
+        const int r = l / L.nx;
+        ix = l - r * L.nx;
+        return b_row3(L, r, iy, iz);
+    }
+    ix = tl.x0 + threadIdx.x;
+    return ix < L.nx && b_row3(L, tl.z0 + threadIdx.y, iy, iz);
 }
 
 #ifndef MFD_B3D_SMEM
@@ -216,9 +234,8 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_h3d_kernel(const BMem
         }
         const HParams<float>& p = MFD_B3D_SMEM ? sp : *M.hp;
         const Div3& d3 = MFD_B3D_SMEM ? sd3 : M.d3;
-        const int ix = tl.x0 + threadIdx.x;
-        int iy, iz;
-        if (ix >= p.L.nx || !b_row3(p.L, tl.z0 + threadIdx.y, iy, iz)) continue;
+        int ix, iy, iz;
+        if (!b_cell3(p.L, tl, ix, iy, iz)) continue;
         switch (flags & (BF_MATH | BF_FAST)) {
             case 0: b_h3d_p<false, false>(p, d3, it, first, ix, iy, iz); break;
             case BF_MATH: b_h3d_p<true, false>(p, d3, it, first, ix, iy, iz); break;
@@ -248,9 +265,8 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_e3d_kernel(const BMem
         }
         const EParams<float, double>& p = MFD_B3D_SMEM ? sp : *M.ep;
         const Div3& d3 = MFD_B3D_SMEM ? sd3 : M.d3;
-        const int ix = tl.x0 + threadIdx.x;
-        int iy, iz;
-        if (ix >= p.L.nx || !b_row3(p.L, tl.z0 + threadIdx.y, iy, iz)) continue;
+        int ix, iy, iz;
+        if (!b_cell3(p.L, tl, ix, iy, iz)) continue;
         switch (flags & (BF_MAT | BF_FAST)) {
             case 0: e3d_cell<float, double, false, false>(p, d3, ix, iy, iz); break;
             case BF_MAT: e3d_cell<float, double, true, false>(p, d3, ix, iy, iz); break;

@@ -1834,8 +1834,13 @@ struct mfd_batch {
             const int mi = (int)i;
             const bool d3 = e->ndim == 3;
             const int rows = d3 ? e->ny * e->nz : e->nz;   // 3-D: rows y + ny z
-            for (int z = 0; z < rows; z += cur_tz)
-                for (int x = 0; x < e->nx; x += cur_tx) (d3 ? tiles3 : tiles).push_back(BTile{mi, x, z, 0});
+            if (d3 && MFD_B3D_LINEAR) {
+                const int ncell = e->nx * rows;
+                for (int l = 0; l < ncell; l += cur_tx * cur_tz) tiles3.push_back(BTile{mi, l, 0, 0});
+            } else {
+                for (int z = 0; z < rows; z += cur_tz)
+                    for (int x = 0; x < e->nx; x += cur_tx) (d3 ? tiles3 : tiles).push_back(BTile{mi, x, z, 0});
+            }
             for (int g : e->response_mats) {
                 const MatDev<float, double>& md = e->mats_host[g - 1];
                 const int y0 = d3 ? md.by0 : 0, y1 = d3 ? md.by0 + md.bny : 1;
