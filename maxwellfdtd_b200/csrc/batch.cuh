@@ -37,8 +37,8 @@ struct BMember {
     Div3 d3;                               // grid-spacing divisors of a 3-D member (div6)
 };
 
-struct BTile {      // cells x0 .. x0+blockDim.x-1 of rows z0 .. z0+blockDim.y-1 of member m (3-D linear tiles: x0 = first cell)
-    int m, x0, z0, pad;
+struct BTile {      // cells x0 .. x0+blockDim.x-1 of rows z0 .. z0+blockDim.y-1 of member m
+    int m, x0, z0, w;  // 3-D linear tiles: (x0, z0, w) = (x, y, z) of the tile's first cell
 };
 
 struct BMatTile {   // one row segment of material g's bounding box: x0 .. x0+blockDim.x-1 at (iy, iz)
@@ -186,15 +186,23 @@ __device__ __forceinline__ bool b_row3(const Layout& L, int r, int& iy, int& iz)
     return true;
 }
 
-// The cell of a 3-D tile's thread: with linear tiles x0 is the tile's first cell in
-// x-fastest order and the block's threads take the next blockDim.x * blockDim.y cells;
-// otherwise the tile is x cells x0.. of rows z0...
+// The cell of a 3-D tile's thread: with linear tiles the block's threads take the
+// blockDim.x * blockDim.y cells in x-fastest order from the tile's first cell (x0, z0, w)
+// = (x, y, z); otherwise the tile is x cells x0.. of rows z0...
 __device__ __forceinline__ bool b_cell3(const Layout& L, const BTile& tl, int& ix, int& iy, int& iz) {
     if (MFD_B3D_LINEAR) {
-        const int l = tl.x0 + (int)(threadIdx.y * blockDim.x + threadIdx.x);
-        const int r = l / L.nx;
-        ix = l - r * L.nx;
-        return b_row3(L, r, iy, iz);
+        // offset / nx row steps, a few at the tile shapes used: cheaper than two divisions
+        ix = tl.x0 + (int)(threadIdx.y * blockDim.x + threadIdx.x);
+        iy = tl.z0;
+        iz = tl.w;
+        while (ix >= L.nx) {
+            ix -= L.nx;
+            if (++iy == L.ny) {
+                iy = 0;
+                ++iz;
+            }
+        }
+        return iz < L.nz;
     }
     ix = tl.x0 + threadIdx.x;
     return ix < L.nx && b_row3(L, tl.z0 + threadIdx.y, iy, iz);

@@ -1836,7 +1836,10 @@ struct mfd_batch {
             const int rows = d3 ? e->ny * e->nz : e->nz;   // 3-D: rows y + ny z
             if (d3 && MFD_B3D_LINEAR) {
                 const int ncell = e->nx * rows;
-                for (int l = 0; l < ncell; l += cur_tx * cur_tz) tiles3.push_back(BTile{mi, l, 0, 0});
+                for (int l = 0; l < ncell; l += cur_tx * cur_tz) {   // (x, y, z) of the tile's first cell
+                    const int r = l / e->nx;
+                    tiles3.push_back(BTile{mi, l - r * e->nx, r % e->ny, r / e->ny});
+                }
             } else {
                 for (int z = 0; z < rows; z += cur_tz)
                     for (int x = 0; x < e->nx; x += cur_tx) (d3 ? tiles3 : tiles).push_back(BTile{mi, x, z, 0});
