@@ -79,6 +79,10 @@ __device__ __forceinline__ void b_stage(P* dst, const P* src) {
 }
 
 
+#ifndef MFD_B2D_CHUNK
+#define MFD_B2D_CHUNK 4  // a block takes runs of this many consecutive tiles (fewer member changes)
+#endif
+
 #ifndef MFD_B2D_SMEM
 #define MFD_B2D_SMEM 1   // 2-D blocks copy the member's parameters to shared memory per tile (42.1 vs 40.8 Gcell/s)
 #endif
@@ -88,7 +92,11 @@ __global__ void __launch_bounds__(512) batch_h2d_kernel(const BMember* __restric
     __shared__ __align__(16) HParams<float> sp;
     const int n = *ntiles;
     int cur = -1;
-    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    // Tile t of the block's k-th turn: runs of MFD_B2D_CHUNK tiles, the runs dealt out to the
+    // blocks in turn, so t grows with k.
+    for (int k = 0;; ++k) {
+        const int t = ((k / MFD_B2D_CHUNK) * (int)gridDim.x + (int)blockIdx.x) * MFD_B2D_CHUNK + k % MFD_B2D_CHUNK;
+        if (t >= n) break;
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
         if (!b_active(M)) continue;   // the same for the whole block
@@ -118,7 +126,11 @@ __global__ void __launch_bounds__(512) batch_e2d_kernel(const BMember* __restric
     __shared__ __align__(16) EParams<float, double> sp;
     const int n = *ntiles;
     int cur = -1;
-    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    // Tile t of the block's k-th turn: runs of MFD_B2D_CHUNK tiles, the runs dealt out to the
+    // blocks in turn, so t grows with k.
+    for (int k = 0;; ++k) {
+        const int t = ((k / MFD_B2D_CHUNK) * (int)gridDim.x + (int)blockIdx.x) * MFD_B2D_CHUNK + k % MFD_B2D_CHUNK;
+        if (t >= n) break;
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
         if (!b_active(M)) continue;   // the same for the whole block
@@ -208,6 +220,10 @@ __device__ __forceinline__ bool b_cell3(const Layout& L, const BTile& tl, int& i
     return ix < L.nx && b_row3(L, tl.z0 + threadIdx.y, iy, iz);
 }
 
+#ifndef MFD_B3D_CHUNK
+#define MFD_B3D_CHUNK 16 // a block takes runs of this many consecutive tiles (fewer member changes)
+#endif
+
 #ifndef MFD_B3D_SMEM
 #define MFD_B3D_SMEM 1   // a block copies the member's update parameters to shared memory per tile
 #endif
@@ -227,7 +243,11 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_h3d_kernel(const BMem
     __shared__ Div3 sd3;
     const int n = *ntiles;
     int cur = -1;
-    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    // Tile t of the block's k-th turn: runs of MFD_B3D_CHUNK tiles, the runs dealt out to the
+    // blocks in turn, so t grows with k.
+    for (int k = 0;; ++k) {
+        const int t = ((k / MFD_B3D_CHUNK) * (int)gridDim.x + (int)blockIdx.x) * MFD_B3D_CHUNK + k % MFD_B3D_CHUNK;
+        if (t >= n) break;
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
         if (!b_active(M)) continue;   // the same for the whole block
@@ -259,7 +279,11 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_e3d_kernel(const BMem
     __shared__ Div3 sd3;
     const int n = *ntiles;
     int cur = -1;
-    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    // Tile t of the block's k-th turn: runs of MFD_B3D_CHUNK tiles, the runs dealt out to the
+    // blocks in turn, so t grows with k.
+    for (int k = 0;; ++k) {
+        const int t = ((k / MFD_B3D_CHUNK) * (int)gridDim.x + (int)blockIdx.x) * MFD_B3D_CHUNK + k % MFD_B3D_CHUNK;
+        if (t >= n) break;
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
         if (!b_active(M)) continue;   // the same for the whole block
