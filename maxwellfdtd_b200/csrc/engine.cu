@@ -1734,7 +1734,7 @@ struct mfd_batch {
     // tiles and autotuning
     int tx = 0, tz = 0;           // fixed shape, or 0 = autotune
     int cur_tx = 32, cur_tz = 8;
-    std::vector<std::pair<int, int>> cands{{32, 4}, {32, 8}, {64, 4}, {128, 2}, {32, 16}, {64, 8}};
+    std::vector<std::pair<int, int>> cands{{32, 4}, {32, 8}, {64, 4}, {128, 2}, {32, 16}, {64, 8}, {32, 2}};
     size_t tune_next = 0;
     std::vector<double> tune_cost;
     bool tuned = false;
