@@ -240,9 +240,11 @@ MFD_API int mfd_read_integral(mfd_handle* h, int32_t which, void* dst);
  * buffer, else MFD_ERR_INVALID with both sizes in mfd_last_error().
  * Nothing in the buffer has to start at zero: each call writes every element it copies out.
  * The buffer is shared by all handles on a device: calls that overlap in time on the same
- * device race on it, so serialise them.  The first call on a device performs the set-up
- * (it looks up the buffer's device address, which makes the driver load the library's
- * device globals): make that first call before any stream capture on that device. */
+ * device race on it, so serialise them.  Each call looks up the buffer's device address on
+ * the current device; the first lookup on a device is the set-up (it makes the driver load
+ * the library's device globals): make that first call before any stream capture on that
+ * device.  A model without plasma returns zeros for JE and rho_end without touching the
+ * device, whatever its plane size, as mfd_read_integral does. */
 #define MFD_NOALLOC_SCRATCH_BYTES (16u << 20)
 MFD_API int mfd_read_integral_noalloc(mfd_handle* h, int32_t which, void* dst);
 

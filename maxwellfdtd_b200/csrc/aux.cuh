@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(256) monitor_fieldsum_kernel(const MonDev<T>* 
 }
 
 // Spectral monitor, per point: S[k][w][j] += F * (2 e_w(t) dt) for each staged step in
-// order (dft.jl:560-566).  A block owns MFD_DFT_W frequencies of 2 * blockDim.x points; each
+// order (dft.jl:43-48).  A block owns MFD_DFT_W frequencies of 2 * blockDim.x points; each
 // thread two points (j and j + blockDim.x, both coalesced).  The block's factors for all
 // staged steps are staged once in shared memory (the same for every point), so the inner
 // loop issues one ring load per point and broadcast shared loads per factor.
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __res
     }
 }
 
-// Spectral monitor with sum: S[k][w] += 2 * sum_j(F_j e_w(t)) * dt (dft.jl:556-559).
+// Spectral monitor with sum: S[k][w] += 2 * sum_j(F_j e_w(t)) * dt (dft.jl:38-41).
 template <typename T>
 __global__ void __launch_bounds__(256) monitor_dftsum_kernel(const MonDev<T>* __restrict__ mon, int ncomp, int nslots,
                                                              long long it0_first, double dt) {
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(256) monitor_dftsum_kernel(const MonDev<T>* __
     if (threadIdx.x == 0) M.S[(long long)k * M.nw + w] = S;
 }
 
-// The per-step DFT factor 2 exp(-i w (t - tshift)) dt of dft.jl:562, from the phasor table.
+// The per-step DFT factor 2 exp(-i w (t - tshift)) dt of dft.jl:44, from the phasor table.
 __global__ void dft_factor_kernel(double2* ph, long long n, double dt) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= n) return;

@@ -166,21 +166,17 @@ static void prefer_shared(const void* f) {
     cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
 }
 
-// Device address of g_read_scratch on the current device, looked up once per device
-// (cudaGetSymbolAddress makes the driver load the module's device globals on first use).
-static void* read_scratch(int dev) {
-    static std::mutex mu;
-    static std::map<int, void*> addr;
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = addr.find(dev);
-    if (it != addr.end()) return it->second;
+// Device address of g_read_scratch on the current device.  Looked up on every call (cheap
+// once the module is loaded; the first lookup makes the driver load the module's device
+// globals), so an address never outlives the context it belongs to: after the host program
+// resets the device, the next call finds the reloaded array.
+static void* read_scratch() {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_read_scratch);
     if (e != cudaSuccess || !p) {
         cudaGetLastError();
         throw Error(MFD_ERR_CUDA, std::string("cudaGetSymbolAddress of the read scratch buffer failed: ") + cudaGetErrorString(e));
     }
-    addr[dev] = p;
     return p;
 }
 
@@ -999,7 +995,7 @@ class Engine : public HandleBase {
                 if (a.nw < 1 || !a.phasor) throw Error(MFD_ERR_INVALID, "spectral monitor needs frequencies");
                 M.S = dalloc<double2>((size_t)ncomp_mon * a.nw * (M.sum ? 1 : a.npts));
                 double2* ph = (double2*)upload(a.phasor, (size_t)nt * a.nw * 2);
-                if (!M.sum) {   // tabulate 2 exp(...) dt once (dft.jl:562)
+                if (!M.sum) {   // tabulate 2 exp(...) dt once (dft.jl:44)
                     const long long n = (long long)nt * a.nw;
                     dft_factor_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ph, n, (double)dt);
                     MFD_CK(cudaGetLastError());
@@ -1573,6 +1569,8 @@ class Engine : public HandleBase {
         if (which == MFD_INT_SA || which == MFD_INT_E2) return read_integral(which, dst);
         if (which != MFD_INT_JE && which != MFD_INT_RHO) { err = "bad integral"; return MFD_ERR_INVALID; }
         const size_t es = which == MFD_INT_JE ? sizeof(T) : sizeof(double);
+        // no plasma: zeros without touching the device, as mfd_read_integral returns them
+        if (!any_plasma || !any_geom) { std::memset(dst, 0, (size_t)N * es); return MFD_OK; }
         const size_t plane = (size_t)nx * ny * es;
         if (plane > (size_t)MFD_NOALLOC_SCRATCH_BYTES) {
             err = "mfd_read_integral_noalloc: one z-plane of this grid is " + std::to_string(plane) +
@@ -1580,8 +1578,7 @@ class Engine : public HandleBase {
                   "-byte scratch buffer; use mfd_read_integral";
             return MFD_ERR_INVALID;
         }
-        if (!any_plasma || !any_geom) { std::memset(dst, 0, (size_t)N * es); return MFD_OK; }
-        unsigned char* scratch = (unsigned char*)read_scratch(dev);
+        unsigned char* scratch = (unsigned char*)read_scratch();
         if (!noalloc_ready) {   // load the kernel now rather than at its first launch
             cudaFuncAttributes fa;
             MFD_CK(cudaFuncGetAttributes(&fa, scatter_state_planes_kernel<T, R>));
@@ -2197,17 +2194,43 @@ int mfd_batch_info(const mfd_batch* b, int32_t* tile_x, int32_t* tile_z, double*
 }
 
 const char* mfd_batch_last_error(const mfd_batch* b) { return b ? b->err.c_str() : "null batch"; }
-int mfd_read_field(mfd_handle* h, int32_t comp, void* dst) { MFD_GUARD(h, h->impl->read_field(comp, dst)); }
-int mfd_write_field(mfd_handle* h, int32_t comp, const void* src) { MFD_GUARD(h, h->impl->write_field(comp, src)); }
-int mfd_read_integral(mfd_handle* h, int32_t which, void* dst) { MFD_GUARD(h, h->impl->read_integral(which, dst)); }
+// A NULL host buffer is an argument error (MFD_ERR_INVALID), never a copy to address 0.
+#define MFD_NEED_BUF(h, buf)                                           \
+    do {                                                               \
+        if (!(h) || !(h)->impl) return MFD_ERR_INVALID;                \
+        if (!(buf)) {                                                  \
+            (h)->impl->err = "null host buffer";                       \
+            return MFD_ERR_INVALID;                                    \
+        }                                                              \
+    } while (0)
+
+int mfd_read_field(mfd_handle* h, int32_t comp, void* dst) {
+    MFD_NEED_BUF(h, dst);
+    MFD_GUARD(h, h->impl->read_field(comp, dst));
+}
+int mfd_write_field(mfd_handle* h, int32_t comp, const void* src) {
+    MFD_NEED_BUF(h, src);
+    MFD_GUARD(h, h->impl->write_field(comp, src));
+}
+int mfd_read_integral(mfd_handle* h, int32_t which, void* dst) {
+    MFD_NEED_BUF(h, dst);
+    MFD_GUARD(h, h->impl->read_integral(which, dst));
+}
 int mfd_read_integral_noalloc(mfd_handle* h, int32_t which, void* dst) {
+    MFD_NEED_BUF(h, dst);
     MFD_GUARD(h, h->impl->read_integral_noalloc(which, dst));
 }
 int mfd_set_snapshots(mfd_handle* h, int32_t ncomp, const int32_t* comps, int64_t nsteps, const int64_t* steps, void* dst) {
     MFD_GUARD(h, h->impl->set_snapshots(ncomp, comps, nsteps, steps, dst));
 }
-int mfd_read_monitor(mfd_handle* h, int32_t m, int32_t comp, void* dst) { MFD_GUARD(h, h->impl->read_monitor(m, comp, dst)); }
-int mfd_read_tfsf_record(mfd_handle* h, int32_t k, void* dst) { MFD_GUARD(h, h->impl->read_record(k, dst)); }
+int mfd_read_monitor(mfd_handle* h, int32_t m, int32_t comp, void* dst) {
+    MFD_NEED_BUF(h, dst);
+    MFD_GUARD(h, h->impl->read_monitor(m, comp, dst));
+}
+int mfd_read_tfsf_record(mfd_handle* h, int32_t k, void* dst) {
+    MFD_NEED_BUF(h, dst);
+    MFD_GUARD(h, h->impl->read_record(k, dst));
+}
 
 int64_t mfd_tfsf_record_size(const mfd_handle* h, int32_t k) {
     if (!h || !h->impl) return 0;

@@ -49,7 +49,7 @@ class DFT:
             ws = np.asarray(w, dtype=np.float64).ravel()
         self.w = ws
         self.Nw = len(ws)
-        # phase exp(-1im*w*(t - tshift)) (dft.jl:545-569): (t - tshift) in T, times -w in double
+        # phase exp(-1im*w*(t - tshift)) (dft.jl:40, 44): (t - tshift) in T, times -w in double
         d = (np.asarray(t_T, dtype=T) - T(tshift)).astype(np.float64)
         theta = (-ws)[None, :] * d[:, None]
         ph = np.empty((Nt, self.Nw, 2))

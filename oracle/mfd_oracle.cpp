@@ -52,6 +52,27 @@ struct OracleBase {
     virtual void status(int64_t* done, int64_t* bad, int32_t* kind) const = 0;
 };
 
+// IonizationRate functor in T precision (examples/5_nonlinear_propagation/IonizationRate.jl:
+// 30-52): 0 for x <= 0, else 10^linterp(log10(x)) on the table's log10 knots X (even
+// spacing, increasing) and log10 rates Y; linterp takes the first segment below X[0], the
+// last above X[n-1], and otherwise segment searchsortedfirst(X, xi) - 1.
+template <typename T>
+T ionization_rate(const T* X, const T* Y, size_t n, T x) {
+    if (x <= 0) return 0;
+    T xi = std::log10(x);
+    size_t i;
+    if (xi <= X[0]) i = 0;
+    else if (xi >= X[n - 1]) i = n - 2;
+    else {
+        size_t j = 0;   // searchsortedfirst(x, xi) - 1 (0-based: first j with X[j] >= xi, minus 1)
+        while (X[j] < xi) ++j;
+        i = j - 1;
+    }
+    T dydx = (Y[i + 1] - Y[i]) / (X[i + 1] - X[i]);
+    T yl = Y[i] + dydx * (xi - X[i]);
+    return std::pow((T)10, yl);
+}
+
 // Layer profile (src/pml.jl:46-52).  0-based: a left layer covers cells [0, ib-1] with pml
 // index ix; a right layer covers [ib-1, n-1] with pml index ix-(ib-1).
 template <typename T>
@@ -467,23 +488,7 @@ struct Oracle : OracleBase {
         }
     }
 
-    // IonizationRate functor, T precision (IonizationRate.jl:42-52).
-    T rate_table(const Mat<T, R>& M, T x) const {
-        if (x <= 0) return 0;
-        T xi = std::log10(x);
-        const std::vector<T>&X = M.rate_x, &Y = M.rate_y;
-        size_t n = X.size(), i;
-        if (xi <= X[0]) i = 0;
-        else if (xi >= X[n - 1]) i = n - 2;
-        else {
-            size_t j = 0;   // searchsortedfirst(x, xi) - 1 (0-based: first j with X[j] >= xi, minus 1)
-            while (X[j] < xi) ++j;
-            i = j - 1;
-        }
-        T dydx = (Y[i + 1] - Y[i]) / (X[i + 1] - X[i]);
-        T yl = Y[i] + dydx * (xi - X[i]);
-        return std::pow((T)10, yl);
-    }
+    T rate_table(const Mat<T, R>& M, T x) const { return ionization_rate<T>(M.rate_x.data(), M.rate_y.data(), M.rate_x.size(), x); }
 
     template <typename Q>
     void plasma_rho(Mat<T, R>& M, size_t c, Q R1, T E2) {
@@ -986,8 +991,27 @@ struct Oracle : OracleBase {
         }
     }
 
+    // Julia's sum over an array (Base.mapreduce_impl, pairwise_blocksize 1024): fewer than 16
+    // terms, or a block of at most 1024, are added left to right; longer ranges split at
+    // their midpoint and add the two halves' sums.  The leaf loop of Base carries @simd, which
+    // lets LLVM reassociate inside a block for the host's vector width, so a Julia run can
+    // differ from this tree in the last bits of a summed monitor; the tree above the blocks
+    // is the same.  val(p) gives the p-th term.
+    template <typename U, typename V>
+    static U julia_sum(size_t lo, size_t hi, const V& val) {   // terms [lo, hi)
+        const size_t n = hi - lo;
+        if (n == 0) return U(0);
+        if (n <= 1024) {
+            U v = val(lo);
+            for (size_t p = lo + 1; p < hi; ++p) v = v + val(p);
+            return v;
+        }
+        const size_t mid = lo + (n - 1) / 2 + 1;   // ifirst + (ilast - ifirst) >> 1, inclusive
+        return julia_sum<U>(lo, mid, val) + julia_sum<U>(mid, hi, val);
+    }
+
     // update_monitor! (monitors.jl:59-69, 107-119, 161-179, 253-258, 299-305, 350-359) and
-    // the DFT accumulation (dft.jl:545-569).
+    // the DFT accumulation (dft.jl:36-51).
     void update_monitors(int64_t it) {
         for (auto& M : mons) {
             size_t np = M.cells.size();
@@ -995,10 +1019,8 @@ struct Oracle : OracleBase {
                 if (!has_comp(comp) || is_D(comp)) continue;
                 const std::vector<T>& FC = F[comp];
                 if (M.kind == MFD_MON_FIELD) {
-                    if (M.sum) {
-                        T s = 0;
-                        for (size_t p = 0; p < np; ++p) s += FC[M.cells[p]];
-                        M.rec[comp][it - 1] = s;
+                    if (M.sum) {   // sum(field.X[inds]) (monitors.jl:62-63, 110-112, 164-169)
+                        M.rec[comp][it - 1] = julia_sum<T>(0, np, [&](size_t p) { return FC[M.cells[p]]; });
                     } else {
                         T* dst = M.rec[comp].data() + (size_t)(it - 1) * np;
                         for (size_t p = 0; p < np; ++p) dst[p] = FC[M.cells[p]];
@@ -1008,12 +1030,9 @@ struct Oracle : OracleBase {
                     double dtd = (double)dt;
                     for (int iw = 0; iw < M.nw; ++iw) {
                         double er = ph[2 * iw], ei = ph[2 * iw + 1];
-                        if (M.sum) {
-                            double sr = 0, si = 0;
-                            for (size_t p = 0; p < np; ++p) {
-                                double f = (double)FC[M.cells[p]];
-                                sr += f * er; si += f * ei;
-                            }
+                        if (M.sum) {   // 2 * sum(F * exp(...)) * dt (dft.jl:40)
+                            const double sr = julia_sum<double>(0, np, [&](size_t p) { return (double)FC[M.cells[p]] * er; });
+                            const double si = julia_sum<double>(0, np, [&](size_t p) { return (double)FC[M.cells[p]] * ei; });
                             std::complex<double>& S = M.S[comp][iw];
                             S = std::complex<double>(S.real() + (2 * sr) * dtd, S.imag() + (2 * si) * dtd);
                         } else {
@@ -1222,6 +1241,21 @@ int64_t oracle_tfsf_record_size(void* h, int32_t k) { return ((OracleBase*)h)->r
 int oracle_status(void* h, int64_t* d, int64_t* b, int32_t* k) { ((OracleBase*)h)->status(d, b, k); return MFD_OK; }
 const char* oracle_last_error(void* h) { return ((OracleBase*)h)->err.c_str(); }
 const char* oracle_create_error(void) { return g_create_error.c_str(); }
+
+// The ionisation-rate table functor on its own (for the tests that pin it to the
+// reference's IonizationRate semantics): x, y are the table's log10 knots as passed in
+// mfd_material.rate_x / rate_y, cast to float when f32 != 0 as the library does.
+int oracle_eval_rate_table(const double* x, const double* y, int32_t n, int32_t f32, const double* I, double* out,
+                           int64_t count) {
+    if (!x || !y || n < 2 || !I || !out || count < 0) return MFD_ERR_INVALID;
+    if (f32) {
+        std::vector<float> X(x, x + n), Y(y, y + n);
+        for (int64_t k = 0; k < count; ++k) out[k] = (double)ionization_rate<float>(X.data(), Y.data(), (size_t)n, (float)I[k]);
+    } else {
+        for (int64_t k = 0; k < count; ++k) out[k] = ionization_rate<double>(x, y, (size_t)n, I[k]);
+    }
+    return MFD_OK;
+}
 int oracle_set_threads(int n) {
 #ifdef _OPENMP
     if (n > 0) omp_set_num_threads(n);

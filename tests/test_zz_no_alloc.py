@@ -4,6 +4,9 @@ The allocation-free read stages JE and rho_end through a fixed device buffer a f
 at a time; it must return exactly what mfd_read_integral returns (tolerance: bit-identical,
 the same values are gathered by the same arithmetic), on two calls in a row, for grids that
 fit in one chunk and grids that need several, and refuse grids whose z-plane does not fit.
+It must also do what it exists for: take no device memory.  The device's default memory
+pool (the one mfd_read_integral's temporary comes from) is watched through the driver API:
+its high-water mark of memory in use must not rise during the reads.
 """
 import ctypes as C
 
@@ -98,5 +101,72 @@ def test_noalloc_refuses_planes_beyond_scratch(gpu_lib):
         ref = st.read_integral(_abi.MFD_INT_JE)
         rc, got = _read_noalloc(st, _abi.MFD_INT_JE)
         assert rc == _abi.MFD_OK and np.array_equal(ref, got)
+    finally:
+        st.close()
+
+
+def test_noalloc_large_planes_without_plasma(gpu_lib):
+    """A model without plasma returns zeros for JE and rho_end from both reads, even when one
+    z-plane would not fit the scratch buffer (nothing is staged)."""
+    g = cases.grid3((1500, 1500, 2))
+    src = M.SoftSource(geometry=(0.0, 0.0, 0.0), waveform=lambda x, y, z, t: cases.pulse(t), component="Ex")
+    model = M.Model(g, src, tmax=1.5 * 0.5 / cases.C0 / np.sqrt(3 / (50e-9) ** 2), pml=0)
+    st = _stepper(model, gpu_lib, np.float32)
+    try:
+        for which in (_abi.MFD_INT_JE, _abi.MFD_INT_RHO):
+            ref = st.read_integral(which)
+            rc, got = _read_noalloc(st, which)
+            assert rc == _abi.MFD_OK, st.lib.last_error(st.h).decode()
+            assert np.array_equal(ref, got) and not got.any()
+    finally:
+        st.close()
+
+
+CU_MEMPOOL_ATTR_USED_MEM_CURRENT, CU_MEMPOOL_ATTR_USED_MEM_HIGH = 7, 8
+
+
+def _default_pool(device=0):
+    """(used_now, used_high, reset_high) of the device's default memory pool (driver API)."""
+    cu = C.CDLL("libcuda.so.1")
+    cu.cuInit.argtypes = [C.c_uint]
+    cu.cuDeviceGet.argtypes = [C.POINTER(C.c_int), C.c_int]
+    cu.cuDeviceGetDefaultMemPool.argtypes = [C.POINTER(C.c_void_p), C.c_int]
+    cu.cuMemPoolGetAttribute.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    cu.cuMemPoolSetAttribute.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    assert cu.cuInit(0) == 0
+    dev = C.c_int()
+    assert cu.cuDeviceGet(C.byref(dev), device) == 0
+    pool = C.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(C.byref(pool), dev.value) == 0
+
+    def get(attr):
+        v = C.c_uint64()
+        assert cu.cuMemPoolGetAttribute(pool, attr, C.byref(v)) == 0
+        return v.value
+
+    def reset_high():   # the only value the high-water mark may be set to is 0 (= current use)
+        z = C.c_uint64(0)
+        assert cu.cuMemPoolSetAttribute(pool, CU_MEMPOOL_ATTR_USED_MEM_HIGH, C.byref(z)) == 0
+
+    return (lambda: get(CU_MEMPOOL_ATTR_USED_MEM_CURRENT)), (lambda: get(CU_MEMPOOL_ATTR_USED_MEM_HIGH)), reset_high
+
+
+def test_noalloc_takes_no_device_memory(gpu_lib):
+    st = _stepper(cases.model_plasma(3, "power"), gpu_lib, np.float32)
+    try:
+        used, high, reset_high = _default_pool()
+        # the watch sees allocations: mfd_read_integral's grid-sized temporary raises the mark
+        reset_high()
+        base = used()
+        st.read_integral(_abi.MFD_INT_JE)
+        assert high() > base
+        # the allocation-free read, every output, twice in a row: the mark stays put
+        reset_high()
+        base = used()
+        for _ in range(2):
+            for which in WHICH:
+                rc, _ = _read_noalloc(st, which)
+                assert rc == _abi.MFD_OK, st.lib.last_error(st.h).decode()
+        assert high() == base == used()
     finally:
         st.close()
