@@ -7,7 +7,12 @@ step of the whole grid (H update with the deferred Sa/E2 sums, E update with CPM
 TFSF injection, monitor gather; the DFT accumulation runs every 64 staged steps).
 
   value   : Gcell-updates/s with all inputs resident in HBM, CUDA events on the library's
-            stream around the K timed steps (one mfd_run call), max over ranks.
+            stream around the K timed steps (one mfd_run call), max over ranks.  The model is
+            the configuration's 4000-step run; the timed steps follow W warm-up steps, and a
+            second window (value_late) times K steps after step 1500, when the pulse fills
+            the TFSF box.  --mode selects the arithmetic of the field updates (fast: the
+            tolerance mode, the default; exact: the reference's operation order bit for bit);
+            other_mode times the same window in the other one.
   e2e     : the same metric through the public API with host buffers: model upload
             (mfd_create), K steps, and the read-back of the final fields, Sa/E2 and the DFT
             spectra, wall-clock with the device synchronised.
@@ -37,9 +42,11 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM traffic of one E and one H update (core + slab kernels) of the 256^3 workload, from one
-# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum of the launches of one step)
-NCU_TRAFFIC_256 = {"E": 760_243_968, "H": 857_313_280}
+# DRAM traffic of one E and one H update (core + slab kernels) of the 256^3 workload, per
+# arithmetic mode, from one ncu capture of the launches of one step (dram__bytes_read.sum +
+# dram__bytes_write.sum); the capture and its command are in NCU_TRAFFIC_SOURCE.
+NCU_TRAFFIC_256 = {("exact", "E"): 760_243_968, ("exact", "H"): 857_313_280}
+NCU_TRAFFIC_SOURCE = "profiles/update_traffic_256.md"
 
 WORKLOAD = "plasmonics_256: 256^3 FP32, Drude+Lorentz sphere r=60nm, 12-cell CPML, TFSF 600nm/3fs, 6x DFT faces x 64 freq FP64"
 
@@ -130,7 +137,8 @@ class ClockSampler:
         except ValueError:
             return None
 
-    def summary(self):
+    def summary(self, window=None):
+        window = window or self.window
         if self.proc is None or not os.path.exists(self.path):
             return None
         rows = []
@@ -142,8 +150,8 @@ class ClockSampler:
         if not rows:
             return None
         inside = rows
-        if self.window is not None:
-            t0, t1 = self.window
+        if window is not None:
+            t0, t1 = window
             stamped = [(self._t(r[0]), r) for r in rows]
             stamped = [(t, r) for t, r in stamped if t is not None]
             inside = [r for t, r in stamped if t0 <= t <= t1]
@@ -177,6 +185,14 @@ def dist_setup():
     return ws, rank, local
 
 
+def _timed_window(st, a, b):
+    """Steps a..b in one mfd_run call: (device ms from CUDA events, kernel launches)."""
+    k0 = st.kernel_times()
+    st.run(a, b)
+    k1 = st.kernel_times()
+    return st.last_run_ms(), int(sum(k1[k][1] - k0[k][1] for k in k1))
+
+
 def run_gpu(args):
     import maxwellfdtd_b200 as M
     from maxwellfdtd_b200 import _abi, workloads
@@ -191,37 +207,49 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     W, K = args.warmup, args.steps
-    nt = W + 2 * K + 2
+    late = max(args.late_start, W + 2 * K) if args.late_start > 0 else 0
+    nt = max(4000, late + K + 1)   # the configuration runs 4000 steps; the TFSF data cover them all
     model, mons = workloads.plasmonics_256(nt=nt, n=args.size)
     dtype = np.float32
     lib = M.load_library()
-    b, meta = model.build_desc(dtype, mons, device=local)
+    b, meta = model.build_desc(dtype, mons, device=local, mode=args.mode)
     st = _abi.Stepper(lib, b, dtype)
     N = model.grid.Nx * model.grid.Ny * model.grid.Nz
     clk = ClockSampler(local).start()
-    # warm-up
-    st.run(1, W)
-    kt0 = st.kernel_times()
+    st.run(1, W)                # warm-up
     if ws > 1:
         dist.barrier()
         torch.cuda.synchronize()
     t_w0 = time.time()
-    st.run(W + 1, W + K)        # timed: K steps in one call, CUDA events around it on the library's stream
-    clk.mark(t_w0, time.time())
-    clk.stop()
-    ms = st.last_run_ms()
-    kt1 = st.kernel_times()
-    launches = int(sum(kt1[k][1] - kt0[k][1] for k in kt1))
+    ms, launches = _timed_window(st, W + 1, W + K)   # timed: K steps, CUDA events on the library's stream
+    win_early = (t_w0, time.time())
     # the next K steps again with an event pair around every launch: per-kernel device times
+    kt0 = st.kernel_times()
     st.set_profiling(True)
     st.run(W + K + 1, W + 2 * K)
     st.set_profiling(False)
-    kt2 = st.kernel_times()
-    kt0, kt1 = kt1, kt2
+    kt1 = st.kernel_times()
+    ms_late = None
+    win_late = None
+    if late:
+        # a second timed window once the pulse fills the TFSF box (steps after `late`)
+        st.run(W + 2 * K + 1, late)
+        if ws > 1:
+            dist.barrier()
+            torch.cuda.synchronize()
+        t_l0 = time.time()
+        ms_late, _ = _timed_window(st, late + 1, late + K)
+        win_late = (t_l0, time.time())
+    clk.stop()
     dev_bytes = st.device_bytes()
     st.close()
     ms_max = max_over_ranks(ms, ws)
     value = N * K * ws / (ms_max * 1e-3) / 1e9
+    late_out = None
+    if late:
+        ms_late = max_over_ranks(ms_late, ws)
+        late_out = {"value": round(N * K * ws / (ms_late * 1e-3) / 1e9, 3), "ms_per_step": round(ms_late / K, 4),
+                    "steps": [late + 1, late + K], "clocks": clk.summary(win_late)}
     h_bytes, e_bytes = algorithmic_bytes(model, meta, dtype)
     # one E update and one H update per step, each a core-rows kernel plus a CPML-slab kernel
     e_ms = (kt1["E"][0] - kt0["E"][0]) / K
@@ -231,13 +259,23 @@ def run_gpu(args):
     h_gbs = h_bytes / (h_ms * 1e-3) / 1e9
     per_kernel = {k: {"ms": round(kt1[k][0] - kt0[k][0], 4), "launches": int(kt1[k][1] - kt0[k][1])} for k in kt1}
 
+    # the other arithmetic mode on the same workload: the same window on its own handle
+    other = "exact" if args.mode == "fast" else "fast"
+    b3, _ = model.build_desc(dtype, mons, device=local, mode=other)
+    st3 = _abi.Stepper(lib, b3, dtype)
+    st3.run(1, W)
+    ms3, _ = _timed_window(st3, W + 1, W + K)
+    st3.close()
+    ms3 = max_over_ranks(ms3, ws)
+    other_out = {"mode": other, "value": round(N * K * ws / (ms3 * 1e-3) / 1e9, 3), "ms_per_step": round(ms3 / K, 4)}
+
     plain = plain_stepper(lib, args, local) if rank == 0 and not args.no_plain else None
 
     # end to end through the public API with host buffers: results land in page-locked
     # buffers the caller owns (allocated once, before the timed region)
     pinned = _pinned_outputs(model, meta, dtype)
     t0 = time.perf_counter()
-    b2, meta2 = model.build_desc(dtype, mons, device=local, host_alloc=_pinned_array)
+    b2, meta2 = model.build_desc(dtype, mons, device=local, host_alloc=_pinned_array, mode=args.mode)
     t_desc = time.perf_counter() - t0
     h2d = sum(a.nbytes for a in b2.keep if isinstance(a, np.ndarray))
     t0 = time.perf_counter()
@@ -262,7 +300,7 @@ def run_gpu(args):
     out = None
     if rank == 0:
         cpu = None if (args.no_cpu or ws > 1) else cpu_baseline(args, model, mons)
-        err = None if (args.no_cpu or ws > 1) else headline_error(lib, local)
+        err = None if (args.no_cpu or ws > 1) else headline_error(lib, local, mode=args.mode)
         out = {
             "metric": "Gcell-updates/s",
             "value": round(value, 3),
@@ -276,8 +314,11 @@ def run_gpu(args):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [args.size] * 3, "cells": N, "steps_per_sim": 4000,
+            "config": {"workload": WORKLOAD, "grid": [args.size] * 3, "cells": N, "steps_per_sim": nt,
+                       "timed_steps": [W + 1, W + K], "mode": args.mode,
                        "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (fields 604 MB)"},
+            "value_late": late_out,
+            "other_mode": other_out,
             "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d / K),
                     "d2h_bytes_per_step": int(d2h / K),
                 "includes": "mfd_create upload from page-locked inputs + K steps + read-back of fields, Sa/E2, spectra into caller-owned page-locked buffers",
@@ -285,11 +326,12 @@ def run_gpu(args):
                     "split_s": {"create": round(t_create, 4), "run": round(t_run, 4), "read_back": round(t_read, 4)}},
             "roofline": {"bound": "hbm", "kernel": "E update (e3d_core_async_kernel + e3d_core_kernel on the material rows + e3d_slab_kernel)", "achieved": round(e_gbs, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4),
-                         "traffic": NCU_TRAFFIC_256["E"] if args.size == 256 else None,
+                         "traffic": NCU_TRAFFIC_256.get((args.mode, "E")) if args.size == 256 else None,
+                         "traffic_source": NCU_TRAFFIC_SOURCE,
                          "algorithmic_bytes_per_launch": e_bytes, "mean_launch_ms": round(e_ms, 5),
                          "peak_kind": peak_kind,
                          "h_kernel": {"achieved": round(h_gbs, 1), "frac": round(h_gbs / peak, 4),
-                                      "traffic": NCU_TRAFFIC_256["H"] if args.size == 256 else None,
+                                      "traffic": NCU_TRAFFIC_256.get((args.mode, "H")) if args.size == 256 else None,
                                       "algorithmic_bytes_per_launch": h_bytes, "mean_launch_ms": round(h_ms, 5)}},
             "kernels": per_kernel,
             "plain_stepper": plain,
@@ -297,7 +339,7 @@ def run_gpu(args):
             "device_bytes": dev_bytes,
             "cpu_baseline": cpu,
             "error_vs_fp64_oracle": err,
-            "clocks": clk.summary(),
+            "clocks": clk.summary(win_early),
         }
         print(json.dumps(out), flush=True)
     if ws > 1:
@@ -632,7 +674,7 @@ def plain_stepper(lib, args, device, steps=20):
     and their HBM roofline fractions, CUDA events per update."""
     from maxwellfdtd_b200 import _abi, workloads
     model, _ = workloads.plain_256(nt=steps + 5, n=args.size)
-    b, meta = model.build_desc(np.float32, None, device=device)
+    b, meta = model.build_desc(np.float32, None, device=device, mode=args.mode)
     st = _abi.Stepper(lib, b, np.float32)
     st.run(1, 3)
     k0 = st.kernel_times()
@@ -647,7 +689,7 @@ def plain_stepper(lib, args, device, steps=20):
     h_ms = (k1["H"][0] - k0["H"][0]) / steps
     e_ms = (k1["E"][0] - k0["E"][0]) / steps
     N = model.grid.Nx * model.grid.Ny * model.grid.Nz
-    return {"workload": f"plain_256: {args.size}^3 FP32 vacuum, 12-cell CPML, soft point source, Sa sum",
+    return {"workload": f"plain_256: {args.size}^3 FP32 vacuum, 12-cell CPML, soft point source, Sa sum, {args.mode} mode",
             "value": round(N * steps / (ms * 1e-3) / 1e9, 3), "unit": "Gcell-updates/s", "steps": steps,
             "h_update": {"ms": round(h_ms, 5), "bytes": h_bytes, "frac": round(h_bytes / (h_ms * 1e-3) / 1e9 / peak, 4)},
             "e_update": {"ms": round(e_ms, 5), "bytes": e_bytes, "frac": round(e_bytes / (e_ms * 1e-3) / 1e9 / peak, 4)},
@@ -680,7 +722,7 @@ def _pinned_outputs(model, meta, dtype):
     return out
 
 
-def headline_error(lib, device, n=96, steps=60):
+def headline_error(lib, device, n=96, steps=60, mode="exact"):
     """Relative L2 error of the single-precision GPU result against the FP64 oracle on an
     n^3 version of the headline configuration (same spacing, sphere, TFSF and monitors
     scaled with the grid): the E and H vectors, Sa, and the DFT spectra; and the distance to
@@ -692,7 +734,7 @@ def headline_error(lib, device, n=96, steps=60):
     model, mons = workloads.plasmonics_256(nt=steps, n=n)
     res = {}
     for tag, lb, dt in (("gpu", lib, np.float32), ("fp64", oracle, np.float64), ("fp32", oracle, np.float32)):
-        b, meta = model.build_desc(dt, mons, device=device if lb is lib else 0)
+        b, meta = model.build_desc(dt, mons, device=device if lb is lib else 0, mode=mode if lb is lib else "exact")
         st = _abi.Stepper(lb, b, dt)
         st.run(1, model.Nt)
         o = {c: st.read_field(comp_index(c)) for c in ("Hx", "Hy", "Hz", "Ex", "Ey", "Ez")}
@@ -711,7 +753,8 @@ def headline_error(lib, device, n=96, steps=60):
         return 0.0 if den == 0 else float(np.linalg.norm(a - b) / den)
     return {"rel_l2": {g: rel(vec(res["gpu"], cs), vec(res["fp64"], cs)) for g, cs in groups.items()},
             "gpu_vs_fp32_oracle": {g: rel(vec(res["gpu"], cs), vec(res["fp32"], cs)) for g, cs in groups.items()},
-            "how": f"{n}^3 version of the workload (dx=2nm, same sphere, TFSF and DFT faces scaled), {steps} steps"}
+            "how": f"{n}^3 version of the workload (dx=2nm, same sphere, TFSF and DFT faces scaled), {steps} steps, "
+                   f"GPU in the {mode} mode"}
 
 
 def _oracle_lib():
@@ -782,6 +825,10 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=40, help="steps of the CPU-baseline sample (about 10 s on 16 cores)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-stepper roofline measurement")
+    ap.add_argument("--mode", default="fast", choices=["fast", "exact"],
+                    help="arithmetic of the field updates (fast: the tolerance mode; exact: bit-identical order)")
+    ap.add_argument("--late-start", type=int, default=1500,
+                    help="plasmonics: steps run before the second timed window (0: no late window)")
     ap.add_argument("--workload", default="plasmonics", choices=["plasmonics", "batch2d", "batch3d", "serve", "dielectric100", "nonlinear"])
     ap.add_argument("--err-steps", type=int, default=300, help="nonlinear: steps of the oracle comparison")
     ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")

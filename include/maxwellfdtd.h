@@ -49,7 +49,7 @@ extern "C" {
 #define MFD_API
 #endif
 
-#define MFD_ABI_VERSION 1
+#define MFD_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------------------ */
 enum {
@@ -65,6 +65,20 @@ enum {
 
 /* ---- element types ---------------------------------------------------------------- */
 enum { MFD_F32 = 0, MFD_F64 = 1 };
+
+/* ---- arithmetic of the field updates (mfd_desc.mode) ---------------------------------
+ * MFD_MODE_EXACT: every cell update in the reference's operation order with no fused
+ *   multiply-add, IEEE square roots and divisions (a division by a grid constant or a CPML
+ *   kappa takes a correction step that the library verifies, per divisor, to give the IEEE
+ *   quotient for every single-precision significand): fields are bit-identical to a CPU
+ *   run of the same order in the same precision.
+ * MFD_MODE_FAST: the tolerance mode.  Derivatives multiply by the reciprocal of the grid
+ *   constant or kappa, the H/D/CPML/running-sum updates are fused multiply-adds and the
+ *   Poynting norm uses the hardware reciprocal square root (single precision).  Results
+ *   stay within relative L2 1e-5 (FP32) / 1e-12 (FP64) of the exact order; the material
+ *   response (ADE, Kerr, plasma), sources and monitors keep the exact arithmetic.  Batch
+ *   members must be MFD_MODE_EXACT. */
+enum { MFD_MODE_EXACT = 0, MFD_MODE_FAST = 1 };
 
 /* ---- boundary conditions: the reference's bc2int codes (src/models.jl:1199-1217) ---- */
 enum { MFD_BC_PERIODIC = 1, MFD_BC_DIRICHLET = 2, MFD_BC_NEUMANN = 3 };
@@ -107,8 +121,20 @@ enum {
  *   1z: incHy, incEz; 2z: incHy, incEz; x1: incHy, incEx; x2: incHy, incEx.
  * 1-D: the 4 arrays of TFSFSource1D (sources.jl:272-279): incHy_1, incEx_1, incHy_2, incEx_2.
  * Each array is [nt][face extent] in T, the face extent laid out as in the reference
- * (column-major (a, b, Nt) => C order [nt][b][a]). */
+ * (column-major (a, b, Nt) => C order [nt][b][a]).
+ *
+ * An array may be passed in a compact form (mfd_tfsf.shape[k]), which the library expands
+ * on the fly: the incident data of a plane wave along a grid axis vary along one face axis
+ * or none, so [nt][b] or [nt] values describe the whole face for every step.  A face's
+ * axes (a, b) are its two in-plane grid axes in x, y, z order (face 1yz: a = y, b = z;
+ * x1z: a = x, b = z; xy1: a = x, b = y; a 2-D face has b of extent 1).
+ *   MFD_INC_FULL    [nt][b][a]  every value (the reference's layout; the default)
+ *   MFD_INC_ALONG_B [nt][b]     the same for every a (value (ia, ib) = v[ib])
+ *   MFD_INC_ALONG_A [nt][a]     the same for every b (value (ia, ib) = v[ia])
+ *   MFD_INC_UNIFORM [nt]        one value per step for the whole face
+ * Device memory and upload then grow with nt times the compact extent only. */
 #define MFD_TFSF_MAX_ARRAYS 24
+enum { MFD_INC_FULL = 0, MFD_INC_ALONG_B = 1, MFD_INC_ALONG_A = 2, MFD_INC_UNIFORM = 3 };
 
 /* One CPML layer profile (reference PMLLayer, src/pml.jl:46-121).  nb = 0: no layer. */
 typedef struct mfd_pml_layer {
@@ -160,6 +186,7 @@ typedef struct mfd_tfsf {
     int32_t i1[3];           /* 1-based (ix1, iy1, iz1)                               */
     int32_t i2[3];           /* 1-based (ix2, iy2, iz2)                               */
     const void* inc[MFD_TFSF_MAX_ARRAYS];
+    int32_t shape[MFD_TFSF_MAX_ARRAYS];   /* MFD_INC_* layout of inc[k] (0: full)   */
 } mfd_tfsf;
 
 /* Field or spectral monitor (reference monitors.jl:7-373, dft.jl:1-51). */
@@ -197,6 +224,7 @@ typedef struct mfd_desc {
     int32_t rec_i1[3];       /* 1-based record box                                   */
     int32_t rec_i2[3];
     int32_t device;          /* CUDA device ordinal                                   */
+    int32_t mode;            /* MFD_MODE_EXACT / MFD_MODE_FAST                         */
 } mfd_desc;
 
 typedef struct mfd_handle mfd_handle;

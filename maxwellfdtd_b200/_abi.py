@@ -5,11 +5,13 @@ import os
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 MFD_OK, MFD_ERR_INVALID, MFD_ERR_OOM, MFD_ERR_CUDA, MFD_ERR_NONFINITE, MFD_ERR_TIMEOUT, \
     MFD_ERR_ADMISSION, MFD_ERR_NODEVICE = range(8)
 MFD_F32, MFD_F64 = 0, 1
+MFD_MODE_EXACT, MFD_MODE_FAST = 0, 1
+MFD_INC_FULL, MFD_INC_ALONG_B, MFD_INC_ALONG_A, MFD_INC_UNIFORM = range(4)
 MFD_INT_SA, MFD_INT_E2, MFD_INT_JE, MFD_INT_RHO = range(4)
 MFD_RATE_NONE, MFD_RATE_POWER, MFD_RATE_TABLE = range(3)
 MFD_MON_FIELD, MFD_MON_SPECTRAL = range(2)
@@ -40,7 +42,7 @@ class Source(C.Structure):
 
 class Tfsf(C.Structure):
     _fields_ = [("enabled", C.c_int32), ("order", C.c_int32), ("i1", C.c_int32 * 3), ("i2", C.c_int32 * 3),
-                ("inc", C.c_void_p * 24)]
+                ("inc", C.c_void_p * 24), ("shape", C.c_int32 * 24)]
 
 
 class Monitor(C.Structure):
@@ -62,7 +64,7 @@ class Desc(C.Structure):
                 ("tfsf", Tfsf),
                 ("nmon", C.c_int32), ("mons", C.POINTER(Monitor)),
                 ("tfsf_record", C.c_int32), ("rec_i1", C.c_int32 * 3), ("rec_i2", C.c_int32 * 3),
-                ("device", C.c_int32)]
+                ("device", C.c_int32), ("mode", C.c_int32)]
 
 
 def dptr(a):

@@ -38,7 +38,10 @@ struct RectStmt {
     int tprec;        // 1: coefficient and product in T; 0: in double
     double coef;
     double coefT;     // T-rounded coefficient for tprec
-    long long len;    // rectangle size (= array length per step)
+    long long len;    // rectangle size
+    int shape;        // MFD_INC_* layout of the incident array (TFSF; record arrays are full)
+    int na;           // extent of the face's first in-plane axis (a)
+    long long clen;   // array values per step: len, len / na, na or 1 by shape
     unsigned long long prev;   // earlier statements of the same component whose rectangle meets this one
     unsigned long long next;   // later ones
 };
@@ -52,6 +55,16 @@ struct RectParams {
     T* arr[24];       // TFSF: incident arrays; record: destination arrays
     RectStmt s[MFD_MAX_STMT];
 };
+
+// Offset within a step's incident values of rectangle element `local` = ia + na * ib.
+__device__ __forceinline__ long long inc_off(const RectStmt& s, long long local) {
+    switch (s.shape) {
+        case MFD_INC_ALONG_B: return local / s.na;
+        case MFD_INC_ALONG_A: return local % s.na;
+        case MFD_INC_UNIFORM: return 0;
+        default: return local;
+    }
+}
 
 __device__ __forceinline__ bool rect_has(const RectStmt& s, int ix, int iy, int iz) {
     return ix >= s.x0 && ix <= s.x1 && iy >= s.y0 && iy <= s.y1 && iz >= s.z0 && iz <= s.z1;
@@ -90,10 +103,10 @@ __device__ __forceinline__ void tfsf_point(const RectParams<T>& p, int si, int l
         if (rect_has(p.s[__ffsll((long long)m) - 1], ix, iy, iz)) return;
     T* F = p.F[s.comp];
     const int c = ix + p.L.px * iy + p.L.sz * iz;
-    T v = tfsf_apply(s, F[c], p.arr[s.k][it0 * s.len + local]);
+    T v = tfsf_apply(s, F[c], p.arr[s.k][it0 * s.clen + inc_off(s, local)]);
     for (unsigned long long m = s.next; m; m &= m - 1) {
         const RectStmt& t = p.s[__ffsll((long long)m) - 1];
-        if (rect_has(t, ix, iy, iz)) v = tfsf_apply(t, v, p.arr[t.k][it0 * t.len + rect_local(t, ix, iy, iz)]);
+        if (rect_has(t, ix, iy, iz)) v = tfsf_apply(t, v, p.arr[t.k][it0 * t.clen + inc_off(t, rect_local(t, ix, iy, iz))]);
     }
     F[c] = v;
 }

@@ -27,7 +27,6 @@
 
 #include "aux.cuh"
 #include "yee.cuh"
-#include "yee3d_tma.cuh"
 #include "yee3d_async.cuh"
 #include "yee3d_split.cuh"
 #include "batch.cuh"
@@ -265,25 +264,6 @@ class DivisorCache {
     std::map<uint32_t, bool> known_;
 };
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed).
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_tiled() {
-    static EncodeTiledFn fn = [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess) {
-            cudaGetLastError();
-            return (EncodeTiledFn) nullptr;
-        }
-        return (EncodeTiledFn)p;
-    }();
-    return fn;
-}
-
 // Lowest |x| of the fast path: 2^-100 keeps x - q0 d an exact float (its quantum stays at or
 // above the subnormal one) with two binades of margin; the device check covers the band's
 // lowest binade as well.
@@ -321,6 +301,7 @@ class Engine : public HandleBase {
     T dx{}, dy{}, dz{}, dt{};
     DivC<T> ddx{}, ddy{}, ddz{};
     bool fastdiv = false;        // every divisor passed the device check
+    bool recip = false;          // tolerance mode: derivatives by reciprocal multiply, fused multiply-adds
     Div3 d3{};                   // grid constants for the branch-free 3-D division (single precision)
     int bc[6] = {1, 1, 1, 1, 1, 1};
     cudaStream_t st = nullptr;
@@ -386,7 +367,6 @@ class Engine : public HandleBase {
     int* d_flags = nullptr;     // [nt] per-step NaN/Inf flags of Ex
     int* h_flags = nullptr;     // host copy
     std::vector<int> h_flags_v;
-    int h_timeout_v = 0;
 
     int64_t done = 0, bad_step = 0;
     int32_t bad_kind = 0;
@@ -402,13 +382,6 @@ class Engine : public HandleBase {
     int mbox[6] = {0, -1, 0, -1, 0, -1};   // bounding box of the material cells (x0, x1, y0, y1, z0, z1; empty: none)
     long long slab_rows = 0;
     int kcount = 1;             // kernels issued by the current launch() call
-    // TMA-fed 3-D kernels (single precision)
-    bool use_tma = false;
-    int tma_zc = 16;
-    HTmaParams htma{};
-    ETmaParams<R> etma{};
-    int* d_timeout = nullptr;   // set by a kernel whose bounded wait ran out
-    int* h_timeout = nullptr;
 
     // timing
     bool profiling = false;
@@ -497,6 +470,7 @@ class Engine : public HandleBase {
         N = (long long)nx * ny * nz;
         nt = d->nt;
         dx = (T)d->dx; dy = (T)d->dy; dz = (T)d->dz; dt = (T)d->dt;
+        recip = d->mode == MFD_MODE_FAST;
         if (Np >= (1ll << 31)) throw Error(MFD_ERR_INVALID, "grid too large: padded cell count must stay below 2^31");
         {
             std::vector<DivC<T>> dv = {make_div<T>(dx), make_div<T>(dy), make_div<T>(dz)};
@@ -686,24 +660,6 @@ class Engine : public HandleBase {
             }
         }
         init_split();
-        d_timeout = dalloc<int>(1);
-        h_timeout = &h_timeout_v;
-        init_tma();
-    }
-
-    // Tensor maps of the TMA-fed 3-D kernels: dims (nx, ny, nz) so cells beyond the grid are
-    // out of bounds (zero-filled); strides of the padded layout (multiples of 16 bytes).
-    bool make_map(CUtensorMap* m, const void* base, bool u8, unsigned bx, unsigned by) {
-        EncodeTiledFn fn = encode_tiled();
-        if (!fn) return false;
-        const size_t es = u8 ? 1 : sizeof(T);
-        cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
-        cuuint64_t strides[2] = {(cuuint64_t)px * es, (cuuint64_t)sz * es};
-        cuuint32_t box[3] = {bx, by, 1};
-        cuuint32_t estr[3] = {1, 1, 1};
-        return fn(m, u8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims,
-                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     }
 
     // The split needs layers that do not overlap in any dimension; MFD_KERNEL3D=unsplit
@@ -735,33 +691,6 @@ class Engine : public HandleBase {
             }
         }
 
-    }
-
-    void init_tma() {
-        if (ndim != 3 || sizeof(T) != 4 || !std::getenv("MFD_TMA")) return;
-        if (const char* z = std::getenv("MFD_TMA_ZC")) tma_zc = std::max(1, std::atoi(z));
-        const uint8_t* gm = geom ? geom : (const uint8_t*)F[MFD_HX];
-        const void* e2 = E2 ? (const void*)E2 : (const void*)Sa;
-        bool ok = true;
-        ok = ok && make_map(&htma.mEx, F[MFD_EX], false, 32, 9);
-        ok = ok && make_map(&htma.mEy, F[MFD_EY], false, 36, 8);
-        ok = ok && make_map(&htma.mEz, F[MFD_EZ], false, 36, 9);
-        ok = ok && make_map(&htma.mHx, F[MFD_HX], false, 32, 8);
-        ok = ok && make_map(&htma.mHy, F[MFD_HY], false, 32, 8);
-        ok = ok && make_map(&htma.mHz, F[MFD_HZ], false, 32, 8);
-        ok = ok && make_map(&htma.mSa, Sa, false, 32, 8);
-        ok = ok && make_map(&htma.mE2, e2, false, 32, 8);
-        ok = ok && make_map(&htma.mG, gm, geom != nullptr, 32, 8);
-        ok = ok && make_map(&etma.mHx, F[MFD_HX], false, 32, 9);
-        ok = ok && make_map(&etma.mHy, F[MFD_HY], false, 36, 8);
-        ok = ok && make_map(&etma.mHz, F[MFD_HZ], false, 36, 9);
-        ok = ok && make_map(&etma.mDx, F[MFD_DX], false, 32, 8);
-        ok = ok && make_map(&etma.mDy, F[MFD_DY], false, 32, 8);
-        ok = ok && make_map(&etma.mDz, F[MFD_DZ], false, 32, 8);
-        ok = ok && make_map(&etma.mG, gm, geom != nullptr, 32, 8);
-        htma.timeout = d_timeout;
-        etma.timeout = d_timeout;
-        use_tma = ok;
     }
 
     // Statement lists: sources.jl:727-773 (3-D), 477-495 (2-D), 326-334 (1-D).
@@ -863,13 +792,24 @@ class Engine : public HandleBase {
         // An incident array that is zero at every step changes nothing (F +- c*0 == F up to
         // the sign of a zero): its statements are dropped and the array is not uploaded.
         const int narr = ndim == 3 ? 24 : ndim == 2 ? 8 : 4;
-        std::vector<long long> alen(24, -1);
-        for (size_t i = 0; i < v.size(); ++i)
-            alen[v[i].k] = (long long)(v[i].x1 - v[i].x0 + 1) * (v[i].y1 - v[i].y0 + 1) * (v[i].z1 - v[i].z0 + 1);
+        // per array: face size, extent of the face's first in-plane axis, values per step
+        std::vector<long long> alen(24, -1), clen(24, -1);
+        std::vector<int> ana(24, 1);
+        for (size_t i = 0; i < v.size(); ++i) {
+            const S6& q = v[i];
+            const int ex = q.x1 - q.x0 + 1, ey = q.y1 - q.y0 + 1, ez = q.z1 - q.z0 + 1;
+            alen[q.k] = (long long)ex * ey * ez;
+            // a: y on the x faces (arrays 0-7), x on the y and z faces; a 2-D face is a line
+            // (its only axis is a), a 1-D face a point
+            ana[q.k] = ndim == 3 ? (q.k < 8 ? ey : ex) : ndim == 2 ? ex * ez : 1;
+        }
         std::vector<bool> nonzero(24, false);
         for (int k = 0; k < narr; ++k) {
             if (!d->tfsf.inc[k]) throw Error(MFD_ERR_INVALID, "missing TFSF incident array");
-            nonzero[k] = any_nonzero_bytes(d->tfsf.inc[k], (size_t)alen[k] * nt * sizeof(T));
+            const int sh = d->tfsf.shape[k];
+            if (sh < MFD_INC_FULL || sh > MFD_INC_UNIFORM) throw Error(MFD_ERR_INVALID, "bad TFSF incident-array shape");
+            clen[k] = sh == MFD_INC_FULL ? alen[k] : sh == MFD_INC_ALONG_B ? alen[k] / ana[k] : sh == MFD_INC_ALONG_A ? ana[k] : 1;
+            nonzero[k] = any_nonzero_bytes(d->tfsf.inc[k], (size_t)clen[k] * nt * sizeof(T));
         }
         RectParams<T>& p = tfsf_p;
         std::memset(&p, 0, sizeof(p));
@@ -882,6 +822,9 @@ class Engine : public HandleBase {
             s.comp = v[i].comp; s.x0 = v[i].x0; s.x1 = v[i].x1; s.y0 = v[i].y0; s.y1 = v[i].y1; s.z0 = v[i].z0; s.z1 = v[i].z1;
             s.k = v[i].k; s.sign = v[i].sign; s.tprec = tp[i]; s.coef = coef[i]; s.coefT = (double)coefT[i];
             s.len = alen[s.k];
+            s.shape = d->tfsf.shape[s.k];
+            s.na = ana[s.k];
+            s.clen = clen[s.k];
         }
         p.n = n;
         auto meets = [](const RectStmt& a, const RectStmt& b) {
@@ -898,7 +841,7 @@ class Engine : public HandleBase {
             if (p.s[i].len >= (1ll << 31)) throw Error(MFD_ERR_INVALID, "TFSF face larger than 2^31 cells");
         }
         for (int k = 0; k < narr; ++k)
-            if (nonzero[k]) p.arr[k] = upload((const T*)d->tfsf.inc[k], (size_t)alen[k] * nt);
+            if (nonzero[k]) p.arr[k] = upload((const T*)d->tfsf.inc[k], (size_t)clen[k] * nt);
         tfsf = n > 0;
         MFD_CK(cudaStreamSynchronize(st));
     }
@@ -952,6 +895,8 @@ class Engine : public HandleBase {
             s.comp = v[i].comp; s.x0 = v[i].x0; s.x1 = v[i].x1; s.y0 = v[i].y0; s.y1 = v[i].y1; s.z0 = v[i].z0; s.z1 = v[i].z1;
             s.k = i;
             s.len = (long long)(s.x1 - s.x0 + 1) * (s.y1 - s.y0 + 1) * (s.z1 - s.z0 + 1);
+            s.shape = MFD_INC_FULL;
+            s.clen = s.len;
             rec_maxlen = std::max(rec_maxlen, s.len);
             if (s.len >= (1ll << 31)) throw Error(MFD_ERR_INVALID, "TFSF record face larger than 2^31 cells");
             p.arr[i] = dalloc<T>((size_t)s.len * nt);
@@ -1081,7 +1026,7 @@ class Engine : public HandleBase {
         return p;
     }
 
-    template <bool MATH, bool FAST>
+    template <bool MATH, int FAST>
     void launch_H_t(const HParams<T>& p) {
         if (ndim == 3) {
             dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
@@ -1095,20 +1040,8 @@ class Engine : public HandleBase {
         }
     }
 
-    template <bool MATH, bool FAST>
-    void launch_H_tma() {
-        dim3 blk(TMA_BX, TMA_BY), grd((nx + TMA_BX - 1) / TMA_BX, (ny + TMA_BY - 1) / TMA_BY, (nz + tma_zc - 1) / tma_zc);
-        h3d_tma_kernel<MATH, FAST><<<grd, blk, TMA_STAGES * HStage::BYTES, st>>>(htma, tma_zc);
-    }
-
-    template <bool MAT, bool FAST>
-    void launch_E_tma() {
-        dim3 blk(TMA_BX, TMA_BY), grd((nx + TMA_BX - 1) / TMA_BX, (ny + TMA_BY - 1) / TMA_BY, (nz + tma_zc - 1) / tma_zc);
-        e3d_tma_kernel<R, MAT, FAST><<<grd, blk, TMA_STAGES * EStage::BYTES, st>>>(etma, tma_zc);
-    }
-
     // 3-D updates split into core rows and CPML slabs (yee3d_split.cuh), either element type
-    template <bool MATH, bool FAST, bool ACC, bool E2S>
+    template <bool MATH, int FAST, bool ACC, bool E2S>
     void launch_H_split(const HParams<T>& p) {
         kcount = 0;
         const int zn = sbox.zr - sbox.zl;
@@ -1136,14 +1069,14 @@ class Engine : public HandleBase {
         }
     }
 
-    template <bool MATH, bool FAST>
+    template <bool MATH, int FAST>
     void launch_H_split_acc(const HParams<T>& p) {
         if (!p.accum) launch_H_split<MATH, FAST, false, false>(p);
         else if (p.sum_e2) launch_H_split<MATH, FAST, true, true>(p);
         else launch_H_split<MATH, FAST, true, false>(p);
     }
 
-    template <bool MAT, bool FAST>
+    template <bool MAT, int FAST>
     void launch_E_split(const EParams<T, R>& p) {
         kcount = 0;
         const int zn = sbox.zr - sbox.zl;
@@ -1189,59 +1122,70 @@ class Engine : public HandleBase {
     }
 
     // single-kernel single-precision 3-D updates (CPML layers that overlap in a dimension)
-    template <bool MATH, bool FAST, bool ACC, bool E2S>
+    template <bool MATH, int FAST, bool ACC, bool E2S>
     void launch_H_f32(const HParams<float>& p) {
         dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
         h3d_f32_kernel<MATH, FAST, ACC, E2S><<<grd, blk, 0, st>>>(p, d3, zc3);
     }
 
-    template <bool MATH, bool FAST>
+    template <bool MATH, int FAST>
     void launch_H_f32_acc(const HParams<float>& p) {
         if (!p.accum) launch_H_f32<MATH, FAST, false, false>(p);
         else if (p.sum_e2) launch_H_f32<MATH, FAST, true, true>(p);
         else launch_H_f32<MATH, FAST, true, false>(p);
     }
 
-    template <bool MAT, bool FAST>
+    template <bool MAT, int FAST>
     void launch_E_f32(const EParams<float, R>& p) {
         dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
         e3d_f32_kernel<R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, zc3);
     }
 
+    // Calls f with the division mode of the model's kernels as a compile-time constant:
+    // DIV_RECIP in the tolerance mode, else DIV_EXACT when every divisor passed the device
+    // check, else DIV_IEEE.
+    template <typename F_>
+    void with_div(F_&& f) {
+        if (recip) f(std::integral_constant<int, DIV_RECIP>{});
+        else if (fastdiv) f(std::integral_constant<int, DIV_EXACT>{});
+        else f(std::integral_constant<int, DIV_IEEE>{});
+    }
+
     void launch_H(int accum, long long prev_step) {
         HParams<T> p = hparams(accum, prev_step);
-        if (ndim == 3 && use_split && !use_tma) {
+        if (ndim == 3 && use_split) {
             launch(KC_H, [&] {
-                if (math_needed) { if (fastdiv) launch_H_split_acc<true, true>(p); else launch_H_split_acc<true, false>(p); }
-                else { if (fastdiv) launch_H_split_acc<false, true>(p); else launch_H_split_acc<false, false>(p); }
+                with_div([&](auto dm) {
+                    constexpr int D = decltype(dm)::value;
+                    if (math_needed) launch_H_split_acc<true, D>(p);
+                    else launch_H_split_acc<false, D>(p);
+                });
             });
             return;
         }
         if constexpr (sizeof(T) == 4) {
-            if (ndim == 3 && !use_tma) {
+            if (ndim == 3) {
                 const HParams<float>& pf = reinterpret_cast<const HParams<float>&>(p);
                 launch(KC_H, [&] {
-                    if (math_needed) { if (fastdiv) launch_H_f32_acc<true, true>(pf); else launch_H_f32_acc<true, false>(pf); }
-                    else { if (fastdiv) launch_H_f32_acc<false, true>(pf); else launch_H_f32_acc<false, false>(pf); }
-                });
-                return;
-            }
-            if (use_tma) {
-                std::memcpy(&htma.p, &p, sizeof(p));
-                launch(KC_H, [&] {
-                    if (math_needed) { if (fastdiv) launch_H_tma<true, true>(); else launch_H_tma<true, false>(); }
-                    else { if (fastdiv) launch_H_tma<false, true>(); else launch_H_tma<false, false>(); }
+                    with_div([&](auto dm) {
+                        constexpr int D = decltype(dm)::value;
+                        if (math_needed) launch_H_f32_acc<true, D>(pf);
+                        else launch_H_f32_acc<false, D>(pf);
+                    });
                 });
                 return;
             }
         }
         launch(KC_H, [&] {
-            if (math_needed) { if (fastdiv) launch_H_t<true, true>(p); else launch_H_t<true, false>(p); }
-            else { if (fastdiv) launch_H_t<false, true>(p); else launch_H_t<false, false>(p); }
+            with_div([&](auto dm) {
+                constexpr int D = decltype(dm)::value;
+                if (math_needed) launch_H_t<true, D>(p);
+                else launch_H_t<false, D>(p);
+            });
         });
     }
 
-    template <bool MAT, bool FAST>
+    template <bool MAT, int FAST>
     void launch_E_t(const EParams<T, R>& p) {
         if (ndim == 3) {
             dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (ny + by3 - 1) / by3, (nz + zc3 - 1) / zc3);
@@ -1257,35 +1201,37 @@ class Engine : public HandleBase {
 
     void launch_E(int cur) {
         EParams<T, R> p = eparams();
-        bool done_tma = false;
-        if (ndim == 3 && use_split && !use_tma) {
+        bool done = false;
+        if (ndim == 3 && use_split) {
             launch(KC_E, [&] {
-                if (any_geom) { if (fastdiv) launch_E_split<true, true>(p); else launch_E_split<true, false>(p); }
-                else { if (fastdiv) launch_E_split<false, true>(p); else launch_E_split<false, false>(p); }
+                with_div([&](auto dm) {
+                    constexpr int D = decltype(dm)::value;
+                    if (any_geom) launch_E_split<true, D>(p);
+                    else launch_E_split<false, D>(p);
+                });
             });
-            done_tma = true;
+            done = true;
         }
         if constexpr (sizeof(T) == 4) {
-            if (ndim == 3 && !use_tma && !done_tma) {
+            if (ndim == 3 && !done) {
                 const EParams<float, R>& pf = reinterpret_cast<const EParams<float, R>&>(p);
                 launch(KC_E, [&] {
-                    if (any_geom) { if (fastdiv) launch_E_f32<true, true>(pf); else launch_E_f32<true, false>(pf); }
-                    else { if (fastdiv) launch_E_f32<false, true>(pf); else launch_E_f32<false, false>(pf); }
+                    with_div([&](auto dm) {
+                        constexpr int D = decltype(dm)::value;
+                        if (any_geom) launch_E_f32<true, D>(pf);
+                        else launch_E_f32<false, D>(pf);
+                    });
                 });
-                done_tma = true;
-            } else if (use_tma && !done_tma) {
-                std::memcpy(&etma.p, &p, sizeof(p));
-                launch(KC_E, [&] {
-                    if (any_geom) { if (fastdiv) launch_E_tma<true, true>(); else launch_E_tma<true, false>(); }
-                    else { if (fastdiv) launch_E_tma<false, true>(); else launch_E_tma<false, false>(); }
-                });
-                done_tma = true;
+                done = true;
             }
         }
-        if (!done_tma)
+        if (!done)
             launch(KC_E, [&] {
-                if (any_geom) { if (fastdiv) launch_E_t<true, true>(p); else launch_E_t<true, false>(p); }
-                else { if (fastdiv) launch_E_t<false, true>(p); else launch_E_t<false, false>(p); }
+                with_div([&](auto dm) {
+                    constexpr int D = decltype(dm)::value;
+                    if (any_geom) launch_E_t<true, D>(p);
+                    else launch_E_t<false, D>(p);
+                });
             });
         // E of dispersive / plasma / Kerr cells: material_flat_kernel for up to 3 poles,
         // material_kernel (poles in a runtime loop) beyond
@@ -1482,14 +1428,7 @@ class Engine : public HandleBase {
         MFD_CK(cudaEventRecord(run_ev[1], st));
         MFD_CK(cudaMemcpyAsync(h_flags + (a - 1), d_flags + (a - 1), (size_t)(b - a + 1) * sizeof(int),
                                cudaMemcpyDeviceToHost, st));
-        MFD_CK(cudaMemcpyAsync(h_timeout, d_timeout, sizeof(int), cudaMemcpyDeviceToHost, st));
         bounded_sync(st);
-        if (*h_timeout) {
-            done = b;
-            bad_step = b;
-            err = "a kernel's bounded wait on its TMA copies ran out";
-            return MFD_ERR_TIMEOUT;
-        }
         float ms = 0;
         MFD_CK(cudaEventElapsedTime(&ms, run_ev[0], run_ev[1]));
         run_ms = ms;
@@ -1789,6 +1728,7 @@ struct mfd_batch {
         if (e->dev != dev) { err = "batch member on another device"; return MFD_ERR_INVALID; }
         if (e->in_batch) { err = "model already in a batch"; return MFD_ERR_INVALID; }
         if (e->record) { err = "batch members cannot record TFSF data"; return MFD_ERR_INVALID; }
+        if (e->recip) { err = "batch members run the exact arithmetic: create the model with MFD_MODE_EXACT"; return MFD_ERR_INVALID; }
         if (e->snap_next < e->snap_steps.size()) { err = "batch members cannot take field snapshots"; return MFD_ERR_INVALID; }
         if (e->bad_step) { err = "the model holds non-finite fields"; return MFD_ERR_NONFINITE; }
         if (last <= e->done || last > e->nt) { err = "the last step must be after the model's current step and within 1..Nt"; return MFD_ERR_INVALID; }
@@ -2066,6 +2006,7 @@ static int validate_desc(const mfd_desc* d) {
     if (d->ndim == 1 && (d->nx != 1 || d->ny != 1)) { g_create_error = "1-D model needs nx = ny = 1"; return MFD_ERR_INVALID; }
     if (d->ndim == 2 && d->ny != 1) { g_create_error = "2-D model needs ny = 1"; return MFD_ERR_INVALID; }
     if (d->dtype != MFD_F32 && d->dtype != MFD_F64) { g_create_error = "bad dtype"; return MFD_ERR_INVALID; }
+    if (d->mode != MFD_MODE_EXACT && d->mode != MFD_MODE_FAST) { g_create_error = "bad mode"; return MFD_ERR_INVALID; }
     if (d->nmat < 0 || d->nmat > 255) { g_create_error = "at most 255 materials"; return MFD_ERR_INVALID; }
     if ((long long)d->nx * d->ny * d->nz > (1ll << 34)) { g_create_error = "grid too large"; return MFD_ERR_INVALID; }
     return MFD_OK;

@@ -61,15 +61,34 @@ struct DivC {
     int ok;          // verified for every significand
 };
 
-template <bool FAST, typename T>
+// Division mode of a kernel (its FAST template parameter):
+//   DIV_IEEE  -- IEEE division (double precision, or a divisor that failed the check);
+//   DIV_EXACT -- the verified correction step above, bit-identical to IEEE division;
+//   DIV_RECIP -- the tolerance mode: x * RN(1/d) (within an ulp of x/d), and the update
+//                expressions fused into multiply-adds (mad below) and the Poynting norm
+//                by the hardware reciprocal square root.  Results are no longer
+//                bit-identical to the reference's operation order; they stay within the
+//                relative L2 tolerance stated for the model's precision.
+enum { DIV_IEEE = 0, DIV_EXACT = 1, DIV_RECIP = 2 };
+
+template <int FAST, typename T>
 __device__ __forceinline__ T cdiv(T x, const DivC<T>& D) {
-    return x / D.d;
+    if constexpr (FAST == DIV_RECIP) return x * D.r;
+    else return x / D.d;
+}
+
+// a * b + c: one fused multiply-add in the tolerance mode, else the product rounded and then
+// the sum rounded, as the reference computes it (the library is built without contraction).
+template <int FAST, typename T>
+__device__ __forceinline__ T mad(T a, T b, T c) {
+    if constexpr (FAST == DIV_RECIP) return fma(a, b, c);
+    else return a * b + c;
 }
 
 __device__ __forceinline__ float qscaled(float x, float d, float r, unsigned lob1, unsigned hib);
 
 template <>
-__device__ __forceinline__ float cdiv<true, float>(float x, const DivC<float>& D) {
+__device__ __forceinline__ float cdiv<DIV_EXACT, float>(float x, const DivC<float>& D) {
     const unsigned ax = __float_as_uint(x) & 0x7fffffffu;
     if (ax - D.lob <= D.span) {
         const float q0 = __fmul_rn(x, D.r);
@@ -116,10 +135,14 @@ __device__ __forceinline__ float qscaled(float x, float d, float r, unsigned lob
     return __fdiv_rn(x, d);
 }
 
-template <bool FAST>
+template <int FAST>
 __device__ __forceinline__ void div6(const Div3& D, const float (&x)[6], float (&q)[6]) {
     const float d[6] = {D.dy, D.dz, D.dx, D.dz, D.dx, D.dy};
-    if (FAST) {
+    if constexpr (FAST == DIV_RECIP) {
+        const float r[6] = {D.ry, D.rz, D.rx, D.rz, D.rx, D.ry};
+#pragma unroll
+        for (int i = 0; i < 6; ++i) q[i] = x[i] * r[i];
+    } else if constexpr (FAST == DIV_EXACT) {
         const float r[6] = {D.ry, D.rz, D.rx, D.rz, D.rx, D.ry};
         unsigned mn = 0xffffffffu, mx = 0u;
 #pragma unroll
@@ -145,6 +168,22 @@ __device__ __forceinline__ void div6(const Div3& D, const float (&x)[6], float (
 template <typename T>
 __device__ __forceinline__ T sqrt0(T v) {
     return v == T(0) ? T(0) : sqrt(v);
+}
+
+// The same in a kernel's division mode: the tolerance mode takes v * rsqrt(v) in single
+// precision (the hardware reciprocal square root, a few ulp) instead of the correctly
+// rounded square root's longer sequence.
+template <int FAST, typename T>
+__device__ __forceinline__ T sqrtm(T v) {
+    if constexpr (FAST == DIV_RECIP && sizeof(T) == 4) return v > T(0) ? v * rsqrtf(v) : T(0);
+    else return sqrt0(v);
+}
+
+// |a|^2 + |b|^2 + |c|^2 of the Poynting vector in the reference's order (a^2 + b^2) + c^2,
+// fused in the tolerance mode.
+template <int FAST, typename T>
+__device__ __forceinline__ T sum3sq(T a, T b, T c) {
+    return mad<FAST>(c, c, mad<FAST>(a, a, b * b));
 }
 
 template <typename T>

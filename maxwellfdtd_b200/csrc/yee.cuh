@@ -78,30 +78,30 @@ __device__ __forceinline__ bool in_layers(const LayerDev<T>& lo, const LayerDev<
 // CPML of the E curl in the H update, one face (models.jl:811-871).  The face's psi pair
 // (psi[2], psi[3]) follows derivatives (da, db); S = +1: h1 += Mh pb, h2 -= Mh pa;
 // S = -1: h1 -= Mh pb, h2 += Mh pa.  Then da, db are divided by kappa.
-template <int S, bool FAST, typename T>
+template <int S, int FAST, typename T>
 __device__ __forceinline__ void cpml_h(const LayerDev<T>& l, int q, int k, T Mh, T& da, T& db, T& h1, T& h2) {
     const T B = l.B[q], A = l.A[q];
-    const T pa = B * l.psi[2][k] + A * da;
-    const T pb = B * l.psi[3][k] + A * db;
+    const T pa = mad<FAST>(B, l.psi[2][k], A * da);
+    const T pb = mad<FAST>(B, l.psi[3][k], A * db);
     l.psi[2][k] = pa;
     l.psi[3][k] = pb;
-    if (S > 0) { h1 += Mh * pb; h2 -= Mh * pa; }
-    else { h1 -= Mh * pb; h2 += Mh * pa; }
+    if (S > 0) { h1 = mad<FAST>(Mh, pb, h1); h2 = mad<FAST>(-Mh, pa, h2); }
+    else { h1 = mad<FAST>(-Mh, pb, h1); h2 = mad<FAST>(Mh, pa, h2); }
     da = cdiv<FAST>(da, l.K[q]);
     db = cdiv<FAST>(db, l.K[q]);
 }
 
 // CPML of the H curl in the E update, one face (models.jl:975-1035), psi pair (psi[0],
 // psi[1]); S = +1: D1 += Md2 pb, D2 -= Md2 pa; S = -1: D1 -= Md2 pb, D2 += Md2 pa.
-template <int S, bool FAST, typename T>
+template <int S, int FAST, typename T>
 __device__ __forceinline__ void cpml_e(const LayerDev<T>& l, int q, int k, T Md2, T& da, T& db, T& d1, T& d2) {
     const T B = l.B[q], A = l.A[q];
-    const T pa = B * l.psi[0][k] + A * da;
-    const T pb = B * l.psi[1][k] + A * db;
+    const T pa = mad<FAST>(B, l.psi[0][k], A * da);
+    const T pb = mad<FAST>(B, l.psi[1][k], A * db);
     l.psi[0][k] = pa;
     l.psi[1][k] = pb;
-    if (S > 0) { d1 += Md2 * pb; d2 -= Md2 * pa; }
-    else { d1 -= Md2 * pb; d2 += Md2 * pa; }
+    if (S > 0) { d1 = mad<FAST>(Md2, pb, d1); d2 = mad<FAST>(-Md2, pa, d2); }
+    else { d1 = mad<FAST>(-Md2, pb, d1); d2 = mad<FAST>(Md2, pa, d2); }
     da = cdiv<FAST>(da, l.K[q]);
     db = cdiv<FAST>(db, l.K[q]);
 }
@@ -139,7 +139,7 @@ __device__ __forceinline__ HLoad<T> h3d_load(const HParams<T>& p, int c, int iz,
     return v;
 }
 
-template <typename T, bool MATH, bool FAST>
+template <typename T, bool MATH, int FAST>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) h3d_kernel(const __grid_constant__ HParams<T> p, const int zc) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -168,9 +168,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) h3d_kernel(const 
         const T ex_zp = zz ? T(0) : cur.exz, ey_zp = zz ? T(0) : cur.eyz;
         T hx = cur.hx, hy = cur.hy, hz = cur.hz;
         if (p.accum) {
-            const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
-            p.Sa[c] = cur.sa + sqrt0(a * a + b * b + d * d) * p.dt;
-            if (p.sum_e2) p.E2[c] = cur.e2 + (ex * ex + ey * ey + ez * ez) * p.dt;
+            const T a = mad<FAST>(ey, hz, -(ez * hy)), b = mad<FAST>(ez, hx, -(ex * hz)), d = mad<FAST>(ex, hy, -(ey * hx));
+            p.Sa[c] = mad<FAST>(sqrtm<FAST>(sum3sq<FAST>(a, b, d)), p.dt, cur.sa);
+            if (p.sum_e2) p.E2[c] = mad<FAST>(sum3sq<FAST>(ex, ey, ez), p.dt, cur.e2);
             guard(p, ex);
         }
         T Mh = p.Mh0;
@@ -200,9 +200,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) h3d_kernel(const 
                 cpml_h<+1, FAST>(lzr, q, ix + sy * (iy + ny * q), Mh, dExz, dEyz, hx, hy);
             }
         }
-        hx -= Mh * (dEzy - dEyz);
-        hy -= Mh * (dExz - dEzx);
-        hz -= Mh * (dEyx - dExy);
+        hx = mad<FAST>(-Mh, dEzy - dEyz, hx);
+        hy = mad<FAST>(-Mh, dExz - dEzx, hy);
+        hz = mad<FAST>(-Mh, dEyx - dExy, hz);
         p.Hx[c] = hx; p.Hy[c] = hy; p.Hz[c] = hz;
         ex = cur.exz;
         ey = cur.eyz;
@@ -233,7 +233,7 @@ __device__ __forceinline__ ELoad<T> e3d_load(const EParams<T, R>& p, int c, int 
     return v;
 }
 
-template <typename T, typename R, bool MAT, bool FAST>
+template <typename T, typename R, bool MAT, int FAST>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) e3d_kernel(const __grid_constant__ EParams<T, R> p, const int zc) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -298,9 +298,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) e3d_kernel(const 
                 cpml_e<-1, FAST>(lzr, q, ix + sy * (iy + ny * q), Md2, dHxz, dHyz, D0, D1);
             }
         }
-        D0 = Md1 * D0 + Md2 * (dHzy - dHyz);
-        D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
-        D2 = Md1 * D2 + Md2 * (dHyx - dHxy);
+        D0 = mad<FAST>(Md1, D0, Md2 * (dHzy - dHyz));
+        D1 = mad<FAST>(Md1, D1, Md2 * (dHxz - dHzx));
+        D2 = mad<FAST>(Md1, D2, Md2 * (dHyx - dHxy));
         p.Dx[c] = D0; p.Dy[c] = D1; p.Dz[c] = D2;
         if (simple) {   // E = (D - 0) Me (models.jl:1136-1153 with no polarisation)
             p.Ex[c] = D0 * Me;
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) e3d_kernel(const 
 // into registers, and the z march is unrolled twice so the prefetched plane is renamed
 // instead of copied.
 // ------------------------------------------------------------------------------------------
-template <bool MATH, bool FAST, bool ACC, bool E2S>
+template <bool MATH, int FAST, bool ACC, bool E2S>
 __global__ void __launch_bounds__(256, 4) h3d_f32_kernel(const __grid_constant__ HParams<float> p, const Div3 D3,
                                                          const int zc) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -381,9 +381,9 @@ __global__ void __launch_bounds__(256, 4) h3d_f32_kernel(const __grid_constant__
         const float ex_zp = zz ? 0.0f : cur.exz, ey_zp = zz ? 0.0f : cur.eyz;
         float hx = cur.hx, hy = cur.hy, hz = cur.hz;
         if (ACC) {
-            const float a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
-            Sa[c] = cur.sa + sqrt0(a * a + b * b + d * d) * dt;
-            if (E2S) E2[c] = cur.e2 + (ex * ex + ey * ey + ez * ez) * dt;
+            const float a = mad<FAST>(ey, hz, -(ez * hy)), b = mad<FAST>(ez, hx, -(ex * hz)), d = mad<FAST>(ex, hy, -(ey * hx));
+            Sa[c] = mad<FAST>(sqrtm<FAST>(sum3sq<FAST>(a, b, d)), dt, cur.sa);
+            if (E2S) E2[c] = mad<FAST>(sum3sq<FAST>(ex, ey, ez), dt, cur.e2);
             if (!(fabsf(ex) <= FLT_MAX)) guard(p, ex);
         }
         float Mh = Mh0;
@@ -411,9 +411,9 @@ __global__ void __launch_bounds__(256, 4) h3d_f32_kernel(const __grid_constant__
                 cpml_h<+1, FAST>(lzr, qq, ix + sy * (iy + ny * qq), Mh, dExz, dEyz, hx, hy);
             }
         }
-        hx -= Mh * (dEzy - dEyz);
-        hy -= Mh * (dExz - dEzx);
-        hz -= Mh * (dEyx - dExy);
+        hx = mad<FAST>(-Mh, dEzy - dEyz, hx);
+        hy = mad<FAST>(-Mh, dExz - dEzx, hy);
+        hz = mad<FAST>(-Mh, dEyx - dExy, hz);
         Hx[c] = hx;
         Hy[c] = hy;
         Hz[c] = hz;
@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(256, 4) h3d_f32_kernel(const __grid_constant__
     }
 }
 
-template <typename R, bool MAT, bool FAST>
+template <typename R, bool MAT, int FAST>
 __global__ void __launch_bounds__(256, 4) e3d_f32_kernel(const __grid_constant__ EParams<float, R> p, const Div3 D3,
                                                          const int zc) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -514,9 +514,9 @@ __global__ void __launch_bounds__(256, 4) e3d_f32_kernel(const __grid_constant__
                 cpml_e<-1, FAST>(lzr, qq, ix + sy * (iy + ny * qq), Md2, dHxz, dHyz, D0, D1);
             }
         }
-        D0 = Md1 * D0 + Md2 * (dHzy - dHyz);
-        D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
-        D2 = Md1 * D2 + Md2 * (dHyx - dHxy);
+        D0 = mad<FAST>(Md1, D0, Md2 * (dHzy - dHyz));
+        D1 = mad<FAST>(Md1, D1, Md2 * (dHxz - dHzx));
+        D2 = mad<FAST>(Md1, D2, Md2 * (dHyx - dHxy));
         Dx[c] = D0;
         Dy[c] = D1;
         Dz[c] = D2;
@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(256, 4) e3d_f32_kernel(const __grid_constant__
 // ------------------------------------------------------------------------------------------
 // One cell of the 2-D H update; `accum` and `prev_step` are the step's running-sum flag and
 // the previous step (p.accum / p.prev_step for a single model, per-member state in a batch).
-template <typename T, bool MATH, bool FAST>
+template <typename T, bool MATH, int FAST>
 __device__ __forceinline__ void h2d_cell(const HParams<T>& p, int accum, long long prev_step, int ix, int iz) {
     const int nx = p.L.nx, nz = p.L.nz;
     const int sz = p.L.sz;
@@ -564,7 +564,7 @@ __device__ __forceinline__ void h2d_cell(const HParams<T>& p, int accum, long lo
             const int q = ix, k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEzx;
             l.psi[1][k] = ps;
-            hy += Mh * ps;
+            hy = mad<FAST>(Mh, ps, hy);
             dEzx = cdiv<FAST>(dEzx, l.K[q]);
         }
     }
@@ -574,7 +574,7 @@ __device__ __forceinline__ void h2d_cell(const HParams<T>& p, int accum, long lo
             const int q = ix - (l.ib - 1), k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEzx;
             l.psi[1][k] = ps;
-            hy += Mh * ps;
+            hy = mad<FAST>(Mh, ps, hy);
             dEzx = cdiv<FAST>(dEzx, l.K[q]);
         }
     }
@@ -584,7 +584,7 @@ __device__ __forceinline__ void h2d_cell(const HParams<T>& p, int accum, long lo
             const int q = iz, k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dExz;
             l.psi[1][k] = ps;
-            hy -= Mh * ps;
+            hy = mad<FAST>(-Mh, ps, hy);
             dExz = cdiv<FAST>(dExz, l.K[q]);
         }
     }
@@ -594,15 +594,15 @@ __device__ __forceinline__ void h2d_cell(const HParams<T>& p, int accum, long lo
             const int q = iz - (l.ib - 1), k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dExz;
             l.psi[1][k] = ps;
-            hy -= Mh * ps;
+            hy = mad<FAST>(-Mh, ps, hy);
             dExz = cdiv<FAST>(dExz, l.K[q]);
         }
     }
-    hy -= Mh * (dExz - dEzx);
+    hy = mad<FAST>(-Mh, dExz - dEzx, hy);
     p.Hy[c] = hy;
 }
 
-template <typename T, bool MATH, bool FAST>
+template <typename T, bool MATH, int FAST>
 __global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParams<T> p) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iz = blockIdx.y * blockDim.y + threadIdx.y;
@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(256) h2d_kernel(const __grid_constant__ HParam
 }
 
 // One cell of the 2-D E update (D with CPML; E of cells without a response material).
-template <typename T, typename R, bool MAT, bool FAST>
+template <typename T, typename R, bool MAT, int FAST>
 __device__ __forceinline__ void e2d_cell(const EParams<T, R>& p, int ix, int iz) {
     const int nx = p.L.nx, nz = p.L.nz;
     const int sz = p.L.sz;
@@ -640,7 +640,7 @@ __device__ __forceinline__ void e2d_cell(const EParams<T, R>& p, int ix, int iz)
             const int q = ix, k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyx;
             l.psi[0][k] = ps;
-            D2 += Md2 * ps;
+            D2 = mad<FAST>(Md2, ps, D2);
             dHyx = cdiv<FAST>(dHyx, l.K[q]);
         }
     }
@@ -650,7 +650,7 @@ __device__ __forceinline__ void e2d_cell(const EParams<T, R>& p, int ix, int iz)
             const int q = ix - (l.ib - 1), k = q + l.nb * iz;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyx;
             l.psi[0][k] = ps;
-            D2 += Md2 * ps;
+            D2 = mad<FAST>(Md2, ps, D2);
             dHyx = cdiv<FAST>(dHyx, l.K[q]);
         }
     }
@@ -660,7 +660,7 @@ __device__ __forceinline__ void e2d_cell(const EParams<T, R>& p, int ix, int iz)
             const int q = iz, k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyz;
             l.psi[0][k] = ps;
-            D0 -= Md2 * ps;
+            D0 = mad<FAST>(-Md2, ps, D0);
             dHyz = cdiv<FAST>(dHyz, l.K[q]);
         }
     }
@@ -670,7 +670,7 @@ __device__ __forceinline__ void e2d_cell(const EParams<T, R>& p, int ix, int iz)
             const int q = iz - (l.ib - 1), k = ix + p.L.px * q;
             const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHyz;
             l.psi[0][k] = ps;
-            D0 -= Md2 * ps;
+            D0 = mad<FAST>(-Md2, ps, D0);
             dHyz = cdiv<FAST>(dHyz, l.K[q]);
         }
     }
@@ -684,7 +684,7 @@ __device__ __forceinline__ void e2d_cell(const EParams<T, R>& p, int ix, int iz)
     }
 }
 
-template <typename T, typename R, bool MAT, bool FAST>
+template <typename T, typename R, bool MAT, int FAST>
 __global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParams<T, R> p) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iz = blockIdx.y * blockDim.y + threadIdx.y;
@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParam
 // ------------------------------------------------------------------------------------------
 // 1-D (z)
 // ------------------------------------------------------------------------------------------
-template <typename T, bool MATH, bool FAST>
+template <typename T, bool MATH, int FAST>
 __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParams<T> p) {
     const int iz = blockIdx.x * blockDim.x + threadIdx.x;
     const int nz = p.L.nz;
@@ -721,7 +721,7 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
             const int q = iz;
             const T ps = l.B[q] * l.psi[1][q] + l.A[q] * dExz;
             l.psi[1][q] = ps;
-            hy -= Mh * ps;
+            hy = mad<FAST>(-Mh, ps, hy);
             dExz = cdiv<FAST>(dExz, l.K[q]);
         }
     }
@@ -731,7 +731,7 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
             const int q = iz - (l.ib - 1);
             const T ps = l.B[q] * l.psi[1][q] + l.A[q] * dExz;
             l.psi[1][q] = ps;
-            hy -= Mh * ps;
+            hy = mad<FAST>(-Mh, ps, hy);
             dExz = cdiv<FAST>(dExz, l.K[q]);
         }
     }
@@ -739,7 +739,7 @@ __global__ void __launch_bounds__(256) h1d_kernel(const __grid_constant__ HParam
     p.Hy[c] = hy;
 }
 
-template <typename T, typename R, bool MAT, bool FAST>
+template <typename T, typename R, bool MAT, int FAST>
 __global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParams<T, R> p) {
     const int iz = blockIdx.x * blockDim.x + threadIdx.x;
     const int nz = p.L.nz;
@@ -766,7 +766,7 @@ __global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParam
             const int q = iz;
             const T ps = l.B[q] * l.psi[0][q] + l.A[q] * dHyz;
             l.psi[0][q] = ps;
-            D0 -= Md2 * ps;
+            D0 = mad<FAST>(-Md2, ps, D0);
             dHyz = cdiv<FAST>(dHyz, l.K[q]);
         }
     }
@@ -776,7 +776,7 @@ __global__ void __launch_bounds__(256) e1d_kernel(const __grid_constant__ EParam
             const int q = iz - (l.ib - 1);
             const T ps = l.B[q] * l.psi[0][q] + l.A[q] * dHyz;
             l.psi[0][q] = ps;
-            D0 -= Md2 * ps;
+            D0 = mad<FAST>(-Md2, ps, D0);
             dHyz = cdiv<FAST>(dHyz, l.K[q]);
         }
     }

@@ -22,10 +22,13 @@
 
 #include <type_traits>
 
-#include "tma.cuh"
 #include "yee3d_split.cuh"
 
 namespace mfd {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
 
 #ifndef MFD_AS_TY
 #define MFD_AS_TY 4   // rows of a staged tile (a block is 32 x MFD_AS_TY threads)
@@ -55,7 +58,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 #define MFD_HASYNC_MINB (1024 / (32 * MFD_AS_TY))   // 1024 resident threads per SM (64 registers)
 #endif
 
-template <bool MATH, bool FAST, bool ACC, bool E2S>
+template <bool MATH, int FAST, bool ACC, bool E2S>
 __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_HASYNC_MINB) h3d_core_async_kernel(const __grid_constant__ HParams<float> p,
                                                                         const Div3 D3, const SplitBox s) {
     __shared__ __align__(16) HAStage S[AS_NST];
@@ -176,9 +179,9 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_HASYNC_MINB) h3d_core_async
         }
         float hx = A.hx[ty][tx], hy = A.hy[ty][tx], hz = A.hz[ty][tx];
         if (ACC) {
-            const float a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
-            p.Sa[c] = A.sa[ty][tx] + sqrt0(a * a + b * b + d * d) * dt;
-            if (E2S) p.E2[c] = A.e2[ty][tx] + (ex * ex + ey * ey + ez * ez) * dt;
+            const float a = mad<FAST>(ey, hz, -(ez * hy)), b = mad<FAST>(ez, hx, -(ex * hz)), d = mad<FAST>(ex, hy, -(ey * hx));
+            p.Sa[c] = mad<FAST>(sqrtm<FAST>(sum3sq<FAST>(a, b, d)), dt, A.sa[ty][tx]);
+            if (E2S) p.E2[c] = mad<FAST>(sum3sq<FAST>(ex, ey, ez), dt, A.e2[ty][tx]);
             if (maybe_nonfinite(ex)) guard(p, ex);
         }
         float Mh = Mh0;
@@ -189,18 +192,18 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_HASYNC_MINB) h3d_core_async
         const float dExy = q[0], dExz = q[1], dEyz = q[3], dEzy = q[5];
         float dEyx = q[2], dEzx = q[4];
         if (xin) {   // cpml_h<+1> of the column's x face
-            const float pa = X.B * cpa + X.A * dEyx;
-            const float pb = X.B * cpb + X.A * dEzx;
+            const float pa = mad<FAST>(X.B, cpa, X.A * dEyx);
+            const float pb = mad<FAST>(X.B, cpb, X.A * dEzx);
             X.pa[k] = pa;
             X.pb[k] = pb;
-            hy += Mh * pb;
-            hz -= Mh * pa;
+            hy = mad<FAST>(Mh, pb, hy);
+            hz = mad<FAST>(-Mh, pa, hz);
             dEyx = cdiv<FAST>(dEyx, X.K);
             dEzx = cdiv<FAST>(dEzx, X.K);
         }
-        hx -= Mh * (dEzy - dEyz);
-        hy -= Mh * (dExz - dEzx);
-        hz -= Mh * (dEyx - dExy);
+        hx = mad<FAST>(-Mh, dEzy - dEyz, hx);
+        hy = mad<FAST>(-Mh, dExz - dEzx, hy);
+        hz = mad<FAST>(-Mh, dEyx - dExy, hz);
         p.Hx[c] = hx;
         p.Hy[c] = hy;
         p.Hz[c] = hz;
@@ -246,7 +249,7 @@ constexpr int EA_NST = 5, EA_AHEAD = EA_NST - 3;   // the copy issued at plane i
 
 // skip (rows y0 .. y1-1, planes z0 .. z1-1, aligned to the tiles; empty when y0 == y1): the
 // blocks there are left to another kernel (the register march with the material map).
-template <typename R, bool MAT, bool FAST>
+template <typename R, bool MAT, int FAST>
 __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_EASYNC_MINB) e3d_core_async_kernel(const __grid_constant__ EParams<float, R> p,
                                                                         const Div3 D3, const SplitBox s, const int4 skip) {
     __shared__ __align__(16) EAStage S[EA_NST];
@@ -372,18 +375,18 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_EASYNC_MINB) e3d_core_async
         }
         float D0 = A.dx[ty][tx], D1 = A.dy[ty][tx], D2 = A.dz[ty][tx];
         if (xin) {   // cpml_e<-1> of the column's x face
-            const float pa = X.B * cpa + X.A * dHyx;
-            const float pb = X.B * cpb + X.A * dHzx;
+            const float pa = mad<FAST>(X.B, cpa, X.A * dHyx);
+            const float pb = mad<FAST>(X.B, cpb, X.A * dHzx);
             X.pa[k] = pa;
             X.pb[k] = pb;
-            D1 -= Md2 * pb;
-            D2 += Md2 * pa;
+            D1 = mad<FAST>(-Md2, pb, D1);
+            D2 = mad<FAST>(Md2, pa, D2);
             dHyx = cdiv<FAST>(dHyx, X.K);
             dHzx = cdiv<FAST>(dHzx, X.K);
         }
-        D0 = Md1 * D0 + Md2 * (dHzy - dHyz);
-        D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
-        D2 = Md1 * D2 + Md2 * (dHyx - dHxy);
+        D0 = mad<FAST>(Md1, D0, Md2 * (dHzy - dHyz));
+        D1 = mad<FAST>(Md1, D1, Md2 * (dHxz - dHzx));
+        D2 = mad<FAST>(Md1, D2, Md2 * (dHyx - dHxy));
         p.Dx[c] = D0;
         p.Dy[c] = D1;
         p.Dz[c] = D2;

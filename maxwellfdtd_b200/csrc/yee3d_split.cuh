@@ -52,14 +52,14 @@ __device__ __forceinline__ void slab_row(const SplitBox& s, int ny, int r, int& 
 
 // The six curl derivatives of a cell, q = num / (dy, dz, dx, dz, dx, dy): for single precision
 // the verified branch-free division (div6), for double precision IEEE division.
-template <typename T, bool FAST>
+template <typename T, int FAST>
 __device__ __forceinline__ void curl_div(const Div3& D3, const DivC<T>& ddx, const DivC<T>& ddy, const DivC<T>& ddz,
                                          const T (&num)[6], T (&q)[6]) {
     if constexpr (sizeof(T) == 4) {
         div6<FAST>(D3, num, q);
     } else {
-        q[0] = num[0] / ddy.d; q[1] = num[1] / ddz.d; q[2] = num[2] / ddx.d;
-        q[3] = num[3] / ddz.d; q[4] = num[4] / ddx.d; q[5] = num[5] / ddy.d;
+        q[0] = cdiv<FAST>(num[0], ddy); q[1] = cdiv<FAST>(num[1], ddz); q[2] = cdiv<FAST>(num[2], ddx);
+        q[3] = cdiv<FAST>(num[3], ddz); q[4] = cdiv<FAST>(num[4], ddx); q[5] = cdiv<FAST>(num[5], ddy);
     }
 }
 
@@ -108,7 +108,7 @@ struct HCoreLoad {
     int g;
 };
 
-template <typename T, bool MATH, bool FAST, bool ACC, bool E2S>
+template <typename T, bool MATH, int FAST, bool ACC, bool E2S>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) h3d_core_kernel(const __grid_constant__ HParams<T> p,
                                                                                const Div3 D3, const SplitBox s) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -170,9 +170,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) h3d_c
         const T ex_zp = zz ? T(0) : cur.exz, ey_zp = zz ? T(0) : cur.eyz;
         T hx = cur.hx, hy = cur.hy, hz = cur.hz;
         if (ACC) {
-            const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
-            Sa[c] = cur.sa + sqrt0(a * a + b * b + d * d) * dt;
-            if (E2S) E2[c] = cur.e2 + (ex * ex + ey * ey + ez * ez) * dt;
+            const T a = mad<FAST>(ey, hz, -(ez * hy)), b = mad<FAST>(ez, hx, -(ex * hz)), d = mad<FAST>(ex, hy, -(ey * hx));
+            Sa[c] = mad<FAST>(sqrtm<FAST>(sum3sq<FAST>(a, b, d)), dt, cur.sa);
+            if (E2S) E2[c] = mad<FAST>(sum3sq<FAST>(ex, ey, ez), dt, cur.e2);
             if (maybe_nonfinite(ex)) guard(p, ex);
         }
         T Mh = Mh0;
@@ -183,18 +183,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) h3d_c
         const T dExy = q[0], dExz = q[1], dEyz = q[3], dEzy = q[5];
         T dEyx = q[2], dEzx = q[4];
         if (X.in) {   // cpml_h<+1> of the column's x face
-            const T pa = X.B * cur.pa + X.A * dEyx;
-            const T pb = X.B * cur.pb + X.A * dEzx;
+            const T pa = mad<FAST>(X.B, cur.pa, X.A * dEyx);
+            const T pb = mad<FAST>(X.B, cur.pb, X.A * dEzx);
             X.pa[k] = pa;
             X.pb[k] = pb;
-            hy += Mh * pb;
-            hz -= Mh * pa;
+            hy = mad<FAST>(Mh, pb, hy);
+            hz = mad<FAST>(-Mh, pa, hz);
             dEyx = cdiv<FAST>(dEyx, X.K);
             dEzx = cdiv<FAST>(dEzx, X.K);
         }
-        hx -= Mh * (dEzy - dEyz);
-        hy -= Mh * (dExz - dEzx);
-        hz -= Mh * (dEyx - dExy);
+        hx = mad<FAST>(-Mh, dEzy - dEyz, hx);
+        hy = mad<FAST>(-Mh, dExz - dEzx, hy);
+        hz = mad<FAST>(-Mh, dEyx - dExy, hz);
         Hx[c] = hx;
         Hy[c] = hy;
         Hz[c] = hz;
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) h3d_c
 
 // One cell of the 3-D H update with every CPML face it lies in (one thread per cell; also the
 // cell code of batched 3-D models).  prev_step indexes the NaN/Inf flags of the running sums.
-template <typename T, bool MATH, bool FAST, bool ACC, bool E2S>
+template <typename T, bool MATH, int FAST, bool ACC, bool E2S>
 __device__ __forceinline__ void h3d_cell(const HParams<T>& p, const Div3& D3, long long prev_step, int ix, int iy, int iz) {
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
     const int sy = p.L.px, sz = p.L.sz;
@@ -223,9 +223,9 @@ __device__ __forceinline__ void h3d_cell(const HParams<T>& p, const Div3& D3, lo
     const T ex_zp = zz ? T(0) : p.Ex[c + oz], ey_zp = zz ? T(0) : p.Ey[c + oz];
     T hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
     if (ACC) {
-        const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
-        p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b + d * d) * p.dt;
-        if (E2S) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
+        const T a = mad<FAST>(ey, hz, -(ez * hy)), b = mad<FAST>(ez, hx, -(ex * hz)), d = mad<FAST>(ex, hy, -(ey * hx));
+        p.Sa[c] = mad<FAST>(sqrtm<FAST>(sum3sq<FAST>(a, b, d)), p.dt, p.Sa[c]);
+        if (E2S) p.E2[c] = mad<FAST>(sum3sq<FAST>(ex, ey, ez), p.dt, p.E2[c]);
         if (maybe_nonfinite(ex)) guard_at(p.flags, prev_step, ex);
     }
     T Mh = p.Mh0;
@@ -254,15 +254,15 @@ __device__ __forceinline__ void h3d_cell(const HParams<T>& p, const Div3& D3, lo
         const int qq = iz - (lzr.ib - 1);
         cpml_h<+1, FAST>(lzr, qq, ix + sy * (iy + ny * qq), Mh, dExz, dEyz, hx, hy);
     }
-    hx -= Mh * (dEzy - dEyz);
-    hy -= Mh * (dExz - dEzx);
-    hz -= Mh * (dEyx - dExy);
+    hx = mad<FAST>(-Mh, dEzy - dEyz, hx);
+    hy = mad<FAST>(-Mh, dExz - dEzx, hy);
+    hz = mad<FAST>(-Mh, dEyx - dExy, hz);
     p.Hx[c] = hx;
     p.Hy[c] = hy;
     p.Hz[c] = hz;
 }
 
-template <typename T, bool MATH, bool FAST, bool ACC, bool E2S>
+template <typename T, bool MATH, int FAST, bool ACC, bool E2S>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) h3d_slab_kernel(const __grid_constant__ HParams<T> p, const Div3 D3,
                                                        const SplitBox s) {
     const int ix = blockIdx.y * blockDim.x + threadIdx.x;
@@ -278,7 +278,7 @@ struct ECoreLoad {
     int g;
 };
 
-template <typename T, typename R, bool MAT, bool FAST>
+template <typename T, typename R, bool MAT, int FAST>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) e3d_core_kernel(const __grid_constant__ EParams<T, R> p,
                                                                                const Div3 D3, const SplitBox s) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -353,18 +353,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) e3d_c
         }
         T D0 = cur.dx, D1 = cur.dy, D2 = cur.dz;
         if (X.in) {   // cpml_e<-1> of the column's x face
-            const T pa = X.B * cur.pa + X.A * dHyx;
-            const T pb = X.B * cur.pb + X.A * dHzx;
+            const T pa = mad<FAST>(X.B, cur.pa, X.A * dHyx);
+            const T pb = mad<FAST>(X.B, cur.pb, X.A * dHzx);
             X.pa[k] = pa;
             X.pb[k] = pb;
-            D1 -= Md2 * pb;
-            D2 += Md2 * pa;
+            D1 = mad<FAST>(-Md2, pb, D1);
+            D2 = mad<FAST>(Md2, pa, D2);
             dHyx = cdiv<FAST>(dHyx, X.K);
             dHzx = cdiv<FAST>(dHzx, X.K);
         }
-        D0 = Md1 * D0 + Md2 * (dHzy - dHyz);
-        D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
-        D2 = Md1 * D2 + Md2 * (dHyx - dHxy);
+        D0 = mad<FAST>(Md1, D0, Md2 * (dHzy - dHyz));
+        D1 = mad<FAST>(Md1, D1, Md2 * (dHxz - dHzx));
+        D2 = mad<FAST>(Md1, D2, Md2 * (dHyx - dHxy));
         Dx[c] = D0;
         Dy[c] = D1;
         Dz[c] = D2;
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) e3d_c
 
 // One cell of the 3-D E update with every CPML face it lies in (also the cell code of batched
 // 3-D models).
-template <typename T, typename R, bool MAT, bool FAST>
+template <typename T, typename R, bool MAT, int FAST>
 __device__ __forceinline__ void e3d_cell(const EParams<T, R>& p, const Div3& D3, int ix, int iy, int iz) {
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
     const int sy = p.L.px, sz = p.L.sz;
@@ -427,9 +427,9 @@ __device__ __forceinline__ void e3d_cell(const EParams<T, R>& p, const Div3& D3,
         const int qq = iz - (lzr.ib - 1);
         cpml_e<-1, FAST>(lzr, qq, ix + sy * (iy + ny * qq), Md2, dHxz, dHyz, D0, D1);
     }
-    D0 = Md1 * D0 + Md2 * (dHzy - dHyz);
-    D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
-    D2 = Md1 * D2 + Md2 * (dHyx - dHxy);
+    D0 = mad<FAST>(Md1, D0, Md2 * (dHzy - dHyz));
+    D1 = mad<FAST>(Md1, D1, Md2 * (dHxz - dHzx));
+    D2 = mad<FAST>(Md1, D2, Md2 * (dHyx - dHxy));
     p.Dx[c] = D0;
     p.Dy[c] = D1;
     p.Dz[c] = D2;
@@ -440,7 +440,7 @@ __device__ __forceinline__ void e3d_cell(const EParams<T, R>& p, const Div3& D3,
     }
 }
 
-template <typename T, typename R, bool MAT, bool FAST>
+template <typename T, typename R, bool MAT, int FAST>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? MFD_SLAB_MINB : 1) e3d_slab_kernel(const __grid_constant__ EParams<T, R> p, const Div3 D3,
                                                        const SplitBox s) {
     const int ix = blockIdx.y * blockDim.x + threadIdx.x;

@@ -125,10 +125,14 @@ class Model:
             return (adapt_range(g.x, dtype), adapt_range(g.z, dtype))
         return (adapt_range(g.x, dtype), adapt_range(g.y, dtype), adapt_range(g.z, dtype))
 
-    def build_desc(self, dtype, monitors=(), tfsf_box=None, rho_fp64=True, device=0, host_alloc=None):
+    def build_desc(self, dtype, monitors=(), tfsf_box=None, rho_fp64=True, device=0, host_alloc=None, mode="exact"):
         """C descriptor for this model in element type ``dtype`` plus host-side metadata.
         ``host_alloc(n, dtype)`` provides the storage of the large input arrays (e.g.
-        page-locked memory)."""
+        page-locked memory).  ``mode`` is the arithmetic of the field updates: "exact" (the
+        reference's operation order, bit for bit) or "fast" (the tolerance mode,
+        MFD_MODE_FAST in include/maxwellfdtd.h)."""
+        if mode not in ("exact", "fast"):
+            raise ValueError("mode must be 'exact' or 'fast'")
         dtype = np.dtype(dtype)
         g = self.grid
         b = _abi.DescBuilder(host_alloc)
@@ -199,13 +203,14 @@ class Model:
                     e.gt = _abi.dptr(b.arr(gt, np.float64))
             d.srcs = sarr
         if self.tfsf is not None:
-            i1, i2, arrays = self.tfsf
+            i1, i2, arrays, shapes = self.tfsf
             d.tfsf.enabled = 1
             d.tfsf.order = self.tfsf_order
             for a in range(3):
                 d.tfsf.i1[a], d.tfsf.i2[a] = i1[a], i2[a]
-            for k, v in enumerate(arrays):
+            for k, (v, sh) in enumerate(zip(arrays, shapes)):
                 d.tfsf.inc[k] = b.arr(v, dtype).ctypes.data
+                d.tfsf.shape[k] = sh
         mon_meta = []
         monitors = [] if monitors is None else (list(monitors) if isinstance(monitors, (list, tuple)) else [monitors])
         if monitors:
@@ -231,6 +236,7 @@ class Model:
                 d.rec_i1[a], d.rec_i2[a] = i1[a], i2[a]
             rec = (tuple(float(v) for v in tfsf_box), i1, i2)
         d.device = device
+        d.mode = _abi.MFD_MODE_FAST if mode == "fast" else _abi.MFD_MODE_EXACT
         meta = {"coords_T": coords_T, "t_T": t_T, "monitors": mon_meta, "record": rec}
         return b, meta
 
@@ -260,14 +266,20 @@ class B200:
     """Backend running the time-step path on a B200 GPU: ``B200(np.float32)`` or
     ``B200(np.float64)``; ``B200()`` is single precision like the reference's ``GPU()``
     (src/backends.jl:19-23).  ``library`` lets a caller supply another library object that
-    exports the same C API."""
+    exports the same C API.  ``mode="fast"`` selects the tolerance-mode field updates
+    (reciprocal multiplies and fused multiply-adds, within relative L2 1e-5 in float32 and
+    1e-12 in float64 of the exact order); the default "exact" keeps the reference's operation
+    order bit for bit."""
 
-    def __init__(self, dtype=np.float32, device=0, rho_fp64=True, library=None):
+    def __init__(self, dtype=np.float32, device=0, rho_fp64=True, library=None, mode="exact"):
         self.dtype = np.dtype(dtype)
         if self.dtype not in (np.dtype(np.float32), np.dtype(np.float64)):
             raise ValueError("B200 backend supports float32 and float64")
+        if mode not in ("exact", "fast"):
+            raise ValueError("mode must be 'exact' or 'fast'")
         self.device = device
         self.rho_fp64 = rho_fp64
+        self.mode = mode
         self._library = library
 
     def library(self):
@@ -333,7 +345,8 @@ def solve(model, *, backend=None, fname=None, nframes=None, nstride=None, dtout=
     if tfsf_record and tfsf_box is None:
         raise ValueError("tfsf_record needs tfsf_box")
     builder, meta = model.build_desc(dtype, monitors, tfsf_box if tfsf_record else None,
-                                     rho_fp64=backend.rho_fp64, device=getattr(backend, "device", 0))
+                                     rho_fp64=backend.rho_fp64, device=getattr(backend, "device", 0),
+                                     mode=getattr(backend, "mode", "exact"))
     st = _abi.Stepper(backend.library(), builder, dtype)
     try:
         return _run(model, st, meta, dtype, fname, nframes, nstride, dtout, components, monitors,

@@ -11,6 +11,7 @@ from typing import Any, Callable, Optional
 
 import numpy as np
 
+from . import _abi
 from .constants import EPS0
 from .geometry import cell_coords, geometry2indices
 
@@ -167,10 +168,10 @@ def _interp_axis(knots, values, q, axis):
     knots = np.asarray(knots, dtype=np.float64)
     q = np.asarray(q, dtype=np.float64)
     n = len(knots)
+    if values.shape[axis] == 1:
+        return np.asarray(values)    # constant along this axis (one knot, or given broadcast)
     if n == len(q) and np.array_equal(knots, q):
         return np.asarray(values)    # queries on the knots: interpolation is the identity
-    if n == 1:
-        return np.repeat(np.take(values, [0], axis=axis), len(q), axis=axis)
     qc = np.clip(q, knots[0], knots[-1])
     i = np.clip(np.searchsorted(knots, qc, side="right") - 1, 0, n - 2)
     w = (qc - knots[i]) / (knots[i + 1] - knots[i])
@@ -196,21 +197,40 @@ def load_tfsf_data(source):
         return {k: f[k] for k in f.files}
 
 
+def _compact(r, extent):
+    """r: resampled incident data (a, b, nt) of a face of `extent` (a, b), an axis of extent 1
+    meaning constant along it.  Axes whose values are the same everywhere are dropped too;
+    returns the C-ordered values per step [nt][...] and the MFD_INC_* layout
+    (include/maxwellfdtd.h)."""
+    if r.shape[0] > 1 and np.array_equal(r, np.broadcast_to(r[:1], r.shape)):
+        r = r[:1]
+    if r.shape[1] > 1 and np.array_equal(r, np.broadcast_to(r[:, :1], r.shape)):
+        r = r[:, :1]
+    A, B, nt = r.shape
+    shape = (_abi.MFD_INC_UNIFORM if A == 1 and B == 1 else _abi.MFD_INC_ALONG_B if A == 1
+             else _abi.MFD_INC_ALONG_A if B == 1 else _abi.MFD_INC_FULL)
+    return np.ascontiguousarray(np.transpose(r, (2, 1, 0)).reshape(nt, -1)), shape
+
+
 def tfsf_struct(source, grid, t):
     """``SourceStruct(::TFSFSource, ...)`` (sources.jl:284-317, 408-466, 592-710): box
     indices on this grid and incident data resampled onto (face coordinates, t), dense in t.
-    Arrays are returned C-ordered [nt][face extent] (the reference's (a, b, Nt) column-major)."""
+    Arrays are returned C-ordered [nt][face extent] (the reference's (a, b, Nt) column-major),
+    each in its compact layout when its values do not vary along a face axis (the dataset may
+    give such an axis with extent 1); returns (i1, i2, arrays, layouts)."""
     d = load_tfsf_data(source)
     box = tuple(float(v) for v in np.asarray(d["box"]).ravel())
     tex = np.asarray(d["t"], dtype=np.float64)
     t = np.asarray(t, dtype=np.float64)
     i1, i2 = box_indices(grid, box)
     arrays = []
+    shapes = []
     if grid.ndim == 1:
         for name in TFSF_NAMES_1D:
             v = np.asarray(d[name], dtype=np.float64).ravel()
             arrays.append(_interp_axis(tex, v, t, 0).reshape(len(t), 1))
-        return i1, i2, arrays
+            shapes.append(_abi.MFD_INC_FULL)
+        return i1, i2, arrays, shapes
     if grid.ndim == 2:
         xex = np.asarray(d["x"], dtype=np.float64)
         zex = np.asarray(d["z"], dtype=np.float64)
@@ -223,8 +243,10 @@ def tfsf_struct(source, grid, t):
             v = _as_col_major(v, 2)
             knots, q = (zex, zq) if name.endswith("z") else (xex, xq)
             r = _interp_grid([knots, tex], v, [q, t])      # (face, nt)
-            arrays.append(np.ascontiguousarray(r.T))
-        return i1, i2, arrays
+            arr, sh = _compact(r[:, None, :], (len(q), 1))
+            arrays.append(arr)
+            shapes.append(sh)
+        return i1, i2, arrays, shapes
     xex = np.asarray(d["x"], dtype=np.float64)
     yex = np.asarray(d["y"], dtype=np.float64)
     zex = np.asarray(d["z"], dtype=np.float64)
@@ -244,8 +266,10 @@ def tfsf_struct(source, grid, t):
     for name, (ka, kb, qa, qb) in zip(TFSF_NAMES_3D, spec):
         v = _as_col_major(np.asarray(d[name], dtype=np.float64), 3)
         r = _interp_grid([ka, kb, tex], v, [qa, qb, t])    # (a, b, nt)
-        arrays.append(np.ascontiguousarray(np.transpose(r, (2, 1, 0)).reshape(len(t), -1)))
-    return i1, i2, arrays
+        arr, sh = _compact(r, (len(qa), len(qb)))
+        arrays.append(arr)
+        shapes.append(sh)
+    return i1, i2, arrays, shapes
 
 
 def _as_col_major(v, nd):

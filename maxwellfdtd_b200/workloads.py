@@ -65,25 +65,19 @@ def _plane_wave_tfsf(grid, i1, i2, t, f, zs, dt):
          "x": grid.x[ix1 - 1:ix2], "y": grid.y[iy1 - 1:iy2], "z": grid.z[iz1 - 1:iz2]}
     zh = z[iz1 - 1:iz2 - 1]      # iz1 .. iz2-1
     zf = z[iz1 - 1:iz2]          # iz1 .. iz2
-    shapes = {}
-    for k, name in enumerate(TFSF_NAMES_3D):
-        face, j = k // 4, k % 4
-        if face < 2:
-            a, b = (Nyi + 1, Nzi) if j in (0, 3) else (Nyi, Nzi + 1)
-        elif face < 4:
-            a, b = (Nxi + 1, Nzi) if j in (0, 3) else (Nxi, Nzi + 1)
-        else:
-            a, b = (Nxi + 1, Nyi) if j in (0, 3) else (Nxi, Nyi + 1)
-        shapes[name] = (nt, b, a)
-        d[name] = np.zeros((nt, b, a), dtype=np.float32)
+    # The wave depends on z and t only, so every array is given with its constant face axes
+    # of extent 1 (the [nt][b][a] layout broadcast): [nt][b][1] on the x and y faces, whose
+    # b axis is z, [nt][1][1] on the z faces, and the components the wave lacks as zeros.
+    for name in TFSF_NAMES_3D:
+        d[name] = np.zeros((nt, 1, 1), dtype=np.float32)
     for name in ("incHy_1yz", "incHy_2yz"):          # (Nyi+1, Nzi): z in iz1..iz2-1
-        d[name][:] = Hy(zh)[:, :, None]
+        d[name] = Hy(zh).astype(np.float32)[:, :, None]
     for name in ("incEx_x1z", "incEx_x2z"):          # (Nxi, Nzi+1): z in iz1..iz2
-        d[name][:] = Ex(zf)[:, :, None]
-    d["incHy_xy1"][:] = Hy(z[iz1 - 2:iz1 - 1])[:, :, None]
-    d["incEx_xy1"][:] = Ex(z[iz1 - 1:iz1])[:, :, None]
-    d["incHy_xy2"][:] = Hy(z[iz2 - 1:iz2])[:, :, None]
-    d["incEx_xy2"][:] = Ex(z[iz2 - 1:iz2])[:, :, None]
+        d[name] = Ex(zf).astype(np.float32)[:, :, None]
+    d["incHy_xy1"] = Hy(z[iz1 - 2:iz1 - 1]).astype(np.float32)[:, :, None]
+    d["incEx_xy1"] = Ex(z[iz1 - 1:iz1]).astype(np.float32)[:, :, None]
+    d["incHy_xy2"] = Hy(z[iz2 - 1:iz2]).astype(np.float32)[:, :, None]
+    d["incEx_xy2"] = Ex(z[iz2 - 1:iz2]).astype(np.float32)[:, :, None]
     return d
 
 
@@ -141,13 +135,13 @@ def _plane_wave_tfsf_2d(grid, i1, i2, t, f, zs, dt):
     d = {"t": np.asarray(t), "box": np.array([grid.x[ix1 - 1], grid.x[ix2 - 1], z[iz1 - 1], z[iz2 - 1]]),
          "x": xk, "z": zk}
     d["incHy_1z"] = Hy(zk).astype(np.float32)
-    d["incEz_1z"] = np.zeros((nt, len(zk)), np.float32)
+    d["incEz_1z"] = np.zeros((nt, 1), np.float32)     # [nt][1]: the same (zero) along the face
     d["incHy_2z"] = d["incHy_1z"]
     d["incEz_2z"] = d["incEz_1z"]
-    d["incHy_x1"] = np.repeat(Hy(z[iz1 - 2:iz1 - 1]), len(xk), axis=1).astype(np.float32)
-    d["incEx_x1"] = np.repeat(Ex(z[iz1 - 1:iz1]), len(xk), axis=1).astype(np.float32)
-    d["incHy_x2"] = np.repeat(Hy(z[iz2 - 1:iz2]), len(xk), axis=1).astype(np.float32)
-    d["incEx_x2"] = np.repeat(Ex(z[iz2 - 1:iz2]), len(xk), axis=1).astype(np.float32)
+    d["incHy_x1"] = Hy(z[iz1 - 2:iz1 - 1]).astype(np.float32)   # [nt][1]: uniform along x
+    d["incEx_x1"] = Ex(z[iz1 - 1:iz1]).astype(np.float32)
+    d["incHy_x2"] = Hy(z[iz2 - 1:iz2]).astype(np.float32)
+    d["incEx_x2"] = Ex(z[iz2 - 1:iz2]).astype(np.float32)
     return d
 
 

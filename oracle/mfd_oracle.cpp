@@ -243,7 +243,20 @@ struct Oracle : OracleBase {
             for (int k = 0; k < narr; ++k) {
                 inc_len[k] = face_len(k, ti1, ti2);
                 const T* p = (const T*)d->tfsf.inc[k];
-                inc[k].assign(p, p + inc_len[k] * nt);
+                const int sh = d->tfsf.shape[k];
+                if (sh == MFD_INC_FULL) {
+                    inc[k].assign(p, p + inc_len[k] * nt);
+                    continue;
+                }
+                // compact layouts (maxwellfdtd.h): expand to the reference's [nt][b][a]
+                const size_t na = face_a(k, ti1, ti2), nb = inc_len[k] / na;
+                const size_t per = sh == MFD_INC_ALONG_B ? nb : sh == MFD_INC_ALONG_A ? na : 1;
+                inc[k].assign(inc_len[k] * nt, 0);
+                for (int64_t it = 0; it < nt; ++it)
+                    for (size_t ib = 0; ib < nb; ++ib)
+                        for (size_t ia = 0; ia < na; ++ia)
+                            inc[k][it * inc_len[k] + ia + na * ib] =
+                                p[it * per + (sh == MFD_INC_ALONG_B ? ib : sh == MFD_INC_ALONG_A ? ia : 0)];
             }
         }
         for (int m = 0; m < d->nmon; ++m) {
@@ -277,6 +290,17 @@ struct Oracle : OracleBase {
         return c == MFD_HY || c == MFD_DX || c == MFD_EX;
     }
     static bool is_D(int c) { return c >= MFD_DX && c <= MFD_DZ; }
+
+    // Extent of a TFSF array's first face axis a (y on the x faces, x on the y and z faces;
+    // the whole line of a 2-D face; 1 in 1-D).
+    size_t face_a(int k, const int* i1, const int* i2) const {
+        size_t Nxi = i2[0] - i1[0], Nyi = i2[1] - i1[1];
+        if (ndim == 1) return 1;
+        if (ndim == 2) return face_len(k, i1, i2);
+        int face = k / 4, j = k % 4;
+        if (face < 2) return (j == 0 || j == 3) ? Nyi + 1 : Nyi;
+        return (j == 0 || j == 3) ? Nxi + 1 : Nxi;
+    }
 
     // Face extents of the TFSF arrays (sources.jl:441-459, 646-699, 804-832).
     size_t face_len(int k, const int* i1, const int* i2) const {

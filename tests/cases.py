@@ -223,9 +223,9 @@ def model_tfsf_replay(ndim, record, nsteps=60):
     return M.Model(g, src, tmax=(nsteps - 0.5) * dt, pml=100e-9, material=mat)
 
 
-def run_all(model, library, dtype, mons=None, tfsf_box_=None, rho_fp64=True, chunks=None):
+def run_all(model, library, dtype, mons=None, tfsf_box_=None, rho_fp64=True, chunks=None, mode="exact"):
     """Run a model on a library; return a dict of every output array."""
-    be = M.B200(dtype, library=library, rho_fp64=rho_fp64)
+    be = M.B200(dtype, library=library, rho_fp64=rho_fp64, mode=mode)
     if chunks is None:
         sol = M.solve(model, backend=be, monitors=mons, tfsf_record=tfsf_box_ is not None, tfsf_box=tfsf_box_,
                       tfsf_fname=None if tfsf_box_ is None else _tmp_name())
@@ -238,7 +238,7 @@ def run_all(model, library, dtype, mons=None, tfsf_box_=None, rho_fp64=True, chu
                 out["rec/" + k] = np.asarray(v)
         return out
     # chunked driving straight through the ABI
-    b, meta = model.build_desc(dtype, mons, rho_fp64=rho_fp64)
+    b, meta = model.build_desc(dtype, mons, rho_fp64=rho_fp64, mode=mode)
     st = _abi.Stepper(library, b, dtype)
     a = 1
     for n in chunks:

@@ -1,0 +1,142 @@
+"""The tolerance mode (MFD_MODE_FAST) against the oracle's exact operation order.
+
+The field updates multiply by reciprocals and fuse multiply-adds, so results are no longer
+bit-identical; the north-star bound is relative L2 <= 1e-5 in Float32 and <= 1e-12 in
+Float64.  Errors are measured per vector quantity (E, D, H as the concatenation of their
+components), per running sum (Sa, E2) and per monitor (all its components together): a
+single component that the exact order keeps at exactly zero by symmetry (Ey of an
+x-polarised source) would otherwise turn rounding noise into a relative error of 1.
+"""
+import numpy as np
+import pytest
+
+import cases as C
+import maxwellfdtd_b200 as M
+import test_gpu_configs as G
+from maxwellfdtd_b200 import _abi
+from maxwellfdtd_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.float32: 1e-5, np.float64: 1e-12}
+TOL_PLASMA_STATE = {np.float32: 1e-4, np.float64: 1e-9}
+
+
+def _groups(out):
+    g = {}
+    for k, v in out.items():
+        if k.startswith("field/"):
+            key = "field/" + k[6]          # E, D or H
+        elif k.startswith("monitors/"):
+            key = "/".join(k.split("/")[:2])
+        else:
+            key = k
+        g.setdefault(key, []).append(np.asarray(v))
+    return g
+
+
+def _rel(parts_a, parts_b):
+    def flat(parts):
+        out = []
+        for p in parts:
+            if np.iscomplexobj(p):
+                out += [np.real(p).ravel(), np.imag(p).ravel()]
+            else:
+                out.append(p.ravel())
+        return np.concatenate(out).astype(np.float64)
+    a, b = flat(parts_a), flat(parts_b)
+    den = max(np.linalg.norm(a), np.linalg.norm(b))
+    return 0.0 if den == 0 else float(np.linalg.norm(a - b) / den)
+
+
+def _check(ref, got, dtype, state_truth=None):
+    ga, gb = _groups(ref), _groups(got)
+    assert set(ga) == set(gb)
+    errs = {k: _rel(ga[k], gb[k]) for k in ga}
+    bad = {k: e for k, e in errs.items() if k not in ("rho_end", "JE") and e > TOL[dtype]}
+    assert not bad, bad
+    for k in ("rho_end", "JE"):
+        if k in errs:
+            assert errs[k] <= TOL_PLASMA_STATE[dtype], (k, errs[k])
+    return errs
+
+
+CASES = {
+    "vacuum": lambda n: (C.model_vacuum(n), C.monitors(n)),
+    "bcs": lambda n: (C.model_bcs(n), None),
+    "materials": lambda n: (C.model_materials(n), C.monitors(n)),
+    "sources": lambda n: (C.model_sources(n), None),
+    "poles": lambda n: (C.model_poles(n, 3, True), None),
+}
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("ndim", [1, 2, 3])
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_fast_mode_within_tolerance(case, ndim, dtype, oracle_lib, gpu_lib):
+    model, mons = CASES[case](ndim)
+    ref = C.run_all(model, oracle_lib, dtype, mons)
+    got = C.run_all(model, gpu_lib, dtype, mons, mode="fast")
+    _check(ref, got, dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("case", ["wide_periodic", "wide_dirichlet", "x_overlap", "y_z_right", "midsize"])
+def test_fast_mode_3d_layouts(case, dtype, oracle_lib, gpu_lib):
+    """Rows across several warps, overlapping layers (the unsplit kernels), layers on some
+    faces only, and the staged kernels' inner tiles."""
+    import test_gpu_parity as P
+    if case.startswith("wide_"):
+        model = C.model_wide_rows(case[5:])
+    elif case == "midsize":
+        model = G._midsize_model((72, 40, 24))
+    else:
+        model = C.model_layers(*P.LAYER_CASES[case])
+    ref = C.run_all(model, oracle_lib, dtype)
+    got = C.run_all(model, gpu_lib, dtype, mode="fast")
+    _check(ref, got, dtype)
+
+
+def test_fast_mode_plasmonics_96(oracle_lib, gpu_lib):
+    """The headline workload's configuration on a 96^3 grid, 60 steps: within 1e-5 of the
+    FP32 oracle, and no further from the FP64 oracle than 1e-5 either."""
+    model, mons = W.plasmonics_256(nt=60, n=96)
+    got = C.run_all(model, gpu_lib, np.float32, mons, mode="fast")
+    ref = C.run_all(model, oracle_lib, np.float32, mons)
+    errs = _check(ref, got, np.float32)
+    truth = C.run_all(model, oracle_lib, np.float64, mons)
+    e64 = {k: _rel(a, b) for (k, a), b in zip(_groups(truth).items(), _groups(got).values())}
+    print("fast mode, plasmonics 96^3, 60 steps: vs FP32 oracle", {k: f"{v:.2e}" for k, v in errs.items()},
+          "vs FP64 oracle", {k: f"{v:.2e}" for k, v in e64.items()})
+    assert max(e64[k] for k in ("field/E", "field/H", "field/D")) <= 1e-5
+
+
+def test_fast_mode_plasma(oracle_lib, gpu_lib):
+    model = C.model_plasma(3, "power")
+    ref = C.run_all(model, oracle_lib, np.float32)
+    got = C.run_all(model, gpu_lib, np.float32, mode="fast")
+    _check(ref, got, np.float32)
+
+
+def test_batch_refuses_fast_members(gpu_lib):
+    model = C.model_vacuum(2)
+    b, _ = model.build_desc(np.float32, None, mode="fast")
+    st = _abi.Stepper(gpu_lib, b, np.float32)
+    batch = _abi.Batch(gpu_lib)
+    try:
+        with pytest.raises(_abi.StepperError) as ei:
+            batch.add(st, model.Nt)
+        assert ei.value.code == _abi.MFD_ERR_INVALID and "EXACT" in str(ei.value)
+    finally:
+        batch.close()
+        st.close()
+
+
+def test_mode_is_validated(gpu_lib):
+    model = C.model_vacuum(1)
+    b, _ = model.build_desc(np.float32, None)
+    b.desc.mode = 7
+    with pytest.raises(_abi.StepperError):
+        _abi.Stepper(gpu_lib, b, np.float32)
+    with pytest.raises(ValueError):
+        M.B200(np.float32, mode="quick")
