@@ -328,6 +328,25 @@ MFD_API int mfd_batch_info(const mfd_batch* b, int32_t* tile_x, int32_t* tile_z,
                            int64_t* cell_updates, int64_t* launches);
 MFD_API const char* mfd_batch_last_error(const mfd_batch* b);
 
+/* ---- model state ------------------------------------------------------------------------
+ * The state a run carries from one step to the next, beyond the nine field components: the
+ * running sums Sa and E2, the CPML psi arrays of every face (the reference's PML struct,
+ * src/pml.jl:227-304), the polarisation of every dispersive material (P, oldP1 of
+ * src/materials.jl:424-426; oldP2 is not needed), the plasma state (rho, drho, the plasma
+ * currents, Pa, JE), the monitors' records and DFT accumulators, the TFSF record arrays,
+ * the NaN/Inf flags and the number of steps done.  mfd_read_state copies it into one host
+ * image of mfd_state_size() bytes; mfd_write_state loads such an image into a handle created
+ * from the same descriptor (same grid, precision, materials, CPML, sources and monitors --
+ * checked against a layout hash in the image), after which mfd_run continues from the
+ * image's step exactly as the run it was taken from would have continued.  The image's
+ * layout is the library's own (not a file format).  Writing clears any pending field
+ * snapshots.  Both calls synchronise the handle's stream; neither may be used on a handle
+ * that a batch is stepping.  Uses: checkpoint and resume, moving a model between devices,
+ * and letting a serving loop evict a model from device memory and restore it later. */
+MFD_API int64_t mfd_state_size(const mfd_handle* h);
+MFD_API int mfd_read_state(mfd_handle* h, void* dst, int64_t bytes);
+MFD_API int mfd_write_state(mfd_handle* h, const void* src, int64_t bytes);
+
 /* Device-time measurement: when on, every kernel launch of mfd_run is bracketed by CUDA
  * events on the handle's stream and its duration is summed per kernel class. */
 MFD_API int mfd_set_profiling(mfd_handle* h, int32_t on);

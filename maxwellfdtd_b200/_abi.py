@@ -142,6 +142,12 @@ class Library:
         if self.has_snapshots:
             self.set_snapshots = fn("set_snapshots", C.c_int, [vp, C.c_int32, C.POINTER(C.c_int32), C.c_int64,
                                                               C.POINTER(C.c_int64), vp])
+        # model state images (CUDA library only)
+        self.has_state = hasattr(L, p + "read_state")
+        if self.has_state:
+            self.state_size = fn("state_size", C.c_int64, [vp])
+            self.read_state = fn("read_state", C.c_int, [vp, vp, C.c_int64])
+            self.write_state = fn("write_state", C.c_int, [vp, vp, C.c_int64])
         # batches of 2-D models (CUDA library only)
         self.has_batch = hasattr(L, p + "batch_create")
         if self.has_batch:
@@ -257,6 +263,17 @@ class Stepper:
 
     def device_bytes(self):
         return int(self.lib.device_bytes(self.h))
+
+    def read_state(self):
+        """The model's state image (mfd_read_state) as a uint8 array."""
+        n = int(self.lib.state_size(self.h))
+        out = np.empty(n, dtype=np.uint8)
+        self._check(self.lib.read_state(self.h, out.ctypes.data_as(C.c_void_p), n))
+        return out
+
+    def write_state(self, image):
+        image = np.ascontiguousarray(image, dtype=np.uint8)
+        self._check(self.lib.write_state(self.h, image.ctypes.data_as(C.c_void_p), image.size))
 
     def read_tfsf_record(self, k):
         n = self.lib.tfsf_record_size(self.h, int(k))

@@ -68,6 +68,18 @@ struct HandleBase {
     virtual int kernel_times(double* ms, int64_t* launches, int n) const = 0;
     virtual double last_run_ms() const = 0;
     virtual int64_t device_bytes() const = 0;
+    virtual int64_t state_size() const = 0;
+    virtual int read_state(void* dst, int64_t n) = 0;
+    virtual int write_state(const void* src, int64_t n) = 0;
+};
+
+// Header of a state image (mfd_read_state): the buffers follow in allocation order.
+struct StateHeader {
+    char magic[8];          // "MFDSTATE"
+    uint32_t version, nbuf;
+    uint64_t layout;        // hash of the model's dimensions, element sizes and buffer sizes
+    int64_t done, bad_step;
+    int32_t bad_kind, pad;
 };
 
 static double wait_timeout_s() {
@@ -381,6 +393,7 @@ class Engine : public HandleBase {
     SplitBox mat_rows{};   // core rows/planes holding material cells, aligned to the staged E tiles
     int mbox[6] = {0, -1, 0, -1, 0, -1};   // bounding box of the material cells (x0, x1, y0, y1, z0, z1; empty: none)
     long long slab_rows = 0;
+    bool resp_fused = false;   // material response inside the E kernel of the core rows (RESP)
     int kcount = 1;             // kernels issued by the current launch() call
 
     // timing
@@ -409,8 +422,13 @@ class Engine : public HandleBase {
         if (st) cudaStreamDestroy(st);
     }
 
+    // Buffers that the steps change (fields, running sums, psi, material and plasma state,
+    // monitor records and accumulators, the record arrays, the per-step flags), in allocation
+    // order: the model state that mfd_read_state / mfd_write_state carry.
+    std::vector<std::pair<void*, size_t>> state_bufs;
+
     template <typename U>
-    U* dalloc(size_t n) {
+    U* dalloc(size_t n, bool state = true) {
         if (n == 0) n = 1;
         void* p = nullptr;
         cudaError_t e = cudaMallocAsync(&p, n * sizeof(U), st);
@@ -421,12 +439,13 @@ class Engine : public HandleBase {
         allocs.push_back(p);
         bytes += (int64_t)(n * sizeof(U));
         MFD_CK(cudaMemsetAsync(p, 0, n * sizeof(U), st));
+        if (state) state_bufs.push_back({p, n * sizeof(U)});
         return (U*)p;
     }
 
     template <typename U>
     U* upload(const U* h, size_t n) {
-        U* d = dalloc<U>(n);
+        U* d = dalloc<U>(n, false);
         if (n) MFD_CK(cudaMemcpyAsync(d, h, n * sizeof(U), cudaMemcpyHostToDevice, st));
         MFD_CK(cudaStreamSynchronize(st));   // the host buffer may be a temporary
         return d;
@@ -679,6 +698,14 @@ class Engine : public HandleBase {
         if (const char* z = std::getenv("MFD_ASYNC_ZC")) async_zc = std::max(1, std::atoi(z));
         // rows and planes of the core box that hold material cells, widened to the staged
         // E kernel's tiles (AS_TY rows, async_zc planes from the core box's corner)
+        // The material response runs inside the core-row E kernel that covers the materials'
+        // rows when every dispersive, Kerr or plasma material lies in the core rows (none in
+        // a y or z layer, where the slab kernel updates the cells).
+        resp_fused = !response_mats.empty();
+        for (int g : response_mats) {
+            const MatDev<T, R>& m = mats_host[g - 1];
+            if (m.by0 < yl || m.by0 + m.bny > yr || m.bz0 < zl || m.bz0 + m.bnz > zr) resp_fused = false;
+        }
         mat_rows = SplitBox{0, 0, 0, 0, async_zc, 0};
         if (mbox[1] >= mbox[0]) {
             const int y0 = std::max(mbox[2], yl), y1 = std::min(mbox[3] + 1, yr);
@@ -1077,7 +1104,7 @@ class Engine : public HandleBase {
     }
 
     template <bool MAT, int FAST>
-    void launch_E_split(const EParams<T, R>& p) {
+    void launch_E_split(const EParams<T, R>& p, int cur) {
         kcount = 0;
         const int zn = sbox.zr - sbox.zl;
         if (sbox.yr > sbox.yl && zn > 0) {
@@ -1103,14 +1130,16 @@ class Engine : public HandleBase {
                         SplitBox sm = mat_rows;
                         sm.zc = zc3;
                         dim3 blk2(bx3, by3), grd2((nx + bx3 - 1) / bx3, (sm.yr - sm.yl + by3 - 1) / by3, (sm.zr - sm.zl + zc3 - 1) / zc3);
-                        e3d_core_kernel<T, R, MAT, FAST><<<grd2, blk2, 0, st>>>(p, d3, sm);
+                        if (resp_fused) e3d_core_kernel<T, R, MAT, FAST, true><<<grd2, blk2, 0, st>>>(p, d3, sm, cur);
+                        else e3d_core_kernel<T, R, MAT, FAST><<<grd2, blk2, 0, st>>>(p, d3, sm);
                         kcount++;
                     }
                 }
             }
             if (!(sizeof(T) == 4 && core_async)) {
                 dim3 blk(bx3, by3), grd((nx + bx3 - 1) / bx3, (sbox.yr - sbox.yl + by3 - 1) / by3, (zn + zc3 - 1) / zc3);
-                e3d_core_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sbox);
+                if (MAT && resp_fused) e3d_core_kernel<T, R, MAT, FAST, true><<<grd, blk, 0, st>>>(p, d3, sbox, cur);
+                else e3d_core_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p, d3, sbox);
                 kcount++;
             }
         }
@@ -1206,8 +1235,8 @@ class Engine : public HandleBase {
             launch(KC_E, [&] {
                 with_div([&](auto dm) {
                     constexpr int D = decltype(dm)::value;
-                    if (any_geom) launch_E_split<true, D>(p);
-                    else launch_E_split<false, D>(p);
+                    if (any_geom) launch_E_split<true, D>(p, cur);
+                    else launch_E_split<false, D>(p, cur);
                 });
             });
             done = true;
@@ -1234,7 +1263,8 @@ class Engine : public HandleBase {
                 });
             });
         // E of dispersive / plasma / Kerr cells: material_flat_kernel for up to 3 poles,
-        // material_kernel (poles in a runtime loop) beyond
+        // material_kernel (poles in a runtime loop) beyond -- unless the E update did it
+        if (ndim == 3 && use_split && resp_fused) return;
         for (int g : response_mats) {
             const MatDev<T, R>& m = mats_host[g - 1];
             launch(KC_MAT, [&] {
@@ -1407,7 +1437,7 @@ class Engine : public HandleBase {
             }
         }
         if (nsteps > 0 && ncomp > snap_cap) {
-            snap_stage = dalloc<T>((size_t)2 * ncomp * Np);   // kept until the handle is destroyed
+            snap_stage = dalloc<T>((size_t)2 * ncomp * Np, false);   // kept until the handle is destroyed
             snap_cap = ncomp;
             MFD_CK(cudaStreamSynchronize(st));
         }
@@ -1584,6 +1614,76 @@ class Engine : public HandleBase {
 
     double last_run_ms() const override { return run_ms; }
     int64_t device_bytes() const override { return bytes; }
+
+    // ---- state images -----------------------------------------------------------------
+    uint64_t layout_hash() const {
+        uint64_t hsh = 1469598103934665603ull;   // FNV-1a over the dimensions and buffer sizes
+        auto mix = [&](uint64_t v) {
+            for (int i = 0; i < 8; ++i) { hsh ^= (v >> (8 * i)) & 0xff; hsh *= 1099511628211ull; }
+        };
+        mix((uint64_t)ndim); mix(sizeof(T)); mix(sizeof(R)); mix((uint64_t)nx); mix((uint64_t)ny); mix((uint64_t)nz);
+        mix((uint64_t)nt); mix(state_bufs.size());
+        for (auto& b : state_bufs) mix(b.second);
+        return hsh;
+    }
+
+    int64_t state_size() const override {
+        int64_t n = (int64_t)sizeof(StateHeader);
+        for (auto& b : state_bufs) n += (int64_t)b.second;
+        return n;
+    }
+
+    int read_state(void* dst, int64_t n) override {
+        if (in_batch) { err = "the model is being stepped by a batch"; return MFD_ERR_INVALID; }
+        if (n < state_size()) { err = "state buffer smaller than mfd_state_size()"; return MFD_ERR_INVALID; }
+        MFD_CK(cudaSetDevice(dev));
+        if (st3) bounded_sync(st3);
+        StateHeader hd{};
+        std::memcpy(hd.magic, "MFDSTATE", 8);
+        hd.version = 1;
+        hd.nbuf = (uint32_t)state_bufs.size();
+        hd.layout = layout_hash();
+        hd.done = done; hd.bad_step = bad_step; hd.bad_kind = bad_kind;
+        char* out = (char*)dst;
+        std::memcpy(out, &hd, sizeof(hd));
+        size_t off = sizeof(hd);
+        for (auto& b : state_bufs) {
+            MFD_CK(cudaMemcpyAsync(out + off, b.first, b.second, cudaMemcpyDeviceToHost, st));
+            off += b.second;
+        }
+        bounded_sync(st);
+        return MFD_OK;
+    }
+
+    int write_state(const void* src, int64_t n) override {
+        if (in_batch) { err = "the model is being stepped by a batch"; return MFD_ERR_INVALID; }
+        if (n < (int64_t)sizeof(StateHeader)) { err = "state image too short"; return MFD_ERR_INVALID; }
+        StateHeader hd;
+        std::memcpy(&hd, src, sizeof(hd));
+        if (std::memcmp(hd.magic, "MFDSTATE", 8) != 0 || hd.version != 1) { err = "not a state image of this library"; return MFD_ERR_INVALID; }
+        if (hd.nbuf != state_bufs.size() || hd.layout != layout_hash() || n < state_size()) {
+            err = "the state image belongs to a model of another layout (create the handle from the same descriptor)";
+            return MFD_ERR_INVALID;
+        }
+        if (hd.done < 0 || hd.done > nt) { err = "state image with a step beyond Nt"; return MFD_ERR_INVALID; }
+        MFD_CK(cudaSetDevice(dev));
+        if (st3) bounded_sync(st3);
+        const char* in = (const char*)src;
+        size_t off = sizeof(hd);
+        for (auto& b : state_bufs) {
+            MFD_CK(cudaMemcpyAsync(b.first, in + off, b.second, cudaMemcpyHostToDevice, st));
+            off += b.second;
+        }
+        bounded_sync(st);
+        done = hd.done;
+        bad_step = hd.bad_step;
+        bad_kind = hd.bad_kind;
+        ring_used = 0;
+        snap_steps.clear();
+        snap_next = 0;
+        snap_busy[0] = snap_busy[1] = false;
+        return MFD_OK;
+    }
 };
 
 thread_local std::string g_create_error;
@@ -2199,6 +2299,21 @@ int mfd_last_run_ms(const mfd_handle* h, double* ms) {
     if (!h || !h->impl || !ms) return MFD_ERR_INVALID;
     *ms = h->impl->last_run_ms();
     return MFD_OK;
+}
+
+int64_t mfd_state_size(const mfd_handle* h) {
+    if (!h || !h->impl) return 0;
+    return h->impl->state_size();
+}
+
+int mfd_read_state(mfd_handle* h, void* dst, int64_t bytes) {
+    MFD_NEED_BUF(h, dst);
+    MFD_GUARD(h, h->impl->read_state(dst, bytes));
+}
+
+int mfd_write_state(mfd_handle* h, const void* src, int64_t bytes) {
+    MFD_NEED_BUF(h, src);
+    MFD_GUARD(h, h->impl->write_state(src, bytes));
 }
 
 int64_t mfd_device_bytes(const mfd_handle* h) {

@@ -278,9 +278,16 @@ struct ECoreLoad {
     int g;
 };
 
-template <typename T, typename R, bool MAT, int FAST>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) e3d_core_kernel(const __grid_constant__ EParams<T, R> p,
-                                                                               const Div3 D3, const SplitBox s) {
+// RESP: the cells of dispersive, Kerr or plasma materials also take their material response
+// here (material_cell, models.jl:1042-1154), right after their D update, instead of in the
+// material kernel that otherwise follows the E update; cur is the ADE ping-pong parity.
+// The response reads only the cell's own E^n (not yet overwritten: such cells skip E = D Me),
+// D, polarisation and plasma state, so doing it cell by cell inside the E update changes
+// nothing.  The engine uses it when every such material lies in the core rows this kernel
+// covers.
+template <typename T, typename R, bool MAT, int FAST, bool RESP = false>
+__global__ void __launch_bounds__(256, RESP ? 2 : (sizeof(T) == 4 ? MFD_CORE_MINB : 2))
+    e3d_core_kernel(const __grid_constant__ EParams<T, R> p, const Div3 D3, const SplitBox s, const int cur = 0) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = s.yl + blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -333,13 +340,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) e3d_c
         v.pb = X.in ? X.pb[kk] : T(0);
         return v;
     };
-    ECoreLoad<T> cur = load(c, k);
+    ECoreLoad<T> ld = load(c, k);
     for (int iz = z0; iz < z1; ++iz, c += sz, k += kstep) {
         ECoreLoad<T> nxt;
         if (iz + 1 < z1) nxt = load(c + sz, k + kstep);
-        const T hx = cur.hx, hy = cur.hy, hz = cur.hz;
-        const T hy_xm = zx ? T(0) : cur.hyx, hz_xm = zx ? T(0) : cur.hzx;
-        const T hx_ym = zy ? T(0) : cur.hxy, hz_ym = zy ? T(0) : cur.hzy;
+        const T hx = ld.hx, hy = ld.hy, hz = ld.hz;
+        const T hy_xm = zx ? T(0) : ld.hyx, hz_xm = zx ? T(0) : ld.hzx;
+        const T hx_ym = zy ? T(0) : ld.hxy, hz_ym = zy ? T(0) : ld.hzy;
         const T num[6] = {hx - hx_ym, hx - hx_zm, hy - hy_xm, hy - hy_zm, hz - hz_xm, hz - hz_ym};
         T q[6];
         curl_div<T, FAST>(D3, p.ddx, p.ddy, p.ddz, num, q);
@@ -347,14 +354,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) e3d_c
         T dHyx = q[2], dHzx = q[4];
         T Md1 = Md10, Md2 = Md20, Me = Me0;
         bool simple = true;
-        if (MAT && cur.g) {
-            const MatDev<T, R>& m = p.mats[cur.g - 1];
+        if (MAT && ld.g) {
+            const MatDev<T, R>& m = p.mats[ld.g - 1];
             Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
         }
-        T D0 = cur.dx, D1 = cur.dy, D2 = cur.dz;
+        T D0 = ld.dx, D1 = ld.dy, D2 = ld.dz;
         if (X.in) {   // cpml_e<-1> of the column's x face
-            const T pa = mad<FAST>(X.B, cur.pa, X.A * dHyx);
-            const T pb = mad<FAST>(X.B, cur.pb, X.A * dHzx);
+            const T pa = mad<FAST>(X.B, ld.pa, X.A * dHyx);
+            const T pb = mad<FAST>(X.B, ld.pb, X.A * dHzx);
             X.pa[k] = pa;
             X.pb[k] = pb;
             D1 = mad<FAST>(-Md2, pb, D1);
@@ -372,10 +379,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MFD_CORE_MINB : 2) e3d_c
             Ex[c] = D0 * Me;
             Ey[c] = D1 * Me;
             Ez[c] = D2 * Me;
+        } else if (RESP) {
+            T* Ep[3] = {Ex, Ey, Ez};
+            const T Dv[3] = {D0, D1, D2};
+            material_cell<T, R, 3>(p.mats + (ld.g - 1), ix, iy, iz, Ep, c, Dv, cur, p.dt);
         }
         hx_zm = hx;
         hy_zm = hy;
-        cur = nxt;
+        ld = nxt;
     }
 }
 
