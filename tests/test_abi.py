@@ -41,7 +41,8 @@ def test_oracle_exports_the_same_api(oracle_lib):
     for n in declared_functions():
         short = n[len("mfd_"):]
         if short in ("set_profiling", "kernel_times", "last_run_ms", "device_bytes", "abi_version",
-                     "read_integral_noalloc", "set_snapshots") or short.startswith("batch_"):
+                     "read_integral_noalloc", "set_snapshots", "state_size", "read_state", "write_state") \
+                or short.startswith(("batch_", "server_")):
             continue
         assert hasattr(oracle_lib.lib, "oracle_" + short), short
 
