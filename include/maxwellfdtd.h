@@ -75,9 +75,10 @@ enum { MFD_F32 = 0, MFD_F64 = 1 };
  * MFD_MODE_FAST: the tolerance mode.  Derivatives multiply by the reciprocal of the grid
  *   constant or kappa, the H/D/CPML/running-sum updates are fused multiply-adds and the
  *   Poynting norm uses the hardware reciprocal square root (single precision).  Results
- *   stay within relative L2 1e-5 (FP32) / 1e-12 (FP64) of the exact order; the material
- *   response (ADE, Kerr, plasma), sources and monitors keep the exact arithmetic.  Batch
- *   members must be MFD_MODE_EXACT. */
+ *   stay within relative L2 1e-5 (FP32) / 1e-12 (FP64) of the exact order; the DFT
+ *   accumulation of spectral monitors fuses its multiply-adds (double precision); the
+ *   material response (ADE, Kerr, plasma), sources and the other monitors keep the exact
+ *   arithmetic.  Batch members must be MFD_MODE_EXACT. */
 enum { MFD_MODE_EXACT = 0, MFD_MODE_FAST = 1 };
 
 /* ---- boundary conditions: the reference's bc2int codes (src/models.jl:1199-1217) ---- */

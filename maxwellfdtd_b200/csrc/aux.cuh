@@ -200,18 +200,20 @@ __global__ void __launch_bounds__(256) monitor_fieldsum_kernel(const MonDev<T>* 
 // order (dft.jl:43-48).  A block owns MFD_DFT_W frequencies of 2 * blockDim.x points; each
 // thread two points (j and j + blockDim.x, both coalesced).  The block's factors for all
 // staged steps are staged once in shared memory (the same for every point), so the inner
-// loop issues one ring load per point and broadcast shared loads per factor.
-#ifndef MFD_DFT_W
+// loop issues one ring load per point and broadcast shared loads per factor.  The grid's
+// fastest axis (blockIdx.x) is the frequency group: the blocks that read the same points'
+// staged values run side by side, so those values come from L2 after the first block has
+// read them from memory, once per flush instead of once per frequency group.
+// FUSED (the tolerance mode): S + F * factor as one fused multiply-add per part.
 #define MFD_DFT_W 4   // frequencies per thread (4 measured faster than 8: fewer registers, more warps)
-#endif
 #define MFD_DFT_MAXSLOTS 64
-template <typename T>
+template <typename T, bool FUSED = false>
 __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __restrict__ mon, int ncomp, int nslots,
                                                           long long it0_first) {
     __shared__ double2 tw[MFD_DFT_MAXSLOTS * MFD_DFT_W];   // [slot][w]
     const MonDev<T>& M = *mon;
-    const int k = blockIdx.y;
-    const int w0 = blockIdx.z * MFD_DFT_W;
+    const int k = blockIdx.z;
+    const int w0 = blockIdx.x * MFD_DFT_W;
     const int nw = M.nw;
     const int wn = min(MFD_DFT_W, nw - w0);
     for (int i = threadIdx.x; i < nslots * MFD_DFT_W; i += blockDim.x) {
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __res
     }
     __syncthreads();
     const long long npts = M.npts;
-    const long long j0 = blockIdx.x * 2LL * blockDim.x + threadIdx.x;
+    const long long j0 = blockIdx.y * 2LL * blockDim.x + threadIdx.x;
     const long long j1 = j0 + blockDim.x;
     if (j0 >= npts) return;
     const bool two = j1 < npts;
@@ -244,10 +246,17 @@ __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __res
 #pragma unroll
         for (int w = 0; w < MFD_DFT_W; ++w) {
             const double2 t = e[w];
-            ar[w] = ar[w] + f * t.x;
-            ai[w] = ai[w] + f * t.y;
-            br[w] = br[w] + g * t.x;
-            bi[w] = bi[w] + g * t.y;
+            if (FUSED) {
+                ar[w] = fma(f, t.x, ar[w]);
+                ai[w] = fma(f, t.y, ai[w]);
+                br[w] = fma(g, t.x, br[w]);
+                bi[w] = fma(g, t.y, bi[w]);
+            } else {
+                ar[w] = ar[w] + f * t.x;
+                ai[w] = ai[w] + f * t.y;
+                br[w] = br[w] + g * t.x;
+                bi[w] = bi[w] + g * t.y;
+            }
         }
     }
 #pragma unroll

@@ -79,13 +79,8 @@ __device__ __forceinline__ void b_stage(P* dst, const P* src) {
 }
 
 
-#ifndef MFD_B2D_CHUNK
 #define MFD_B2D_CHUNK 4  // a block takes runs of this many consecutive tiles (fewer member changes)
-#endif
 
-#ifndef MFD_B2D_SMEM
-#define MFD_B2D_SMEM 1   // 2-D blocks copy the member's parameters to shared memory per tile (42.1 vs 40.8 Gcell/s)
-#endif
 
 __global__ void __launch_bounds__(512) batch_h2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
@@ -103,13 +98,13 @@ __global__ void __launch_bounds__(512) batch_h2d_kernel(const BMember* __restric
         const int acc = M.it > M.first ? 1 : 0;
         const long long prev = M.it - 1;
         const int flags = M.flags;
-        if (MFD_B2D_SMEM && tl.m != cur) {
+        if (tl.m != cur) {   // the block copies the member's parameters to shared memory (42.1 vs 40.8 Gcell/s)
             __syncthreads();          // the previous member's parameters are no longer read
             b_stage(&sp, M.hp);
             __syncthreads();
             cur = tl.m;
         }
-        const HParams<float>& p = MFD_B2D_SMEM ? sp : *M.hp;
+        const HParams<float>& p = sp;
         const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
         if (ix >= p.L.nx || iz >= p.L.nz) continue;
         switch (flags & (BF_MATH | BF_FAST)) {
@@ -135,13 +130,13 @@ __global__ void __launch_bounds__(512) batch_e2d_kernel(const BMember* __restric
         const BMember& M = mem[tl.m];
         if (!b_active(M)) continue;   // the same for the whole block
         const int flags = M.flags;
-        if (MFD_B2D_SMEM && tl.m != cur) {
+        if (tl.m != cur) {   // the block copies the member's parameters to shared memory (42.1 vs 40.8 Gcell/s)
             __syncthreads();
             b_stage(&sp, M.ep);
             __syncthreads();
             cur = tl.m;
         }
-        const EParams<float, double>& p = MFD_B2D_SMEM ? sp : *M.ep;
+        const EParams<float, double>& p = sp;
         const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
         if (ix >= p.L.nx || iz >= p.L.nz) continue;
         switch (flags & (BF_MAT | BF_FAST)) {
@@ -182,51 +177,29 @@ __global__ void __launch_bounds__(128) batch_material2d_kernel(const BMember* __
     }
 }
 
-#ifndef MFD_B3D_MINB
 #define MFD_B3D_MINB 3   // batched 3-D updates held to 40 registers (measured 16.0 against 15.0 Gcell/s at 58)
-#endif
 
-#ifndef MFD_B3D_LINEAR
-#define MFD_B3D_LINEAR 1   // 3-D tiles are runs of cells in x-fastest order (no idle lanes at short rows)
-#endif
 
-// 3-D members: tile rows are (y, z) rows numbered y + ny z.
-__device__ __forceinline__ bool b_row3(const Layout& L, int r, int& iy, int& iz) {
-    if (r >= L.ny * L.nz) return false;
-    iz = r / L.ny;
-    iy = r - iz * L.ny;
-    return true;
-}
-
-// The cell of a 3-D tile's thread: with linear tiles the block's threads take the
-// blockDim.x * blockDim.y cells in x-fastest order from the tile's first cell (x0, z0, w)
-// = (x, y, z); otherwise the tile is x cells x0.. of rows z0...
+// The cell of a 3-D tile's thread.  A 3-D tile is a run of cells in x-fastest order (no
+// idle lanes at rows shorter than the block): the block's threads take the
+// blockDim.x * blockDim.y cells from the tile's first cell (x0, z0, w) = (x, y, z).
 __device__ __forceinline__ bool b_cell3(const Layout& L, const BTile& tl, int& ix, int& iy, int& iz) {
-    if (MFD_B3D_LINEAR) {
-        // offset / nx row steps, a few at the tile shapes used: cheaper than two divisions
-        ix = tl.x0 + (int)(threadIdx.y * blockDim.x + threadIdx.x);
-        iy = tl.z0;
-        iz = tl.w;
-        while (ix >= L.nx) {
-            ix -= L.nx;
-            if (++iy == L.ny) {
-                iy = 0;
-                ++iz;
-            }
+    // offset / nx row steps, a few at the tile shapes used: cheaper than two divisions
+    ix = tl.x0 + (int)(threadIdx.y * blockDim.x + threadIdx.x);
+    iy = tl.z0;
+    iz = tl.w;
+    while (ix >= L.nx) {
+        ix -= L.nx;
+        if (++iy == L.ny) {
+            iy = 0;
+            ++iz;
         }
-        return iz < L.nz;
     }
-    ix = tl.x0 + threadIdx.x;
-    return ix < L.nx && b_row3(L, tl.z0 + threadIdx.y, iy, iz);
+    return iz < L.nz;
 }
 
-#ifndef MFD_B3D_CHUNK
 #define MFD_B3D_CHUNK 16 // a block takes runs of this many consecutive tiles (fewer member changes)
-#endif
 
-#ifndef MFD_B3D_SMEM
-#define MFD_B3D_SMEM 1   // a block copies the member's update parameters to shared memory per tile
-#endif
 
 // The running sums of the previous step are added from a member's second step on.
 template <bool MATH, bool FAST>
@@ -253,15 +226,15 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_h3d_kernel(const BMem
         if (!b_active(M)) continue;   // the same for the whole block
         const long long it = M.it, first = M.first;
         const int flags = M.flags;
-        if (MFD_B3D_SMEM && tl.m != cur) {
+        if (tl.m != cur) {   // the block copies the member's parameters to shared memory
             __syncthreads();          // the previous member's parameters are no longer read
             b_stage(&sp, M.hp);
             if (threadIdx.x == 0 && threadIdx.y == 0) sd3 = M.d3;
             __syncthreads();
             cur = tl.m;
         }
-        const HParams<float>& p = MFD_B3D_SMEM ? sp : *M.hp;
-        const Div3& d3 = MFD_B3D_SMEM ? sd3 : M.d3;
+        const HParams<float>& p = sp;
+        const Div3& d3 = sd3;
         int ix, iy, iz;
         if (!b_cell3(p.L, tl, ix, iy, iz)) continue;
         switch (flags & (BF_MATH | BF_FAST)) {
@@ -288,15 +261,15 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_e3d_kernel(const BMem
         const BMember& M = mem[tl.m];
         if (!b_active(M)) continue;   // the same for the whole block
         const int flags = M.flags;
-        if (MFD_B3D_SMEM && tl.m != cur) {
+        if (tl.m != cur) {   // the block copies the member's parameters to shared memory
             __syncthreads();
             b_stage(&sp, M.ep);
             if (threadIdx.x == 0 && threadIdx.y == 0) sd3 = M.d3;
             __syncthreads();
             cur = tl.m;
         }
-        const EParams<float, double>& p = MFD_B3D_SMEM ? sp : *M.ep;
-        const Div3& d3 = MFD_B3D_SMEM ? sd3 : M.d3;
+        const EParams<float, double>& p = sp;
+        const Div3& d3 = sd3;
         int ix, iy, iz;
         if (!b_cell3(p.L, tl, ix, iy, iz)) continue;
         switch (flags & (BF_MAT | BF_FAST)) {

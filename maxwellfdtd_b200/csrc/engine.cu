@@ -279,9 +279,7 @@ class DivisorCache {
 // Lowest |x| of the fast path: 2^-100 keeps x - q0 d an exact float (its quantum stays at or
 // above the subnormal one) with two binades of margin; the device check covers the band's
 // lowest binade as well.
-#ifndef MFD_DIV_LO_EXP
 #define MFD_DIV_LO_EXP -100
-#endif
 
 template <typename T>
 static DivC<T> make_div(T d) {
@@ -391,6 +389,7 @@ class Engine : public HandleBase {
     bool use_split = false;
     SplitBox sbox{};
     SplitBox mat_rows{};   // core rows/planes holding material cells, aligned to the staged E tiles
+    int mat_x0 = 0, mat_x1 = 0;   // ... and their columns, aligned to the tiles of both E kernels
     int mbox[6] = {0, -1, 0, -1, 0, -1};   // bounding box of the material cells (x0, x1, y0, y1, z0, z1; empty: none)
     long long slab_rows = 0;
     bool resp_fused = false;   // material response inside the E kernel of the core rows (RESP)
@@ -671,13 +670,6 @@ class Engine : public HandleBase {
         h_flags_v.assign((size_t)nt, 0);
         h_flags = h_flags_v.data();
         MFD_CK(cudaStreamSynchronize(st));
-        const char* tune = std::getenv("MFD_TILE3D");
-        if (tune) {
-            int a, b, c;
-            if (std::sscanf(tune, "%d,%d,%d", &a, &b, &c) == 3 && a > 0 && b > 0 && c > 0 && a * b <= 256 && a % 32 == 0) {
-                bx3 = a; by3 = b; zc3 = c;
-            }
-        }
         init_split();
     }
 
@@ -715,6 +707,8 @@ class Engine : public HandleBase {
                 mat_rows.yr = std::min(yr, yl + (y1 - yl + AS_TY - 1) / AS_TY * AS_TY);
                 mat_rows.zl = zl + (z0 - zl) / async_zc * async_zc;
                 mat_rows.zr = std::min(zr, zl + (z1 - zl + async_zc - 1) / async_zc * async_zc);
+                mat_x0 = mbox[0] / bx3 * bx3;
+                mat_x1 = std::min(nx, (mbox[1] + bx3) / bx3 * bx3);
             }
         }
 
@@ -941,6 +935,8 @@ class Engine : public HandleBase {
         for (int m = 0; m < d->nmon; ++m) {
             const mfd_monitor& a = d->mons[m];
             if (a.npts < 1) throw Error(MFD_ERR_INVALID, "monitor without points");
+            if (a.kind == MFD_MON_SPECTRAL && (a.npts + 511) / 512 > 65535)
+                throw Error(MFD_ERR_INVALID, "a spectral monitor has more than 33553920 points");
             if (a.kind == MFD_MON_SPECTRAL || a.sum) ring_vals += (long long)ncomp_mon * a.npts;
         }
         need_ring = ring_vals > 0;
@@ -1118,9 +1114,10 @@ class Engine : public HandleBase {
                     prefer_shared((const void*)e3d_core_async_kernel<R, false, FAST>);
                     SplitBox sa = sbox;
                     sa.zc = async_zc;
-                    const int4 skip = MAT ? make_int4(mat_rows.yl, mat_rows.yr, mat_rows.zl, mat_rows.zr) : make_int4(0, 0, 0, 0);
-                    const bool all_mat = MAT && mat_rows.yl == sbox.yl && mat_rows.yr == sbox.yr && mat_rows.zl == sbox.zl &&
-                                         mat_rows.zr == sbox.zr;   // nothing left for the staged kernel
+                    const TileSkip skip = MAT ? TileSkip{mat_x0, mat_x1, mat_rows.yl, mat_rows.yr, mat_rows.zl, mat_rows.zr}
+                                              : TileSkip{0, 0, 0, 0, 0, 0};
+                    const bool all_mat = MAT && mat_x0 == 0 && mat_x1 >= nx && mat_rows.yl == sbox.yl && mat_rows.yr == sbox.yr &&
+                                         mat_rows.zl == sbox.zl && mat_rows.zr == sbox.zr;   // nothing left for the staged kernel
                     dim3 blk(AS_TX, AS_TY), grd((nx + AS_TX - 1) / AS_TX, (sbox.yr - sbox.yl + AS_TY - 1) / AS_TY, (zn + async_zc - 1) / async_zc);
                     if (!all_mat) {
                         e3d_core_async_kernel<R, false, FAST><<<grd, blk, 0, st>>>(p, d3, sa, skip);
@@ -1129,9 +1126,10 @@ class Engine : public HandleBase {
                     if (MAT && mat_rows.yr > mat_rows.yl && mat_rows.zr > mat_rows.zl) {
                         SplitBox sm = mat_rows;
                         sm.zc = zc3;
-                        dim3 blk2(bx3, by3), grd2((nx + bx3 - 1) / bx3, (sm.yr - sm.yl + by3 - 1) / by3, (sm.zr - sm.zl + zc3 - 1) / zc3);
-                        if (resp_fused) e3d_core_kernel<T, R, MAT, FAST, true><<<grd2, blk2, 0, st>>>(p, d3, sm, cur);
-                        else e3d_core_kernel<T, R, MAT, FAST><<<grd2, blk2, 0, st>>>(p, d3, sm);
+                        dim3 blk2(bx3, by3), grd2((mat_x1 - mat_x0 + bx3 - 1) / bx3, (sm.yr - sm.yl + by3 - 1) / by3,
+                                                  (sm.zr - sm.zl + zc3 - 1) / zc3);
+                        if (resp_fused) e3d_core_kernel<T, R, MAT, FAST, true><<<grd2, blk2, 0, st>>>(p, d3, sm, cur, mat_x0);
+                        else e3d_core_kernel<T, R, MAT, FAST><<<grd2, blk2, 0, st>>>(p, d3, sm, 0, mat_x0);
                         kcount++;
                     }
                 }
@@ -1332,8 +1330,9 @@ class Engine : public HandleBase {
                 });
             } else if (M.kind == MFD_MON_SPECTRAL && !M.sum) {
                 launch(KC_DFT, [&] {
-                    dim3 grd((unsigned)((M.npts + 511) / 512), ncomp_mon, (M.nw + MFD_DFT_W - 1) / MFD_DFT_W);
-                    monitor_dft_kernel<T><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first);
+                    dim3 grd((M.nw + MFD_DFT_W - 1) / MFD_DFT_W, (unsigned)((M.npts + 511) / 512), ncomp_mon);
+                    if (recip) monitor_dft_kernel<T, true><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first);
+                    else monitor_dft_kernel<T><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first);
                 });
             } else if (M.kind == MFD_MON_SPECTRAL) {
                 launch(KC_DFT, [&] {
@@ -1871,7 +1870,7 @@ struct mfd_batch {
             const int mi = (int)i;
             const bool d3 = e->ndim == 3;
             const int rows = d3 ? e->ny * e->nz : e->nz;   // 3-D: rows y + ny z
-            if (d3 && MFD_B3D_LINEAR) {
+            if (d3) {
                 const int ncell = e->nx * rows;
                 for (int l = 0; l < ncell; l += cur_tx * cur_tz) {   // (x, y, z) of the tile's first cell
                     const int r = l / e->nx;

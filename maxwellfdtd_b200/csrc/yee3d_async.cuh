@@ -30,9 +30,7 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-#ifndef MFD_AS_TY
 #define MFD_AS_TY 4   // rows of a staged tile (a block is 32 x MFD_AS_TY threads)
-#endif
 constexpr int AS_TX = 32, AS_TY = MFD_AS_TY, AS_NST = 5, AS_AHEAD = 3;
 constexpr int AS_EW = AS_TX + 4;   // E rows: the tile's 32 columns and the 16-byte chunk holding x+1
 static_assert(AS_NST - AS_AHEAD == 2, "one barrier per plane needs two stages of slack");
@@ -54,9 +52,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-#ifndef MFD_HASYNC_MINB
 #define MFD_HASYNC_MINB (1024 / (32 * MFD_AS_TY))   // 1024 resident threads per SM (64 registers)
-#endif
 
 template <bool MATH, int FAST, bool ACC, bool E2S>
 __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_HASYNC_MINB) h3d_core_async_kernel(const __grid_constant__ HParams<float> p,
@@ -243,15 +239,13 @@ constexpr int EA_NO = 3 * AS_TY * (AS_TX / 4);
 constexpr int EA_SLOTS = (AS_NE + EA_NO + AS_TX * AS_TY - 1) / (AS_TX * AS_TY);
 constexpr int EA_NST = 5, EA_AHEAD = EA_NST - 3;   // the copy issued at plane iz lands in the stage last read at iz - 2
 
-#ifndef MFD_EASYNC_MINB
 #define MFD_EASYNC_MINB (1024 / (32 * MFD_AS_TY))   // 1024 resident threads per SM (64 registers)
-#endif
 
-// skip (rows y0 .. y1-1, planes z0 .. z1-1, aligned to the tiles; empty when y0 == y1): the
-// blocks there are left to another kernel (the register march with the material map).
+// skip: the tiles of the materials' columns, rows and planes, left to another kernel (the
+// register march with the material map).
 template <typename R, bool MAT, int FAST>
 __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_EASYNC_MINB) e3d_core_async_kernel(const __grid_constant__ EParams<float, R> p,
-                                                                        const Div3 D3, const SplitBox s, const int4 skip) {
+                                                                        const Div3 D3, const SplitBox s, const TileSkip skip) {
     __shared__ __align__(16) EAStage S[EA_NST];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AS_TX * ty;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -259,7 +253,7 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, MFD_EASYNC_MINB) e3d_core_async
     const int x0 = blockIdx.x * AS_TX;
     const int y0 = s.yl + blockIdx.y * AS_TY;
     const int z0 = s.zl + blockIdx.z * s.zc;
-    if (y0 >= skip.x && y0 < skip.y && z0 >= skip.z && z0 < skip.w) return;   // block-uniform
+    if (x0 >= skip.x0 && x0 < skip.x1 && y0 >= skip.y0 && y0 < skip.y1 && z0 >= skip.z0 && z0 < skip.z1) return;   // block-uniform
     const int z1 = min(z0 + s.zc, s.zr);
     const int ix = x0 + tx, iy = y0 + ty;
     const bool act = ix < nx && iy < s.yr;

@@ -17,12 +17,8 @@
 
 #include "yee.cuh"
 
-#ifndef MFD_CORE_MINB
 #define MFD_CORE_MINB 4   // single-precision core kernels: blocks of 256 threads' worth per SM (64 registers)
-#endif
-#ifndef MFD_SLAB_MINB
 #define MFD_SLAB_MINB 16  // single-precision slab kernels: 16 blocks of 128 threads per SM (32 registers; measured faster than 40)
-#endif
 
 namespace mfd {
 
@@ -34,6 +30,13 @@ struct SplitBox {
     int yl, yr, zl, zr;
     int zc;     // planes per core block
     int nzr;    // slab rows in z layers
+};
+
+// Tiles of the core rows that the staged E kernel leaves to the register march with the
+// material map: columns x0 .. x1-1, rows y0 .. y1-1, planes z0 .. z1-1 (aligned to the
+// tiles; empty when y0 == y1).
+struct TileSkip {
+    int x0, x1, y0, y1, z0, z1;
 };
 
 __device__ __forceinline__ void slab_row(const SplitBox& s, int ny, int r, int& iy, int& iz) {
@@ -287,8 +290,9 @@ struct ECoreLoad {
 // covers.
 template <typename T, typename R, bool MAT, int FAST, bool RESP = false>
 __global__ void __launch_bounds__(256, RESP ? 2 : (sizeof(T) == 4 ? MFD_CORE_MINB : 2))
-    e3d_core_kernel(const __grid_constant__ EParams<T, R> p, const Div3 D3, const SplitBox s, const int cur = 0) {
-    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    e3d_core_kernel(const __grid_constant__ EParams<T, R> p, const Div3 D3, const SplitBox s, const int cur = 0,
+                    const int xoff = 0) {
+    const int ix = xoff + blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = s.yl + blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
     if (ix >= nx || iy >= s.yr) return;
