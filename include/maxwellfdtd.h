@@ -75,10 +75,9 @@ enum { MFD_F32 = 0, MFD_F64 = 1 };
  * MFD_MODE_FAST: the tolerance mode.  Derivatives multiply by the reciprocal of the grid
  *   constant or kappa, the H/D/CPML/running-sum updates are fused multiply-adds and the
  *   Poynting norm uses the hardware reciprocal square root (single precision).  Results
- *   stay within relative L2 1e-5 (FP32) / 1e-12 (FP64) of the exact order; the DFT
- *   accumulation of spectral monitors fuses its multiply-adds (double precision); the
- *   material response (ADE, Kerr, plasma), sources and the other monitors keep the exact
- *   arithmetic.  Batch members must be MFD_MODE_EXACT. */
+ *   stay within relative L2 1e-5 (FP32) / 1e-12 (FP64) of the exact order; the material
+ *   response (ADE, Kerr, plasma), sources and monitors keep the exact arithmetic.  Batch
+ *   members must be MFD_MODE_EXACT. */
 enum { MFD_MODE_EXACT = 0, MFD_MODE_FAST = 1 };
 
 /* ---- boundary conditions: the reference's bc2int codes (src/models.jl:1199-1217) ---- */
@@ -347,6 +346,46 @@ MFD_API const char* mfd_batch_last_error(const mfd_batch* b);
 MFD_API int64_t mfd_state_size(const mfd_handle* h);
 MFD_API int mfd_read_state(mfd_handle* h, void* dst, int64_t bytes);
 MFD_API int mfd_write_state(mfd_handle* h, const void* src, int64_t bytes);
+
+/* ---- serving ----------------------------------------------------------------------------
+ * No counterpart in the reference, which runs one solve! at a time.  A server solves a stream
+ * of requests on one device.  mfd_server_submit queues a model descriptor; the server admits
+ * queued requests in arrival order when the request's device-memory footprint (computed from
+ * the descriptor before anything is allocated, mfd_server_footprint) fits the budget next to
+ * the admitted requests and fewer than max_active requests are computing, and uploads it.
+ * 2-D and small 3-D (at most 2^20 cells) single-precision requests in MFD_MODE_EXACT with
+ * rho_fp64 and no TFSF recording join one running batch (mfd_batch_*), which takes new
+ * members between its runs of steps (continuous batching); every other request runs as a
+ * solo lane on its own host thread and stream, at most max_solo at a time.  A request that
+ * waits only for a solo lane does not hold back batch requests behind it; one that waits for
+ * memory does.  Every request computes exactly what mfd_create + mfd_run(1, nt) compute.
+ *
+ * The descriptor and every array it points to must stay valid until mfd_server_poll reports
+ * the request MFD_REQ_RUNNING (uploaded) or later.  A finished request (MFD_REQ_DONE) keeps
+ * its handle and its share of the budget until mfd_server_release: read its results through
+ * mfd_server_handle and the mfd_read_* calls first (do not run, write or destroy that
+ * handle).  A failed request (MFD_REQ_FAILED; its status code is returned by poll and wait)
+ * gives its memory back at once.  Times are seconds since the server's creation: submitted,
+ * admitted, running (uploaded), finished.  The calls are safe from any host thread.
+ * mfd_server_destroy waits for admitted requests to finish, drops queued ones and frees
+ * every handle. */
+enum { MFD_REQ_QUEUED = 0, MFD_REQ_ADMITTED = 1, MFD_REQ_RUNNING = 2, MFD_REQ_DONE = 3, MFD_REQ_FAILED = 4 };
+typedef struct mfd_server mfd_server;
+MFD_API int mfd_server_create(int32_t device, double budget_bytes, int32_t max_active, int32_t max_solo, mfd_server** out);
+MFD_API void mfd_server_destroy(mfd_server* s);
+/* MFD_ERR_ADMISSION when the request could never fit the budget. */
+MFD_API int mfd_server_submit(mfd_server* s, const mfd_desc* desc, int64_t* id);
+/* state, times[4] (may be NULL) and the footprint in bytes (may be NULL). */
+MFD_API int mfd_server_poll(mfd_server* s, int64_t id, int32_t* state, double* times, int64_t* bytes);
+/* Waits up to timeout_s seconds for the request to finish (MFD_ERR_TIMEOUT if it has not). */
+MFD_API int mfd_server_wait(mfd_server* s, int64_t id, double timeout_s, int32_t* state);
+MFD_API int mfd_server_handle(mfd_server* s, int64_t id, mfd_handle** h);
+MFD_API int mfd_server_release(mfd_server* s, int64_t id);
+MFD_API int mfd_server_info(mfd_server* s, int64_t* queued, int64_t* running, int64_t* done, int64_t* failed,
+                            double* used_bytes, double* peak_used_bytes, int32_t* peak_active);
+/* Device bytes mfd_create would allocate for the descriptor (-1: invalid descriptor). */
+MFD_API int64_t mfd_server_footprint(const mfd_desc* desc);
+MFD_API const char* mfd_server_last_error(mfd_server* s);
 
 /* Device-time measurement: when on, every kernel launch of mfd_run is bracketed by CUDA
  * events on the handle's stream and its duration is summed per kernel class. */

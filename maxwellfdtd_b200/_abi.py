@@ -12,6 +12,7 @@ MFD_OK, MFD_ERR_INVALID, MFD_ERR_OOM, MFD_ERR_CUDA, MFD_ERR_NONFINITE, MFD_ERR_T
 MFD_F32, MFD_F64 = 0, 1
 MFD_MODE_EXACT, MFD_MODE_FAST = 0, 1
 MFD_INC_FULL, MFD_INC_ALONG_B, MFD_INC_ALONG_A, MFD_INC_UNIFORM = range(4)
+MFD_REQ_QUEUED, MFD_REQ_ADMITTED, MFD_REQ_RUNNING, MFD_REQ_DONE, MFD_REQ_FAILED = range(5)
 MFD_INT_SA, MFD_INT_E2, MFD_INT_JE, MFD_INT_RHO = range(4)
 MFD_RATE_NONE, MFD_RATE_POWER, MFD_RATE_TABLE = range(3)
 MFD_MON_FIELD, MFD_MON_SPECTRAL = range(2)
@@ -148,6 +149,23 @@ class Library:
             self.state_size = fn("state_size", C.c_int64, [vp])
             self.read_state = fn("read_state", C.c_int, [vp, vp, C.c_int64])
             self.write_state = fn("write_state", C.c_int, [vp, vp, C.c_int64])
+        # the serving loop (CUDA library only)
+        self.has_server = hasattr(L, p + "server_create")
+        if self.has_server:
+            self.server_create = fn("server_create", C.c_int, [C.c_int32, C.c_double, C.c_int32, C.c_int32, C.POINTER(vp)])
+            self.server_destroy = fn("server_destroy", None, [vp])
+            self.server_submit = fn("server_submit", C.c_int, [vp, C.POINTER(Desc), C.POINTER(C.c_int64)])
+            self.server_poll = fn("server_poll", C.c_int, [vp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                                           C.POINTER(C.c_int64)])
+            self.server_wait = fn("server_wait", C.c_int, [vp, C.c_int64, C.c_double, C.POINTER(C.c_int32)])
+            self.server_handle = fn("server_handle", C.c_int, [vp, C.c_int64, C.POINTER(vp)])
+            self.server_release = fn("server_release", C.c_int, [vp, C.c_int64])
+            self.server_info = fn("server_info", C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                                           C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                                           C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                           C.POINTER(C.c_int32)])
+            self.server_footprint = fn("server_footprint", C.c_int64, [C.POINTER(Desc)])
+            self.server_last_error = fn("server_last_error", C.c_char_p, [vp])
         # batches of 2-D models (CUDA library only)
         self.has_batch = hasattr(L, p + "batch_create")
         if self.has_batch:
@@ -335,3 +353,89 @@ class Batch:
         except Exception:
             pass
 
+
+
+class Borrowed(Stepper):
+    """A handle owned by someone else (a server's finished request): readable like a
+    Stepper, never destroyed by this object."""
+
+    def __init__(self, lib, h, builder, dtype):
+        self.lib = lib
+        self.builder = builder
+        self.dtype = np.dtype(dtype)
+        d = builder.desc
+        self.shape3 = (d.nx, d.ny, d.nz)
+        self.N = d.nx * d.ny * d.nz
+        self.h = h
+
+    def close(self):
+        self.h = None
+
+
+class Server:
+    """The library's serving loop (mfd_server_*): submit descriptors, poll, read the finished
+    requests' handles, release them."""
+
+    def __init__(self, lib, device=0, budget_bytes=160e9, max_active=64, max_solo=16):
+        if not getattr(lib, "has_server", False):
+            raise RuntimeError("this library has no server entry points")
+        self.lib = lib
+        s = C.c_void_p()
+        st = lib.server_create(int(device), float(budget_bytes), int(max_active), int(max_solo), C.byref(s))
+        if st != MFD_OK:
+            raise StepperError(st, f"server create failed ({st}): {lib.create_error().decode()}")
+        self.s = s
+        self._keep = {}
+
+    def _check(self, st):
+        if st != MFD_OK:
+            raise StepperError(st, self.lib.server_last_error(self.s).decode())
+
+    def submit(self, builder):
+        """Queue a descriptor (its DescBuilder is kept alive until the request is released)."""
+        rid = C.c_int64()
+        self._check(self.lib.server_submit(self.s, C.byref(builder.desc), C.byref(rid)))
+        self._keep[rid.value] = builder
+        return rid.value
+
+    def poll(self, rid):
+        """(state, [submitted, admitted, running, finished] seconds, footprint bytes, status)."""
+        state, t, nb = C.c_int32(), (C.c_double * 4)(), C.c_int64()
+        st = self.lib.server_poll(self.s, int(rid), C.byref(state), t, C.byref(nb))
+        if st != MFD_OK and state.value != MFD_REQ_FAILED:
+            self._check(st)
+        return state.value, list(t), nb.value, st
+
+    def wait(self, rid, timeout_s=3600.0):
+        state = C.c_int32()
+        self._check(self.lib.server_wait(self.s, int(rid), float(timeout_s), C.byref(state)))
+        return state.value
+
+    def handle(self, rid, dtype):
+        h = C.c_void_p()
+        self._check(self.lib.server_handle(self.s, int(rid), C.byref(h)))
+        return Borrowed(self.lib, h, self._keep[rid], dtype)
+
+    def release(self, rid):
+        self._check(self.lib.server_release(self.s, int(rid)))
+        self._keep.pop(rid, None)
+
+    def info(self):
+        q, r, d, f = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        u, pu, pa = C.c_double(), C.c_double(), C.c_int32()
+        self._check(self.lib.server_info(self.s, C.byref(q), C.byref(r), C.byref(d), C.byref(f), C.byref(u),
+                                         C.byref(pu), C.byref(pa)))
+        return {"queued": q.value, "running": r.value, "done": d.value, "failed": f.value, "used_bytes": u.value,
+                "peak_used_bytes": pu.value, "peak_active": pa.value}
+
+    def close(self):
+        if getattr(self, "s", None):
+            self.lib.server_destroy(self.s)
+            self.s = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

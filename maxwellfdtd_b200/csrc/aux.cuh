@@ -204,10 +204,9 @@ __global__ void __launch_bounds__(256) monitor_fieldsum_kernel(const MonDev<T>* 
 // fastest axis (blockIdx.x) is the frequency group: the blocks that read the same points'
 // staged values run side by side, so those values come from L2 after the first block has
 // read them from memory, once per flush instead of once per frequency group.
-// FUSED (the tolerance mode): S + F * factor as one fused multiply-add per part.
 #define MFD_DFT_W 4   // frequencies per thread (4 measured faster than 8: fewer registers, more warps)
 #define MFD_DFT_MAXSLOTS 64
-template <typename T, bool FUSED = false>
+template <typename T>
 __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __restrict__ mon, int ncomp, int nslots,
                                                           long long it0_first) {
     __shared__ double2 tw[MFD_DFT_MAXSLOTS * MFD_DFT_W];   // [slot][w]
@@ -246,17 +245,10 @@ __global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __res
 #pragma unroll
         for (int w = 0; w < MFD_DFT_W; ++w) {
             const double2 t = e[w];
-            if (FUSED) {
-                ar[w] = fma(f, t.x, ar[w]);
-                ai[w] = fma(f, t.y, ai[w]);
-                br[w] = fma(g, t.x, br[w]);
-                bi[w] = fma(g, t.y, bi[w]);
-            } else {
-                ar[w] = ar[w] + f * t.x;
-                ai[w] = ai[w] + f * t.y;
-                br[w] = br[w] + g * t.x;
-                bi[w] = bi[w] + g * t.y;
-            }
+            ar[w] = ar[w] + f * t.x;
+            ai[w] = ai[w] + f * t.y;
+            br[w] = br[w] + g * t.x;
+            bi[w] = bi[w] + g * t.y;
         }
     }
 #pragma unroll

@@ -1331,8 +1331,7 @@ class Engine : public HandleBase {
             } else if (M.kind == MFD_MON_SPECTRAL && !M.sum) {
                 launch(KC_DFT, [&] {
                     dim3 grd((M.nw + MFD_DFT_W - 1) / MFD_DFT_W, (unsigned)((M.npts + 511) / 512), ncomp_mon);
-                    if (recip) monitor_dft_kernel<T, true><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first);
-                    else monitor_dft_kernel<T><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first);
+                    monitor_dft_kernel<T><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first);
                 });
             } else if (M.kind == MFD_MON_SPECTRAL) {
                 launch(KC_DFT, [&] {
@@ -2328,3 +2327,5 @@ const char* mfd_last_error(const mfd_handle* h) {
 const char* mfd_create_error(void) { return g_create_error.c_str(); }
 
 }  // extern "C"
+
+#include "serve.cuh"

@@ -1,5 +1,10 @@
 """Serving loop: a stream of solves of mixed size and kind on one GPU.
 
+The loop itself is the library's native server (mfd_server_*, csrc/serve.cuh), reachable
+from any host language through the C ABI; Server below drives it from Python.  For a
+library without one (the CPU oracle, which the host-logic tests use) the same policy runs
+in Python threads.
+
 No counterpart in the reference, which runs one solve! at a time.  Requests arrive over
 time; each is admitted when its device-memory footprint fits the budget and a slot is
 free, in arrival order.  Its state then stays resident on the device until it completes.
@@ -272,6 +277,55 @@ class Server:
         for r in reqs:
             if r.bytes > self.budget:
                 raise ValueError(f"request {r.id} needs {r.bytes} bytes, more than the budget")
+        if getattr(self.lib, "has_server", False) and self.use_batch:
+            return self._run_native(reqs, realtime)
+        return self._run_python(reqs, realtime)
+
+    def _run_native(self, reqs, realtime):
+        """The library's server: requests are submitted at their arrival times; finished ones
+        are read (their results kept when keep_results) and released."""
+        srv = _abi.Server(self.lib, self.device, self.budget, self.max_active, self.max_solo)
+        t0 = time.time()
+        waiting = deque(reqs)
+        live = {}
+        try:
+            while waiting or live:
+                now = time.time() - t0
+                while waiting and (not realtime or waiting[0].arrival <= now):
+                    r = waiting.popleft()
+                    r.t_submit = t0 + (r.arrival if realtime else 0.0)
+                    live[srv.submit(r.builder)] = r
+                for rid in list(live):
+                    state, times, _, code = srv.poll(rid)
+                    if state not in (_abi.MFD_REQ_DONE, _abi.MFD_REQ_FAILED):
+                        continue
+                    r = live.pop(rid)
+                    r.t_admit, r.t_created, r.t_ran = t0 + times[1], t0 + times[2], t0 + times[3]
+                    if state == _abi.MFD_REQ_DONE:
+                        st = srv.handle(rid, r.dtype)
+                        try:
+                            if self.keep_results:
+                                r.out = read_results(st, r, self.read_fields)
+                            r.status = st.status()
+                        except Exception as e:
+                            r.error = e
+                    else:
+                        r.error = _abi.StepperError(code, self.lib.server_last_error(srv.s).decode())
+                    srv.release(rid)
+                    r.t_done = time.time()
+                    self.done.append(r)
+                    if r.error is not None:
+                        self.errors.append(r)
+                time.sleep(0.002)
+            info = srv.info()
+        finally:
+            srv.close()
+        self.admitted = [r.id for r in sorted(reqs, key=lambda r: (r.t_admit, r.arrival))]
+        self.peak_used = info["peak_used_bytes"]
+        self.peak_active = info["peak_active"]
+        return self.stats(reqs, t0)
+
+    def _run_python(self, reqs, realtime):
         self.stopping = False
         if self.use_batch:
             self.batch = _abi.Batch(self.lib, self.device)

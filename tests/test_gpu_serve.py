@@ -50,3 +50,58 @@ def test_serve_mix_matches_alone(gpu_lib):
         assert tuple(r.status) == tuple(status)
         bad = [key for key in ref if not np.array_equal(ref[key], r.out[key], equal_nan=True)]
         assert not bad, (r.id, r.batchable, bad)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_native_footprint_bounds_device_bytes(dtype, gpu_lib):
+    """mfd_server_footprint, the admission estimate the native server uses."""
+    for model, mons in footprint_models():
+        b, meta = model.build_desc(dtype, mons)
+        est = gpu_lib.server_footprint(C_byref(b))
+        st = _abi.Stepper(gpu_lib, b, dtype)
+        got = st.device_bytes()
+        st.close()
+        assert got <= est <= 1.1 * got + (1 << 20), (model.grid.ndim, got, est)
+
+
+def C_byref(builder):
+    import ctypes
+    return ctypes.byref(builder.desc)
+
+
+def test_native_server_api(gpu_lib):
+    """Submit, wait, read through the request's handle, release; a request larger than the
+    budget is refused at submission; unknown ids are refused."""
+    models = [(C.model_materials(3), C.monitors(3)), (C.model_materials(2), C.monitors(2)),
+              (C.model_bcs(1), None)]
+    builders = [m.build_desc(np.float32, mo) for m, mo in models]
+    budget = 4 * max(gpu_lib.server_footprint(C_byref(b)) for b, _ in builders)
+    srv = _abi.Server(gpu_lib, budget_bytes=budget, max_active=2, max_solo=1)
+    try:
+        ids = [srv.submit(b) for b, _ in builders]
+        for rid, (b, meta), (model, mons) in zip(ids, builders, models):
+            assert srv.wait(rid, 300.0) == _abi.MFD_REQ_DONE
+            state, times, nbytes, code = srv.poll(rid)
+            assert state == _abi.MFD_REQ_DONE and code == _abi.MFD_OK and nbytes > 0
+            assert times[0] <= times[1] <= times[2] <= times[3]
+            h = srv.handle(rid, np.float32)
+            got = h.read_field(6)
+            alone = _abi.Stepper(gpu_lib, b, np.float32)
+            alone.run(1, model.Nt)
+            assert np.array_equal(got, alone.read_field(6))
+            alone.close()
+            assert h.status()[0] == model.Nt
+            srv.release(rid)
+        info = srv.info()
+        assert info["done"] == len(ids) and info["failed"] == 0 and info["used_bytes"] == 0
+        assert info["peak_used_bytes"] <= budget and info["peak_active"] <= 2
+        big, _ = C.model_materials(3).build_desc(np.float32, C.monitors(3))
+        small_srv = _abi.Server(gpu_lib, budget_bytes=1e5, max_active=1, max_solo=1)
+        with pytest.raises(_abi.StepperError) as ei:
+            small_srv.submit(big)
+        assert ei.value.code == _abi.MFD_ERR_ADMISSION
+        small_srv.close()
+        with pytest.raises(_abi.StepperError):
+            srv.poll(12345)
+    finally:
+        srv.close()

@@ -50,3 +50,15 @@ def test_serve_rejects_request_beyond_budget(oracle_lib):
     srv = serve.Server(oracle_lib, budget_bytes=min(r.bytes for r in reqs) - 1, use_batch=False)
     with pytest.raises(ValueError):
         srv.run(reqs)
+
+
+def test_native_footprint_without_gpu():
+    """The library's admission estimate (mfd_server_footprint) is host code: it runs without a
+    device and agrees with the Python estimate within 10 %."""
+    from maxwellfdtd_b200 import _abi
+    import ctypes
+    lib = M.load_library()
+    for r in small_requests(6) + [serve.Request(9, C.model_materials(3), C.monitors(3), 0.0)]:
+        est = lib.server_footprint(ctypes.byref(r.builder.desc))
+        assert est > 0
+        assert abs(est - r.bytes) <= 0.1 * r.bytes + (1 << 16), (est, r.bytes)
