@@ -1374,6 +1374,30 @@ class Engine : public HandleBase {
 
     bool in_batch = false;     // stepped by a batch until it retires
 
+    // A run that ends before the last step leaves two things for later, so that the cost of
+    // a step does not depend on where the caller splits a run into calls: the values staged
+    // for summed and spectral monitors stay in the ring until it is full (the fold every
+    // ring_k steps), and the running sums of the run's last step are added by the next run's
+    // first H update (as within a run).  settle() completes both; every read that sees them,
+    // a field write, a state image and joining a batch settle first.
+    bool sums_pending = false;   // the running sums of step `done` are not yet added
+
+    void launch_guard(int64_t step) {
+        launch(KC_SUMS, [&] {
+            dim3 grd((nx + 255) / 256, ny, nz);
+            guard_kernel<T><<<grd, 256, 0, st>>>(F[MFD_EX], layout(), d_flags, step);
+        });
+    }
+
+    void settle() {
+        MFD_CK(cudaSetDevice(dev));
+        flush_monitors();
+        if (sums_pending) {
+            launch_sums(done);
+            sums_pending = false;
+        }
+    }
+
     int run(int64_t a, int64_t b) override {
         if (in_batch) { err = "the model is being stepped by a batch"; return MFD_ERR_INVALID; }
         if (bad_step) { err = "the model holds non-finite fields from step " + std::to_string(bad_step); return MFD_ERR_NONFINITE; }
@@ -1382,14 +1406,15 @@ class Engine : public HandleBase {
         MFD_CK(cudaSetDevice(dev));
         MFD_CK(cudaEventRecord(run_ev[0], st));
         for (int64_t it = a; it <= b; ++it) {
-            launch_H(it > a ? 1 : 0, it - 1);
+            launch_H((it > a || sums_pending) ? 1 : 0, it - 1);
+            sums_pending = false;
             launch_E((int)((it - 1) & 1));
             launch_sources(it);
             launch_monitors(it);
             if (record) launch_record(it);
             if (snap_next < snap_steps.size() && snap_steps[snap_next] == it) snapshot();
         }
-        return finish(a, b);
+        return finish(a, b, true);
     }
 
     // Frame snap_next: device copies into a free staging slot, then the host copies on st3.
@@ -1448,10 +1473,17 @@ class Engine : public HandleBase {
     }
 
     // End of a run of steps a..b (also of a batch member's window): staged monitors, the
-    // running sums of step b, and the per-step NaN/Inf flags.
-    int finish(int64_t a, int64_t b) {
-        flush_monitors();
-        launch_sums(b);
+    // running sums of step b, and the per-step NaN/Inf flags.  With defer (mfd_run) and b
+    // before the last step, the monitors' ring and the sums of step b are left for later
+    // (settle) and only the NaN/Inf guard of step b runs now.
+    int finish(int64_t a, int64_t b, bool defer = false) {
+        if (defer && b < nt) {
+            launch_guard(b);
+            sums_pending = true;
+        } else {
+            flush_monitors();
+            launch_sums(b);
+        }
         if (st3 && (snap_busy[0] || snap_busy[1])) bounded_sync(st3);   // frames of steps <= b are on the host
         MFD_CK(cudaEventRecord(run_ev[1], st));
         MFD_CK(cudaMemcpyAsync(h_flags + (a - 1), d_flags + (a - 1), (size_t)(b - a + 1) * sizeof(int),
@@ -1491,7 +1523,7 @@ class Engine : public HandleBase {
 
     int write_field(int comp, const void* src) override {
         if (comp < 0 || comp > 8 || !F[comp]) { err = "bad component"; return MFD_ERR_INVALID; }
-        MFD_CK(cudaSetDevice(dev));
+        settle();   // the pending running sums belong to the fields before the write
         MFD_CK(cudaMemcpy2DAsync(F[comp], (size_t)px * sizeof(T), src, (size_t)nx * sizeof(T), (size_t)nx * sizeof(T),
                                  (size_t)ny * nz, cudaMemcpyHostToDevice, st));
         bounded_sync(st);
@@ -1499,7 +1531,7 @@ class Engine : public HandleBase {
     }
 
     int read_integral(int which, void* dst) override {
-        MFD_CK(cudaSetDevice(dev));
+        settle();
         if (which == MFD_INT_SA) { copy_out(Sa, dst, sizeof(T)); return MFD_OK; }
         if (which == MFD_INT_E2) {
             if (E2) copy_out(E2, dst, sizeof(T));
@@ -1570,6 +1602,7 @@ class Engine : public HandleBase {
         if (k < 0) { err = "bad monitor component"; return MFD_ERR_INVALID; }
         const MonDev<T>& M = mons_host[m];
         MFD_CK(cudaSetDevice(dev));
+        flush_monitors();   // the values still staged in the ring
         if (M.kind == MFD_MON_FIELD) {
             const size_t n = M.sum ? (size_t)nt : (size_t)nt * M.npts;
             MFD_CK(cudaMemcpyAsync(dst, M.hist + (size_t)k * n, n * sizeof(T), cudaMemcpyDeviceToHost, st));
@@ -1634,7 +1667,7 @@ class Engine : public HandleBase {
     int read_state(void* dst, int64_t n) override {
         if (in_batch) { err = "the model is being stepped by a batch"; return MFD_ERR_INVALID; }
         if (n < state_size()) { err = "state buffer smaller than mfd_state_size()"; return MFD_ERR_INVALID; }
-        MFD_CK(cudaSetDevice(dev));
+        settle();   // the image holds no staged values and no pending sums
         if (st3) bounded_sync(st3);
         StateHeader hd{};
         std::memcpy(hd.magic, "MFDSTATE", 8);
@@ -1677,6 +1710,7 @@ class Engine : public HandleBase {
         bad_step = hd.bad_step;
         bad_kind = hd.bad_kind;
         ring_used = 0;
+        sums_pending = false;
         snap_steps.clear();
         snap_next = 0;
         snap_busy[0] = snap_busy[1] = false;
@@ -1830,6 +1864,8 @@ struct mfd_batch {
         if (e->snap_next < e->snap_steps.size()) { err = "batch members cannot take field snapshots"; return MFD_ERR_INVALID; }
         if (e->bad_step) { err = "the model holds non-finite fields"; return MFD_ERR_NONFINITE; }
         if (last <= e->done || last > e->nt) { err = "the last step must be after the model's current step and within 1..Nt"; return MFD_ERR_INVALID; }
+        e->settle();   // a member starts with an empty ring and its sums added
+        bounded_sync(e->st);
         MFD_CK(cudaSetDevice(dev));
         Member m{};
         m.h = h; m.e = e; m.first = e->done + 1; m.last = last; m.it = m.first;

@@ -877,4 +877,13 @@ __global__ void __launch_bounds__(256) sums_kernel(const __grid_constant__ HPara
     guard(p, ex);
 }
 
+// NaN/Inf guard of Ex for one step (models.jl:202-209), for a step whose running sums (and
+// the guard done with them) are left to the next H update.
+template <typename T>
+__global__ void __launch_bounds__(256) guard_kernel(const T* __restrict__ Ex, const Layout L, int* flags, const long long step) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ix >= L.nx) return;
+    guard_at(flags, step, Ex[ix + L.px * (int)blockIdx.y + L.sz * (int)blockIdx.z]);
+}
+
 }  // namespace mfd
