@@ -338,7 +338,8 @@ def solve(model, *, backend=None, fname=None, nframes=None, nstride=None, dtout=
     """``solve!(model; backend, ...)`` (models.jl:166-242).  Returns a Solution whose
     ``field`` holds the final fields and whose ``out`` holds what the reference writes to
     its output file (Sa, E2, rho_end, JE, field snapshots, monitors); with ``fname`` the
-    same datasets are saved as an .npz file."""
+    same datasets are saved: an HDF5 file in the reference's layout when the name ends in
+    .hdf, .h5 or .hdf5 (the reference's default is "out.hdf"), else an .npz file."""
     backend = backend or B200()
     dtype = backend.dtype
     g = model.grid
@@ -458,8 +459,28 @@ def _run(model, st, meta, dtype, fname, nframes, nstride, dtout, components, mon
         d = os.path.dirname(fname)
         if d:
             os.makedirs(d, exist_ok=True)
-        np.savez(fname, **{k: v for k, v in out.items() if isinstance(v, (np.ndarray, bool, int, float))})
+        saved = {k: v for k, v in out.items() if isinstance(v, (np.ndarray, bool, np.bool_, int, float))}
+        if os.path.splitext(fname)[1].lower() in (".hdf", ".h5", ".hdf5"):
+            write_hdf5(fname, saved)
+        else:
+            np.savez(fname, **saved)
     return Solution(model, Field(fields), out, np.asarray(t_T), np.dtype(dtype))
+
+
+def write_hdf5(fname, out):
+    """The reference's output file (outputs.jl, monitors.jl write_monitor) in HDF5: each
+    "a/b/c" key a dataset c in group a/b.  The arrays here have the reference's Julia shapes
+    (column-major, x fastest); HDF5.jl stores such an array with its dimensions reversed and
+    its bytes unchanged, which is what transposing a column-major view to C order gives."""
+    from . import hdf5
+    tree = {}
+    for key, v in out.items():
+        parts = key.split("/")
+        node = tree
+        for p in parts[:-1]:
+            node = node.setdefault(p, {})
+        node[parts[-1]] = np.asarray(v).T
+    hdf5.write(fname, tree)
 
 
 def _cartesian(grid, cells):
