@@ -197,67 +197,91 @@ __global__ void __launch_bounds__(256) monitor_fieldsum_kernel(const MonDev<T>* 
 }
 
 // Spectral monitor, per point: S[k][w][j] += F * (2 e_w(t) dt) for each staged step in
-// order (dft.jl:43-48).  A block owns MFD_DFT_W frequencies of 2 * blockDim.x points; each
-// thread two points (j and j + blockDim.x, both coalesced).  The block's factors for all
-// staged steps are staged once in shared memory (the same for every point), so the inner
-// loop issues one ring load per point and broadcast shared loads per factor.  The grid's
-// fastest axis (blockIdx.x) is the frequency group: the blocks that read the same points'
-// staged values run side by side, so those values come from L2 after the first block has
-// read them from memory, once per flush instead of once per frequency group.
-#define MFD_DFT_W 4   // frequencies per thread (4 measured faster than 8: fewer registers, more warps)
-#define MFD_DFT_MAXSLOTS 64
+// order (dft.jl:43-48), every product and sum rounded in double as the reference does.
+// The fold is a [points x steps] . [steps x frequencies] product in FP64, bound by the FP64
+// pipe once its operands come from shared memory.  A block owns DFT_PT points of one
+// component and a tile of up to DFT_WT frequencies: it stages the points' staged values
+// for every slot (the ring tile) and the tile's factors for every slot in shared memory
+// once, then each thread accumulates DFT_PS points x DFT_W frequencies in registers over
+// the slots -- per slot DFT_PS ring loads (consecutive threads, consecutive points) and
+// DFT_W factor loads (one address per warp: a broadcast) feed 4 * DFT_PS * DFT_W FP64
+// operations.  threadIdx.x picks the points (j, j + 32, ...), threadIdx.y the frequency
+// group of DFT_W.
+constexpr int MFD_DFT_MAXSLOTS = 64;
+constexpr int DFT_W = 4, DFT_PS = 2, DFT_PT = 32 * DFT_PS, DFT_WT = 32;
+
 template <typename T>
-__global__ void __launch_bounds__(256) monitor_dft_kernel(const MonDev<T>* __restrict__ mon, int ncomp, int nslots,
-                                                          long long it0_first) {
-    __shared__ double2 tw[MFD_DFT_MAXSLOTS * MFD_DFT_W];   // [slot][w]
+__global__ void __launch_bounds__(32 * DFT_WT / DFT_W, 2) monitor_dft_kernel(const MonDev<T>* __restrict__ mon, int ncomp,
+                                                                              int nslots, long long it0_first) {
+    extern __shared__ __align__(16) unsigned char dft_smem[];
+    double2* tw = reinterpret_cast<double2*>(dft_smem);                                  // [slot][w of the tile]
+    T* rt = reinterpret_cast<T*>(dft_smem + sizeof(double2) * MFD_DFT_MAXSLOTS * DFT_WT);   // [slot][point of the tile]
     const MonDev<T>& M = *mon;
-    const int k = blockIdx.z;
-    const int w0 = blockIdx.x * MFD_DFT_W;
+    const int k = blockIdx.y;
     const int nw = M.nw;
-    const int wn = min(MFD_DFT_W, nw - w0);
-    for (int i = threadIdx.x; i < nslots * MFD_DFT_W; i += blockDim.x) {
-        const int sl = i / MFD_DFT_W, w = i - sl * MFD_DFT_W;
-        tw[i] = w < wn ? M.phasor[(it0_first + sl) * nw + w0 + w] : make_double2(0.0, 0.0);
+    const int wt0 = blockIdx.z * DFT_WT;
+    const int wtn = min(DFT_WT, nw - wt0);
+    const long long npts = M.npts;
+    const long long p0 = (long long)blockIdx.x * DFT_PT;
+    const int tid = threadIdx.x + 32 * threadIdx.y, nth = 32 * blockDim.y;
+    for (int i = tid; i < nslots * DFT_WT; i += nth) {
+        const int sl = i / DFT_WT, w = i - sl * DFT_WT;
+        tw[i] = w < wtn ? M.phasor[(it0_first + sl) * nw + wt0 + w] : make_double2(0.0, 0.0);
+    }
+    const long long rstride = (long long)ncomp * npts;
+    const T* ring = M.ring + (long long)k * npts;
+    for (int i = tid; i < nslots * DFT_PT; i += nth) {
+        const int sl = i / DFT_PT, q = i - sl * DFT_PT;
+        rt[i] = p0 + q < npts ? ring[sl * rstride + p0 + q] : T(0);
     }
     __syncthreads();
-    const long long npts = M.npts;
-    const long long j0 = blockIdx.y * 2LL * blockDim.x + threadIdx.x;
-    const long long j1 = j0 + blockDim.x;
-    if (j0 >= npts) return;
-    const bool two = j1 < npts;
-    double ar[MFD_DFT_W], ai[MFD_DFT_W], br[MFD_DFT_W], bi[MFD_DFT_W];
-    double2* S = M.S + ((long long)k * nw + w0) * npts;
+    const int w0 = DFT_W * threadIdx.y;          // within the tile
+    if (w0 >= wtn) return;
+    const int wn = min(DFT_W, wtn - w0);
+    double ar[DFT_PS][DFT_W], ai[DFT_PS][DFT_W];
+    double2* S = M.S + ((long long)k * nw + wt0 + w0) * npts;
 #pragma unroll
-    for (int w = 0; w < MFD_DFT_W; ++w) {
-        ar[w] = ai[w] = br[w] = bi[w] = 0.0;
-        if (w < wn) {
-            const double2 a = S[(long long)w * npts + j0];
-            ar[w] = a.x; ai[w] = a.y;
-            if (two) { const double2 b = S[(long long)w * npts + j1]; br[w] = b.x; bi[w] = b.y; }
+    for (int a = 0; a < DFT_PS; ++a) {
+        const long long j = p0 + threadIdx.x + 32 * a;
+#pragma unroll
+        for (int w = 0; w < DFT_W; ++w) {
+            ar[a][w] = ai[a][w] = 0.0;
+            if (w < wn && j < npts) {
+                const double2 v = S[(long long)w * npts + j];
+                ar[a][w] = v.x;
+                ai[a][w] = v.y;
+            }
         }
     }
-    const T* ring = M.ring + (long long)k * npts;
-    const long long rstride = (long long)ncomp * npts;
     for (int sl = 0; sl < nslots; ++sl) {
-        const double f = (double)ring[sl * rstride + j0];
-        const double g = two ? (double)ring[sl * rstride + j1] : 0.0;
-        const double2* e = tw + sl * MFD_DFT_W;
+        double f[DFT_PS];
 #pragma unroll
-        for (int w = 0; w < MFD_DFT_W; ++w) {
+        for (int a = 0; a < DFT_PS; ++a) f[a] = (double)rt[sl * DFT_PT + threadIdx.x + 32 * a];
+        const double2* e = tw + sl * DFT_WT + w0;
+#pragma unroll
+        for (int w = 0; w < DFT_W; ++w) {
             const double2 t = e[w];
-            ar[w] = ar[w] + f * t.x;
-            ai[w] = ai[w] + f * t.y;
-            br[w] = br[w] + g * t.x;
-            bi[w] = bi[w] + g * t.y;
+#pragma unroll
+            for (int a = 0; a < DFT_PS; ++a) {
+                ar[a][w] = ar[a][w] + f[a] * t.x;
+                ai[a][w] = ai[a][w] + f[a] * t.y;
+            }
         }
     }
 #pragma unroll
-    for (int w = 0; w < MFD_DFT_W; ++w) {
-        if (w < wn) {
-            S[(long long)w * npts + j0] = make_double2(ar[w], ai[w]);
-            if (two) S[(long long)w * npts + j1] = make_double2(br[w], bi[w]);
-        }
+    for (int a = 0; a < DFT_PS; ++a) {
+        const long long j = p0 + threadIdx.x + 32 * a;
+        if (j >= npts) continue;
+#pragma unroll
+        for (int w = 0; w < DFT_W; ++w)
+            if (w < wn) S[(long long)w * npts + j] = make_double2(ar[a][w], ai[a][w]);
     }
+}
+
+// Shared memory of monitor_dft_kernel: the factor tile and the ring tile.
+template <typename T>
+constexpr size_t dft_smem_bytes() {
+    return sizeof(double2) * MFD_DFT_MAXSLOTS * DFT_WT + sizeof(T) * MFD_DFT_MAXSLOTS * DFT_PT;
 }
 
 // Spectral monitor with sum: S[k][w] += 2 * sum_j(F_j e_w(t)) * dt (dft.jl:38-41).

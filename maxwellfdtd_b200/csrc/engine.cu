@@ -935,11 +935,12 @@ class Engine : public HandleBase {
         for (int m = 0; m < d->nmon; ++m) {
             const mfd_monitor& a = d->mons[m];
             if (a.npts < 1) throw Error(MFD_ERR_INVALID, "monitor without points");
-            if (a.kind == MFD_MON_SPECTRAL && (a.npts + 511) / 512 > 65535)
-                throw Error(MFD_ERR_INVALID, "a spectral monitor has more than 33553920 points");
+            if (a.kind == MFD_MON_SPECTRAL && (a.nw + DFT_WT - 1) / DFT_WT > 65535)
+                throw Error(MFD_ERR_INVALID, "a spectral monitor has more than 4194240 frequencies");
             if (a.kind == MFD_MON_SPECTRAL || a.sum) ring_vals += (long long)ncomp_mon * a.npts;
         }
         need_ring = ring_vals > 0;
+        MFD_CK(cudaFuncSetAttribute(monitor_dft_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dft_smem_bytes<T>()));
         if (need_ring) {
             // staging depth: up to 64 steps, at most ~512 MB of staged values
             long long cap = (512ll << 20) / ((long long)sizeof(T) * ring_vals);
@@ -1330,8 +1331,11 @@ class Engine : public HandleBase {
                 });
             } else if (M.kind == MFD_MON_SPECTRAL && !M.sum) {
                 launch(KC_DFT, [&] {
-                    dim3 grd((M.nw + MFD_DFT_W - 1) / MFD_DFT_W, (unsigned)((M.npts + 511) / 512), ncomp_mon);
-                    monitor_dft_kernel<T><<<grd, 256, 0, st>>>(md, ncomp_mon, ring_used, ring_first);
+                    // blocks of 32 x (frequency groups of the tile), tiles of DFT_PT points
+                    const int wtile = std::min(DFT_WT, (M.nw + DFT_W - 1) / DFT_W * DFT_W);
+                    dim3 blk(32, wtile / DFT_W);
+                    dim3 grd((unsigned)((M.npts + DFT_PT - 1) / DFT_PT), ncomp_mon, (M.nw + DFT_WT - 1) / DFT_WT);
+                    monitor_dft_kernel<T><<<grd, blk, dft_smem_bytes<T>(), st>>>(md, ncomp_mon, ring_used, ring_first);
                 });
             } else if (M.kind == MFD_MON_SPECTRAL) {
                 launch(KC_DFT, [&] {
