@@ -195,3 +195,40 @@ def test_descriptor_inputs_in_caller_storage(oracle_lib):
         st.close()
     assert got_alloc, "no array went to the caller's storage"
     assert np.array_equal(outs[0], outs[1])
+
+
+def _c_fields(src, name):
+    body = re.search(r"typedef struct " + name + r" \{(.*?)\} " + name + ";", src, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        decl = re.sub(r"\[[^\]]*\]", "", decl)
+        names += [re.findall(r"(\w+)\s*$", v.strip())[0] for v in decl.split(",")]   # the declarator names
+    return names
+
+
+def _julia_fields(src, name):
+    body = re.search(r"struct " + name + r"\n(.*?)\nend", src, re.S).group(1)
+    return re.findall(r"(\w+)::", body)
+
+
+def test_julia_shim_mirrors_header():
+    """julia/MaxwellFDTDB200.jl declares the descriptor structs with the header's fields in the
+    header's order (the shim cannot run here: no Julia)."""
+    with open(HEADER) as f:
+        c = f.read()
+    with open(os.path.join(ROOT, "julia", "MaxwellFDTDB200.jl")) as f:
+        jl = f.read()
+    for cname, jname in (("mfd_pml_layer", "MfdPmlLayer"), ("mfd_material", "MfdMaterial"), ("mfd_source", "MfdSource"),
+                         ("mfd_tfsf", "MfdTFSF"), ("mfd_monitor", "MfdMonitor"), ("mfd_desc", "MfdDesc")):
+        assert _c_fields(c, cname) == _julia_fields(jl, jname), cname
+    for fn in declared_functions():
+        if fn.startswith(("mfd_batch_", "mfd_set_profiling", "mfd_kernel_times", "mfd_last_run_ms", "mfd_device_bytes",
+                          "mfd_abi_version", "mfd_status", "mfd_write_field", "mfd_read_tfsf_record",
+                          "mfd_tfsf_record_size", "mfd_set_snapshots", "mfd_server_poll", "mfd_server_info",
+                          "mfd_server_footprint")):
+            continue
+        assert ":" + fn + "," in jl, fn
