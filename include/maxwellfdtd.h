@@ -199,6 +199,33 @@ typedef struct mfd_monitor {
     const double* phasor;    /* spectral: [nt][nw][2] = exp(-i w (t_it - tshift))     */
 } mfd_monitor;
 
+/* ---- analytic geometry evaluated on the device ------------------------------------------
+ * The reference evaluates each material's geometry(x, y, z) at every grid point on the host
+ * and writes the material index, later materials winning (src/util.jl:1-31,
+ * src/models.jl:85-98).  For the shapes below the library builds the uint8 material map on
+ * the device instead: shapes are applied in order (a later shape overwrites the cells it
+ * covers), each writing its material index, and every test is the double-precision
+ * expression written here, evaluated left to right with no fused multiply-add, at the grid
+ * coordinates mfd_desc.coords -- so a host evaluating the same expression (numpy, Julia)
+ * gets the same map bit for bit.  2-D grids use (x, z) and 1-D grids z only: the missing
+ * coordinates are taken as 0.
+ *   MFD_SHAPE_BALL       p = cx, cy, cz, r:
+ *                        ((x-cx)*(x-cx) + (y-cy)*(y-cy)) + (z-cz)*(z-cz) <= r*r
+ *   MFD_SHAPE_BOX        p = x0, x1, y0, y1, z0, z1:  x0 <= x <= x1 && y0 <= y <= y1 && z0 <= z <= z1
+ *   MFD_SHAPE_ELLIPSOID  p = cx, cy, cz, ax, ay, az:
+ *                        (((x-cx)/ax)*((x-cx)/ax) + ((y-cy)/ay)*((y-cy)/ay)) + ((z-cz)/az)*((z-cz)/az) <= 1
+ *   MFD_SHAPE_CYLINDER   p = cx, cy, r, z0, z1 (axis along z):
+ *                        (x-cx)*(x-cx) + (y-cy)*(y-cy) <= r*r && z0 <= z <= z1
+ *   MFD_SHAPE_HALFSPACE  p = nx, ny, nz, d:  (nx*x + ny*y) + nz*z >= d
+ *   MFD_SHAPE_ALL        every cell */
+enum { MFD_SHAPE_BALL = 1, MFD_SHAPE_BOX = 2, MFD_SHAPE_ELLIPSOID = 3, MFD_SHAPE_CYLINDER = 4, MFD_SHAPE_HALFSPACE = 5,
+       MFD_SHAPE_ALL = 6 };
+typedef struct mfd_shape {
+    int32_t kind;            /* MFD_SHAPE_*                                            */
+    int32_t material;        /* 1..nmat, written into the cells the shape covers      */
+    double p[8];             /* parameters by kind                                    */
+} mfd_shape;
+
 /* Complete description of one model (reference Model, src/models.jl:1-122). */
 typedef struct mfd_desc {
     int32_t abi_version;     /* MFD_ABI_VERSION                                       */
@@ -225,6 +252,9 @@ typedef struct mfd_desc {
     int32_t rec_i2[3];
     int32_t device;          /* CUDA device ordinal                                   */
     int32_t mode;            /* MFD_MODE_EXACT / MFD_MODE_FAST                         */
+    int32_t nshape;          /* shapes evaluated on the device (geometry must be NULL) */
+    const mfd_shape* shapes;
+    const double* coords[3]; /* grid coordinates x[nx], y[ny], z[nz] (for the shapes)  */
 } mfd_desc;
 
 typedef struct mfd_handle mfd_handle;
@@ -243,6 +273,10 @@ MFD_API int mfd_run(mfd_handle* h, int64_t it_first, int64_t it_last);
 
 /* Number of steps completed and the first step whose Ex held NaN (bit 0) or Inf (bit 1). */
 MFD_API int mfd_status(const mfd_handle* h, int64_t* steps_done, int64_t* bad_step, int32_t* bad_kind);
+
+/* The material index map as the library holds it (nx*ny*nz bytes, x fastest): the
+ * descriptor's geometry, or the map built on the device from its shapes. */
+MFD_API int mfd_read_geometry(mfd_handle* h, uint8_t* dst);
 
 /* Dense field component (MFD_HX..MFD_EZ) to/from host memory, nx*ny*nz elements of T. */
 MFD_API int mfd_read_field(mfd_handle* h, int32_t comp, void* dst);

@@ -53,6 +53,10 @@ struct MfdMonitor
     kind::Int32; sum::Int32; npts::Int64; cells::Ptr{Int64}; nw::Int32; phasor::Ptr{Cdouble}
 end
 
+struct MfdShape
+    kind::Int32; material::Int32; p::NTuple{8,Cdouble}
+end
+
 struct MfdDesc
     abi_version::Int32; ndim::Int32; dtype::Int32; nx::Int32; ny::Int32; nz::Int32
     dx::Cdouble; dy::Cdouble; dz::Cdouble; dt::Cdouble; nt::Int64
@@ -61,6 +65,7 @@ struct MfdDesc
     geometry::Ptr{UInt8}; nmat::Int32; mats::Ptr{MfdMaterial}; rho_fp64::Int32
     nsrc::Int32; srcs::Ptr{MfdSource}; tfsf::MfdTFSF; nmon::Int32; mons::Ptr{MfdMonitor}
     tfsf_record::Int32; rec_i1::NTuple{3,Int32}; rec_i2::NTuple{3,Int32}; device::Int32; mode::Int32
+    nshape::Int32; shapes::Ptr{MfdShape}; coords::NTuple{3,Ptr{Cdouble}}
 end
 
 # ---- descriptor from a reference Model ------------------------------------------------------
@@ -172,7 +177,8 @@ function build_desc(model, ::Type{T}, monitors; mode=MFD_MODE_EXACT, device=0, i
     d = MfdDesc(MFD_ABI_VERSION, nd, T == Float64 ? MFD_F64 : MFD_F32, nx, ny, nz, dx, dy, grid.dz, dt, Nt,
                 Tuple(Int32.(bc6)), lay, Mh, Me, Md1, Md2, _ptr(keep, UInt8.(geometry)), length(mats),
                 isempty(mats) ? C_NULL : _ptr(keep, mats), 1, length(srcs), isempty(srcs) ? C_NULL : _ptr(keep, srcs),
-                tfsf, length(mons), isempty(mons) ? C_NULL : _ptr(keep, mons), 0, (0, 0, 0), (0, 0, 0), device, mode)
+                tfsf, length(mons), isempty(mons) ? C_NULL : _ptr(keep, mons), 0, (0, 0, 0), (0, 0, 0), device, mode,
+                0, C_NULL, (C_NULL, C_NULL, C_NULL))   # closures: the host map above, no device shapes
     return d, keep
 end
 
@@ -181,6 +187,7 @@ _check(h, st) = st == MFD_OK ||
 
 # readers: Julia Arrays are column-major with x fastest, the library's layout -> no transpose
 read_field!(h, comp, A::Array) = _check(h, ccall((:mfd_read_field, libmfd), Cint, (Ptr{Cvoid}, Int32, Ptr{Cvoid}), h, comp, A))
+read_geometry!(h, A::Array{UInt8}) = _check(h, ccall((:mfd_read_geometry, libmfd), Cint, (Ptr{Cvoid}, Ptr{UInt8}), h, A))
 read_integral!(h, which, A::Array) = _check(h, ccall((:mfd_read_integral, libmfd), Cint, (Ptr{Cvoid}, Int32, Ptr{Cvoid}), h, which, A))
 read_integral_noalloc!(h, which, A::Array) =
     _check(h, ccall((:mfd_read_integral_noalloc, libmfd), Cint, (Ptr{Cvoid}, Int32, Ptr{Cvoid}), h, which, A))

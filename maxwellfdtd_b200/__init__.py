@@ -6,6 +6,7 @@ Model, solve!).  The time-step path itself runs in libmaxwellfdtd_b200.so, hand-
 CUDA for sm_100a behind the C ABI in include/maxwellfdtd.h.
 """
 from .constants import C0, EPS0, HBAR, ME, MU0, QE
+from .geometry import Ball, Box, Cylinder, Ellipsoid, Everywhere, HalfSpace, Shape
 from .grids import Grid1D, Grid2D, Grid3D, make_grid as Grid
 from .materials import (DebyeSusceptibility, DrudeSusceptibility, IonizationRate, LorentzSusceptibility,
                         Material, Plasma, PowerLawRate, susceptibility)
@@ -19,6 +20,7 @@ solve_ = solve   # Julia's solve! spelling is not a Python identifier
 __all__ = [
     "C0", "EPS0", "MU0", "QE", "ME", "HBAR",
     "Grid", "Grid1D", "Grid2D", "Grid3D",
+    "Shape", "Ball", "Box", "Ellipsoid", "Cylinder", "HalfSpace", "Everywhere",
     "Material", "Plasma", "DebyeSusceptibility", "DrudeSusceptibility", "LorentzSusceptibility",
     "PowerLawRate", "IonizationRate", "susceptibility",
     "CPML", "SoftSource", "HardSource", "TFSFSource", "SeparableWaveform",

@@ -51,6 +51,10 @@ class Monitor(C.Structure):
                 ("cells", C.POINTER(C.c_int64)), ("nw", C.c_int32), ("phasor", _dp)]
 
 
+class Shape(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("material", C.c_int32), ("p", C.c_double * 8)]
+
+
 class Desc(C.Structure):
     _fields_ = [("abi_version", C.c_int32), ("ndim", C.c_int32), ("dtype", C.c_int32),
                 ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
@@ -65,7 +69,8 @@ class Desc(C.Structure):
                 ("tfsf", Tfsf),
                 ("nmon", C.c_int32), ("mons", C.POINTER(Monitor)),
                 ("tfsf_record", C.c_int32), ("rec_i1", C.c_int32 * 3), ("rec_i2", C.c_int32 * 3),
-                ("device", C.c_int32), ("mode", C.c_int32)]
+                ("device", C.c_int32), ("mode", C.c_int32),
+                ("nshape", C.c_int32), ("shapes", C.POINTER(Shape)), ("coords", _dp * 3)]
 
 
 def dptr(a):
@@ -123,6 +128,7 @@ class Library:
         self.destroy = fn("destroy", None, [vp])
         self.run = fn("run", C.c_int, [vp, C.c_int64, C.c_int64])
         self.read_field = fn("read_field", C.c_int, [vp, C.c_int32, vp])
+        self.read_geometry = fn("read_geometry", C.c_int, [vp, vp])
         self.write_field = fn("write_field", C.c_int, [vp, C.c_int32, vp])
         self.read_integral = fn("read_integral", C.c_int, [vp, C.c_int32, vp])
         self.read_monitor = fn("read_monitor", C.c_int, [vp, C.c_int32, C.c_int32, vp])
@@ -233,6 +239,12 @@ class Stepper:
     def read_field(self, comp, out=None):
         out = self._dest(out, self.N, self.dtype)
         self._check(self.lib.read_field(self.h, int(comp), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def read_geometry(self):
+        """The material index map the library holds (nx*ny*nz bytes, x fastest)."""
+        out = np.empty(self.N, dtype=np.uint8)
+        self._check(self.lib.read_geometry(self.h, out.ctypes.data_as(C.c_void_p)))
         return out
 
     def write_field(self, comp, values):

@@ -30,6 +30,7 @@
 #include "yee3d_async.cuh"
 #include "yee3d_split.cuh"
 #include "batch.cuh"
+#include "geometry.cuh"
 
 namespace mfd {
 
@@ -56,6 +57,7 @@ struct HandleBase {
     virtual ~HandleBase() = default;
     virtual int run(int64_t a, int64_t b) = 0;
     virtual int read_field(int comp, void* dst) = 0;
+    virtual int read_geometry(uint8_t* dst) = 0;
     virtual int write_field(int comp, const void* src) = 0;
     virtual int read_integral(int which, void* dst) = 0;
     virtual int read_integral_noalloc(int which, void* dst) = 0;
@@ -473,6 +475,42 @@ class Engine : public HandleBase {
         return c == MFD_HY || c == MFD_DX || c == MFD_EX;
     }
 
+    // The material map built on the device from the descriptor's shapes (geometry.cuh), and
+    // each material's bounding box read back for the compact state.  geom stays allocated
+    // only when some cell holds a material.
+    void device_geometry(const mfd_desc* d, std::vector<int>& bx0, std::vector<int>& bx1, std::vector<int>& by0,
+                         std::vector<int>& by1, std::vector<int>& bz0, std::vector<int>& bz1) {
+        if (d->geometry) throw Error(MFD_ERR_INVALID, "give either a geometry array or shapes, not both");
+        if (!d->shapes || !d->coords[2] || (ndim >= 2 && !d->coords[0]) || (ndim == 3 && !d->coords[1]))
+            throw Error(MFD_ERR_INVALID, "shapes need the shape list and the grid coordinates");
+        for (int i = 0; i < d->nshape; ++i) {
+            const mfd_shape& sh = d->shapes[i];
+            if (sh.kind < MFD_SHAPE_BALL || sh.kind > MFD_SHAPE_ALL) throw Error(MFD_ERR_INVALID, "unknown shape kind");
+            if (sh.material < 1 || sh.material > nmat) throw Error(MFD_ERR_INVALID, "shape material beyond nmat");
+        }
+        mfd_shape* ds = upload(d->shapes, (size_t)d->nshape);
+        const double* xs = ndim >= 2 ? upload(d->coords[0], (size_t)nx) : nullptr;
+        const double* ys = ndim == 3 ? upload(d->coords[1], (size_t)ny) : nullptr;
+        const double* zs = upload(d->coords[2], (size_t)nz);
+        geom = dalloc<uint8_t>((size_t)Np, false);
+        std::vector<int> box(6 * (size_t)nmat);
+        for (int g = 0; g < nmat; ++g)
+            for (int k = 0; k < 6; ++k) box[6 * g + k] = (k % 2) ? -1 : INT32_MAX;
+        int* dbox = upload(box.data(), box.size());
+        const dim3 grd((nx + 255) / 256, ny, nz);
+        geometry_kernel<<<grd, 256, 0, st>>>(geom, layout(), ds, d->nshape, xs, ys, zs);
+        MFD_CK(cudaGetLastError());
+        geometry_box_kernel<<<grd, 256, 0, st>>>(geom, layout(), dbox);
+        MFD_CK(cudaGetLastError());
+        MFD_CK(cudaMemcpyAsync(box.data(), dbox, box.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+        MFD_CK(cudaStreamSynchronize(st));
+        for (int g = 1; g <= nmat; ++g) {
+            const int* b = box.data() + 6 * (g - 1);
+            bx0[g] = b[0]; bx1[g] = b[1]; by0[g] = b[2]; by1[g] = b[3]; bz0[g] = b[4]; bz1[g] = b[5];
+            if (b[1] >= 0) any_geom = true;
+        }
+    }
+
     // ---------------------------------------------------------------------------------
     void init(const mfd_desc* d) {
         dev = d->device;
@@ -552,6 +590,10 @@ class Engine : public HandleBase {
                 }
             });
             if (bad) throw Error(MFD_ERR_INVALID, "geometry index beyond nmat");
+        } else if (d->nshape > 0) {
+            device_geometry(d, bx0, bx1, by0, by1, bz0, bz1);
+        }
+        if (d->geometry || d->nshape > 0) {
             for (int g = 1; g <= nmat; ++g) {
                 if (bx1[g] < 0) continue;
                 const bool first = mbox[1] < mbox[0];
@@ -561,7 +603,7 @@ class Engine : public HandleBase {
             }
         }
         if (any_geom) {
-            geom = upload(gpad.data(), gpad.size());
+            if (!geom) geom = upload(gpad.data(), gpad.size());
             E2 = dalloc<T>(Np);
         }
         const int nc = ndim;   // field components per vector quantity
@@ -1519,6 +1561,12 @@ class Engine : public HandleBase {
         bounded_sync(st);
     }
 
+    int read_geometry(uint8_t* dst) override {
+        if (geom) copy_out(geom, dst, 1);
+        else std::memset(dst, 0, (size_t)N);
+        return MFD_OK;
+    }
+
     int read_field(int comp, void* dst) override {
         if (comp < 0 || comp > 8 || !F[comp]) { err = "bad component"; return MFD_ERR_INVALID; }
         copy_out(F[comp], dst, sizeof(T));
@@ -2286,6 +2334,10 @@ const char* mfd_batch_last_error(const mfd_batch* b) { return b ? b->err.c_str()
 int mfd_read_field(mfd_handle* h, int32_t comp, void* dst) {
     MFD_NEED_BUF(h, dst);
     MFD_GUARD(h, h->impl->read_field(comp, dst));
+}
+int mfd_read_geometry(mfd_handle* h, uint8_t* dst) {
+    MFD_NEED_BUF(h, dst);
+    MFD_GUARD(h, h->impl->read_geometry(dst));
 }
 int mfd_write_field(mfd_handle* h, int32_t comp, const void* src) {
     MFD_NEED_BUF(h, src);

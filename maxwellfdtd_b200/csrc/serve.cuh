@@ -42,12 +42,19 @@ static int64_t desc_footprint(const mfd_desc* d) {
     std::vector<int> x0(nmat + 1, INT32_MAX), x1(nmat + 1, -1), y0(nmat + 1, INT32_MAX), y1(nmat + 1, -1),
         z0(nmat + 1, INT32_MAX), z1(nmat + 1, -1);
     bool any = false;
-    if (d->geometry) {
+    if (d->geometry || (d->nshape > 0 && d->shapes && d->coords[2])) {
         for (int iz = 0; iz < d->nz; ++iz)
             for (int iy = 0; iy < d->ny; ++iy) {
-                const uint8_t* row = d->geometry + (size_t)d->nx * (iy + (size_t)d->ny * iz);
+                const uint8_t* row = d->geometry ? d->geometry + (size_t)d->nx * (iy + (size_t)d->ny * iz) : nullptr;
                 for (int ix = 0; ix < d->nx; ++ix) {
-                    const int g = row[ix];
+                    int g = 0;
+                    if (row) g = row[ix];
+                    else {   // the shapes, as the device evaluates them (geometry.cuh)
+                        const double x = nd >= 2 && d->coords[0] ? d->coords[0][ix] : 0.0;
+                        const double y = nd == 3 && d->coords[1] ? d->coords[1][iy] : 0.0;
+                        for (int k = 0; k < d->nshape; ++k)
+                            if (shape_covers(d->shapes[k], x, y, d->coords[2][iz])) g = d->shapes[k].material;
+                    }
                     if (!g || g > nmat) continue;
                     any = true;
                     x0[g] = std::min(x0[g], ix); x1[g] = std::max(x1[g], ix);

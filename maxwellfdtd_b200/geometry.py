@@ -88,3 +88,142 @@ def cell_coords(grid, cells, coords=None):
     iy = (cells // grid.Nx) % grid.Ny
     iz = cells // (grid.Nx * grid.Ny)
     return (np.asarray(cs[0])[ix], np.asarray(cs[1])[iy], np.asarray(cs[2])[iz])
+
+
+# ------------------------------------------------------------------------------------------
+# Analytic shapes: geometries the library evaluates on the device (mfd_shape,
+# include/maxwellfdtd.h).  Each is also a geometry function like the reference's closures:
+# called with the grid coordinates it evaluates the same double-precision expression, in the
+# same order, as the device does, so the map is the same whichever side builds it.  A 2-D
+# grid's coordinates are (x, z) and a 1-D grid's z: the missing ones are 0, and a shape's
+# points and vectors are given in the grid's own coordinates (2-D: (x, z); 1-D: (z,)).
+# ------------------------------------------------------------------------------------------
+def _to3(v, ndim):
+    v = [float(a) for a in np.atleast_1d(v)]
+    if len(v) == 3:
+        return v
+    if ndim == 2 and len(v) == 2:
+        return [v[0], 0.0, v[1]]
+    if ndim == 1 and len(v) == 1:
+        return [0.0, 0.0, v[0]]
+    raise ValueError("a shape's points and vectors need one value per grid dimension")
+
+
+def _xyz(cs):
+    z0 = np.zeros(1)
+    if len(cs) == 3:
+        return cs
+    if len(cs) == 2:
+        return cs[0], z0, cs[1]
+    return z0, z0, cs[0]
+
+
+class Shape:
+    kind = 0
+
+    def params(self, ndim):
+        raise NotImplementedError
+
+    def __call__(self, *cs):
+        x, y, z = _xyz([np.asarray(c, dtype=np.float64) for c in cs])
+        return self._covers(self.params(len(cs)), x, y, z)
+
+
+class Ball(Shape):
+    """((x-cx)^2 + (y-cy)^2) + (z-cz)^2 <= r^2."""
+    kind = 1
+
+    def __init__(self, center, radius):
+        self.center, self.radius = center, float(radius)
+
+    def params(self, ndim):
+        return _to3(self.center, ndim) + [self.radius]
+
+    @staticmethod
+    def _covers(p, x, y, z):
+        a, b, c = x - p[0], y - p[1], z - p[2]
+        return (a * a + b * b) + c * c <= p[3] * p[3]
+
+
+class Box(Shape):
+    """lo <= (x, y, z) <= hi on every axis."""
+    kind = 2
+
+    def __init__(self, lo, hi):
+        self.lo, self.hi = lo, hi
+
+    def params(self, ndim):
+        lo, hi = _to3(self.lo, ndim), _to3(self.hi, ndim)
+        if ndim < 3:   # the missing axes are 0: the box spans them
+            for k in ((1,) if ndim == 2 else (0, 1)):
+                lo[k], hi[k] = -np.inf, np.inf
+        return [lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]]
+
+    @staticmethod
+    def _covers(p, x, y, z):
+        return (p[0] <= x) & (x <= p[1]) & (p[2] <= y) & (y <= p[3]) & (p[4] <= z) & (z <= p[5])
+
+
+class Ellipsoid(Shape):
+    """(((x-cx)/ax)^2 + ((y-cy)/ay)^2) + ((z-cz)/az)^2 <= 1."""
+    kind = 3
+
+    def __init__(self, center, semiaxes):
+        self.center, self.semiaxes = center, semiaxes
+
+    def params(self, ndim):
+        ax = _to3(self.semiaxes, ndim)
+        if ndim < 3:
+            ax = [a if a != 0.0 else 1.0 for a in ax]   # a missing axis (coordinate 0, centre 0) adds 0
+        return _to3(self.center, ndim) + ax
+
+    @staticmethod
+    def _covers(p, x, y, z):
+        a, b, c = (x - p[0]) / p[3], (y - p[1]) / p[4], (z - p[2]) / p[5]
+        return (a * a + b * b) + c * c <= 1.0
+
+
+class Cylinder(Shape):
+    """A circular cylinder along z: (x-cx)^2 + (y-cy)^2 <= r^2 and z0 <= z <= z1 (3-D)."""
+    kind = 4
+
+    def __init__(self, center_xy, radius, z0, z1):
+        self.center_xy, self.radius, self.z0, self.z1 = center_xy, float(radius), float(z0), float(z1)
+
+    def params(self, ndim):
+        if ndim != 3:
+            raise ValueError("Cylinder is a 3-D shape")
+        cx, cy = (float(v) for v in self.center_xy)
+        return [cx, cy, self.radius, self.z0, self.z1]
+
+    @staticmethod
+    def _covers(p, x, y, z):
+        a, b = x - p[0], y - p[1]
+        return (a * a + b * b <= p[2] * p[2]) & (p[3] <= z) & (z <= p[4])
+
+
+class HalfSpace(Shape):
+    """(nx x + ny y) + nz z >= d."""
+    kind = 5
+
+    def __init__(self, normal, d):
+        self.normal, self.d = normal, float(d)
+
+    def params(self, ndim):
+        return _to3(self.normal, ndim) + [self.d]
+
+    @staticmethod
+    def _covers(p, x, y, z):
+        return (p[0] * x + p[1] * y) + p[2] * z >= p[3]
+
+
+class Everywhere(Shape):
+    """Every cell (a whole-domain material)."""
+    kind = 6
+
+    def params(self, ndim):
+        return []
+
+    @staticmethod
+    def _covers(p, x, y, z):
+        return np.ones(np.broadcast_shapes(np.shape(x), np.shape(y), np.shape(z)), dtype=bool)

@@ -14,7 +14,7 @@ import numpy as np
 
 from . import _abi
 from .constants import C0
-from .geometry import geometry2bool
+from .geometry import Shape, geometry2bool
 from .grids import adapt_range
 from .materials import IonizationRate, Material, PowerLawRate, material_struct
 from .monitors import FieldMonitor, SpectralMonitor, monitor_struct
@@ -108,13 +108,30 @@ class Model:
         mats = [] if material is None else (list(material) if isinstance(material, (list, tuple)) else [material])
         if len(mats) > 255:
             raise ValueError("at most 255 materials")
-        geom = np.zeros(grid.shape, dtype=np.uint8)
-        for imat, m in enumerate(mats, start=1):
-            geom[geometry2bool(m.geometry, grid)] = imat   # later materials win (models.jl:91-98)
-        self.geometry = geom
+        self._mat_geometries = [m.geometry for m in mats]
+        self._geometry = None
         self.materials = [material_struct(m, self.dt) for m in mats]
         self.Mh, self.Me, self.Md1, self.Md2 = self.dt / 1.25663706212e-6, 1 / 8.8541878128e-12, 1.0, self.dt
         self.isplasma = any(m.isplasma for m in self.materials)
+
+    @property
+    def geometry(self):
+        """The material index map (models.jl:85-98: later materials win), evaluated on the
+        host when first asked for.  A model whose materials are all analytic shapes
+        (geometry.Shape) does not need it: its descriptor passes the shapes and the library
+        builds the map on the device."""
+        if self._geometry is None:
+            geom = np.zeros(self.grid.shape, dtype=np.uint8)
+            for imat, g in enumerate(self._mat_geometries, start=1):
+                geom[geometry2bool(g, self.grid)] = imat
+            self._geometry = geom
+        return self._geometry
+
+    def shapes(self):
+        """[(material index, Shape)] when every material's geometry is a Shape, else None."""
+        if self._mat_geometries and all(isinstance(g, Shape) for g in self._mat_geometries):
+            return [(i, g) for i, g in enumerate(self._mat_geometries, start=1)]
+        return None
 
     # ------------------------------------------------------------------------------------
     def coords(self, dtype):
@@ -125,12 +142,15 @@ class Model:
             return (adapt_range(g.x, dtype), adapt_range(g.z, dtype))
         return (adapt_range(g.x, dtype), adapt_range(g.y, dtype), adapt_range(g.z, dtype))
 
-    def build_desc(self, dtype, monitors=(), tfsf_box=None, rho_fp64=True, device=0, host_alloc=None, mode="exact"):
+    def build_desc(self, dtype, monitors=(), tfsf_box=None, rho_fp64=True, device=0, host_alloc=None, mode="exact",
+                   device_geometry=None):
         """C descriptor for this model in element type ``dtype`` plus host-side metadata.
         ``host_alloc(n, dtype)`` provides the storage of the large input arrays (e.g.
         page-locked memory).  ``mode`` is the arithmetic of the field updates: "exact" (the
         reference's operation order, bit for bit) or "fast" (the tolerance mode,
-        MFD_MODE_FAST in include/maxwellfdtd.h)."""
+        MFD_MODE_FAST in include/maxwellfdtd.h).  ``device_geometry``: None passes the
+        materials' shapes for the device to evaluate when every geometry is a Shape (else
+        the host map), True requires that, False always passes the host map."""
         if mode not in ("exact", "fast"):
             raise ValueError("mode must be 'exact' or 'fast'")
         dtype = np.dtype(dtype)
@@ -154,8 +174,26 @@ class Model:
                 d.pml[f].A = _abi.dptr(b.arr(L.A, np.float64))
                 d.pml[f].B = _abi.dptr(b.arr(L.B, np.float64))
         d.Mh0, d.Me0, d.Md10, d.Md20 = self.Mh, self.Me, self.Md1, self.Md2
-        geo = b.arr(self.geometry.ravel(order="F"), np.uint8)
-        d.geometry = geo.ctypes.data_as(_abi.C.POINTER(_abi.C.c_uint8))
+        shapes = self.shapes() if device_geometry is not False else None
+        if device_geometry and shapes is None:
+            raise ValueError("device_geometry needs every material's geometry to be a Shape")
+        if shapes:   # the library builds the map on the device
+            sarr = (_abi.Shape * len(shapes))()
+            b.keep.append(sarr)
+            for k, (imat, shp) in enumerate(shapes):
+                sarr[k].kind = shp.kind
+                sarr[k].material = imat
+                for j, v in enumerate(shp.params(g.ndim)):
+                    sarr[k].p[j] = v
+            d.nshape = len(shapes)
+            d.shapes = sarr
+            axes = (g.x, g.y, g.z) if g.ndim == 3 else (g.x, None, g.z) if g.ndim == 2 else (None, None, g.z)
+            for k, c in enumerate(axes):
+                if c is not None:
+                    d.coords[k] = _abi.dptr(b.arr(np.asarray(c, dtype=np.float64), np.float64))
+        else:
+            geo = b.arr(self.geometry.ravel(order="F"), np.uint8)
+            d.geometry = geo.ctypes.data_as(_abi.C.POINTER(_abi.C.c_uint8))
         nm = len(self.materials)
         d.nmat = nm
         if nm:

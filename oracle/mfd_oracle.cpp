@@ -44,6 +44,7 @@ struct OracleBase {
     virtual ~OracleBase() = default;
     virtual int run(int64_t a, int64_t b) = 0;
     virtual int read_field(int comp, void* dst) = 0;
+    virtual int read_geometry(uint8_t* dst) = 0;
     virtual int write_field(int comp, const void* src) = 0;
     virtual int read_integral(int which, void* dst) = 0;
     virtual int read_monitor(int m, int comp, void* dst) = 0;
@@ -71,6 +72,31 @@ T ionization_rate(const T* X, const T* Y, size_t n, T x) {
     T dydx = (Y[i + 1] - Y[i]) / (X[i + 1] - X[i]);
     T yl = Y[i] + dydx * (xi - X[i]);
     return std::pow((T)10, yl);
+}
+
+// An analytic shape covers (x, y, z): the header's double-precision test for its kind,
+// left to right (the host restatement of the geometry closures of util.jl:1-31 for the
+// shapes include/maxwellfdtd.h defines).
+bool shape_covers(const mfd_shape& s, double x, double y, double z) {
+    const double* p = s.p;
+    switch (s.kind) {
+        case MFD_SHAPE_BALL: {
+            const double a = x - p[0], b = y - p[1], c = z - p[2];
+            return (a * a + b * b) + c * c <= p[3] * p[3];
+        }
+        case MFD_SHAPE_BOX: return p[0] <= x && x <= p[1] && p[2] <= y && y <= p[3] && p[4] <= z && z <= p[5];
+        case MFD_SHAPE_ELLIPSOID: {
+            const double a = (x - p[0]) / p[3], b = (y - p[1]) / p[4], c = (z - p[2]) / p[5];
+            return (a * a + b * b) + c * c <= 1.0;
+        }
+        case MFD_SHAPE_CYLINDER: {
+            const double a = x - p[0], b = y - p[1];
+            return a * a + b * b <= p[2] * p[2] && p[3] <= z && z <= p[4];
+        }
+        case MFD_SHAPE_HALFSPACE: return (p[0] * x + p[1] * y) + p[2] * z >= p[3];
+        case MFD_SHAPE_ALL: return true;
+        default: return false;
+    }
 }
 
 // Layer profile (src/pml.jl:46-52).  0-based: a left layer covers cells [0, ib-1] with pml
@@ -176,6 +202,19 @@ struct Oracle : OracleBase {
                 if (geometry[i] > d->nmat) { err = "geometry index beyond nmat"; return MFD_ERR_INVALID; }
                 if (geometry[i] > 0) isgeometry = true;
             }
+        else if (d->nshape > 0) {   // the material map from analytic shapes (the reference's geometry2bool, util.jl:1-31)
+            for (int iz = 0; iz < nz; ++iz)
+                for (int iy = 0; iy < ny; ++iy)
+                    for (int ix = 0; ix < nx; ++ix) {
+                        const double x = ndim >= 2 ? d->coords[0][ix] : 0.0, y = ndim == 3 ? d->coords[1][iy] : 0.0;
+                        const double z = d->coords[2][iz];
+                        int g = 0;
+                        for (int k = 0; k < d->nshape; ++k)
+                            if (shape_covers(d->shapes[k], x, y, z)) g = d->shapes[k].material;
+                        geometry[id(ix, iy, iz)] = g;
+                        if (g > 0) isgeometry = true;
+                    }
+        }
         for (int m = 0; m < d->nmat; ++m) {
             const mfd_material& s = d->mats[m];
             Mat<T, R> M;
@@ -1137,6 +1176,11 @@ struct Oracle : OracleBase {
         return MFD_OK;
     }
 
+    int read_geometry(uint8_t* dst) override {
+        for (size_t i = 0; i < N; ++i) dst[i] = (uint8_t)geometry[i];
+        return MFD_OK;
+    }
+
     int read_field(int comp, void* dst) override {
         if (comp < 0 || comp > 8 || !has_comp(comp)) { err = "bad component"; return MFD_ERR_INVALID; }
         std::memcpy(dst, F[comp].data(), N * sizeof(T));
@@ -1257,6 +1301,7 @@ int oracle_create(const mfd_desc* d, void** out) {
 void oracle_destroy(void* h) { delete (OracleBase*)h; }
 int oracle_run(void* h, int64_t a, int64_t b) { return ((OracleBase*)h)->run(a, b); }
 int oracle_read_field(void* h, int32_t comp, void* dst) { return ((OracleBase*)h)->read_field(comp, dst); }
+int oracle_read_geometry(void* h, uint8_t* dst) { return ((OracleBase*)h)->read_geometry(dst); }
 int oracle_write_field(void* h, int32_t comp, const void* src) { return ((OracleBase*)h)->write_field(comp, src); }
 int oracle_read_integral(void* h, int32_t which, void* dst) { return ((OracleBase*)h)->read_integral(which, dst); }
 int oracle_read_monitor(void* h, int32_t m, int32_t comp, void* dst) { return ((OracleBase*)h)->read_monitor(m, comp, dst); }

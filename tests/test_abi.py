@@ -63,7 +63,9 @@ int main(void) {
   F(mfd_desc, dt) F(mfd_desc, nt) F(mfd_desc, bc) F(mfd_desc, pml) F(mfd_desc, Mh0) F(mfd_desc, geometry)
   F(mfd_desc, nmat) F(mfd_desc, mats) F(mfd_desc, rho_fp64) F(mfd_desc, nsrc) F(mfd_desc, srcs)
   F(mfd_desc, tfsf) F(mfd_desc, nmon) F(mfd_desc, mons) F(mfd_desc, tfsf_record) F(mfd_desc, rec_i1)
-  F(mfd_desc, rec_i2) F(mfd_desc, device)
+  F(mfd_desc, rec_i2) F(mfd_desc, device) F(mfd_desc, mode) F(mfd_desc, nshape) F(mfd_desc, shapes) F(mfd_desc, coords)
+  printf("mfd_shape %zu\n", sizeof(mfd_shape));
+  F(mfd_shape, material) F(mfd_shape, p) F(mfd_tfsf, shape)
   F(mfd_material, nq) F(mfd_material, Aq) F(mfd_material, kerr) F(mfd_material, plasma) F(mfd_material, Rava)
   F(mfd_material, rate_kind) F(mfd_material, rate_order) F(mfd_material, rate_n) F(mfd_material, rate_y)
   F(mfd_source, coeff) F(mfd_source, npts) F(mfd_source, cells) F(mfd_source, gt)
@@ -85,7 +87,7 @@ int main(void) {
 def test_ctypes_layout_matches_c():
     lay = _c_layout()
     types = {"mfd_pml_layer": _abi.PmlLayer, "mfd_material": _abi.Material, "mfd_source": _abi.Source,
-             "mfd_tfsf": _abi.Tfsf, "mfd_monitor": _abi.Monitor, "mfd_desc": _abi.Desc}
+             "mfd_tfsf": _abi.Tfsf, "mfd_monitor": _abi.Monitor, "mfd_desc": _abi.Desc, "mfd_shape": _abi.Shape}
     for k, v in lay.items():
         if "." in k:
             s, m = k.split(".")
@@ -222,7 +224,7 @@ def test_julia_shim_mirrors_header():
         c = f.read()
     with open(os.path.join(ROOT, "julia", "MaxwellFDTDB200.jl")) as f:
         jl = f.read()
-    for cname, jname in (("mfd_pml_layer", "MfdPmlLayer"), ("mfd_material", "MfdMaterial"), ("mfd_source", "MfdSource"),
+    for cname, jname in (("mfd_shape", "MfdShape"), ("mfd_pml_layer", "MfdPmlLayer"), ("mfd_material", "MfdMaterial"), ("mfd_source", "MfdSource"),
                          ("mfd_tfsf", "MfdTFSF"), ("mfd_monitor", "MfdMonitor"), ("mfd_desc", "MfdDesc")):
         assert _c_fields(c, cname) == _julia_fields(jl, jname), cname
     for fn in declared_functions():
