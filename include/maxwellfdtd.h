@@ -93,6 +93,15 @@ enum {
     MFD_EX = 6, MFD_EY = 7, MFD_EZ = 8
 };
 
+/* ---- the 2-D field set (mfd_desc.polarization; ignored by 1-D and 3-D models) --------
+ * MFD_POL_HY: Hy, Dx, Dz, Ex, Ez -- the reference's Field2D (src/fields.jl:36-55).
+ * MFD_POL_EY: Hx, Hz, Dy, Ey -- the other polarisation of an x-z model, which the
+ *   reference does not have.  Its updates are the reference's 3-D updates
+ *   (src/models.jl:735-1162) with every y derivative zero, in the same operation order, so
+ *   a run equals the Hx, Hz, Dy, Ey of a 3-D run with ny = 1 and periodic y bit for bit;
+ *   Sa is that run's Poynting norm and the NaN/Inf guard reads Ey (there is no Ex). */
+enum { MFD_POL_HY = 0, MFD_POL_EY = 1 };
+
 /* ---- integral outputs (reference Output.Sa/E2, model.JE, rho_end: outputs.jl:46-65) -- */
 enum { MFD_INT_SA = 0, MFD_INT_E2 = 1, MFD_INT_JE = 2, MFD_INT_RHO = 3 };
 
@@ -119,6 +128,9 @@ enum {
  *   incEz;  face x2z: same;  face xy1: incHx, incHy, incEx, incEy;  face xy2: same.
  * 2-D: the 8 arrays of TFSFSource2D (sources.jl:390-403):
  *   1z: incHy, incEz; 2z: incHy, incEz; x1: incHy, incEx; x2: incHy, incEx.
+ * 2-D, MFD_POL_EY: 1z: incHz, incEy; 2z: incHz, incEy; x1: incHx, incEy; x2: incHx, incEy,
+ *   each over the face's Nzi + 1 (x faces) or Nxi + 1 (z faces) nodes, as the 3-D faces
+ *   1yz / 2yz / xy1 / xy2 hold Hz, Ey and Hx, Ey.
  * 1-D: the 4 arrays of TFSFSource1D (sources.jl:272-279): incHy_1, incEx_1, incHy_2, incEx_2.
  * Each array is [nt][face extent] in T, the face extent laid out as in the reference
  * (column-major (a, b, Nt) => C order [nt][b][a]).
@@ -255,6 +267,7 @@ typedef struct mfd_desc {
     int32_t nshape;          /* shapes evaluated on the device (geometry must be NULL) */
     const mfd_shape* shapes;
     const double* coords[3]; /* grid coordinates x[nx], y[ny], z[nz] (for the shapes)  */
+    int32_t polarization;    /* 2-D field set: MFD_POL_HY (0) or MFD_POL_EY            */
 } mfd_desc;
 
 typedef struct mfd_handle mfd_handle;

@@ -19,6 +19,7 @@ const MFD_ABI_VERSION = 2
 const MFD_OK, MFD_ERR_INVALID, MFD_ERR_OOM, MFD_ERR_CUDA, MFD_ERR_NONFINITE = 0, 1, 2, 3, 4
 const MFD_F32, MFD_F64 = 0, 1
 const MFD_MODE_EXACT, MFD_MODE_FAST = 0, 1
+const MFD_POL_HY, MFD_POL_EY = 0, 1
 const MFD_SRC_SOFT, MFD_SRC_HARD = 0, 1
 const MFD_MON_FIELD, MFD_MON_SPECTRAL = 0, 1
 const MFD_RATE_NONE, MFD_RATE_POWER, MFD_RATE_TABLE = 0, 1, 2
@@ -65,7 +66,7 @@ struct MfdDesc
     geometry::Ptr{UInt8}; nmat::Int32; mats::Ptr{MfdMaterial}; rho_fp64::Int32
     nsrc::Int32; srcs::Ptr{MfdSource}; tfsf::MfdTFSF; nmon::Int32; mons::Ptr{MfdMonitor}
     tfsf_record::Int32; rec_i1::NTuple{3,Int32}; rec_i2::NTuple{3,Int32}; device::Int32; mode::Int32
-    nshape::Int32; shapes::Ptr{MfdShape}; coords::NTuple{3,Ptr{Cdouble}}
+    nshape::Int32; shapes::Ptr{MfdShape}; coords::NTuple{3,Ptr{Cdouble}}; polarization::Int32
 end
 
 # ---- descriptor from a reference Model ------------------------------------------------------
@@ -178,7 +179,8 @@ function build_desc(model, ::Type{T}, monitors; mode=MFD_MODE_EXACT, device=0, i
                 Tuple(Int32.(bc6)), lay, Mh, Me, Md1, Md2, _ptr(keep, UInt8.(geometry)), length(mats),
                 isempty(mats) ? C_NULL : _ptr(keep, mats), 1, length(srcs), isempty(srcs) ? C_NULL : _ptr(keep, srcs),
                 tfsf, length(mons), isempty(mons) ? C_NULL : _ptr(keep, mons), 0, (0, 0, 0), (0, 0, 0), device, mode,
-                0, C_NULL, (C_NULL, C_NULL, C_NULL))   # closures: the host map above, no device shapes
+                0, C_NULL, (C_NULL, C_NULL, C_NULL),   # closures: the host map above, no device shapes
+                MFD_POL_HY)                          # the reference's Field2D (fields.jl:36-55)
     return d, keep
 end
 

@@ -11,6 +11,7 @@ MFD_OK, MFD_ERR_INVALID, MFD_ERR_OOM, MFD_ERR_CUDA, MFD_ERR_NONFINITE, MFD_ERR_T
     MFD_ERR_ADMISSION, MFD_ERR_NODEVICE = range(8)
 MFD_F32, MFD_F64 = 0, 1
 MFD_MODE_EXACT, MFD_MODE_FAST = 0, 1
+MFD_POL_HY, MFD_POL_EY = 0, 1
 MFD_INC_FULL, MFD_INC_ALONG_B, MFD_INC_ALONG_A, MFD_INC_UNIFORM = range(4)
 MFD_REQ_QUEUED, MFD_REQ_ADMITTED, MFD_REQ_RUNNING, MFD_REQ_DONE, MFD_REQ_FAILED = range(5)
 MFD_INT_SA, MFD_INT_E2, MFD_INT_JE, MFD_INT_RHO = range(4)
@@ -70,7 +71,8 @@ class Desc(C.Structure):
                 ("nmon", C.c_int32), ("mons", C.POINTER(Monitor)),
                 ("tfsf_record", C.c_int32), ("rec_i1", C.c_int32 * 3), ("rec_i2", C.c_int32 * 3),
                 ("device", C.c_int32), ("mode", C.c_int32),
-                ("nshape", C.c_int32), ("shapes", C.POINTER(Shape)), ("coords", _dp * 3)]
+                ("nshape", C.c_int32), ("shapes", C.POINTER(Shape)), ("coords", _dp * 3),
+                ("polarization", C.c_int32)]
 
 
 def dptr(a):

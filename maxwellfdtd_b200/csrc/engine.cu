@@ -308,6 +308,7 @@ template <typename T, typename R>
 class Engine : public HandleBase {
    public:
     int ndim = 0, nx = 0, ny = 0, nz = 0, px = 0, dev = 0;
+    bool ey2 = false;           // the second 2-D field set (Hx, Hz, Dy, Ey: MFD_POL_EY)
     long long sz = 0, Np = 0, N = 0;
     int64_t nt = 0;
     T dx{}, dy{}, dz{}, dt{};
@@ -471,9 +472,13 @@ class Engine : public HandleBase {
 
     bool has_comp(int c) const {
         if (ndim == 3) return true;
+        if (ey2) return c == MFD_HX || c == MFD_HZ || c == MFD_DY || c == MFD_EY;
         if (ndim == 2) return c == MFD_HY || c == MFD_DX || c == MFD_DZ || c == MFD_EX || c == MFD_EZ;
         return c == MFD_HY || c == MFD_DX || c == MFD_EX;
     }
+    // The component the NaN/Inf guard reads: Ex (models.jl:202-209), Ey in the second 2-D
+    // field set, which has no Ex.
+    int guard_comp() const { return ey2 ? MFD_EY : MFD_EX; }
 
     // The material map built on the device from the descriptor's shapes (geometry.cuh), and
     // each material's bounding box read back for the compact state.  geom stays allocated
@@ -520,6 +525,7 @@ class Engine : public HandleBase {
         MFD_CK(cudaEventCreate(&run_ev[0]));
         MFD_CK(cudaEventCreate(&run_ev[1]));
         ndim = d->ndim; nx = d->nx; ny = d->ny; nz = d->nz;
+        ey2 = ndim == 2 && d->polarization == MFD_POL_EY;
         px = ndim == 1 ? 1 : (int)round_up(nx, 32);
         sz = (long long)px * ny;
         Np = sz * nz;
@@ -826,6 +832,24 @@ class Engine : public HandleBase {
             add(MFD_EY, X1, X2, Y1, Y2 - 1, Z2, Z2, 20, +1, cez, 0, 0);
             add(MFD_DX, X1, X2 - 1, Y1, Y2, Z2, Z2, 21, -1, cdz, 0, 0);
             add(MFD_DY, X1, X2, Y1, Y2 - 1, Z2, Z2, 20, +1, cdz, 0, 0);
+        } else if (ey2) {
+            // the 3-D faces 1yz, 2yz, xy1, xy2 restricted to Hz, Ey / Hx, Ey (sources.jl:728-776),
+            // with the 2-D coefficients (sources.jl:478-495)
+            const double cmx = (double)dt / (MU0 * (double)dx), cex = (double)dt / (EPS0 * (double)dx);
+            const double cmz = (double)dt / (MU0 * (double)dz), cez = (double)dt / (EPS0 * (double)dz);
+            const T cdx = dt / dx, cdz = dt / dz;
+            add(MFD_HZ, X1 - 1, X1 - 1, 0, 0, Z1, Z2, 1, +1, cmx, 0, 0);
+            add(MFD_EY, X1, X1, 0, 0, Z1, Z2, 0, +1, cex, 0, 0);
+            add(MFD_DY, X1, X1, 0, 0, Z1, Z2, 0, +1, 0, 1, cdx);
+            add(MFD_HZ, X2, X2, 0, 0, Z1, Z2, 3, -1, cmx, 0, 0);
+            add(MFD_EY, X2, X2, 0, 0, Z1, Z2, 2, -1, cex, 0, 0);
+            add(MFD_DY, X2, X2, 0, 0, Z1, Z2, 2, -1, 0, 1, cdx);
+            add(MFD_HX, X1, X2, 0, 0, Z1 - 1, Z1 - 1, 5, -1, cmz, 0, 0);
+            add(MFD_EY, X1, X2, 0, 0, Z1, Z1, 4, -1, cez, 0, 0);
+            add(MFD_DY, X1, X2, 0, 0, Z1, Z1, 4, -1, 0, 1, cdz);
+            add(MFD_HX, X1, X2, 0, 0, Z2, Z2, 7, +1, cmz, 0, 0);
+            add(MFD_EY, X1, X2, 0, 0, Z2, Z2, 6, +1, cez, 0, 0);
+            add(MFD_DY, X1, X2, 0, 0, Z2, Z2, 6, +1, 0, 1, cdz);
         } else if (ndim == 2) {
             const double cmx = (double)dt / (MU0 * (double)dx), cex = (double)dt / (EPS0 * (double)dx);
             const double cmz = (double)dt / (MU0 * (double)dz), cez = (double)dt / (EPS0 * (double)dz);
@@ -938,6 +962,11 @@ class Engine : public HandleBase {
             add(MFD_EX, X1, X2 - 1, Y1, Y2, Z1, Z1); add(MFD_EY, X1, X2, Y1, Y2 - 1, Z1, Z1);
             add(MFD_HX, X1, X2, Y1, Y2 - 1, Z2, Z2); add(MFD_HY, X1, X2 - 1, Y1, Y2, Z2, Z2);
             add(MFD_EX, X1, X2 - 1, Y1, Y2, Z2, Z2); add(MFD_EY, X1, X2, Y1, Y2 - 1, Z2, Z2);
+        } else if (ey2) {
+            add(MFD_HZ, X1 - 1, X1 - 1, 0, 0, Z1, Z2); add(MFD_EY, X1, X1, 0, 0, Z1, Z2);
+            add(MFD_HZ, X2, X2, 0, 0, Z1, Z2); add(MFD_EY, X2, X2, 0, 0, Z1, Z2);
+            add(MFD_HX, X1, X2, 0, 0, Z1 - 1, Z1 - 1); add(MFD_EY, X1, X2, 0, 0, Z1, Z1);
+            add(MFD_HX, X1, X2, 0, 0, Z2, Z2); add(MFD_EY, X1, X2, 0, 0, Z2, Z2);
         } else if (ndim == 2) {
             add(MFD_HY, X1 - 1, X1 - 1, 0, 0, Z1, Z2 - 1); add(MFD_EZ, X1, X1, 0, 0, Z1, Z2 - 1);
             add(MFD_HY, X2, X2, 0, 0, Z1, Z2 - 1); add(MFD_EZ, X2, X2, 0, 0, Z1, Z2 - 1);
@@ -970,9 +999,10 @@ class Engine : public HandleBase {
         if (d->nmon <= 0) return;
         static const int c3[6] = {MFD_HX, MFD_HY, MFD_HZ, MFD_EX, MFD_EY, MFD_EZ};
         static const int c2[3] = {MFD_HY, MFD_EX, MFD_EZ};
+        static const int c2e[3] = {MFD_HX, MFD_HZ, MFD_EY};
         static const int c1[2] = {MFD_HY, MFD_EX};
         ncomp_mon = ndim == 3 ? 6 : ndim == 2 ? 3 : 2;
-        for (int k = 0; k < ncomp_mon; ++k) mon_comps[k] = ndim == 3 ? c3[k] : ndim == 2 ? c2[k] : c1[k];
+        for (int k = 0; k < ncomp_mon; ++k) mon_comps[k] = ndim == 3 ? c3[k] : ey2 ? c2e[k] : ndim == 2 ? c2[k] : c1[k];
         long long ring_vals = 0;
         for (int m = 0; m < d->nmon; ++m) {
             const mfd_monitor& a = d->mons[m];
@@ -1099,7 +1129,8 @@ class Engine : public HandleBase {
             h3d_kernel<T, MATH, FAST><<<grd, blk, 0, st>>>(p, zc3);
         } else if (ndim == 2) {
             dim3 blk(32, 8), grd((nx + 31) / 32, (nz + 7) / 8);
-            h2d_kernel<T, MATH, FAST><<<grd, blk, 0, st>>>(p);
+            if (ey2) h2e_kernel<T, MATH, FAST><<<grd, blk, 0, st>>>(p);
+            else h2d_kernel<T, MATH, FAST><<<grd, blk, 0, st>>>(p);
         } else {
             dim3 blk(256), grd((nz + 255) / 256);
             h1d_kernel<T, MATH, FAST><<<grd, blk, 0, st>>>(p);
@@ -1262,7 +1293,8 @@ class Engine : public HandleBase {
             e3d_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p, zc3);
         } else if (ndim == 2) {
             dim3 blk(32, 8), grd((nx + 31) / 32, (nz + 7) / 8);
-            e2d_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p);
+            if (ey2) e2e_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p);
+            else e2d_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p);
         } else {
             dim3 blk(256), grd((nz + 255) / 256);
             e1d_kernel<T, R, MAT, FAST><<<grd, blk, 0, st>>>(p);
@@ -1311,11 +1343,15 @@ class Engine : public HandleBase {
             launch(KC_MAT, [&] {
                 if (m.nq <= 3 && ndim >= 2) {
                     if (ndim == 3) launch_mat_flat<3>(g, m, cur);
+                    else if (ey2) launch_mat_flat<1>(g, m, cur);
                     else launch_mat_flat<2>(g, m, cur);
                     return;
                 }
                 dim3 grd((m.bnx + 127) / 128, m.bny, m.bnz);
-                if (ndim == 3)
+                if (ey2)   // one component: Dy, Ey
+                    material_kernel<T, R, 1><<<grd, 128, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DY], nullptr, nullptr,
+                                                                  F[MFD_EY], nullptr, nullptr, cur, dt);
+                else if (ndim == 3)
                     material_kernel<T, R, 3><<<grd, 128, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], F[MFD_DY], F[MFD_DZ],
                                                                   F[MFD_EX], F[MFD_EY], F[MFD_EZ], cur, dt);
                 else if (ndim == 2)
@@ -1331,13 +1367,18 @@ class Engine : public HandleBase {
     template <int NC>
     void launch_mat_flat(int g, const MatDev<T, R>& m, int cur) {
         const unsigned blocks = (unsigned)((m.bsize + 255) / 256);
+        // NC = 3: x, y, z; 2: x, z; 1: the one component (Dy, Ey of the second 2-D field set)
+        T* D0 = NC == 1 ? F[MFD_DY] : F[MFD_DX];
+        T* E0 = NC == 1 ? F[MFD_EY] : F[MFD_EX];
         T* Dy = NC == 3 ? F[MFD_DY] : nullptr;
         T* Ey = NC == 3 ? F[MFD_EY] : nullptr;
+        T* Dz = NC == 1 ? nullptr : F[MFD_DZ];
+        T* Ez = NC == 1 ? nullptr : F[MFD_EZ];
         switch (m.nq) {
-            case 0: material_flat_kernel<T, R, NC, 0><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], Dy, F[MFD_DZ], F[MFD_EX], Ey, F[MFD_EZ], cur, dt); break;
-            case 1: material_flat_kernel<T, R, NC, 1><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], Dy, F[MFD_DZ], F[MFD_EX], Ey, F[MFD_EZ], cur, dt); break;
-            case 2: material_flat_kernel<T, R, NC, 2><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], Dy, F[MFD_DZ], F[MFD_EX], Ey, F[MFD_EZ], cur, dt); break;
-            default: material_flat_kernel<T, R, NC, 3><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), F[MFD_DX], Dy, F[MFD_DZ], F[MFD_EX], Ey, F[MFD_EZ], cur, dt); break;
+            case 0: material_flat_kernel<T, R, NC, 0><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), D0, Dy, Dz, E0, Ey, Ez, cur, dt); break;
+            case 1: material_flat_kernel<T, R, NC, 1><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), D0, Dy, Dz, E0, Ey, Ez, cur, dt); break;
+            case 2: material_flat_kernel<T, R, NC, 2><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), D0, Dy, Dz, E0, Ey, Ez, cur, dt); break;
+            default: material_flat_kernel<T, R, NC, 3><<<blocks, 256, 0, st>>>(mats_dev, g, geom, layout(), D0, Dy, Dz, E0, Ey, Ez, cur, dt); break;
         }
     }
 
@@ -1414,7 +1455,7 @@ class Engine : public HandleBase {
         HParams<T> p = hparams(1, step);
         launch(KC_SUMS, [&] {
             dim3 grd((nx + 255) / 256, ny, nz);
-            sums_kernel<T><<<grd, 256, 0, st>>>(p, ndim);
+            sums_kernel<T><<<grd, 256, 0, st>>>(p, ey2 ? FSET_EY2 : ndim);
         });
     }
 
@@ -1431,7 +1472,7 @@ class Engine : public HandleBase {
     void launch_guard(int64_t step) {
         launch(KC_SUMS, [&] {
             dim3 grd((nx + 255) / 256, ny, nz);
-            guard_kernel<T><<<grd, 256, 0, st>>>(F[MFD_EX], layout(), d_flags, step);
+            guard_kernel<T><<<grd, 256, 0, st>>>(F[guard_comp()], layout(), d_flags, step);
         });
     }
 
@@ -1704,7 +1745,7 @@ class Engine : public HandleBase {
         auto mix = [&](uint64_t v) {
             for (int i = 0; i < 8; ++i) { hsh ^= (v >> (8 * i)) & 0xff; hsh *= 1099511628211ull; }
         };
-        mix((uint64_t)ndim); mix(sizeof(T)); mix(sizeof(R)); mix((uint64_t)nx); mix((uint64_t)ny); mix((uint64_t)nz);
+        mix((uint64_t)ndim); mix((uint64_t)ey2); mix(sizeof(T)); mix(sizeof(R)); mix((uint64_t)nx); mix((uint64_t)ny); mix((uint64_t)nz);
         mix((uint64_t)nt); mix(state_bufs.size());
         for (auto& b : state_bufs) mix(b.second);
         return hsh;
@@ -1909,6 +1950,7 @@ struct mfd_batch {
         E* e = dynamic_cast<E*>(h->impl.get());
         if (!e) { err = "batch members must be single precision with double-precision plasma density (the default)"; return MFD_ERR_INVALID; }
         if (e->ndim < 2) { err = "batch members must be 2-D or 3-D models"; return MFD_ERR_INVALID; }
+        if (e->ey2) { err = "batch members use the first 2-D field set (MFD_POL_HY)"; return MFD_ERR_INVALID; }
         if (e->dev != dev) { err = "batch member on another device"; return MFD_ERR_INVALID; }
         if (e->in_batch) { err = "model already in a batch"; return MFD_ERR_INVALID; }
         if (e->record) { err = "batch members cannot record TFSF data"; return MFD_ERR_INVALID; }
@@ -2193,6 +2235,9 @@ static int validate_desc(const mfd_desc* d) {
     if (d->ndim == 2 && d->ny != 1) { g_create_error = "2-D model needs ny = 1"; return MFD_ERR_INVALID; }
     if (d->dtype != MFD_F32 && d->dtype != MFD_F64) { g_create_error = "bad dtype"; return MFD_ERR_INVALID; }
     if (d->mode != MFD_MODE_EXACT && d->mode != MFD_MODE_FAST) { g_create_error = "bad mode"; return MFD_ERR_INVALID; }
+    if (d->polarization != MFD_POL_HY && (d->ndim != 2 || d->polarization != MFD_POL_EY)) {
+        g_create_error = "polarization must be MFD_POL_HY, or MFD_POL_EY for a 2-D model"; return MFD_ERR_INVALID;
+    }
     if (d->nmat < 0 || d->nmat > 255) { g_create_error = "at most 255 materials"; return MFD_ERR_INVALID; }
     if ((long long)d->nx * d->ny * d->nz > (1ll << 34)) { g_create_error = "grid too large"; return MFD_ERR_INVALID; }
     return MFD_OK;

@@ -37,7 +37,8 @@ static int64_t desc_footprint(const mfd_desc* d) {
     const int64_t px = nd == 1 ? d->nx : (d->nx + 31) / 32 * 32;
     const int64_t Np = px * d->ny * d->nz;
     static const int ncomp[4] = {0, 3, 5, 9};
-    int64_t b = (ncomp[nd] + 1) * Np * T + d->nt * 4 + 4;
+    const bool ey2 = nd == 2 && d->polarization == MFD_POL_EY;   // Hx, Hz, Dy, Ey
+    int64_t b = ((ey2 ? 4 : ncomp[nd]) + 1) * Np * T + d->nt * 4 + 4;
     const int nmat = d->nmat;
     std::vector<int> x0(nmat + 1, INT32_MAX), x1(nmat + 1, -1), y0(nmat + 1, INT32_MAX), y1(nmat + 1, -1),
         z0(nmat + 1, INT32_MAX), z1(nmat + 1, -1);
@@ -64,7 +65,7 @@ static int64_t desc_footprint(const mfd_desc* d) {
             }
     }
     if (any) b += Np + Np * T;
-    const int nc = nd;
+    const int nc = ey2 ? 1 : nd;
     for (int g = 1; g <= nmat; ++g) {
         const mfd_material& m = d->mats[g - 1];
         b += T + 512;
@@ -101,7 +102,7 @@ static int64_t desc_footprint(const mfd_desc* d) {
         int64_t sum = 0;
         for (int k = 0; k < narr; ++k) {
             int64_t a = 1, bb = 1;
-            if (nd == 2) a = k < 4 ? Nz : Nx;
+            if (nd == 2) a = (k < 4 ? Nz : Nx) + (ey2 ? 1 : 0);   // the second field set spans the nodes
             if (nd == 3) {
                 const int face = k / 4, j = k % 4;
                 const bool p = j == 0 || j == 3;
@@ -351,7 +352,8 @@ int mfd_server_submit(mfd_server* s, const mfd_desc* desc, int64_t* id) {
     r->desc = *desc;
     r->bytes = desc_footprint(desc);
     const long long cells = (long long)desc->nx * desc->ny * desc->nz;
-    r->batchable = (desc->ndim == 2 || (desc->ndim == 3 && cells <= MFD_SERVER_BATCH_3D_CELLS)) && desc->dtype == MFD_F32 &&
+    r->batchable = ((desc->ndim == 2 && desc->polarization == MFD_POL_HY) ||
+                    (desc->ndim == 3 && cells <= MFD_SERVER_BATCH_3D_CELLS)) && desc->dtype == MFD_F32 &&
                    desc->rho_fp64 && !desc->tfsf_record && desc->mode == MFD_MODE_EXACT;
     std::lock_guard<std::mutex> lk(s->mu);
     if ((double)r->bytes > s->budget) {

@@ -693,6 +693,127 @@ __global__ void __launch_bounds__(256) e2d_kernel(const __grid_constant__ EParam
 }
 
 // ------------------------------------------------------------------------------------------
+// 2-D, second field set (Hx, Hz, Dy, Ey): the 3-D cell updates with every y derivative zero,
+// in their operation order (src/models.jl:735-878, 895-1162).  psi[0] of a layer holds
+// psiHzx / psiHxz (E update), psi[1] psiEyx / psiEyz (H update).
+// ------------------------------------------------------------------------------------------
+template <typename T, bool MATH, int FAST>
+__device__ __forceinline__ void h2e_cell(const HParams<T>& p, int accum, long long prev_step, int ix, int iz) {
+    const int nx = p.L.nx, nz = p.L.nz;
+    const int sz = p.L.sz;
+    const int c = ix + sz * iz;
+    const T ey = p.Ey[c];
+    T ey_xp, ey_zp;
+    if (ix < nx - 1) ey_xp = p.Ey[c + 1];
+    else { const int b = p.bc[MFD_XR]; ey_xp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ey[c - (nx - 1)] : T(0), ey); }
+    if (iz < nz - 1) ey_zp = p.Ey[c + sz];
+    else { const int b = p.bc[MFD_ZR]; ey_zp = bc_value(b, b == MFD_BC_PERIODIC ? p.Ey[c - (nz - 1) * sz] : T(0), ey); }
+    T hx = p.Hx[c], hz = p.Hz[c];
+    if (accum) {
+        const T a = ey * hz, d = T(0) - ey * hx;
+        p.Sa[c] = p.Sa[c] + sqrt0(a * a + d * d) * p.dt;
+        if (p.sum_e2) p.E2[c] = p.E2[c] + ey * ey * p.dt;
+        guard_at(p.flags, prev_step, ey);
+    }
+    T Mh = p.Mh0;
+    if (MATH) { const int g = p.geom[c]; if (g) Mh = p.matMh[g - 1]; }
+    T dEyx = cdiv<FAST>(ey_xp - ey, p.ddx);
+    T dEyz = cdiv<FAST>(ey_zp - ey, p.ddz);
+#pragma unroll
+    for (int f = MFD_XL; f <= MFD_XR; ++f) {
+        const LayerDev<T>& l = p.lay[f];
+        if (l.nb && (f == MFD_XL ? ix < l.ib : ix >= l.ib - 1)) {
+            const int q = f == MFD_XL ? ix : ix - (l.ib - 1), k = q + l.nb * iz;
+            const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEyx;
+            l.psi[1][k] = ps;
+            hz = mad<FAST>(-Mh, ps, hz);
+            dEyx = cdiv<FAST>(dEyx, l.K[q]);
+        }
+    }
+#pragma unroll
+    for (int f = MFD_ZL; f <= MFD_ZR; ++f) {
+        const LayerDev<T>& l = p.lay[f];
+        if (l.nb && (f == MFD_ZL ? iz < l.ib : iz >= l.ib - 1)) {
+            const int q = f == MFD_ZL ? iz : iz - (l.ib - 1), k = ix + p.L.px * q;
+            const T ps = l.B[q] * l.psi[1][k] + l.A[q] * dEyz;
+            l.psi[1][k] = ps;
+            hx = mad<FAST>(Mh, ps, hx);
+            dEyz = cdiv<FAST>(dEyz, l.K[q]);
+        }
+    }
+    hx = mad<FAST>(-Mh, T(0) - dEyz, hx);
+    hz = mad<FAST>(-Mh, dEyx - T(0), hz);
+    p.Hx[c] = hx;
+    p.Hz[c] = hz;
+}
+
+template <typename T, bool MATH, int FAST>
+__global__ void __launch_bounds__(256) h2e_kernel(const __grid_constant__ HParams<T> p) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= p.L.nx || iz >= p.L.nz) return;
+    h2e_cell<T, MATH, FAST>(p, p.accum, p.prev_step, ix, iz);
+}
+
+template <typename T, typename R, bool MAT, int FAST>
+__device__ __forceinline__ void e2e_cell(const EParams<T, R>& p, int ix, int iz) {
+    const int nx = p.L.nx, nz = p.L.nz;
+    const int sz = p.L.sz;
+    const int c = ix + sz * iz;
+    const T hx = p.Hx[c], hz = p.Hz[c];
+    T hz_xm, hx_zm;
+    if (ix > 0) hz_xm = p.Hz[c - 1];
+    else { const int b = p.bc[MFD_XL]; hz_xm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hz[c + (nx - 1)] : T(0), hz); }
+    if (iz > 0) hx_zm = p.Hx[c - sz];
+    else { const int b = p.bc[MFD_ZL]; hx_zm = bc_value(b, b == MFD_BC_PERIODIC ? p.Hx[c + (nz - 1) * sz] : T(0), hx); }
+    T dHxz = cdiv<FAST>(hx - hx_zm, p.ddz);
+    T dHzx = cdiv<FAST>(hz - hz_xm, p.ddx);
+    T Md1 = p.Md10, Md2 = p.Md20, Me = p.Me0;
+    bool simple = true;
+    if (MAT) {
+        const int g = p.geom[c];
+        if (g) {
+            const MatDev<T, R>& m = p.mats[g - 1];
+            Md1 = m.Md1; Md2 = m.Md2; Me = m.Me; simple = m.simple != 0;
+        }
+    }
+    T D1 = p.Dy[c];
+#pragma unroll
+    for (int f = MFD_XL; f <= MFD_XR; ++f) {
+        const LayerDev<T>& l = p.lay[f];
+        if (l.nb && (f == MFD_XL ? ix < l.ib : ix >= l.ib - 1)) {
+            const int q = f == MFD_XL ? ix : ix - (l.ib - 1), k = q + l.nb * iz;
+            const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHzx;
+            l.psi[0][k] = ps;
+            D1 = mad<FAST>(-Md2, ps, D1);
+            dHzx = cdiv<FAST>(dHzx, l.K[q]);
+        }
+    }
+#pragma unroll
+    for (int f = MFD_ZL; f <= MFD_ZR; ++f) {
+        const LayerDev<T>& l = p.lay[f];
+        if (l.nb && (f == MFD_ZL ? iz < l.ib : iz >= l.ib - 1)) {
+            const int q = f == MFD_ZL ? iz : iz - (l.ib - 1), k = ix + p.L.px * q;
+            const T ps = l.B[q] * l.psi[0][k] + l.A[q] * dHxz;
+            l.psi[0][k] = ps;
+            D1 = mad<FAST>(Md2, ps, D1);
+            dHxz = cdiv<FAST>(dHxz, l.K[q]);
+        }
+    }
+    D1 = Md1 * D1 + Md2 * (dHxz - dHzx);
+    p.Dy[c] = D1;
+    if (simple) p.Ey[c] = D1 * Me;
+}
+
+template <typename T, typename R, bool MAT, int FAST>
+__global__ void __launch_bounds__(256) e2e_kernel(const __grid_constant__ EParams<T, R> p) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= p.L.nx || iz >= p.L.nz) return;
+    e2e_cell<T, R, MAT, FAST>(p, ix, iz);
+}
+
+// ------------------------------------------------------------------------------------------
 // 1-D (z)
 // ------------------------------------------------------------------------------------------
 template <typename T, bool MATH, int FAST>
@@ -850,20 +971,32 @@ __global__ void __launch_bounds__(256) material_flat_kernel(const MatDev<T, R>* 
 
 // Running sums and NaN/Inf guard for the last step of a run (the H kernel of the next step
 // does this for every other step).
+// fset: the model's field set -- 3, 2 or 1 (its dimension) or FSET_EY2 (the second 2-D
+// field set: Hx, Hz, Dy, Ey).
+constexpr int FSET_EY2 = 4;
+
 template <typename T>
-__global__ void __launch_bounds__(256) sums_kernel(const __grid_constant__ HParams<T> p, const int ndim) {
+__global__ void __launch_bounds__(256) sums_kernel(const __grid_constant__ HParams<T> p, const int fset) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y;
     const int iz = blockIdx.z;
     if (ix >= p.L.nx) return;
     const int c = ix + p.L.px * iy + p.L.sz * iz;
+    if (fset == FSET_EY2) {   // the 3-D norm with Ex = Ez = Hy = 0
+        const T ey = p.Ey[c], hx = p.Hx[c], hz = p.Hz[c];
+        const T a = ey * hz, d = T(0) - ey * hx;
+        p.Sa[c] = p.Sa[c] + sqrt0(a * a + d * d) * p.dt;
+        if (p.sum_e2) p.E2[c] = p.E2[c] + ey * ey * p.dt;
+        guard(p, ey);
+        return;
+    }
     const T ex = p.Ex[c];
-    if (ndim == 3) {
+    if (fset == 3) {
         const T ey = p.Ey[c], ez = p.Ez[c], hx = p.Hx[c], hy = p.Hy[c], hz = p.Hz[c];
         const T a = ey * hz - ez * hy, b = ez * hx - ex * hz, d = ex * hy - ey * hx;
         p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b + d * d) * p.dt;
         if (p.sum_e2) p.E2[c] = p.E2[c] + (ex * ex + ey * ey + ez * ez) * p.dt;
-    } else if (ndim == 2) {
+    } else if (fset == 2) {
         const T ez = p.Ez[c], hy = p.Hy[c];
         const T a = -ez * hy, b = ex * hy;
         p.Sa[c] = p.Sa[c] + sqrt0(a * a + b * b) * p.dt;
@@ -877,7 +1010,7 @@ __global__ void __launch_bounds__(256) sums_kernel(const __grid_constant__ HPara
     guard(p, ex);
 }
 
-// NaN/Inf guard of Ex for one step (models.jl:202-209), for a step whose running sums (and
+// NaN/Inf guard of Ex (Ey in the second 2-D field set) for one step (models.jl:202-209), for a step whose running sums (and
 // the guard done with them) are left to the next H update.
 template <typename T>
 __global__ void __launch_bounds__(256) guard_kernel(const T* __restrict__ Ex, const Layout L, int* flags, const long long step) {

@@ -20,7 +20,7 @@ from .materials import IonizationRate, Material, PowerLawRate, material_struct
 from .monitors import FieldMonitor, SpectralMonitor, monitor_struct
 from .pml import make_pml
 from .sources import (HardSource, SoftSource, TFSFSource, box_indices, comp_index, field_components,
-                      source_struct_point, tabulate_waveform, tfsf_names, tfsf_struct)
+                      polarization_name, source_struct_point, tabulate_waveform, tfsf_names, tfsf_struct)
 
 _BC = {"periodic": 1, "dirichlet": 2, "neumann": 3}
 
@@ -70,10 +70,15 @@ def adapt_time(t, dtype):
 
 
 class Model:
-    """``Model(grid, source; tmax, CN=0.5, bc=:periodic, pml=0, material=nothing)``."""
+    """``Model(grid, source; tmax, CN=0.5, bc=:periodic, pml=0, material=nothing)``.
+    ``polarization`` chooses the field set of a 2-D model: "Hy" (Hy, Dx, Dz, Ex, Ez, the
+    reference's) or "Ey" (Hx, Hz, Dy, Ey, which the reference does not have)."""
 
-    def __init__(self, grid, source, *, tmax, CN=0.5, bc="periodic", pml=0, material=None):
+    def __init__(self, grid, source, *, tmax, CN=0.5, bc="periodic", pml=0, material=None, polarization="Hy"):
         self.grid = grid
+        self.polarization = polarization_name(polarization)
+        if grid.ndim != 2 and self.polarization != "Hy":
+            raise ValueError("polarization applies to 2-D models")
         self.dt = time_step(grid, CN)
         self.t = time_range(self.dt, tmax)
         self.Nt = len(self.t)
@@ -87,10 +92,10 @@ class Model:
             if isinstance(s, TFSFSource):
                 if self.tfsf is not None:
                     raise ValueError("one TFSF source per model")
-                self.tfsf = tfsf_struct(s, grid, self.t)
+                self.tfsf = tfsf_struct(s, grid, self.t, self.polarization)
                 self.tfsf_order = len(self.point_sources)
             elif isinstance(s, (SoftSource, HardSource)):
-                self.point_sources.append(source_struct_point(s, grid))
+                self.point_sources.append(source_struct_point(s, grid, self.polarization))
             else:
                 raise TypeError(f"unknown source type {type(s).__name__}")
         nfaces = 2 * grid.ndim
@@ -275,6 +280,7 @@ class Model:
             rec = (tuple(float(v) for v in tfsf_box), i1, i2)
         d.device = device
         d.mode = _abi.MFD_MODE_FAST if mode == "fast" else _abi.MFD_MODE_EXACT
+        d.polarization = _abi.MFD_POL_EY if self.polarization == "Ey" else _abi.MFD_POL_HY
         meta = {"coords_T": coords_T, "t_T": t_T, "monitors": mon_meta, "record": rec}
         return b, meta
 
@@ -400,7 +406,7 @@ def _run(model, st, meta, dtype, fname, nframes, nstride, dtout, components, mon
     shape = _grid_shape(g)
     Nt = model.Nt
     t_T = meta["t_T"]
-    comps_all = [c for c in field_components(g.ndim) if not c.startswith("D")]
+    comps_all = [c for c in field_components(g.ndim, model.polarization) if not c.startswith("D")]
     isfields = not (nstride is None and nframes is None and dtout is None)
     out_steps = output_times(t_T, nstride, nframes, dtout) if isfields else []
     if components is None:
@@ -479,10 +485,11 @@ def _run(model, st, meta, dtype, fname, nframes, nstride, dtout, components, mon
                 shp = (Nt,) if ms["sum"] else (Nt, len(cells))
             v = st.read_monitor(n - 1, comp_index(c), shp, spectral)
             out[pre + c] = v if ms["sum"] else v.T
-    fields = {c: st.read_field(comp_index(c)).reshape(shape, order="F") for c in field_components(g.ndim)}
+    fields = {c: st.read_field(comp_index(c)).reshape(shape, order="F")
+              for c in field_components(g.ndim, model.polarization)}
     if tfsf_record:
         _, i1, i2 = meta["record"]
-        rec = _record_dataset(g, st, meta, i1, i2)
+        rec = _record_dataset(g, st, meta, i1, i2, model.polarization)
         if tfsf_fname is None:
             base = fname if fname is not None else "out.npz"
             root, ext = os.path.splitext(base)
@@ -531,8 +538,9 @@ def _cartesian(grid, cells):
                      cells // (grid.Nx * grid.Ny) + 1], axis=1)
 
 
-def _record_dataset(g, st, meta, i1, i2):
-    """The TFSF record file content (sources.jl:349-369, 500-531, 779-836)."""
+def _record_dataset(g, st, meta, i1, i2, polarization="Hy"):
+    """The TFSF record file content (sources.jl:349-369, 500-531, 779-836); the second 2-D
+    field set records its faces over the nodes i1..i2."""
     box, _, _ = meta["record"]
     cs = meta["coords_T"]
     t_T = meta["t_T"]
@@ -541,14 +549,15 @@ def _record_dataset(g, st, meta, i1, i2):
     ix1, iy1, iz1 = i1
     ix2, iy2, iz2 = i2
     if g.ndim == 2:
-        rec["x"] = np.asarray(cs[0][ix1 - 1:ix2 - 1])
-        rec["z"] = np.asarray(cs[1][iz1 - 1:iz2 - 1])
+        e = 1 if polarization == "Ey" else 0
+        rec["x"] = np.asarray(cs[0][ix1 - 1:ix2 - 1 + e])
+        rec["z"] = np.asarray(cs[1][iz1 - 1:iz2 - 1 + e])
     elif g.ndim == 3:
         rec["x"] = np.asarray(cs[0][ix1 - 1:ix2])
         rec["y"] = np.asarray(cs[1][iy1 - 1:iy2])
         rec["z"] = np.asarray(cs[2][iz1 - 1:iz2])
     Nxi, Nyi, Nzi = ix2 - ix1, iy2 - iy1, iz2 - iz1
-    for k, name in enumerate(tfsf_names(g.ndim)):
+    for k, name in enumerate(tfsf_names(g.ndim, polarization)):
         v = st.read_tfsf_record(k)
         if g.ndim == 1:
             rec[name] = v.reshape(nt)

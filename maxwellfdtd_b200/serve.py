@@ -136,11 +136,12 @@ def read_results(st, req, fields=True):
     """The request's outputs: every monitor's record and, with fields, the final fields and Sa."""
     from .sources import comp_index, field_components
     nd = req.model.grid.ndim
+    pol = getattr(req.model, "polarization", "Hy")
     out = {}
     if fields:
-        out = {f"field/{c}": st.read_field(comp_index(c)) for c in field_components(nd)}
+        out = {f"field/{c}": st.read_field(comp_index(c)) for c in field_components(nd, pol)}
         out["Sa"] = st.read_integral(_abi.MFD_INT_SA)
-    comps = {3: ("Hx", "Hy", "Hz", "Ex", "Ey", "Ez"), 2: ("Hy", "Ex", "Ez"), 1: ("Hy", "Ex")}[nd]
+    comps = [c for c in field_components(nd, pol) if not c.startswith("D")]
     for k, mm in enumerate(req.meta["monitors"]):
         npts = len(mm["cells"])
         spectral = mm["kind"] == 1

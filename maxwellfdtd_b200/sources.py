@@ -18,10 +18,23 @@ from .geometry import cell_coords, geometry2indices
 _COMP = {"Hx": 0, "Hy": 1, "Hz": 2, "Dx": 3, "Dy": 4, "Dz": 5, "Ex": 6, "Ey": 7, "Ez": 8}
 COMPONENTS_3D = ("Hx", "Hy", "Hz", "Dx", "Dy", "Dz", "Ex", "Ey", "Ez")
 COMPONENTS_2D = ("Hy", "Dx", "Dz", "Ex", "Ez")
+COMPONENTS_2D_EY = ("Hx", "Hz", "Dy", "Ey")
 COMPONENTS_1D = ("Hy", "Dx", "Ex")
+POLARIZATIONS = ("Hy", "Ey")
 
 
-def field_components(ndim):
+def polarization_name(p):
+    """The 2-D field set: "Hy" (Hy, Dx, Dz, Ex, Ez -- the reference's Field2D,
+    fields.jl:36-55) or "Ey" (Hx, Hz, Dy, Ey; MFD_POL_EY in include/maxwellfdtd.h)."""
+    p = str(p).lstrip(":")
+    if p not in POLARIZATIONS:
+        raise ValueError(f"polarization must be one of {POLARIZATIONS}, not {p!r}")
+    return p
+
+
+def field_components(ndim, polarization="Hy"):
+    if ndim == 2 and polarization == "Ey":
+        return COMPONENTS_2D_EY
     return {1: COMPONENTS_1D, 2: COMPONENTS_2D, 3: COMPONENTS_3D}[ndim]
 
 
@@ -78,12 +91,12 @@ class PointSourceStruct:
     p: Any
 
 
-def source_struct_point(source, grid):
+def source_struct_point(source, grid, polarization="Hy"):
     cells = geometry2indices(source.geometry, grid)
     if len(cells) == 0:
         raise ValueError("I did not find any grid points which satisfy your source geometry.")
     comp = str(source.component).lstrip(":")
-    if comp not in field_components(grid.ndim):
+    if comp not in field_components(grid.ndim, polarization):
         raise ValueError(f"{grid.ndim}-D field has no component {comp}")
     if isinstance(source, SoftSource):
         if comp in ("Ex", "Ey", "Ez") and not source.explicit:
@@ -133,7 +146,15 @@ TFSF_NAMES_3D = ("incHy_1yz", "incHz_1yz", "incEy_1yz", "incEz_1yz",
                  "incHx_xy2", "incHy_xy2", "incEx_xy2", "incEy_xy2")
 
 
-def tfsf_names(ndim):
+# The second 2-D field set: Hz, Ey on the x faces and Hx, Ey on the z faces, over the nodes
+# i1..i2 (the 3-D faces 1yz, 2yz, xy1, xy2 restricted to those components).
+TFSF_NAMES_2D_EY = ("incHz_1z", "incEy_1z", "incHz_2z", "incEy_2z",
+                    "incHx_x1", "incEy_x1", "incHx_x2", "incEy_x2")
+
+
+def tfsf_names(ndim, polarization="Hy"):
+    if ndim == 2 and polarization == "Ey":
+        return TFSF_NAMES_2D_EY
     return {1: TFSF_NAMES_1D, 2: TFSF_NAMES_2D, 3: TFSF_NAMES_3D}[ndim]
 
 
@@ -212,7 +233,7 @@ def _compact(r, extent):
     return np.ascontiguousarray(np.transpose(r, (2, 1, 0)).reshape(nt, -1)), shape
 
 
-def tfsf_struct(source, grid, t):
+def tfsf_struct(source, grid, t, polarization="Hy"):
     """``SourceStruct(::TFSFSource, ...)`` (sources.jl:284-317, 408-466, 592-710): box
     indices on this grid and incident data resampled onto (face coordinates, t), dense in t.
     Arrays are returned C-ordered [nt][face extent] (the reference's (a, b, Nt) column-major),
@@ -236,9 +257,14 @@ def tfsf_struct(source, grid, t):
         zex = np.asarray(d["z"], dtype=np.float64)
         ix1, iz1 = i1[0], i1[2]
         ix2, iz2 = i2[0], i2[2]
-        zq = grid.z[iz1 - 1:iz2 - 1]
-        xq = grid.x[ix1 - 1:ix2 - 1]
-        for name in TFSF_NAMES_2D:
+        names = tfsf_names(2, polarization)
+        if any(n not in d for n in names):
+            raise ValueError(f"the TFSF data do not hold the {polarization} polarisation's arrays "
+                             + ", ".join(names))
+        e = 1 if polarization == "Ey" else 0   # node ranges i1..i2 in the Ey field set
+        zq = grid.z[iz1 - 1:iz2 - 1 + e]
+        xq = grid.x[ix1 - 1:ix2 - 1 + e]
+        for name in names:
             v = np.asarray(d[name], dtype=np.float64)   # (face, Nt) column-major in the file
             v = _as_col_major(v, 2)
             knots, q = (zex, zq) if name.endswith("z") else (xex, xq)

@@ -148,6 +148,7 @@ struct Monitor {
 template <typename T, typename R>
 struct Oracle : OracleBase {
     int ndim, nx, ny, nz;
+    int pol = MFD_POL_HY;   // the 2-D field set (include/maxwellfdtd.h)
     size_t N;
     T dx, dy, dz, dt;
     int64_t nt;
@@ -161,7 +162,8 @@ struct Oracle : OracleBase {
     // psi arrays in the reference's shapes (src/pml.jl:133-304).
     // 3-D: x faces (Nb,Ny,Nz): Hyx,Hzx,Eyx,Ezx; y faces (Nx,Nb,Nz): Hxy,Hzy,Exy,Ezy;
     //      z faces (Nx,Ny,Nb): Hxz,Hyz,Exz,Eyz.  2-D: x faces (Nb,Nz): Hyx,Ezx;
-    //      z faces (Nx,Nb): Hyz,Exz.  1-D: z faces (Nb): Hyz,Exz.
+    //      z faces (Nx,Nb): Hyz,Exz (second 2-D field set: Hzx,Eyx and Hxz,Eyz).
+    //      1-D: z faces (Nb): Hyz,Exz.
     std::vector<T> psi[6][4];
     std::vector<T> JE, Sa, E2;
     std::vector<Source<T>> srcs;
@@ -182,6 +184,7 @@ struct Oracle : OracleBase {
 
     int init(const mfd_desc* d) {
         ndim = d->ndim; nx = d->nx; ny = d->ny; nz = d->nz;
+        pol = ndim == 2 ? d->polarization : MFD_POL_HY;
         N = (size_t)nx * ny * nz;
         dx = (T)d->dx; dy = (T)d->dy; dz = (T)d->dz; dt = (T)d->dt;
         nt = d->nt;
@@ -325,6 +328,7 @@ struct Oracle : OracleBase {
 
     bool has_comp(int c) const {
         if (ndim == 3) return true;
+        if (ndim == 2 && pol == MFD_POL_EY) return c == MFD_HX || c == MFD_HZ || c == MFD_DY || c == MFD_EY;
         if (ndim == 2) return c == MFD_HY || c == MFD_DX || c == MFD_DZ || c == MFD_EX || c == MFD_EZ;
         return c == MFD_HY || c == MFD_DX || c == MFD_EX;
     }
@@ -345,6 +349,7 @@ struct Oracle : OracleBase {
     size_t face_len(int k, const int* i1, const int* i2) const {
         size_t Nxi = i2[0] - i1[0], Nyi = i2[1] - i1[1], Nzi = i2[2] - i1[2];
         if (ndim == 1) return 1;
+        if (ndim == 2 && pol == MFD_POL_EY) return k < 4 ? Nzi + 1 : Nxi + 1;   // Hz, Ey / Hx, Ey on the nodes
         if (ndim == 2) return k < 4 ? Nzi : Nxi;
         int face = k / 4, j = k % 4;
         if (face < 2) return (j == 0 || j == 3) ? (Nyi + 1) * Nzi : Nyi * (Nzi + 1);
@@ -813,6 +818,107 @@ struct Oracle : OracleBase {
             }
     }
 
+    // 2-D updates of the second field set (Hx, Hz, Dy, Ey): the 3-D update_H_kernel! /
+    // update_E_kernel! (src/models.jl:735-878, 895-1162) with every y derivative zero, in
+    // the 3-D operation order.  psi[xface][0]=psiHzx, [1]=psiEyx; psi[zface][0]=psiHxz,
+    // [1]=psiEyz.
+    void update_H2ey() {
+        std::vector<T>&Hx = F[MFD_HX], &Hz = F[MFD_HZ];
+        const std::vector<T>& Ey = F[MFD_EY];
+#pragma omp parallel for schedule(static)
+        for (int iz = 0; iz < nz; ++iz)
+            for (int ix = 0; ix < nx; ++ix) {
+                size_t c = id(ix, 0, iz);
+                int64_t g = geometry[c];
+                T Mh = g > 0 ? mats[g - 1].Mh : Mh0;
+                T Ey_ixp1, Ey_izp1;
+                if (ix == nx - 1) {
+                    int b = bc[MFD_XR];
+                    if (b == MFD_BC_PERIODIC) Ey_ixp1 = Ey[id(0, 0, iz)];
+                    else if (b == MFD_BC_DIRICHLET) Ey_ixp1 = 0;
+                    else Ey_ixp1 = Ey[c];
+                } else Ey_ixp1 = Ey[id(ix + 1, 0, iz)];
+                if (iz == nz - 1) {
+                    int b = bc[MFD_ZR];
+                    if (b == MFD_BC_PERIODIC) Ey_izp1 = Ey[id(ix, 0, 0)];
+                    else if (b == MFD_BC_DIRICHLET) Ey_izp1 = 0;
+                    else Ey_izp1 = Ey[c];
+                } else Ey_izp1 = Ey[id(ix, 0, iz + 1)];
+                T dEyx = (Ey_ixp1 - Ey[c]) / dx;
+                T dEyz = (Ey_izp1 - Ey[c]) / dz;
+                for (int f : {MFD_XL, MFD_XR}) {
+                    const Layer<T>& l = L[f];
+                    if (!l.nb || (f == MFD_XL ? ix >= l.ib : ix < l.ib - 1)) continue;
+                    int p = f == MFD_XL ? ix : ix - (l.ib - 1);
+                    T& ps = psi[f][1][(size_t)p + (size_t)l.nb * iz];
+                    ps = l.B[p] * ps + l.A[p] * dEyx;
+                    Hz[c] -= Mh * ps;
+                    dEyx = dEyx / l.K[p];
+                }
+                for (int f : {MFD_ZL, MFD_ZR}) {
+                    const Layer<T>& l = L[f];
+                    if (!l.nb || (f == MFD_ZL ? iz >= l.ib : iz < l.ib - 1)) continue;
+                    int p = f == MFD_ZL ? iz : iz - (l.ib - 1);
+                    T& ps = psi[f][1][(size_t)ix + (size_t)nx * p];
+                    ps = l.B[p] * ps + l.A[p] * dEyz;
+                    Hx[c] += Mh * ps;
+                    dEyz = dEyz / l.K[p];
+                }
+                Hx[c] -= Mh * (0 - dEyz);
+                Hz[c] -= Mh * (dEyx - 0);
+            }
+    }
+
+    void update_E2ey() {
+        std::vector<T>& Dy = F[MFD_DY];
+        const std::vector<T>&Hx = F[MFD_HX], &Hz = F[MFD_HZ];
+        static const int Dc[1] = {MFD_DY}, Ec[1] = {MFD_EY}, Ps[1] = {1};
+#pragma omp parallel for schedule(static)
+        for (int iz = 0; iz < nz; ++iz)
+            for (int ix = 0; ix < nx; ++ix) {
+                size_t c = id(ix, 0, iz);
+                int64_t g = geometry[c];
+                T Md1, Md2;
+                if (g > 0) { Md1 = mats[g - 1].Md1; Md2 = mats[g - 1].Md2; }
+                else { Md1 = Md10; Md2 = Md20; }
+                T Hz_ixm1, Hx_izm1;
+                if (ix == 0) {
+                    int b = bc[MFD_XL];
+                    if (b == MFD_BC_PERIODIC) Hz_ixm1 = Hz[id(nx - 1, 0, iz)];
+                    else if (b == MFD_BC_DIRICHLET) Hz_ixm1 = 0;
+                    else Hz_ixm1 = Hz[c];
+                } else Hz_ixm1 = Hz[id(ix - 1, 0, iz)];
+                if (iz == 0) {
+                    int b = bc[MFD_ZL];
+                    if (b == MFD_BC_PERIODIC) Hx_izm1 = Hx[id(ix, 0, nz - 1)];
+                    else if (b == MFD_BC_DIRICHLET) Hx_izm1 = 0;
+                    else Hx_izm1 = Hx[c];
+                } else Hx_izm1 = Hx[id(ix, 0, iz - 1)];
+                T dHxz = (Hx[c] - Hx_izm1) / dz;
+                T dHzx = (Hz[c] - Hz_ixm1) / dx;
+                for (int f : {MFD_XL, MFD_XR}) {
+                    const Layer<T>& l = L[f];
+                    if (!l.nb || (f == MFD_XL ? ix >= l.ib : ix < l.ib - 1)) continue;
+                    int p = f == MFD_XL ? ix : ix - (l.ib - 1);
+                    T& ps = psi[f][0][(size_t)p + (size_t)l.nb * iz];
+                    ps = l.B[p] * ps + l.A[p] * dHzx;
+                    Dy[c] -= Md2 * ps;
+                    dHzx = dHzx / l.K[p];
+                }
+                for (int f : {MFD_ZL, MFD_ZR}) {
+                    const Layer<T>& l = L[f];
+                    if (!l.nb || (f == MFD_ZL ? iz >= l.ib : iz < l.ib - 1)) continue;
+                    int p = f == MFD_ZL ? iz : iz - (l.ib - 1);
+                    T& ps = psi[f][0][(size_t)ix + (size_t)nx * p];
+                    ps = l.B[p] * ps + l.A[p] * dHxz;
+                    Dy[c] += Md2 * ps;
+                    dHxz = dHxz / l.K[p];
+                }
+                Dy[c] = Md1 * Dy[c] + Md2 * (dHxz - dHzx);
+                materials_and_E(c, g, 1, Dc, Ec, Ps);
+            }
+    }
+
     // 1-D kernels (src/models.jl:248-437).  psi[zface][0]=psiHyz, [1]=psiExz.
     void update_H1() {
         std::vector<T>& Hy = F[MFD_HY];
@@ -968,6 +1074,28 @@ struct Oracle : OracleBase {
             tfsf_apply<double>(MFD_EY, ix1, ix2, iy1, iy2 - 1, iz2, iz2, 20, it, cez, +1);
             tfsf_apply<double>(MFD_DX, ix1, ix2 - 1, iy1, iy2, iz2, iz2, 21, it, cdz, -1);
             tfsf_apply<double>(MFD_DY, ix1, ix2, iy1, iy2 - 1, iz2, iz2, 20, it, cdz, +1);
+        } else if (ndim == 2 && pol == MFD_POL_EY) {
+            // The 3-D faces 1yz, 2yz, xy1, xy2 restricted to Hz, Ey / Hx, Ey (their signs and
+            // node ranges, sources.jl:728-776) with the 2-D coefficients (sources.jl:478-495).
+            double cmx = (double)dt / (MU0 * (double)dx), cex = (double)dt / (EPS0 * (double)dx);
+            double cmz = (double)dt / (MU0 * (double)dz), cez = (double)dt / (EPS0 * (double)dz);
+            T cdx = dt / dx, cdz = dt / dz;
+            // 1z
+            tfsf_apply<double>(MFD_HZ, ix1 - 1, ix1 - 1, 1, 1, iz1, iz2, 1, it, cmx, +1);
+            tfsf_apply<double>(MFD_EY, ix1, ix1, 1, 1, iz1, iz2, 0, it, cex, +1);
+            tfsf_apply<T>(MFD_DY, ix1, ix1, 1, 1, iz1, iz2, 0, it, cdx, +1);
+            // 2z
+            tfsf_apply<double>(MFD_HZ, ix2, ix2, 1, 1, iz1, iz2, 3, it, cmx, -1);
+            tfsf_apply<double>(MFD_EY, ix2, ix2, 1, 1, iz1, iz2, 2, it, cex, -1);
+            tfsf_apply<T>(MFD_DY, ix2, ix2, 1, 1, iz1, iz2, 2, it, cdx, -1);
+            // x1
+            tfsf_apply<double>(MFD_HX, ix1, ix2, 1, 1, iz1 - 1, iz1 - 1, 5, it, cmz, -1);
+            tfsf_apply<double>(MFD_EY, ix1, ix2, 1, 1, iz1, iz1, 4, it, cez, -1);
+            tfsf_apply<T>(MFD_DY, ix1, ix2, 1, 1, iz1, iz1, 4, it, cdz, -1);
+            // x2
+            tfsf_apply<double>(MFD_HX, ix1, ix2, 1, 1, iz2, iz2, 7, it, cmz, +1);
+            tfsf_apply<double>(MFD_EY, ix1, ix2, 1, 1, iz2, iz2, 6, it, cez, +1);
+            tfsf_apply<T>(MFD_DY, ix1, ix2, 1, 1, iz2, iz2, 6, it, cdz, +1);
         } else if (ndim == 2) {
             // dt/(MU0*dx) and dt/(EPS0*dx) promote to double; dt/dx stays T (sources.jl:478-495)
             double cmx = (double)dt / (MU0 * (double)dx), cex = (double)dt / (EPS0 * (double)dx);
@@ -1037,6 +1165,15 @@ struct Oracle : OracleBase {
             rec_copy(MFD_HY, ix1, ix2 - 1, iy1, iy2, iz2, iz2, 21, it);
             rec_copy(MFD_EX, ix1, ix2 - 1, iy1, iy2, iz2, iz2, 22, it);
             rec_copy(MFD_EY, ix1, ix2, iy1, iy2 - 1, iz2, iz2, 23, it);
+        } else if (ndim == 2 && pol == MFD_POL_EY) {
+            rec_copy(MFD_HZ, ix1 - 1, ix1 - 1, 1, 1, iz1, iz2, 0, it);
+            rec_copy(MFD_EY, ix1, ix1, 1, 1, iz1, iz2, 1, it);
+            rec_copy(MFD_HZ, ix2, ix2, 1, 1, iz1, iz2, 2, it);
+            rec_copy(MFD_EY, ix2, ix2, 1, 1, iz1, iz2, 3, it);
+            rec_copy(MFD_HX, ix1, ix2, 1, 1, iz1 - 1, iz1 - 1, 4, it);
+            rec_copy(MFD_EY, ix1, ix2, 1, 1, iz1, iz1, 5, it);
+            rec_copy(MFD_HX, ix1, ix2, 1, 1, iz2, iz2, 6, it);
+            rec_copy(MFD_EY, ix1, ix2, 1, 1, iz2, iz2, 7, it);
         } else if (ndim == 2) {
             rec_copy(MFD_HY, ix1 - 1, ix1 - 1, 1, 1, iz1, iz2 - 1, 0, it);
             rec_copy(MFD_EZ, ix1, ix1, 1, 1, iz1, iz2 - 1, 1, it);
@@ -1122,6 +1259,12 @@ struct Oracle : OracleBase {
                 T a = Ey * Hz - Ez * Hy, b = Ez * Hx - Ex * Hz, d = Ex * Hy - Ey * Hx;
                 Sa[c] += std::sqrt(a * a + b * b + d * d) * dt;
                 if (isgeometry) E2[c] += (Ex * Ex + Ey * Ey + Ez * Ez) * dt;
+            } else if (ndim == 2 && pol == MFD_POL_EY) {
+                // the 3-D norm with Ex = Ez = Hy = 0: a = Ey Hz, b = 0, d = -Ey Hx
+                T Hx = F[MFD_HX][c], Hz = F[MFD_HZ][c], Ey = F[MFD_EY][c];
+                T a = Ey * Hz, d = 0 - Ey * Hx;
+                Sa[c] += std::sqrt(a * a + d * d) * dt;
+                if (isgeometry) E2[c] += Ey * Ey * dt;
             } else if (ndim == 2) {
                 T Hy = F[MFD_HY][c], Ex = F[MFD_EX][c], Ez = F[MFD_EZ][c];
                 T a = -Ez * Hy, b = Ex * Hy;
@@ -1137,7 +1280,7 @@ struct Oracle : OracleBase {
     }
 
     int check_finite(int64_t it) {
-        const std::vector<T>& Ex = F[MFD_EX];
+        const std::vector<T>& Ex = F[pol == MFD_POL_EY ? MFD_EY : MFD_EX];   // Ey when the model has no Ex
         bool nan = false, inf = false;
         for (size_t c = 0; c < N; ++c) {
             if (std::isnan(Ex[c])) nan = true;
@@ -1160,6 +1303,7 @@ struct Oracle : OracleBase {
         for (int64_t it = a; it <= b; ++it) {
             // step! (models.jl:125-132)
             if (ndim == 3) { update_H3(); update_E3(); }
+            else if (ndim == 2 && pol == MFD_POL_EY) { update_H2ey(); update_E2ey(); }
             else if (ndim == 2) { update_H2(); update_E2(); }
             else { update_H1(); update_E1(); }
             for (size_t s = 0; s <= srcs.size(); ++s) {
@@ -1242,6 +1386,9 @@ int validate(const mfd_desc* d) {
     if (d->ndim == 1 && (d->nx != 1 || d->ny != 1)) { g_create_error = "1-D model needs nx = ny = 1"; return MFD_ERR_INVALID; }
     if (d->ndim == 2 && d->ny != 1) { g_create_error = "2-D model needs ny = 1"; return MFD_ERR_INVALID; }
     if (d->dtype != MFD_F32 && d->dtype != MFD_F64) { g_create_error = "bad dtype"; return MFD_ERR_INVALID; }
+    if (d->polarization != MFD_POL_HY && (d->ndim != 2 || d->polarization != MFD_POL_EY)) {
+        g_create_error = "polarization must be MFD_POL_HY, or MFD_POL_EY for a 2-D model"; return MFD_ERR_INVALID;
+    }
     if (d->tfsf.enabled) {
         for (int a = 0; a < 3; ++a) {
             if (d->ndim == 3 || (d->ndim == 2 && a != 1) || (d->ndim == 1 && a == 2)) {

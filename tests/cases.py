@@ -229,7 +229,7 @@ def run_all(model, library, dtype, mons=None, tfsf_box_=None, rho_fp64=True, chu
     if chunks is None:
         sol = M.solve(model, backend=be, monitors=mons, tfsf_record=tfsf_box_ is not None, tfsf_box=tfsf_box_,
                       tfsf_fname=None if tfsf_box_ is None else _tmp_name())
-        out = {f"field/{c}": np.asarray(sol.field[c]) for c in field_components(model.grid.ndim)}
+        out = {f"field/{c}": np.asarray(sol.field[c]) for c in field_components(model.grid.ndim, model.polarization)}
         for k, v in sol.out.items():
             if isinstance(v, np.ndarray) and k != "t":
                 out[k] = v
@@ -245,7 +245,7 @@ def run_all(model, library, dtype, mons=None, tfsf_box_=None, rho_fp64=True, chu
         st.run(a, a + n - 1)
         a += n
     st.run(a, model.Nt)
-    out = {f"field/{c}": st.read_field(comp_index(c)) for c in field_components(model.grid.ndim)}
+    out = {f"field/{c}": st.read_field(comp_index(c)) for c in field_components(model.grid.ndim, model.polarization)}
     out["Sa"] = st.read_integral(_abi.MFD_INT_SA)
     st.close()
     return out

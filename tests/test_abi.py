@@ -63,7 +63,7 @@ int main(void) {
   F(mfd_desc, dt) F(mfd_desc, nt) F(mfd_desc, bc) F(mfd_desc, pml) F(mfd_desc, Mh0) F(mfd_desc, geometry)
   F(mfd_desc, nmat) F(mfd_desc, mats) F(mfd_desc, rho_fp64) F(mfd_desc, nsrc) F(mfd_desc, srcs)
   F(mfd_desc, tfsf) F(mfd_desc, nmon) F(mfd_desc, mons) F(mfd_desc, tfsf_record) F(mfd_desc, rec_i1)
-  F(mfd_desc, rec_i2) F(mfd_desc, device) F(mfd_desc, mode) F(mfd_desc, nshape) F(mfd_desc, shapes) F(mfd_desc, coords)
+  F(mfd_desc, rec_i2) F(mfd_desc, device) F(mfd_desc, mode) F(mfd_desc, nshape) F(mfd_desc, shapes) F(mfd_desc, coords) F(mfd_desc, polarization)
   printf("mfd_shape %zu\n", sizeof(mfd_shape));
   F(mfd_shape, material) F(mfd_shape, p) F(mfd_tfsf, shape)
   F(mfd_material, nq) F(mfd_material, Aq) F(mfd_material, kerr) F(mfd_material, plasma) F(mfd_material, Rava)
