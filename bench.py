@@ -45,7 +45,8 @@ sys.path.insert(0, ROOT)
 # DRAM traffic of one E and one H update (core + slab kernels) of the 256^3 workload, per
 # arithmetic mode, from one ncu capture of the launches of one step (dram__bytes_read.sum +
 # dram__bytes_write.sum); the capture and its command are in NCU_TRAFFIC_SOURCE.
-NCU_TRAFFIC_256 = {("exact", "E"): 760_243_968, ("exact", "H"): 857_313_280}
+NCU_TRAFFIC_256 = {("exact", "E"): 760_243_968, ("exact", "H"): 857_313_280,
+                   ("fast", "E"): 791_582_720, ("fast", "H"): 855_493_888}
 NCU_TRAFFIC_SOURCE = "profiles/update_traffic_256.md"
 
 WORKLOAD = "plasmonics_256: 256^3 FP32, Drude+Lorentz sphere r=60nm, 12-cell CPML, TFSF 600nm/3fs, 6x DFT faces x 64 freq FP64"

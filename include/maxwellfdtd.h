@@ -400,8 +400,8 @@ MFD_API int mfd_write_state(mfd_handle* h, const void* src, int64_t bytes);
  * queued requests in arrival order when the request's device-memory footprint (computed from
  * the descriptor before anything is allocated, mfd_server_footprint) fits the budget next to
  * the admitted requests and fewer than max_active requests are computing, and uploads it.
- * 2-D and small 3-D (at most 2^20 cells) single-precision requests in MFD_MODE_EXACT with
- * rho_fp64 and no TFSF recording join one running batch (mfd_batch_*), which takes new
+ * 2-D (first field set, MFD_POL_HY) and small 3-D (at most 2^20 cells) single-precision
+ * requests in MFD_MODE_EXACT with rho_fp64 and no TFSF recording join one running batch (mfd_batch_*), which takes new
  * members between its runs of steps (continuous batching); every other request runs as a
  * solo lane on its own host thread and stream, at most max_solo at a time.  A request that
  * waits only for a solo lane does not hold back batch requests behind it; one that waits for
