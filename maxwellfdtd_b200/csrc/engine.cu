@@ -382,6 +382,7 @@ class Engine : public HandleBase {
     long long mon_maxpts = 0;
     long long ring_first = 0;
     bool need_ring = false;
+    bool mon_apart = false;     // no monitor cell is written by a source: gather beside them
 
     int* d_flags = nullptr;     // [nt] per-step NaN/Inf flags of Ex
     int* h_flags = nullptr;     // host copy
@@ -732,6 +733,15 @@ class Engine : public HandleBase {
         h_flags = h_flags_v.data();
         MFD_CK(cudaStreamSynchronize(st));
         init_split();
+        mon_apart = overlap && monitors_apart_from_sources(d);
+        if (mon_apart) make_side_stream();
+    }
+
+    void make_side_stream() {
+        if (st_side) return;
+        MFD_CK(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking));
+        MFD_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        MFD_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     }
 
     // The split needs layers that do not overlap in any dimension; MFD_KERNEL3D=unsplit
@@ -747,11 +757,7 @@ class Engine : public HandleBase {
         sbox = SplitBox{yl, yr, zl, zr, zc3, (zl + nz - zr) * ny};
         slab_rows = (long long)sbox.nzr + (long long)(zr - zl) * (yl + ny - yr);
         use_split = true;
-        if (overlap && !st_side) {
-            MFD_CK(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking));
-            MFD_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-            MFD_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
-        }
+        if (overlap) make_side_stream();
         if (const char* a = std::getenv("MFD_CORE_ASYNC")) core_async = std::atoi(a) != 0;
         if (const char* z = std::getenv("MFD_ASYNC_ZC")) async_zc = std::max(1, std::atoi(z));
         // rows and planes of the core box that hold material cells, widened to the staged
@@ -1011,6 +1017,28 @@ class Engine : public HandleBase {
             if (s.len >= (1ll << 31)) throw Error(MFD_ERR_INVALID, "TFSF record face larger than 2^31 cells");
             p.arr[i] = dalloc<T>((size_t)s.len * nt);
         }
+    }
+
+    // True when no source (point source or TFSF statement) writes a cell that a monitor
+    // reads.  The monitor gather of a step then runs on the side stream while the sources
+    // run: it reads only its points' own cells, and the sources write only theirs.
+    bool monitors_apart_from_sources(const mfd_desc* d) const {
+        if (d->nmon <= 0) return false;
+        std::vector<bool> mark((size_t)N, false);
+        for (int m = 0; m < d->nmon; ++m)
+            for (long long j = 0; j < d->mons[m].npts; ++j) mark[(size_t)d->mons[m].cells[j]] = true;
+        for (int i = 0; i < d->nsrc; ++i)
+            for (long long j = 0; j < d->srcs[i].npts; ++j)
+                if (mark[(size_t)d->srcs[i].cells[j]]) return false;
+        if (tfsf)
+            for (int i = 0; i < tfsf_p.n; ++i) {
+                const RectStmt& q = tfsf_p.s[i];
+                for (int z = q.z0; z <= q.z1; ++z)
+                    for (int y = q.y0; y <= q.y1; ++y)
+                        for (int x = q.x0; x <= q.x1; ++x)
+                            if (mark[(size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z)]) return false;
+            }
+        return true;
     }
 
     void init_monitors(const mfd_desc* d) {
@@ -1467,18 +1495,19 @@ class Engine : public HandleBase {
         ring_used = 0;
     }
 
-    void launch_monitors(int64_t it) {
+    void launch_monitors(int64_t it, cudaStream_t s = nullptr) {
         if (mons_host.empty()) return;
         if (need_ring && ring_used == 0) ring_first = it - 1;
         const int slot = ring_used;
         launch(KC_MON, [&] {
             const long long nb = (mon_maxpts + 255) / 256;
-            monitor_gather_kernel<T><<<dim3((unsigned)nb, mon_p.nmon), 256, 0, st>>>(mon_p, it - 1, slot);
+            monitor_gather_kernel<T><<<dim3((unsigned)nb, mon_p.nmon), 256, 0, s ? s : st>>>(mon_p, it - 1, slot);
         });
-        if (need_ring) {
-            ring_used++;
-            if (ring_used == ring_k) flush_monitors();
-        }
+        if (need_ring) ring_used++;
+    }
+    // The ring fold when the ring is full (on st, after the gather has joined).
+    void fold_if_full() {
+        if (need_ring && ring_used == ring_k) flush_monitors();
     }
 
     void launch_record(int64_t it) {
@@ -1534,8 +1563,16 @@ class Engine : public HandleBase {
             launch_H((it > a || sums_pending) ? 1 : 0, it - 1);
             sums_pending = false;
             launch_E((int)((it - 1) & 1));
-            launch_sources(it);
-            launch_monitors(it);
+            if (mon_apart && !profiling) {   // gather beside the sources (disjoint cells)
+                fork();
+                launch_monitors(it, st_side);
+                launch_sources(it);
+                join();
+            } else {
+                launch_sources(it);
+                launch_monitors(it);
+            }
+            fold_if_full();
             if (record) launch_record(it);
             if (snap_next < snap_steps.size() && snap_steps[snap_next] == it) snapshot();
         }
