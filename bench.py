@@ -402,7 +402,7 @@ def run_batch2d(args, three=False):
     wb = _abi.Batch(lib, local)
     warm = []
     for m, mo in models[:8]:
-        b, meta = m.build_desc(np.float32, mo, device=local)
+        b, meta = m.build_desc(np.float32, mo, device=local, mode=args.mode)
         st = _abi.Stepper(lib, b, np.float32)
         wb.add(st, min(m.Nt, 3 * 16))
         warm.append(st)
@@ -416,7 +416,7 @@ def run_batch2d(args, three=False):
     held = []
     h2d = 0
     for m, mo in models:
-        b, meta = m.build_desc(np.float32, mo, device=local)
+        b, meta = m.build_desc(np.float32, mo, device=local, mode=args.mode)
         h2d += sum(a.nbytes for a in b.keep if isinstance(a, np.ndarray))
         st = _abi.Stepper(lib, b, np.float32)
         batch.add(st, m.Nt)
@@ -444,7 +444,7 @@ def run_batch2d(args, three=False):
     seq = [models[i] for i in np.random.default_rng(args.seed + 1).choice(len(models), min(args.seq_sims, len(models)), replace=False)]
     seq_ms, seq_cu = 0.0, 0
     for m, mo in seq:
-        b, meta = m.build_desc(np.float32, mo, device=local)
+        b, meta = m.build_desc(np.float32, mo, device=local, mode=args.mode)
         st = _abi.Stepper(lib, b, np.float32)
         st.run(1, m.Nt)
         seq_ms += st.last_run_ms()
@@ -464,7 +464,7 @@ def run_batch2d(args, three=False):
                                 f"1-20 ellipses eps in [1,12] (half Debye), Ricker point source, 4 point monitors, "
                                 f"steps 2000-6000 x {args.steps_scale}"),
                    "cells": int(sum(ncell(m) for m, _ in models)), "cell_updates": int(cu_total),
-                   "seed": args.seed, "parallelism": "one batch, persistent launches, CUDA graph",
+                   "seed": args.seed, "mode": args.mode, "parallelism": "one batch, persistent launches, CUDA graph",
                    "l2": "inputs larger than L2", "tile": list(info["tile"])},
         "e2e": {"value": round(cu_total / (t_end - t0) / 1e9, 3), "unit": "Gcell-updates/s",
                 "h2d_bytes_per_step": int(h2d / max(1, max(m.Nt for m, _ in models))),

@@ -76,8 +76,8 @@ enum { MFD_F32 = 0, MFD_F64 = 1 };
  *   constant or kappa, the H/D/CPML/running-sum updates are fused multiply-adds and the
  *   Poynting norm uses the hardware reciprocal square root (single precision).  Results
  *   stay within relative L2 1e-5 (FP32) / 1e-12 (FP64) of the exact order; the material
- *   response (ADE, Kerr, plasma), sources and monitors keep the exact arithmetic.  Batch
- *   members must be MFD_MODE_EXACT. */
+ *   response (ADE, Kerr, plasma), sources and monitors keep the exact arithmetic.  A batch
+ *   takes members of either mode, each with its own arithmetic. */
 enum { MFD_MODE_EXACT = 0, MFD_MODE_FAST = 1 };
 
 /* ---- boundary conditions: the reference's bc2int codes (src/models.jl:1199-1217) ---- */
@@ -401,7 +401,7 @@ MFD_API int mfd_write_state(mfd_handle* h, const void* src, int64_t bytes);
  * the descriptor before anything is allocated, mfd_server_footprint) fits the budget next to
  * the admitted requests and fewer than max_active requests are computing, and uploads it.
  * 2-D (first field set, MFD_POL_HY) and small 3-D (at most 2^20 cells) single-precision
- * requests in MFD_MODE_EXACT with rho_fp64 and no TFSF recording join one running batch (mfd_batch_*), which takes new
+ * requests (either mode) with rho_fp64 and no TFSF recording join one running batch (mfd_batch_*), which takes new
  * members between its runs of steps (continuous batching); every other request runs as a
  * solo lane on its own host thread and stream, at most max_solo at a time.  A request that
  * waits only for a solo lane does not hold back batch requests behind it; one that waits for

@@ -21,7 +21,11 @@
 
 namespace mfd {
 
-enum { BF_MATH = 1, BF_MAT = 2, BF_FAST = 4, BF_3D = 8 };
+enum { BF_MATH = 1, BF_MAT = 2, BF_FAST = 4, BF_3D = 8, BF_RECIP = 16 };
+
+// The division mode of a member's cell code (mfd_device.cuh DIV_*): the tolerance mode's
+// reciprocal multiplies, else the verified constant division, else IEEE division.
+__device__ __forceinline__ int b_div(int flags) { return (flags & BF_RECIP) ? DIV_RECIP : (flags & BF_FAST) ? DIV_EXACT : DIV_IEEE; }
 
 // Per-member state (device).  Steps are 1-based; the member runs steps first..last.
 struct BMember {
@@ -107,11 +111,13 @@ __global__ void __launch_bounds__(512) batch_h2d_kernel(const BMember* __restric
         const HParams<float>& p = sp;
         const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
         if (ix >= p.L.nx || iz >= p.L.nz) continue;
-        switch (flags & (BF_MATH | BF_FAST)) {
-            case 0: h2d_cell<float, false, false>(p, acc, prev, ix, iz); break;
-            case BF_MATH: h2d_cell<float, true, false>(p, acc, prev, ix, iz); break;
-            case BF_FAST: h2d_cell<float, false, true>(p, acc, prev, ix, iz); break;
-            default: h2d_cell<float, true, true>(p, acc, prev, ix, iz); break;
+        switch ((flags & BF_MATH) | (b_div(flags) << 1)) {
+            case 0: h2d_cell<float, false, DIV_IEEE>(p, acc, prev, ix, iz); break;
+            case 1: h2d_cell<float, true, DIV_IEEE>(p, acc, prev, ix, iz); break;
+            case 2: h2d_cell<float, false, DIV_EXACT>(p, acc, prev, ix, iz); break;
+            case 3: h2d_cell<float, true, DIV_EXACT>(p, acc, prev, ix, iz); break;
+            case 4: h2d_cell<float, false, DIV_RECIP>(p, acc, prev, ix, iz); break;
+            default: h2d_cell<float, true, DIV_RECIP>(p, acc, prev, ix, iz); break;
         }
     }
 }
@@ -139,11 +145,13 @@ __global__ void __launch_bounds__(512) batch_e2d_kernel(const BMember* __restric
         const EParams<float, double>& p = sp;
         const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
         if (ix >= p.L.nx || iz >= p.L.nz) continue;
-        switch (flags & (BF_MAT | BF_FAST)) {
-            case 0: e2d_cell<float, double, false, false>(p, ix, iz); break;
-            case BF_MAT: e2d_cell<float, double, true, false>(p, ix, iz); break;
-            case BF_FAST: e2d_cell<float, double, false, true>(p, ix, iz); break;
-            default: e2d_cell<float, double, true, true>(p, ix, iz); break;
+        switch ((flags & BF_MAT ? 1 : 0) | (b_div(flags) << 1)) {
+            case 0: e2d_cell<float, double, false, DIV_IEEE>(p, ix, iz); break;
+            case 1: e2d_cell<float, double, true, DIV_IEEE>(p, ix, iz); break;
+            case 2: e2d_cell<float, double, false, DIV_EXACT>(p, ix, iz); break;
+            case 3: e2d_cell<float, double, true, DIV_EXACT>(p, ix, iz); break;
+            case 4: e2d_cell<float, double, false, DIV_RECIP>(p, ix, iz); break;
+            default: e2d_cell<float, double, true, DIV_RECIP>(p, ix, iz); break;
         }
     }
 }
@@ -202,7 +210,7 @@ __device__ __forceinline__ bool b_cell3(const Layout& L, const BTile& tl, int& i
 
 
 // The running sums of the previous step are added from a member's second step on.
-template <bool MATH, bool FAST>
+template <bool MATH, int FAST>
 __device__ __forceinline__ void b_h3d_p(const HParams<float>& p, const Div3& d3, long long it, long long first, int ix, int iy,
                                         int iz) {
     if (it == first) h3d_cell<float, MATH, FAST, false, false>(p, d3, it - 1, ix, iy, iz);
@@ -237,11 +245,13 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_h3d_kernel(const BMem
         const Div3& d3 = sd3;
         int ix, iy, iz;
         if (!b_cell3(p.L, tl, ix, iy, iz)) continue;
-        switch (flags & (BF_MATH | BF_FAST)) {
-            case 0: b_h3d_p<false, false>(p, d3, it, first, ix, iy, iz); break;
-            case BF_MATH: b_h3d_p<true, false>(p, d3, it, first, ix, iy, iz); break;
-            case BF_FAST: b_h3d_p<false, true>(p, d3, it, first, ix, iy, iz); break;
-            default: b_h3d_p<true, true>(p, d3, it, first, ix, iy, iz); break;
+        switch ((flags & BF_MATH) | (b_div(flags) << 1)) {
+            case 0: b_h3d_p<false, DIV_IEEE>(p, d3, it, first, ix, iy, iz); break;
+            case 1: b_h3d_p<true, DIV_IEEE>(p, d3, it, first, ix, iy, iz); break;
+            case 2: b_h3d_p<false, DIV_EXACT>(p, d3, it, first, ix, iy, iz); break;
+            case 3: b_h3d_p<true, DIV_EXACT>(p, d3, it, first, ix, iy, iz); break;
+            case 4: b_h3d_p<false, DIV_RECIP>(p, d3, it, first, ix, iy, iz); break;
+            default: b_h3d_p<true, DIV_RECIP>(p, d3, it, first, ix, iy, iz); break;
         }
     }
 }
@@ -272,11 +282,13 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_e3d_kernel(const BMem
         const Div3& d3 = sd3;
         int ix, iy, iz;
         if (!b_cell3(p.L, tl, ix, iy, iz)) continue;
-        switch (flags & (BF_MAT | BF_FAST)) {
-            case 0: e3d_cell<float, double, false, false>(p, d3, ix, iy, iz); break;
-            case BF_MAT: e3d_cell<float, double, true, false>(p, d3, ix, iy, iz); break;
-            case BF_FAST: e3d_cell<float, double, false, true>(p, d3, ix, iy, iz); break;
-            default: e3d_cell<float, double, true, true>(p, d3, ix, iy, iz); break;
+        switch ((flags & BF_MAT ? 1 : 0) | (b_div(flags) << 1)) {
+            case 0: e3d_cell<float, double, false, DIV_IEEE>(p, d3, ix, iy, iz); break;
+            case 1: e3d_cell<float, double, true, DIV_IEEE>(p, d3, ix, iy, iz); break;
+            case 2: e3d_cell<float, double, false, DIV_EXACT>(p, d3, ix, iy, iz); break;
+            case 3: e3d_cell<float, double, true, DIV_EXACT>(p, d3, ix, iy, iz); break;
+            case 4: e3d_cell<float, double, false, DIV_RECIP>(p, d3, ix, iy, iz); break;
+            default: e3d_cell<float, double, true, DIV_RECIP>(p, d3, ix, iy, iz); break;
         }
     }
 }

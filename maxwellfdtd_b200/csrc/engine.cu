@@ -366,8 +366,8 @@ class Engine : public HandleBase {
     // concurrently with the core-row launch: within one half-step the launches write
     // disjoint cells and only read the other field (fork / join below).
     bool overlap = true;
-    cudaStream_t st_side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t st_side = nullptr, st_side2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
     cudaEvent_t ev_snap_ready[2] = {nullptr, nullptr}, ev_snap_free[2] = {nullptr, nullptr};
     RectParams<T> rec_p{};
     int rec_narr = 0;
@@ -434,6 +434,8 @@ class Engine : public HandleBase {
         if (st3) cudaStreamDestroy(st3);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (ev_join2) cudaEventDestroy(ev_join2);
+        if (st_side2) { cudaStreamSynchronize(st_side2); cudaStreamDestroy(st_side2); }
         if (st_side) cudaStreamDestroy(st_side);
         if (st) cudaStreamDestroy(st);
     }
@@ -740,8 +742,10 @@ class Engine : public HandleBase {
     void make_side_stream() {
         if (st_side) return;
         MFD_CK(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking));
+        MFD_CK(cudaStreamCreateWithFlags(&st_side2, cudaStreamNonBlocking));
         MFD_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         MFD_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        MFD_CK(cudaEventCreateWithFlags(&ev_join2, cudaEventDisableTiming));
     }
 
     // The split needs layers that do not overlap in any dimension; MFD_KERNEL3D=unsplit
@@ -1024,19 +1028,27 @@ class Engine : public HandleBase {
     // run: it reads only its points' own cells, and the sources write only theirs.
     bool monitors_apart_from_sources(const mfd_desc* d) const {
         if (d->nmon <= 0) return false;
-        std::vector<bool> mark((size_t)N, false);
+        long long lo = N, hi = -1;   // the monitored cells' index range: the marks cover only it
         for (int m = 0; m < d->nmon; ++m)
-            for (long long j = 0; j < d->mons[m].npts; ++j) mark[(size_t)d->mons[m].cells[j]] = true;
+            for (long long j = 0; j < d->mons[m].npts; ++j) {
+                lo = std::min(lo, (long long)d->mons[m].cells[j]);
+                hi = std::max(hi, (long long)d->mons[m].cells[j]);
+            }
+        if (hi < lo) return true;
+        std::vector<bool> mark((size_t)(hi - lo + 1), false);
+        for (int m = 0; m < d->nmon; ++m)
+            for (long long j = 0; j < d->mons[m].npts; ++j) mark[(size_t)(d->mons[m].cells[j] - lo)] = true;
+        auto marked = [&](long long c) { return c >= lo && c <= hi && mark[(size_t)(c - lo)]; };
         for (int i = 0; i < d->nsrc; ++i)
             for (long long j = 0; j < d->srcs[i].npts; ++j)
-                if (mark[(size_t)d->srcs[i].cells[j]]) return false;
+                if (marked(d->srcs[i].cells[j])) return false;
         if (tfsf)
             for (int i = 0; i < tfsf_p.n; ++i) {
                 const RectStmt& q = tfsf_p.s[i];
                 for (int z = q.z0; z <= q.z1; ++z)
                     for (int y = q.y0; y <= q.y1; ++y)
                         for (int x = q.x0; x <= q.x1; ++x)
-                            if (mark[(size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z)]) return false;
+                            if (marked((long long)x + (long long)nx * ((long long)y + (long long)ny * z))) return false;
             }
         return true;
     }
@@ -1127,14 +1139,20 @@ class Engine : public HandleBase {
 
     // Side-stream launches of a split update: fork() before the core launch, the side
     // launches on st_side, join() after them (the next work on st waits for both).
-    void fork() {
+    void fork(bool two = false) {
         MFD_CK(cudaEventRecord(ev_fork, st));
         MFD_CK(cudaStreamWaitEvent(st_side, ev_fork, 0));
+        if (two) MFD_CK(cudaStreamWaitEvent(st_side2, ev_fork, 0));
     }
-    void join() {
+    void join(bool two = false) {
         MFD_CK(cudaEventRecord(ev_join, st_side));
         MFD_CK(cudaStreamWaitEvent(st, ev_join, 0));
+        if (two) {
+            MFD_CK(cudaEventRecord(ev_join2, st_side2));
+            MFD_CK(cudaStreamWaitEvent(st, ev_join2, 0));
+        }
     }
+
 
     void collect_times() {
         for (auto& pe : pend) {
@@ -1199,9 +1217,10 @@ class Engine : public HandleBase {
     void launch_H_split(const HParams<T>& p) {
         kcount = 0;
         const int zn = sbox.zr - sbox.zl;
-        const bool ov = st_side && slab_rows && sbox.yr > sbox.yl && zn > 0;
+        const bool core = sbox.yr > sbox.yl && zn > 0;
+        const bool ov = st_side && slab_rows && core;
         if (ov) fork();
-        if (sbox.yr > sbox.yl && zn > 0) {
+        if (core) {
             if constexpr (sizeof(T) == 4) {
                 if (core_async) {
                     prefer_shared((const void*)h3d_core_async_kernel<MATH, FAST, ACC, E2S>);
@@ -1237,10 +1256,10 @@ class Engine : public HandleBase {
     void launch_E_split(const EParams<T, R>& p, int cur) {
         kcount = 0;
         const int zn = sbox.zr - sbox.zl;
-        const bool ov = st_side && sbox.yr > sbox.yl && zn > 0;
-        const cudaStream_t ss = ov ? st_side : st;
-        if (ov) fork();
-        if (sbox.yr > sbox.yl && zn > 0) {
+        const bool core = sbox.yr > sbox.yl && zn > 0;
+        const bool ov = st_side && core;
+        if (ov) fork(true);
+        if (core) {
             // The staged E kernel has no material-map variant (compiled with the map it
             // measured slower than e3d_core_kernel: 0.239 vs 0.218 ms per E update at 256^3
             // with a dispersive sphere).  With a map, the staged kernel without it updates
@@ -1256,15 +1275,16 @@ class Engine : public HandleBase {
                     const bool all_mat = MAT && mat_x0 == 0 && mat_x1 >= nx && mat_rows.yl == sbox.yl && mat_rows.yr == sbox.yr &&
                                          mat_rows.zl == sbox.zl && mat_rows.zr == sbox.zr;   // nothing left for the staged kernel
                     dim3 blk(AS_TX, AS_TY), grd((nx + AS_TX - 1) / AS_TX, (sbox.yr - sbox.yl + AS_TY - 1) / AS_TY, (zn + async_zc - 1) / async_zc);
-                    // the material rows first, on the side stream: their few long-running
-                    // blocks then share the SMs with the staged kernel's
+                    // the material rows first, on their own side stream: their few
+                    // long-running blocks then share the SMs with the staged kernel's
                     if (MAT && mat_rows.yr > mat_rows.yl && mat_rows.zr > mat_rows.zl) {
                         SplitBox sm = mat_rows;
                         sm.zc = zc_mat;
                         dim3 blk2(bx3, by3), grd2((mat_x1 - mat_x0 + bx3 - 1) / bx3, (sm.yr - sm.yl + by3 - 1) / by3,
                                                   (sm.zr - sm.zl + zc_mat - 1) / zc_mat);
-                        if (resp_fused) e3d_core_kernel<T, R, MAT, FAST, true><<<grd2, blk2, 0, ss>>>(p, d3, sm, cur, mat_x0);
-                        else e3d_core_kernel<T, R, MAT, FAST><<<grd2, blk2, 0, ss>>>(p, d3, sm, 0, mat_x0);
+                        const cudaStream_t s2 = ov ? st_side2 : st;
+                        if (resp_fused) e3d_core_kernel<T, R, MAT, FAST, true><<<grd2, blk2, 0, s2>>>(p, d3, sm, cur, mat_x0);
+                        else e3d_core_kernel<T, R, MAT, FAST><<<grd2, blk2, 0, s2>>>(p, d3, sm, 0, mat_x0);
                         kcount++;
                     }
                     if (!all_mat) {
@@ -1282,10 +1302,10 @@ class Engine : public HandleBase {
         }
         if (slab_rows) {
             dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
-            e3d_slab_kernel<T, R, MAT, FAST><<<grd, 128, 0, ss>>>(p, d3, sbox);
+            e3d_slab_kernel<T, R, MAT, FAST><<<grd, 128, 0, ov ? st_side : st>>>(p, d3, sbox);
             kcount++;
         }
-        if (ov) join();
+        if (ov) join(true);
     }
 
     // single-kernel single-precision 3-D updates (CPML layers that overlap in a dimension)
@@ -2029,7 +2049,6 @@ struct mfd_batch {
         if (e->dev != dev) { err = "batch member on another device"; return MFD_ERR_INVALID; }
         if (e->in_batch) { err = "model already in a batch"; return MFD_ERR_INVALID; }
         if (e->record) { err = "batch members cannot record TFSF data"; return MFD_ERR_INVALID; }
-        if (e->recip) { err = "batch members run the exact arithmetic: create the model with MFD_MODE_EXACT"; return MFD_ERR_INVALID; }
         if (e->snap_next < e->snap_steps.size()) { err = "batch members cannot take field snapshots"; return MFD_ERR_INVALID; }
         if (e->bad_step) { err = "the model holds non-finite fields"; return MFD_ERR_NONFINITE; }
         if (last <= e->done || last > e->nt) { err = "the last step must be after the model's current step and within 1..Nt"; return MFD_ERR_INVALID; }
@@ -2038,7 +2057,8 @@ struct mfd_batch {
         MFD_CK(cudaSetDevice(dev));
         Member m{};
         m.h = h; m.e = e; m.first = e->done + 1; m.last = last; m.it = m.first;
-        m.flags = (e->math_needed ? BF_MATH : 0) | (e->any_geom ? BF_MAT : 0) | (e->fastdiv ? BF_FAST : 0) | (e->ndim == 3 ? BF_3D : 0);
+        m.flags = (e->math_needed ? BF_MATH : 0) | (e->any_geom ? BF_MAT : 0) | (e->fastdiv ? BF_FAST : 0) | (e->ndim == 3 ? BF_3D : 0) |
+                  (e->recip ? BF_RECIP : 0);
         m.cells = (long long)e->nx * e->ny * e->nz;
         try {
             m.hp = copy_struct(e->hparams(0, 0));

@@ -354,7 +354,7 @@ int mfd_server_submit(mfd_server* s, const mfd_desc* desc, int64_t* id) {
     const long long cells = (long long)desc->nx * desc->ny * desc->nz;
     r->batchable = ((desc->ndim == 2 && desc->polarization == MFD_POL_HY) ||
                     (desc->ndim == 3 && cells <= MFD_SERVER_BATCH_3D_CELLS)) && desc->dtype == MFD_F32 &&
-                   desc->rho_fp64 && !desc->tfsf_record && desc->mode == MFD_MODE_EXACT;
+                   desc->rho_fp64 && !desc->tfsf_record;
     std::lock_guard<std::mutex> lk(s->mu);
     if ((double)r->bytes > s->budget) {
         s->err = "submit: the request needs " + std::to_string(r->bytes) + " device bytes, more than the server's budget";

@@ -131,17 +131,43 @@ def test_fast_mode_plasma(oracle_lib, gpu_lib):
     _check(ref, got, np.float32, lambda: C.run_all(model, oracle_lib, np.float64))
 
 
-def test_batch_refuses_fast_members(gpu_lib):
-    model = C.model_vacuum(2)
-    b, _ = model.build_desc(np.float32, None, mode="fast")
-    st = _abi.Stepper(gpu_lib, b, np.float32)
+def test_batch_takes_fast_members(oracle_lib, gpu_lib):
+    """Tolerance-mode members in a batch, beside exact ones: a 2-D member equals its solo run
+    bit for bit (both run h2d_cell / e2d_cell); every member's fields and Sa are within the
+    bound of the exact-order oracle."""
+    import test_gpu_batch as TB
+
+    def make(model, mons, mode):
+        b, meta = model.build_desc(np.float32, mons, mode=mode)
+        return _abi.Stepper(gpu_lib, b, np.float32), b, meta
+
+    members = [(TB.member_model(s), "fast") for s in range(4)] + [(TB.member_model(7), "exact")] + \
+              [((C.model_materials(3), None), "fast"), ((C.model_bcs(3), None), "fast")]
+    solo = []
+    for (m, mo), mode in members[:5]:
+        st, b, meta = make(m, mo, mode)
+        st.run(1, m.Nt)
+        solo.append(TB.outputs_nd(st, m, meta))
+        st.close()
     batch = _abi.Batch(gpu_lib)
-    try:
-        with pytest.raises(_abi.StepperError) as ei:
-            batch.add(st, model.Nt)
-        assert ei.value.code == _abi.MFD_ERR_INVALID and "EXACT" in str(ei.value)
-    finally:
-        batch.close()
+    held = []
+    for (m, mo), mode in members:
+        st, b, meta = make(m, mo, mode)
+        batch.add(st, m.Nt)
+        held.append((st, b, meta, m))
+    batch.run_all(chunk=17)
+    got = [TB.outputs_nd(st, m, meta) for st, b, meta, m in held]
+    for r, g in zip(solo, got[:5]):
+        TB.same(r, g)
+    for ((m, mo), mode), g in zip(members, got):
+        ref = C.run_all(m, oracle_lib, np.float32)
+        for group in ("E", "D", "H"):
+            keys = [k for k in ref if k.startswith("field/" + group)]
+            e = _rel([ref[k] for k in keys], [g[k] for k in keys])
+            assert e <= TOL[np.float32], (group, e)
+        assert _rel([ref["Sa"]], [g["Sa"]]) <= TOL[np.float32]
+    batch.close()
+    for st, *_ in held:
         st.close()
 
 
