@@ -23,9 +23,12 @@ namespace mfd {
 
 enum { BF_MATH = 1, BF_MAT = 2, BF_FAST = 4, BF_3D = 8, BF_RECIP = 16 };
 
-// The division mode of a member's cell code (mfd_device.cuh DIV_*): the tolerance mode's
-// reciprocal multiplies, else the verified constant division, else IEEE division.
-__device__ __forceinline__ int b_div(int flags) { return (flags & BF_RECIP) ? DIV_RECIP : (flags & BF_FAST) ? DIV_EXACT : DIV_IEEE; }
+// The half-step kernels come in two sets: DSET 0 runs the members of the exact arithmetic
+// (IEEE or the verified constant division), DSET 1 those of the tolerance mode (reciprocal
+// multiplies), each launched only when the batch holds such members.  One kernel for both
+// measured slower: the extra cell code raised the 2-D E kernel from 32 to 40 registers.
+template <int DSET>
+__device__ __forceinline__ bool b_other_set(int flags) { return ((flags & BF_RECIP) != 0) != (DSET == 1); }
 
 // Per-member state (device).  Steps are 1-based; the member runs steps first..last.
 struct BMember {
@@ -84,9 +87,12 @@ __device__ __forceinline__ void b_stage(P* dst, const P* src) {
 
 
 #define MFD_B2D_CHUNK 4  // a block takes runs of this many consecutive tiles (fewer member changes)
+#define MFD_B2D_MINB 4   // batched 2-D updates of the exact set: 4 blocks of 512 threads per SM (32 registers; the
+                         // tolerance set takes 3 blocks: at 32 registers its E kernel spills)
 
 
-__global__ void __launch_bounds__(512) batch_h2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
+template <int DSET>
+__global__ void __launch_bounds__(512, DSET == 0 ? MFD_B2D_MINB : 3) batch_h2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
     __shared__ __align__(16) HParams<float> sp;
     const int n = *ntiles;
@@ -98,7 +104,7 @@ __global__ void __launch_bounds__(512) batch_h2d_kernel(const BMember* __restric
         if (t >= n) break;
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
-        if (!b_active(M)) continue;   // the same for the whole block
+        if (!b_active(M) || b_other_set<DSET>(M.flags)) continue;   // the same for the whole block
         const int acc = M.it > M.first ? 1 : 0;
         const long long prev = M.it - 1;
         const int flags = M.flags;
@@ -111,18 +117,22 @@ __global__ void __launch_bounds__(512) batch_h2d_kernel(const BMember* __restric
         const HParams<float>& p = sp;
         const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
         if (ix >= p.L.nx || iz >= p.L.nz) continue;
-        switch ((flags & BF_MATH) | (b_div(flags) << 1)) {
-            case 0: h2d_cell<float, false, DIV_IEEE>(p, acc, prev, ix, iz); break;
-            case 1: h2d_cell<float, true, DIV_IEEE>(p, acc, prev, ix, iz); break;
-            case 2: h2d_cell<float, false, DIV_EXACT>(p, acc, prev, ix, iz); break;
-            case 3: h2d_cell<float, true, DIV_EXACT>(p, acc, prev, ix, iz); break;
-            case 4: h2d_cell<float, false, DIV_RECIP>(p, acc, prev, ix, iz); break;
-            default: h2d_cell<float, true, DIV_RECIP>(p, acc, prev, ix, iz); break;
+        if constexpr (DSET == 1) {
+            if (flags & BF_MATH) h2d_cell<float, true, DIV_RECIP>(p, acc, prev, ix, iz);
+            else h2d_cell<float, false, DIV_RECIP>(p, acc, prev, ix, iz);
+        } else {
+            switch (flags & (BF_MATH | BF_FAST)) {
+                case 0: h2d_cell<float, false, DIV_IEEE>(p, acc, prev, ix, iz); break;
+                case BF_MATH: h2d_cell<float, true, DIV_IEEE>(p, acc, prev, ix, iz); break;
+                case BF_FAST: h2d_cell<float, false, DIV_EXACT>(p, acc, prev, ix, iz); break;
+                default: h2d_cell<float, true, DIV_EXACT>(p, acc, prev, ix, iz); break;
+            }
         }
     }
 }
 
-__global__ void __launch_bounds__(512) batch_e2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
+template <int DSET>
+__global__ void __launch_bounds__(512, DSET == 0 ? MFD_B2D_MINB : 3) batch_e2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
     __shared__ __align__(16) EParams<float, double> sp;
     const int n = *ntiles;
@@ -134,7 +144,7 @@ __global__ void __launch_bounds__(512) batch_e2d_kernel(const BMember* __restric
         if (t >= n) break;
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
-        if (!b_active(M)) continue;   // the same for the whole block
+        if (!b_active(M) || b_other_set<DSET>(M.flags)) continue;   // the same for the whole block
         const int flags = M.flags;
         if (tl.m != cur) {   // the block copies the member's parameters to shared memory (42.1 vs 40.8 Gcell/s)
             __syncthreads();
@@ -145,13 +155,16 @@ __global__ void __launch_bounds__(512) batch_e2d_kernel(const BMember* __restric
         const EParams<float, double>& p = sp;
         const int ix = tl.x0 + threadIdx.x, iz = tl.z0 + threadIdx.y;
         if (ix >= p.L.nx || iz >= p.L.nz) continue;
-        switch ((flags & BF_MAT ? 1 : 0) | (b_div(flags) << 1)) {
-            case 0: e2d_cell<float, double, false, DIV_IEEE>(p, ix, iz); break;
-            case 1: e2d_cell<float, double, true, DIV_IEEE>(p, ix, iz); break;
-            case 2: e2d_cell<float, double, false, DIV_EXACT>(p, ix, iz); break;
-            case 3: e2d_cell<float, double, true, DIV_EXACT>(p, ix, iz); break;
-            case 4: e2d_cell<float, double, false, DIV_RECIP>(p, ix, iz); break;
-            default: e2d_cell<float, double, true, DIV_RECIP>(p, ix, iz); break;
+        if constexpr (DSET == 1) {
+            if (flags & BF_MAT) e2d_cell<float, double, true, DIV_RECIP>(p, ix, iz);
+            else e2d_cell<float, double, false, DIV_RECIP>(p, ix, iz);
+        } else {
+            switch (flags & (BF_MAT | BF_FAST)) {
+                case 0: e2d_cell<float, double, false, DIV_IEEE>(p, ix, iz); break;
+                case BF_MAT: e2d_cell<float, double, true, DIV_IEEE>(p, ix, iz); break;
+                case BF_FAST: e2d_cell<float, double, false, DIV_EXACT>(p, ix, iz); break;
+                default: e2d_cell<float, double, true, DIV_EXACT>(p, ix, iz); break;
+            }
         }
     }
 }
@@ -218,6 +231,7 @@ __device__ __forceinline__ void b_h3d_p(const HParams<float>& p, const Div3& d3,
     else h3d_cell<float, MATH, FAST, true, false>(p, d3, it - 1, ix, iy, iz);
 }
 
+template <int DSET>
 __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_h3d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
     __shared__ __align__(16) HParams<float> sp;
@@ -231,7 +245,7 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_h3d_kernel(const BMem
         if (t >= n) break;
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
-        if (!b_active(M)) continue;   // the same for the whole block
+        if (!b_active(M) || b_other_set<DSET>(M.flags)) continue;   // the same for the whole block
         const long long it = M.it, first = M.first;
         const int flags = M.flags;
         if (tl.m != cur) {   // the block copies the member's parameters to shared memory
@@ -245,17 +259,21 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_h3d_kernel(const BMem
         const Div3& d3 = sd3;
         int ix, iy, iz;
         if (!b_cell3(p.L, tl, ix, iy, iz)) continue;
-        switch ((flags & BF_MATH) | (b_div(flags) << 1)) {
-            case 0: b_h3d_p<false, DIV_IEEE>(p, d3, it, first, ix, iy, iz); break;
-            case 1: b_h3d_p<true, DIV_IEEE>(p, d3, it, first, ix, iy, iz); break;
-            case 2: b_h3d_p<false, DIV_EXACT>(p, d3, it, first, ix, iy, iz); break;
-            case 3: b_h3d_p<true, DIV_EXACT>(p, d3, it, first, ix, iy, iz); break;
-            case 4: b_h3d_p<false, DIV_RECIP>(p, d3, it, first, ix, iy, iz); break;
-            default: b_h3d_p<true, DIV_RECIP>(p, d3, it, first, ix, iy, iz); break;
+        if constexpr (DSET == 1) {
+            if (flags & BF_MATH) b_h3d_p<true, DIV_RECIP>(p, d3, it, first, ix, iy, iz);
+            else b_h3d_p<false, DIV_RECIP>(p, d3, it, first, ix, iy, iz);
+        } else {
+            switch (flags & (BF_MATH | BF_FAST)) {
+                case 0: b_h3d_p<false, DIV_IEEE>(p, d3, it, first, ix, iy, iz); break;
+                case BF_MATH: b_h3d_p<true, DIV_IEEE>(p, d3, it, first, ix, iy, iz); break;
+                case BF_FAST: b_h3d_p<false, DIV_EXACT>(p, d3, it, first, ix, iy, iz); break;
+                default: b_h3d_p<true, DIV_EXACT>(p, d3, it, first, ix, iy, iz); break;
+            }
         }
     }
 }
 
+template <int DSET>
 __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_e3d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
     __shared__ __align__(16) EParams<float, double> sp;
@@ -269,7 +287,7 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_e3d_kernel(const BMem
         if (t >= n) break;
         const BTile tl = tiles[t];
         const BMember& M = mem[tl.m];
-        if (!b_active(M)) continue;   // the same for the whole block
+        if (!b_active(M) || b_other_set<DSET>(M.flags)) continue;   // the same for the whole block
         const int flags = M.flags;
         if (tl.m != cur) {   // the block copies the member's parameters to shared memory
             __syncthreads();
@@ -282,13 +300,16 @@ __global__ void __launch_bounds__(512, MFD_B3D_MINB) batch_e3d_kernel(const BMem
         const Div3& d3 = sd3;
         int ix, iy, iz;
         if (!b_cell3(p.L, tl, ix, iy, iz)) continue;
-        switch ((flags & BF_MAT ? 1 : 0) | (b_div(flags) << 1)) {
-            case 0: e3d_cell<float, double, false, DIV_IEEE>(p, d3, ix, iy, iz); break;
-            case 1: e3d_cell<float, double, true, DIV_IEEE>(p, d3, ix, iy, iz); break;
-            case 2: e3d_cell<float, double, false, DIV_EXACT>(p, d3, ix, iy, iz); break;
-            case 3: e3d_cell<float, double, true, DIV_EXACT>(p, d3, ix, iy, iz); break;
-            case 4: e3d_cell<float, double, false, DIV_RECIP>(p, d3, ix, iy, iz); break;
-            default: e3d_cell<float, double, true, DIV_RECIP>(p, d3, ix, iy, iz); break;
+        if constexpr (DSET == 1) {
+            if (flags & BF_MAT) e3d_cell<float, double, true, DIV_RECIP>(p, d3, ix, iy, iz);
+            else e3d_cell<float, double, false, DIV_RECIP>(p, d3, ix, iy, iz);
+        } else {
+            switch (flags & (BF_MAT | BF_FAST)) {
+                case 0: e3d_cell<float, double, false, DIV_IEEE>(p, d3, ix, iy, iz); break;
+                case BF_MAT: e3d_cell<float, double, true, DIV_IEEE>(p, d3, ix, iy, iz); break;
+                case BF_FAST: e3d_cell<float, double, false, DIV_EXACT>(p, d3, ix, iy, iz); break;
+                default: e3d_cell<float, double, true, DIV_EXACT>(p, d3, ix, iy, iz); break;
+            }
         }
     }
 }

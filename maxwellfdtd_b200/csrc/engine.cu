@@ -1982,6 +1982,7 @@ struct mfd_batch {
     // tiles, [5 + k] points of source pass k
     DevBuf<int> d_counts;
     int ntiles = 0, nmtiles = 0, nmpts = 0, ntiles3 = 0, nmtiles3 = 0;
+    bool has_set[2] = {false, false};   // members of the exact arithmetic / the tolerance mode
     std::vector<int> spass_n;
     // graph
     cudaGraphExec_t gexec = nullptr;
@@ -2087,9 +2088,11 @@ struct mfd_batch {
         std::vector<std::vector<BRow>> tpasses;
         std::vector<int> tlen;
         std::vector<BPoint> mpts;
+        has_set[0] = has_set[1] = false;
         for (size_t i = 0; i < mem.size(); ++i) {
             const Member& m = mem[i];
             E* e = m.e;
+            has_set[(m.flags & BF_RECIP) ? 1 : 0] = true;
             hm.push_back(BMember{m.hp, m.ep, m.mp, m.rp, m.it, m.first, m.last, e->ring_first, m.flags, 0, e->d3});
             const int mi = (int)i;
             const bool d3 = e->ndim == 3;
@@ -2185,21 +2188,36 @@ struct mfd_batch {
 
     void launch_step() {
         const dim3 blk(cur_tx, cur_tz);
-        if (ntiles) {
-            const int gt = grid_for((const void*)batch_h2d_kernel, cur_tx * cur_tz, ntiles);
-            batch_h2d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+        // the half-step kernels of each arithmetic set the batch holds (batch.cuh)
+        for (int set = 0; set < 2; ++set) {
+            if (!has_set[set]) continue;
+            if (ntiles) {
+                const void* k = set ? (const void*)batch_h2d_kernel<1> : (const void*)batch_h2d_kernel<0>;
+                const int gt = grid_for(k, cur_tx * cur_tz, ntiles);
+                if (set) batch_h2d_kernel<1><<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+                else batch_h2d_kernel<0><<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+            }
+            if (ntiles3) {
+                const void* k = set ? (const void*)batch_h3d_kernel<1> : (const void*)batch_h3d_kernel<0>;
+                const int gt = grid_for(k, cur_tx * cur_tz, ntiles3);
+                if (set) batch_h3d_kernel<1><<<gt, blk, 0, st>>>(d_mem.p, d_tiles3.p, d_counts.p + 3);
+                else batch_h3d_kernel<0><<<gt, blk, 0, st>>>(d_mem.p, d_tiles3.p, d_counts.p + 3);
+            }
         }
-        if (ntiles3) {
-            const int gt = grid_for((const void*)batch_h3d_kernel, cur_tx * cur_tz, ntiles3);
-            batch_h3d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles3.p, d_counts.p + 3);
-        }
-        if (ntiles) {
-            const int gt = grid_for((const void*)batch_e2d_kernel, cur_tx * cur_tz, ntiles);
-            batch_e2d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
-        }
-        if (ntiles3) {
-            const int gt = grid_for((const void*)batch_e3d_kernel, cur_tx * cur_tz, ntiles3);
-            batch_e3d_kernel<<<gt, blk, 0, st>>>(d_mem.p, d_tiles3.p, d_counts.p + 3);
+        for (int set = 0; set < 2; ++set) {
+            if (!has_set[set]) continue;
+            if (ntiles) {
+                const void* k = set ? (const void*)batch_e2d_kernel<1> : (const void*)batch_e2d_kernel<0>;
+                const int gt = grid_for(k, cur_tx * cur_tz, ntiles);
+                if (set) batch_e2d_kernel<1><<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+                else batch_e2d_kernel<0><<<gt, blk, 0, st>>>(d_mem.p, d_tiles.p, d_counts.p + 0);
+            }
+            if (ntiles3) {
+                const void* k = set ? (const void*)batch_e3d_kernel<1> : (const void*)batch_e3d_kernel<0>;
+                const int gt = grid_for(k, cur_tx * cur_tz, ntiles3);
+                if (set) batch_e3d_kernel<1><<<gt, blk, 0, st>>>(d_mem.p, d_tiles3.p, d_counts.p + 3);
+                else batch_e3d_kernel<0><<<gt, blk, 0, st>>>(d_mem.p, d_tiles3.p, d_counts.p + 3);
+            }
         }
         if (nmtiles) {
             const int g = grid_for((const void*)batch_material2d_kernel, 128, nmtiles);

@@ -185,7 +185,10 @@ class Server:
         self.peak_active = 0
 
     # -- lanes ---------------------------------------------------------------------------
-    def _finish(self, req, st):
+    def _finish(self, req, st, solo=False):
+        """Reads a finished request and gives its memory, slot and (solo=True) its lane back,
+        all in one critical section, so admission never sees a lane free while its request
+        still counts as active."""
         req.t_ran = time.time()
         try:
             if self.keep_results:
@@ -199,6 +202,8 @@ class Server:
             req.t_done = time.time()
             self.used -= req.bytes
             self.active -= 1
+            if solo:
+                self.solo -= 1
             self.done.append(req)
             if req.error is not None:
                 self.errors.append(req)
@@ -222,9 +227,7 @@ class Server:
                 self.errors.append(req)
                 self.wake.notify_all()
             return
-        with self.lock:
-            self.solo -= 1
-        self._finish(req, st)
+        self._finish(req, st, solo=True)
 
     def _batch_loop(self):
         """The batch's own thread: adds newly admitted members between graph replays
