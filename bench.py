@@ -495,7 +495,7 @@ def run_serve(args):
     ws, rank, local = dist_setup()
     lib = M.load_library()
     stream = workloads.served(n=args.requests, rate=args.rate, seed=args.seed, steps_scale=args.steps_scale)
-    reqs = [serve.Request(i, m, mo, a) for i, (a, m, mo) in enumerate(stream)]   # client-side descriptors
+    reqs = [serve.Request(i, m, mo, a, mode=args.mode) for i, (a, m, mo) in enumerate(stream)]   # client-side descriptors
     # warm-up: two small requests alone (loads the kernels)
     for _, m, mo in workloads.served(n=2, seed=args.seed + 7, steps_scale=0.01, n2=(64, 96), n3=(24, 32)):
         serve.solve_alone(lib, serve.Request(-1, m, mo, 0.0))
@@ -525,6 +525,7 @@ def run_serve(args):
                                f"64-256 (dx=10nm), 500-5000 steps x {args.steps_scale}, dielectric/Drude/Lorentz, "
                                f"TFSF or soft plane source, spectral monitor 8-32 freq FP64",
                    "budget_gb": args.budget_gb, "slots": args.slots, "solo_lanes": args.solo_lanes, "seed": args.seed,
+                   "mode": args.mode,
                    "parallelism": "one GPU: continuous batch of 2-D requests + concurrent solo lanes"},
         "latency": {"p50_s": round(stats["latency_p50_s"], 4), "p99_s": round(stats["latency_p99_s"], 4),
                     "queue_wait_p50_s": round(stats["queue_wait_p50_s"], 4),

@@ -111,19 +111,20 @@ def footprint(builder, model, dtype=np.float32):
 class Request:
     """One solve: model + monitors, its descriptor (built by the client), times and results."""
 
-    def __init__(self, rid, model, monitors, arrival, dtype=np.float32):
+    def __init__(self, rid, model, monitors, arrival, dtype=np.float32, mode="exact"):
         self.id = rid
         self.model = model
         self.monitors = monitors
         self.arrival = float(arrival)
         self.dtype = np.dtype(dtype)
-        self.builder, self.meta = model.build_desc(dtype, monitors)
+        self.builder, self.meta = model.build_desc(dtype, monitors, mode=mode)
         self.bytes = footprint(self.builder, model, dtype)
         g = model.grid
         self.cells = g.Nx * g.Ny * g.Nz
         self.cell_updates = self.cells * model.Nt
         d = self.builder.desc
-        small = g.ndim == 2 or (g.ndim == 3 and self.cells <= BATCH_3D_MAX_CELLS)
+        small = (g.ndim == 2 and getattr(model, "polarization", "Hy") == "Hy") or \
+            (g.ndim == 3 and self.cells <= BATCH_3D_MAX_CELLS)
         self.batchable = small and self.dtype == np.float32 and bool(d.rho_fp64) and not d.tfsf_record
         self.t_submit = self.t_admit = self.t_done = None
         self.t_created = self.t_ran = None       # upload finished, last step finished
