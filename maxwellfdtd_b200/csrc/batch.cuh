@@ -87,12 +87,12 @@ __device__ __forceinline__ void b_stage(P* dst, const P* src) {
 
 
 #define MFD_B2D_CHUNK 4  // a block takes runs of this many consecutive tiles (fewer member changes)
-#define MFD_B2D_MINB 4   // batched 2-D updates of the exact set: 4 blocks of 512 threads per SM (32 registers; the
-                         // tolerance set takes 3 blocks: at 32 registers its E kernel spills)
+#define MFD_B2D_MINB 4   // batched 2-D updates: 4 blocks of 512 threads per SM (32 registers; the tolerance set's E
+                         // kernel spills 36 bytes there, and still measured 43.9 against 41.4 Gcell/s at 3 blocks)
 
 
 template <int DSET>
-__global__ void __launch_bounds__(512, DSET == 0 ? MFD_B2D_MINB : 3) batch_h2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
+__global__ void __launch_bounds__(512, MFD_B2D_MINB) batch_h2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
     __shared__ __align__(16) HParams<float> sp;
     const int n = *ntiles;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(512, DSET == 0 ? MFD_B2D_MINB : 3) batch_h2d_k
 }
 
 template <int DSET>
-__global__ void __launch_bounds__(512, DSET == 0 ? MFD_B2D_MINB : 3) batch_e2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
+__global__ void __launch_bounds__(512, MFD_B2D_MINB) batch_e2d_kernel(const BMember* __restrict__ mem, const BTile* __restrict__ tiles,
                                                         const int* __restrict__ ntiles) {
     __shared__ __align__(16) EParams<float, double> sp;
     const int n = *ntiles;

@@ -2360,7 +2360,12 @@ extern "C" {
 
 int mfd_abi_version(void) { return MFD_ABI_VERSION; }
 
-int mfd_create(const mfd_desc* desc, mfd_handle** out) {
+}  // extern "C"
+
+// mfd_create with the split updates' side streams on or off (the server's lanes run several
+// models at once and leave them off: their streams would share the device's few hardware
+// queues with every other lane's).
+static int create_handle(const mfd_desc* desc, mfd_handle** out, bool overlap) {
     if (!out) return MFD_ERR_INVALID;
     *out = nullptr;
     int st = validate_desc(desc);
@@ -2376,14 +2381,17 @@ int mfd_create(const mfd_desc* desc, mfd_handle** out) {
     try {
         if (desc->dtype == MFD_F64) {
             auto e = std::make_unique<Engine<double, double>>();
+            e->overlap = overlap;
             e->init(desc);
             h->impl = std::move(e);
         } else if (desc->rho_fp64) {
             auto e = std::make_unique<Engine<float, double>>();
+            e->overlap = overlap;
             e->init(desc);
             h->impl = std::move(e);
         } else {
             auto e = std::make_unique<Engine<float, float>>();
+            e->overlap = overlap;
             e->init(desc);
             h->impl = std::move(e);
         }
@@ -2397,6 +2405,10 @@ int mfd_create(const mfd_desc* desc, mfd_handle** out) {
     *out = h.release();
     return MFD_OK;
 }
+
+extern "C" {
+
+int mfd_create(const mfd_desc* desc, mfd_handle** out) { return create_handle(desc, out, true); }
 
 void mfd_destroy(mfd_handle* h) { delete h; }
 

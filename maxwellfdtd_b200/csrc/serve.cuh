@@ -188,7 +188,7 @@ struct mfd_server {
 
     void solo_lane(Req* r) {
         mfd_handle* h = nullptr;
-        int rc = mfd_create(&r->desc, &h);
+        int rc = create_handle(&r->desc, &h, false);
         std::string msg;
         if (rc != MFD_OK) msg = mfd_create_error();
         {
@@ -259,7 +259,7 @@ struct mfd_server {
         if (r->batchable && use_batch) {
             lk.unlock();
             mfd_handle* h = nullptr;
-            const int rc = mfd_create(&r->desc, &h);
+            const int rc = create_handle(&r->desc, &h, false);
             const std::string msg = rc == MFD_OK ? "" : mfd_create_error();
             lk.lock();
             r->h = h;

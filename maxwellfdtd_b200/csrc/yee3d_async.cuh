@@ -53,9 +53,12 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 #define MFD_HASYNC_MINB (1024 / (32 * MFD_AS_TY))   // 1024 resident threads per SM (64 registers)
+// The tolerance mode's shorter cell code fits 10 blocks per SM (48 registers): 256^3 plasmonics
+// 42.2 against 41.9 Gcell/s; the exact code there lost more (37.1 against 40.1), so it keeps 8.
+#define MFD_ASYNC_MINB_RECIP 10
 
 template <bool MATH, int FAST, bool ACC, bool E2S>
-__global__ void __launch_bounds__(AS_TX * AS_TY, MFD_HASYNC_MINB) h3d_core_async_kernel(const __grid_constant__ HParams<float> p,
+__global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_MINB_RECIP : MFD_HASYNC_MINB) h3d_core_async_kernel(const __grid_constant__ HParams<float> p,
                                                                         const Div3 D3, const SplitBox s) {
     __shared__ __align__(16) HAStage S[AS_NST];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AS_TX * ty;
@@ -244,7 +247,7 @@ constexpr int EA_NST = 5, EA_AHEAD = EA_NST - 3;   // the copy issued at plane i
 // skip: the tiles of the materials' columns, rows and planes, left to another kernel (the
 // register march with the material map).
 template <typename R, bool MAT, int FAST>
-__global__ void __launch_bounds__(AS_TX * AS_TY, MFD_EASYNC_MINB) e3d_core_async_kernel(const __grid_constant__ EParams<float, R> p,
+__global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_MINB_RECIP : MFD_EASYNC_MINB) e3d_core_async_kernel(const __grid_constant__ EParams<float, R> p,
                                                                         const Div3 D3, const SplitBox s, const TileSkip skip) {
     __shared__ __align__(16) EAStage S[EA_NST];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AS_TX * ty;
