@@ -559,11 +559,11 @@ def _fields(st, ndim):
     return {c: st.read_field(comp_index(c)) for c in field_components(ndim) if not c.startswith("D")}
 
 
-def _timed_solve(lib, model, mons, dtype, W, K, local, profile_steps=0):
+def _timed_solve(lib, model, mons, dtype, W, K, local, profile_steps=0, mode="exact"):
     """Warm-up W steps, then steps W+1..W+K in one timed call, then profile_steps more with
     per-launch events; returns (stepper, ms, meta, per-kernel ms per step)."""
     from maxwellfdtd_b200 import _abi
-    b, meta = model.build_desc(dtype, mons, device=local)
+    b, meta = model.build_desc(dtype, mons, device=local, mode=mode)
     st = _abi.Stepper(lib, b, dtype)
     st.run(1, W)
     st.run(W + 1, W + K)
@@ -604,7 +604,7 @@ def run_config(args):
         K = model.Nt - W - 20
         clk = ClockSampler(local).start()
         t0 = time.time()
-        st, ms, meta, per = _timed_solve(lib, model, mons, dtype, W, K, local, profile_steps=20)
+        st, ms, meta, per = _timed_solve(lib, model, mons, dtype, W, K, local, profile_steps=20, mode=args.mode)
         clk.mark(t0, time.time())
         clk.stop()
         gpu = _fields(st, 3)
@@ -621,7 +621,7 @@ def run_config(args):
         so.close()
         err = {c: _rel_l2(gpu[c], ref[c]) for c in gpu}
         err["monitor_Ex"] = _rel_l2(gpu_mon, ref_mon)
-        err_note = "full configuration, all 1000 steps, FP64 GPU vs FP64 oracle"
+        err_note = f"full configuration, all 1000 steps, FP64 GPU ({args.mode} mode) vs FP64 oracle"
         wl = "dielectric100: 100^3 FP64, dx=20nm, 10-cell CPML, sphere r=500nm eps=2.25, TFSF 800nm/10fs from a vacuum record run, 1000 steps"
         cpu = {"value": round(model.grid.Nx * model.grid.Ny * model.grid.Nz * model.Nt / cpu_s / 1e9, 5),
                "unit": "Gcell-updates/s", "cores": int(threads), "kind": "port", "sample": f"all {model.Nt} steps ({cpu_s:.1f} s)"}
@@ -631,7 +631,7 @@ def run_config(args):
         model, mons = workloads.nonlinear_192(nt=W + K + 22)
         clk = ClockSampler(local).start()
         t0 = time.time()
-        st, ms, meta, per = _timed_solve(lib, model, mons, dtype, W, K, local, profile_steps=20)
+        st, ms, meta, per = _timed_solve(lib, model, mons, dtype, W, K, local, profile_steps=20, mode=args.mode)
         clk.mark(t0, time.time())
         clk.stop()
         st.close()
@@ -641,7 +641,7 @@ def run_config(args):
         out = {}
         cpu_s = None
         for tag, lib_, dt_ in (("gpu", lib, np.float32), ("fp64", oracle, np.float64), ("fp32", oracle, np.float32)):
-            b, meta = small.build_desc(dt_, None)
+            b, meta = small.build_desc(dt_, None, mode=args.mode if tag == "gpu" else "exact")
             sx = _abi.Stepper(lib_, b, dt_)
             t = time.perf_counter()
             sx.run(1, small.Nt)
@@ -654,7 +654,8 @@ def run_config(args):
         err = {g: _rel_l2(vec(out["gpu"], cs), vec(out["fp64"], cs)) for g, cs in groups.items()}
         err["oracle_fp32_vs_fp64"] = {g: _rel_l2(vec(out["fp32"], cs), vec(out["fp64"], cs)) for g, cs in groups.items()}
         err["gpu_vs_fp32_oracle"] = {g: _rel_l2(vec(out["gpu"], cs), vec(out["fp32"], cs)) for g, cs in groups.items()}
-        err_note = f"{n_small[0]}x{n_small[1]}x{n_small[2]} grid of the same configuration, {steps_small} steps, FP32 GPU (rho FP64) vs FP64 oracle"
+        err_note = (f"{n_small[0]}x{n_small[1]}x{n_small[2]} grid of the same configuration, {steps_small} steps, "
+                    f"FP32 GPU ({args.mode} mode, rho FP64) vs FP64 oracle")
         wl = ("nonlinear: 192x192x1024 FP32, dx=dy=100nm dz=20nm, 16-cell CPML, glass: 3 Sellmeier Lorentz poles + Kerr "
               "n2=2.5e-20 + 8-photon plasma (rho FP64), Gaussian beam w0=3um 800nm 30fs 5e17 W/m^2")
         Ns = n_small[0] * n_small[1] * n_small[2]
@@ -667,7 +668,7 @@ def run_config(args):
     out = {"metric": "Gcell-updates/s", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": 1, "steps": K,
            "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64" if dtype == np.float64 else "f32", "data": "synthetic",
-           "config": {"workload": wl, "grid": [model.grid.Nx, model.grid.Ny, model.grid.Nz], "cells": N},
+           "config": {"workload": wl, "grid": [model.grid.Nx, model.grid.Ny, model.grid.Nz], "cells": N, "mode": args.mode},
            "roofline": {"bound": "hbm", "kernel": "whole step (H + E updates, material response, sources, monitors)",
                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                         "traffic": None, "algorithmic_bytes_per_step": int(h_bytes + e_bytes), "peak_kind": kind},
