@@ -398,6 +398,16 @@ class Engine : public HandleBase {
     // planes per block of the material-row E launch: one (more, shorter-lived blocks beside
     // the staged kernel's; 256^3 plasmonics: E 0.193 ms per update against 0.198 at 4)
     int zc_mat = 1;
+    // The y- and z-layer cells of the single-precision split updates go through the staged
+    // kernels (LAY 1 / 2) instead of the one-cell-per-thread slab kernels: in the tolerance
+    // mode, for the H update (256^3 plasmonics: 43.5 against 42.5 Gcell/s with both updates
+    // layered; the exact mode's layer code needs 80 registers and measured slower, 38.0
+    // against 40.2).
+    bool lay_H = true, lay_E = true;
+    // planes per block of a z-layer launch (12-plane layers at 256^3 plasmonics: 6 gave 43.9,
+    // 4 gave 43.4-43.5, 12 gave 42.2 Gcell/s)
+    int zc_lay = 6;
+    bool mat_in_layers = false;       // some material cell lies in a y or z layer
     // single-precision 3-D updates split into core rows and CPML slabs (yee3d_split.cuh)
     bool use_split = false;
     SplitBox sbox{};
@@ -775,6 +785,7 @@ class Engine : public HandleBase {
             if (m.by0 < yl || m.by0 + m.bny > yr || m.bz0 < zl || m.bz0 + m.bnz > zr) resp_fused = false;
         }
         mat_rows = SplitBox{0, 0, 0, 0, async_zc, 0};
+        mat_in_layers = mbox[1] >= mbox[0] && (mbox[2] < yl || mbox[3] >= yr || mbox[4] < zl || mbox[5] >= zr);
         if (mbox[1] >= mbox[0]) {
             const int y0 = std::max(mbox[2], yl), y1 = std::min(mbox[3] + 1, yr);
             const int z0 = std::max(mbox[4], zl), z1 = std::min(mbox[5] + 1, zr);
@@ -1218,8 +1229,11 @@ class Engine : public HandleBase {
         kcount = 0;
         const int zn = sbox.zr - sbox.zl;
         const bool core = sbox.yr > sbox.yl && zn > 0;
+        const bool lay = sizeof(T) == 4 && core_async && lay_H && recip && core && slab_rows;
         const bool ov = st_side && slab_rows && core;
-        if (ov) fork();
+        if (ov) fork(lay);
+        if constexpr (sizeof(T) == 4)
+            if (lay) launch_H_layers<MATH, FAST, ACC, E2S>(p, ov ? st_side : st, ov ? st_side2 : st);
         if (core) {
             if constexpr (sizeof(T) == 4) {
                 if (core_async) {
@@ -1237,12 +1251,38 @@ class Engine : public HandleBase {
                 kcount++;
             }
         }
-        if (slab_rows) {
+        if (slab_rows && !lay) {
             dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
             h3d_slab_kernel<T, MATH, FAST, ACC, E2S><<<grd, 128, 0, ov ? st_side : st>>>(p, d3, sbox);
             kcount++;
         }
-        if (ov) join();
+        if (ov) join(lay);
+    }
+
+    // The y-layer rows over the core planes (LAY 1, on sy_) and the z-layer planes (LAY 2,
+    // every row, on sz_) of a single-precision H update, by the staged kernel.
+    template <bool MATH, int FAST, bool ACC, bool E2S>
+    void launch_H_layers(const HParams<float>& p, cudaStream_t sy_, cudaStream_t sz_) {
+        const dim3 blk(AS_TX, AS_TY);
+        const int zn = sbox.zr - sbox.zl;
+        for (int side = 0; side < 2; ++side) {
+            const int ya = side ? sbox.yr : 0, yb = side ? ny : sbox.yl;
+            if (yb <= ya || zn <= 0) continue;
+            prefer_shared((const void*)h3d_core_async_kernel<MATH, FAST, ACC, E2S, 1>);
+            const SplitBox sl{ya, yb, sbox.zl, sbox.zr, async_zc, 0};
+            const dim3 grd((nx + AS_TX - 1) / AS_TX, (yb - ya + AS_TY - 1) / AS_TY, (zn + async_zc - 1) / async_zc);
+            h3d_core_async_kernel<MATH, FAST, ACC, E2S, 1><<<grd, blk, 0, sy_>>>(p, d3, sl);
+            kcount++;
+        }
+        for (int side = 0; side < 2; ++side) {
+            const int za = side ? sbox.zr : 0, zb = side ? nz : sbox.zl;
+            if (zb <= za) continue;
+            prefer_shared((const void*)h3d_core_async_kernel<MATH, FAST, ACC, E2S, 2>);
+            const SplitBox sl{0, ny, za, zb, zc_lay, 0};
+            const dim3 grd((nx + AS_TX - 1) / AS_TX, (ny + AS_TY - 1) / AS_TY, (zb - za + zc_lay - 1) / zc_lay);
+            h3d_core_async_kernel<MATH, FAST, ACC, E2S, 2><<<grd, blk, 0, sz_>>>(p, d3, sl);
+            kcount++;
+        }
     }
 
     template <bool MATH, int FAST>
@@ -1300,12 +1340,47 @@ class Engine : public HandleBase {
                 kcount++;
             }
         }
-        if (slab_rows) {
+        const bool lay = sizeof(T) == 4 && core_async && lay_E && recip && core && slab_rows;
+        if constexpr (sizeof(T) == 4) {
+            if (lay) {
+                if (MAT && mat_in_layers) launch_E_layers<true, FAST>(p, ov ? st_side : st, ov ? st_side2 : st);
+                else launch_E_layers<false, FAST>(p, ov ? st_side : st, ov ? st_side2 : st);
+            }
+        }
+        if (slab_rows && !lay) {
             dim3 grd((unsigned)slab_rows, (nx + 127) / 128);
             e3d_slab_kernel<T, R, MAT, FAST><<<grd, 128, 0, ov ? st_side : st>>>(p, d3, sbox);
             kcount++;
         }
         if (ov) join(true);
+    }
+
+    // The y-layer rows over the core planes (LAY 1, on sy_) and the z-layer planes (LAY 2, on
+    // sz_) of a single-precision E update, by the staged kernel; MAT when a material cell lies
+    // in a layer.
+    template <bool MAT, int FAST>
+    void launch_E_layers(const EParams<float, R>& p, cudaStream_t sy_, cudaStream_t sz_) {
+        const dim3 blk(AS_TX, AS_TY);
+        const TileSkip none{0, 0, 0, 0, 0, 0};
+        const int zn = sbox.zr - sbox.zl;
+        for (int side = 0; side < 2; ++side) {
+            const int ya = side ? sbox.yr : 0, yb = side ? ny : sbox.yl;
+            if (yb <= ya || zn <= 0) continue;
+            prefer_shared((const void*)e3d_core_async_kernel<R, MAT, FAST, 1>);
+            const SplitBox sl{ya, yb, sbox.zl, sbox.zr, async_zc, 0};
+            const dim3 grd((nx + AS_TX - 1) / AS_TX, (yb - ya + AS_TY - 1) / AS_TY, (zn + async_zc - 1) / async_zc);
+            e3d_core_async_kernel<R, MAT, FAST, 1><<<grd, blk, 0, sy_>>>(p, d3, sl, none);
+            kcount++;
+        }
+        for (int side = 0; side < 2; ++side) {
+            const int za = side ? sbox.zr : 0, zb = side ? nz : sbox.zl;
+            if (zb <= za) continue;
+            prefer_shared((const void*)e3d_core_async_kernel<R, MAT, FAST, 2>);
+            const SplitBox sl{0, ny, za, zb, zc_lay, 0};
+            const dim3 grd((nx + AS_TX - 1) / AS_TX, (ny + AS_TY - 1) / AS_TY, (zb - za + zc_lay - 1) / zc_lay);
+            e3d_core_async_kernel<R, MAT, FAST, 2><<<grd, blk, 0, sz_>>>(p, d3, sl, none);
+            kcount++;
+        }
     }
 
     // single-kernel single-precision 3-D updates (CPML layers that overlap in a dimension)

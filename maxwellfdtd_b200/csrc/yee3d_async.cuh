@@ -56,10 +56,18 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // The tolerance mode's shorter cell code fits 10 blocks per SM (48 registers): 256^3 plasmonics
 // 42.2 against 41.9 Gcell/s; the exact code there lost more (37.1 against 40.1), so it keeps 8.
 #define MFD_ASYNC_MINB_RECIP 10
+// The layer launches' exact-mode cell code (x, y and z faces) spills at 64 registers: 6 blocks.
+#define MFD_ASYNC_MINB_LAY 6
 
-template <bool MATH, int FAST, bool ACC, bool E2S>
-__global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_MINB_RECIP : MFD_HASYNC_MINB) h3d_core_async_kernel(const __grid_constant__ HParams<float> p,
-                                                                        const Div3 D3, const SplitBox s) {
+// LAY: 0 the core rows; 1 the rows of the y layers over the core planes (s.yl .. s.yr is
+// one y layer's rows); 2 the planes of one z layer (s.zl .. s.zr), every row.  A thread's row
+// keeps its y face along the march and a plane's z face holds for the whole block, so a layer
+// cell costs its psi pair (prefetched with the next plane like the x face's) and a few flops,
+// in the CPML slab kernels' face order (x, y, z).
+template <bool MATH, int FAST, bool ACC, bool E2S, int LAY = 0>
+__global__ void __launch_bounds__(AS_TX * AS_TY, LAY ? (FAST == DIV_RECIP ? MFD_HASYNC_MINB : MFD_ASYNC_MINB_LAY)
+                                                      : (FAST == DIV_RECIP ? MFD_ASYNC_MINB_RECIP : MFD_HASYNC_MINB))
+    h3d_core_async_kernel(const __grid_constant__ HParams<float> p, const Div3 D3, const SplitBox s) {
     __shared__ __align__(16) HAStage S[AS_NST];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AS_TX * ty;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -129,11 +137,24 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_M
     // the next plane's material index and x-layer psi pair, prefetched in registers
     int g_next = (MATH && act) ? (int)p.geom[c] : 0;
     float pa_next = xin ? X.pa[k] : 0.0f, pb_next = xin ? X.pb[k] : 0.0f;
+    // the row's y face (LAY >= 1) and the planes' z face (LAY 2)
+    const XCol<float> Y = LAY ? xcol<float>(p.lay[MFD_YL], p.lay[MFD_YR], act ? iy : 0, 2, 3) : XCol<float>{};
+    const bool yin = LAY && act && Y.in;
+    const int kystep = sy * Y.nb;
+    int ky = ix + sy * (Y.q + Y.nb * z0);
+    float ya_next = yin ? Y.pa[ky] : 0.0f, yb_next = yin ? Y.pb[ky] : 0.0f;
+    const bool zlo = p.lay[MFD_ZL].nb && z0 < p.lay[MFD_ZL].ib;
+    const LayerDev<float>& LZ = p.lay[zlo ? MFD_ZL : MFD_ZR];
+    const int zq0 = zlo ? 0 : LZ.ib - 1;   // plane iz is the layer's point iz - zq0
+    const bool zin = LAY == 2 && act;
+    int kz = ix + sy * (iy + ny * (z0 - zq0));
+    float za_next = zin ? LZ.psi[2][kz] : 0.0f, zb_next = zin ? LZ.psi[3][kz] : 0.0f;
 
     // Blocks away from the upper x and y faces, on planes below the last, need no boundary
     // condition and no activity test (a block-uniform choice of the code path).
     const bool inner_xy = x0 + AS_TX <= nx - 1 && y0 + AS_TY <= s.yr && y0 + AS_TY <= ny - 1;
-    auto cell = [&](auto inner_tag, const HAStage& A, const HAStage& Bn, int iz, int g, float cpa, float cpb) {
+    auto cell = [&](auto inner_tag, const HAStage& A, const HAStage& Bn, int iz, int g, float cpa, float cpb, float cya,
+                    float cyb, float cza, float czb) {
         constexpr bool IN = decltype(inner_tag)::value;
         const float ex = A.ex[ty][tx], ey = A.ey[ty][tx], ez = A.ez[ty][tx];
         float ey_xp, ez_xp, ex_yp, ez_yp, ex_zp, ey_zp;
@@ -188,7 +209,7 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_M
         const float num[6] = {ex_yp - ex, ex_zp - ex, ey_xp - ey, ey_zp - ey, ez_xp - ez, ez_yp - ez};
         float q[6];
         div6<FAST>(D3, num, q);
-        const float dExy = q[0], dExz = q[1], dEyz = q[3], dEzy = q[5];
+        float dExy = q[0], dExz = q[1], dEyz = q[3], dEzy = q[5];
         float dEyx = q[2], dEzx = q[4];
         if (xin) {   // cpml_h<+1> of the column's x face
             const float pa = mad<FAST>(X.B, cpa, X.A * dEyx);
@@ -199,6 +220,28 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_M
             hz = mad<FAST>(-Mh, pa, hz);
             dEyx = cdiv<FAST>(dEyx, X.K);
             dEzx = cdiv<FAST>(dEzx, X.K);
+        }
+        if (LAY && yin) {   // cpml_h<-1> of the row's y face
+            const float pa = mad<FAST>(Y.B, cya, Y.A * dExy);
+            const float pb = mad<FAST>(Y.B, cyb, Y.A * dEzy);
+            Y.pa[ky] = pa;
+            Y.pb[ky] = pb;
+            hx = mad<FAST>(-Mh, pb, hx);
+            hz = mad<FAST>(Mh, pa, hz);
+            dExy = cdiv<FAST>(dExy, Y.K);
+            dEzy = cdiv<FAST>(dEzy, Y.K);
+        }
+        if (LAY == 2) {   // cpml_h<+1> of the plane's z face
+            const int qz = iz - zq0;
+            const float B = LZ.B[qz], A = LZ.A[qz];
+            const float pa = mad<FAST>(B, cza, A * dExz);
+            const float pb = mad<FAST>(B, czb, A * dEyz);
+            LZ.psi[2][kz] = pa;
+            LZ.psi[3][kz] = pb;
+            hx = mad<FAST>(Mh, pb, hx);
+            hy = mad<FAST>(-Mh, pa, hy);
+            dExz = cdiv<FAST>(dExz, LZ.K[qz]);
+            dEyz = cdiv<FAST>(dEyz, LZ.K[qz]);
         }
         hx = mad<FAST>(-Mh, dEzy - dEyz, hx);
         hy = mad<FAST>(-Mh, dExz - dEzx, hy);
@@ -211,20 +254,28 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_M
 #pragma unroll
     for (int j = 0; j < AS_AHEAD; ++j) issue(z0 + j);
     int sc = z0 % AS_NST;   // stage of plane iz
-    for (int iz = z0; iz < z1; ++iz, c += sz, k += kstep) {
+    for (int iz = z0; iz < z1; ++iz, c += sz, k += kstep, ky += kystep, kz += sy * ny) {
         issue(iz + AS_AHEAD);
         const int g = g_next;
-        const float cpa = pa_next, cpb = pb_next;
+        const float cpa = pa_next, cpb = pb_next, cya = ya_next, cyb = yb_next, cza = za_next, czb = zb_next;
         if (iz + 1 < z1) {
             g_next = (MATH && act) ? (int)p.geom[c + sz] : 0;
             pa_next = xin ? X.pa[k + kstep] : 0.0f;
             pb_next = xin ? X.pb[k + kstep] : 0.0f;
+            if (LAY) {
+                ya_next = yin ? Y.pa[ky + kystep] : 0.0f;
+                yb_next = yin ? Y.pb[ky + kystep] : 0.0f;
+            }
+            if (LAY == 2) {
+                za_next = zin ? LZ.psi[2][kz + sy * ny] : 0.0f;
+                zb_next = zin ? LZ.psi[3][kz + sy * ny] : 0.0f;
+            }
         }
         const int sn = sc == AS_NST - 1 ? 0 : sc + 1;
         cp_async_wait<AS_AHEAD - 1>();   // this thread's copies of planes iz and iz+1 have landed
         __syncthreads();                 // ... and every other thread's
-        if (inner_xy && iz < nz - 1) cell(std::true_type{}, S[sc], S[sn], iz, g, cpa, cpb);
-        else if (act) cell(std::false_type{}, S[sc], S[sn], iz, g, cpa, cpb);
+        if (inner_xy && iz < nz - 1) cell(std::true_type{}, S[sc], S[sn], iz, g, cpa, cpb, cya, cyb, cza, czb);
+        else if (act) cell(std::false_type{}, S[sc], S[sn], iz, g, cpa, cpb, cya, cyb, cza, czb);
         sc = sn;
     }
     cp_async_wait<0>();
@@ -246,9 +297,11 @@ constexpr int EA_NST = 5, EA_AHEAD = EA_NST - 3;   // the copy issued at plane i
 
 // skip: the tiles of the materials' columns, rows and planes, left to another kernel (the
 // register march with the material map).
-template <typename R, bool MAT, int FAST>
-__global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_MINB_RECIP : MFD_EASYNC_MINB) e3d_core_async_kernel(const __grid_constant__ EParams<float, R> p,
-                                                                        const Div3 D3, const SplitBox s, const TileSkip skip) {
+// LAY as for h3d_core_async_kernel: the rows of a y layer (1) or the planes of a z layer (2).
+template <typename R, bool MAT, int FAST, int LAY = 0>
+__global__ void __launch_bounds__(AS_TX * AS_TY, LAY ? (FAST == DIV_RECIP ? MFD_EASYNC_MINB : MFD_ASYNC_MINB_LAY)
+                                                      : (FAST == DIV_RECIP ? MFD_ASYNC_MINB_RECIP : MFD_EASYNC_MINB))
+    e3d_core_async_kernel(const __grid_constant__ EParams<float, R> p, const Div3 D3, const SplitBox s, const TileSkip skip) {
     __shared__ __align__(16) EAStage S[EA_NST];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AS_TX * ty;
     const int nx = p.L.nx, ny = p.L.ny, nz = p.L.nz;
@@ -312,11 +365,24 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_M
     // the next plane's material index and x-layer psi pair, prefetched in registers
     int g_next = (MAT && act) ? (int)p.geom[c] : 0;
     float pa_next = xin ? X.pa[k] : 0.0f, pb_next = xin ? X.pb[k] : 0.0f;
+    // the row's y face (LAY >= 1) and the planes' z face (LAY 2)
+    const XCol<float> Y = LAY ? xcol<float>(p.lay[MFD_YL], p.lay[MFD_YR], act ? iy : 0, 0, 1) : XCol<float>{};
+    const bool yin = LAY && act && Y.in;
+    const int kystep = sy * Y.nb;
+    int ky = ix + sy * (Y.q + Y.nb * z0);
+    float ya_next = yin ? Y.pa[ky] : 0.0f, yb_next = yin ? Y.pb[ky] : 0.0f;
+    const bool zlo = p.lay[MFD_ZL].nb && z0 < p.lay[MFD_ZL].ib;
+    const LayerDev<float>& LZ = p.lay[zlo ? MFD_ZL : MFD_ZR];
+    const int zq0 = zlo ? 0 : LZ.ib - 1;   // plane iz is the layer's point iz - zq0
+    const bool zin = LAY == 2 && act;
+    int kz = ix + sy * (iy + ny * (z0 - zq0));
+    float za_next = zin ? LZ.psi[0][kz] : 0.0f, zb_next = zin ? LZ.psi[1][kz] : 0.0f;
 
     // Blocks away from the lower x and y faces (and the grid's x end), on planes above the
     // first, need no boundary condition and no activity test.
     const bool inner_xy = x0 > 0 && x0 + AS_TX <= nx && y0 > 0 && y0 + AS_TY <= s.yr;
-    auto cell = [&](auto inner_tag, const EAStage& A, const EAStage& P, int iz, int g, float cpa, float cpb) {
+    auto cell = [&](auto inner_tag, const EAStage& A, const EAStage& P, int iz, int g, float cpa, float cpb, float cya,
+                    float cyb, float cza, float czb) {
         constexpr bool IN = decltype(inner_tag)::value;
         const float hx = A.hx[ty + 1][tx + 4], hy = A.hy[ty + 1][tx + 4], hz = A.hz[ty + 1][tx + 4];
         float hy_xm, hz_xm, hx_ym, hz_ym, hx_zm, hy_zm;
@@ -362,7 +428,7 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_M
         const float num[6] = {hx - hx_ym, hx - hx_zm, hy - hy_xm, hy - hy_zm, hz - hz_xm, hz - hz_ym};
         float q[6];
         div6<FAST>(D3, num, q);
-        const float dHxy = q[0], dHxz = q[1], dHyz = q[3], dHzy = q[5];
+        float dHxy = q[0], dHxz = q[1], dHyz = q[3], dHzy = q[5];
         float dHyx = q[2], dHzx = q[4];
         float Md1 = Md10, Md2 = Md20, Me = Me0;
         bool simple = true;
@@ -381,6 +447,28 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_M
             dHyx = cdiv<FAST>(dHyx, X.K);
             dHzx = cdiv<FAST>(dHzx, X.K);
         }
+        if (LAY && yin) {   // cpml_e<+1> of the row's y face
+            const float pa = mad<FAST>(Y.B, cya, Y.A * dHxy);
+            const float pb = mad<FAST>(Y.B, cyb, Y.A * dHzy);
+            Y.pa[ky] = pa;
+            Y.pb[ky] = pb;
+            D0 = mad<FAST>(Md2, pb, D0);
+            D2 = mad<FAST>(-Md2, pa, D2);
+            dHxy = cdiv<FAST>(dHxy, Y.K);
+            dHzy = cdiv<FAST>(dHzy, Y.K);
+        }
+        if (LAY == 2) {   // cpml_e<-1> of the plane's z face
+            const int qz = iz - zq0;
+            const float B = LZ.B[qz], A = LZ.A[qz];
+            const float pa = mad<FAST>(B, cza, A * dHxz);
+            const float pb = mad<FAST>(B, czb, A * dHyz);
+            LZ.psi[0][kz] = pa;
+            LZ.psi[1][kz] = pb;
+            D0 = mad<FAST>(-Md2, pb, D0);
+            D1 = mad<FAST>(Md2, pa, D1);
+            dHxz = cdiv<FAST>(dHxz, LZ.K[qz]);
+            dHyz = cdiv<FAST>(dHyz, LZ.K[qz]);
+        }
         D0 = mad<FAST>(Md1, D0, Md2 * (dHzy - dHyz));
         D1 = mad<FAST>(Md1, D1, Md2 * (dHxz - dHzx));
         D2 = mad<FAST>(Md1, D2, Md2 * (dHyx - dHxy));
@@ -398,19 +486,27 @@ __global__ void __launch_bounds__(AS_TX * AS_TY, FAST == DIV_RECIP ? MFD_ASYNC_M
     for (int j = -1; j < EA_AHEAD; ++j) issue(z0 + j);
     int sc = z0 % EA_NST;                             // stage of plane iz
     int sp = sc == 0 ? EA_NST - 1 : sc - 1;           // ... of plane iz - 1
-    for (int iz = z0; iz < z1; ++iz, c += sz, k += kstep) {
+    for (int iz = z0; iz < z1; ++iz, c += sz, k += kstep, ky += kystep, kz += sy * ny) {
         issue(iz + EA_AHEAD);
         const int g = g_next;
-        const float cpa = pa_next, cpb = pb_next;
+        const float cpa = pa_next, cpb = pb_next, cya = ya_next, cyb = yb_next, cza = za_next, czb = zb_next;
         if (iz + 1 < z1) {
             g_next = (MAT && act) ? (int)p.geom[c + sz] : 0;
             pa_next = xin ? X.pa[k + kstep] : 0.0f;
             pb_next = xin ? X.pb[k + kstep] : 0.0f;
+            if (LAY) {
+                ya_next = yin ? Y.pa[ky + kystep] : 0.0f;
+                yb_next = yin ? Y.pb[ky + kystep] : 0.0f;
+            }
+            if (LAY == 2) {
+                za_next = zin ? LZ.psi[0][kz + sy * ny] : 0.0f;
+                zb_next = zin ? LZ.psi[1][kz + sy * ny] : 0.0f;
+            }
         }
         cp_async_wait<EA_AHEAD>();   // this thread's copies of planes up to iz have landed
         __syncthreads();             // ... and every other thread's
-        if (inner_xy && iz > 0) cell(std::true_type{}, S[sc], S[sp], iz, g, cpa, cpb);
-        else if (act) cell(std::false_type{}, S[sc], S[sp], iz, g, cpa, cpb);
+        if (inner_xy && iz > 0) cell(std::true_type{}, S[sc], S[sp], iz, g, cpa, cpb, cya, cyb, cza, czb);
+        else if (act) cell(std::false_type{}, S[sc], S[sp], iz, g, cpa, cpb, cya, cyb, cza, czb);
         sp = sc;
         sc = sc == EA_NST - 1 ? 0 : sc + 1;
     }
