@@ -751,8 +751,15 @@ class Engine : public HandleBase {
 
     void make_side_stream() {
         if (st_side) return;
-        MFD_CK(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking));
-        MFD_CK(cudaStreamCreateWithFlags(&st_side2, cudaStreamNonBlocking));
+        // The side streams take the device's highest priority: the block scheduler then
+        // places the slab, layer and material-row blocks ahead of the core-row launch's,
+        // whose many short blocks fill the SMs behind them (256^3 plasmonics: 44.4-44.5
+        // against 43.8 Gcell/s at the default priority, 43.4 with the core rows' stream
+        // first).
+        int pr_least = 0, pr_greatest = 0;
+        MFD_CK(cudaDeviceGetStreamPriorityRange(&pr_least, &pr_greatest));
+        MFD_CK(cudaStreamCreateWithPriority(&st_side, cudaStreamNonBlocking, pr_greatest));
+        MFD_CK(cudaStreamCreateWithPriority(&st_side2, cudaStreamNonBlocking, pr_greatest));
         MFD_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         MFD_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         MFD_CK(cudaEventCreateWithFlags(&ev_join2, cudaEventDisableTiming));
