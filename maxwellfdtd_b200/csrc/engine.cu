@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "aux.cuh"
+#include "dft_tc.cuh"
 #include "yee.cuh"
 #include "yee3d_async.cuh"
 #include "yee3d_split.cuh"
@@ -383,6 +384,12 @@ class Engine : public HandleBase {
     long long ring_first = 0;
     bool need_ring = false;
     bool mon_apart = false;     // no monitor cell is written by a source: gather beside them
+    // Tolerance mode, Float32: spectral monitors folded on the tensor cores (dft_tc.cuh)
+    bool tc_fold = false;
+    int tc_sms = 1;
+    double tc_bscale = 1.0;     // power of two bringing the factors 2 e^{-iwt} dt near 1
+    int* d_tcfault = nullptr;   // set by a fold whose tensor-core wait ran out
+    int h_tcfault = 0;
 
     int* d_flags = nullptr;     // [nt] per-step NaN/Inf flags of Ex
     int* h_flags = nullptr;     // host copy
@@ -1122,6 +1129,18 @@ class Engine : public HandleBase {
             if (a.kind == MFD_MON_SPECTRAL || M.sum) M.ring = dalloc<T>((size_t)ring_k * ncomp_mon * a.npts);
             mons_host.push_back(M);
         }
+        if constexpr (sizeof(T) == 4) {
+            bool spectral = false;
+            for (const MonDev<T>& M : mons_host) spectral |= M.kind == MFD_MON_SPECTRAL && !M.sum;
+            if (recip && spectral) {
+                tc_fold = true;
+                MFD_CK(cudaFuncSetAttribute(monitor_dft_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)dft_tc_smem_bytes));
+                MFD_CK(cudaDeviceGetAttribute(&tc_sms, cudaDevAttrMultiProcessorCount, dev));
+                tc_bscale = std::ldexp(1.0, -std::ilogb(2.0 * (double)dt));
+                d_tcfault = dalloc<int>(1, false);
+            }
+        }
         mons_dev = upload(mons_host.data(), mons_host.size());
         mon_p.nmon = (int)mons_host.size();
         mon_p.ncomp = ncomp_mon;
@@ -1570,6 +1589,12 @@ class Engine : public HandleBase {
         }
     }
 
+    // A tensor-core fold whose completion wait ran out leaves its spectra incomplete.
+    void check_fold() const {
+        if (tc_fold && h_tcfault)
+            throw Error(MFD_ERR_TIMEOUT, "a spectral monitor's tensor-core fold did not complete within its wait limit");
+    }
+
     void flush_monitors() {
         if (!need_ring || ring_used == 0) return;
         const double dtd = (double)dt;
@@ -1580,6 +1605,19 @@ class Engine : public HandleBase {
                 launch(KC_DFT, [&] {
                     monitor_fieldsum_kernel<T><<<dim3(ncomp_mon, ring_used), 256, 0, st>>>(md, ncomp_mon, nt, ring_first);
                 });
+            } else if (M.kind == MFD_MON_SPECTRAL && !M.sum && tc_fold) {
+                if constexpr (sizeof(T) == 4) {
+                    launch(KC_DFT, [&] {
+                        // persistent: two blocks per SM, G blocks per frequency tile over the
+                        // (component, point tile) items
+                        const long long nwt = (M.nw + TC_W - 1) / TC_W;
+                        const long long items = (long long)ncomp_mon * ((M.npts + TC_M - 1) / TC_M);
+                        const long long G = std::max(1ll, std::min(items, 2ll * tc_sms / nwt));
+                        const int grid = (int)(nwt * G);
+                        monitor_dft_tc_kernel<<<grid, TC_THREADS, dft_tc_smem_bytes, st>>>(md, ncomp_mon, ring_used, ring_first,
+                                                                                          tc_bscale, d_tcfault);
+                    });
+                }
             } else if (M.kind == MFD_MON_SPECTRAL && !M.sum) {
                 launch(KC_DFT, [&] {
                     // blocks of 32 x (frequency groups of the tile), tiles of DFT_PT points
@@ -1752,7 +1790,9 @@ class Engine : public HandleBase {
         MFD_CK(cudaEventRecord(run_ev[1], st));
         MFD_CK(cudaMemcpyAsync(h_flags + (a - 1), d_flags + (a - 1), (size_t)(b - a + 1) * sizeof(int),
                                cudaMemcpyDeviceToHost, st));
+        if (tc_fold) MFD_CK(cudaMemcpyAsync(&h_tcfault, d_tcfault, sizeof(int), cudaMemcpyDeviceToHost, st));
         bounded_sync(st);
+        check_fold();
         float ms = 0;
         MFD_CK(cudaEventElapsedTime(&ms, run_ev[0], run_ev[1]));
         run_ms = ms;
@@ -1880,7 +1920,9 @@ class Engine : public HandleBase {
             const size_t n = (size_t)M.nw * (M.sum ? 1 : M.npts);
             MFD_CK(cudaMemcpyAsync(dst, M.S + (size_t)k * n, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
         }
+        if (tc_fold) MFD_CK(cudaMemcpyAsync(&h_tcfault, d_tcfault, sizeof(int), cudaMemcpyDeviceToHost, st));
         bounded_sync(st);
+        check_fold();
         return MFD_OK;
     }
 

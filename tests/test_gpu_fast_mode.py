@@ -183,3 +183,35 @@ def test_mode_is_validated(gpu_lib):
         _abi.Stepper(gpu_lib, b, np.float32)
     with pytest.raises(ValueError):
         M.B200(np.float32, mode="quick")
+
+
+def test_tensor_core_fold_against_fp64_sum(gpu_lib):
+    """Float32 spectral monitors in the tolerance mode are folded on the tensor cores (TF32
+    high and low parts, three products per 8 staged steps, FP32 partial sums per fold of at
+    most 64 steps, added to the FP64 spectra).  Checked against an FP64 sum over the same
+    run's recorded time series (a field monitor on the same plane): 80 frequencies (a full
+    and a partial 64-frequency tile), a plane whose point count is no multiple of the
+    128-point tile, and 75 steps (a full fold and a partial one of 11 steps)."""
+    from maxwellfdtd_b200.monitors import DFT
+    model = C.model_vacuum(3, nsteps=75)
+    plane = C._plane(3, 150e-9)
+    w = np.linspace(1.0e15, 4.0e15, 80)
+    mons = [M.FieldMonitor(plane), M.SpectralMonitor(plane, w=w)]
+    sol = M.solve(model, backend=M.B200(np.float32, library=gpu_lib, mode="fast"), monitors=mons)
+    out = sol.out
+    t_T = np.asarray(out["t"], dtype=np.float32)
+    assert len(t_T) == 75
+    dft = DFT(t_T, np.float32, w=w)
+    fac = 2.0 * (dft.phasor[..., 0] + 1j * dft.phasor[..., 1]) * float(np.float32(model.dt))   # [Nt][Nw]
+    npts = out["monitors/1/Ex"].shape[0]
+    assert npts % 128 != 0
+    for c in ("Hx", "Hy", "Hz", "Ex", "Ey", "Ez"):
+        ref = out[f"monitors/1/{c}"].astype(np.float64) @ fac      # (npts, Nw)
+        got = out[f"monitors/2/{c}"]
+        assert got.shape == ref.shape
+        den = np.linalg.norm(ref)
+        if den == 0:
+            assert not np.any(got)
+            continue
+        rel = float(np.linalg.norm(got - ref) / den)
+        assert rel <= 1e-5, (c, rel)
