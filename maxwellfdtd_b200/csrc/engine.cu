@@ -411,9 +411,10 @@ class Engine : public HandleBase {
     // layered; the exact mode's layer code needs 80 registers and measured slower, 38.0
     // against 40.2).
     bool lay_H = true, lay_E = true;
-    // planes per block of a z-layer launch (12-plane layers at 256^3 plasmonics: 6 gave 43.9,
-    // 4 gave 43.4-43.5, 12 gave 42.2 Gcell/s)
-    int zc_lay = 6;
+    // planes per block of a z-layer launch (12-plane layers at 256^3 plasmonics, side streams
+    // at the highest priority: 12 gave 44.26, 6 gave 44.08-44.10, 4 gave 43.86 Gcell/s; before
+    // the priority streams 6 gave 43.9 and 12 gave 42.2)
+    int zc_lay = 12;
     bool mat_in_layers = false;       // some material cell lies in a y or z layer
     // single-precision 3-D updates split into core rows and CPML slabs (yee3d_split.cuh)
     bool use_split = false;
