@@ -589,13 +589,12 @@ class Engine : public HandleBase {
         Sa = dalloc<T>(Np);
         // materials
         nmat = d->nmat;
-        std::vector<uint8_t> gpad;
         std::vector<int> bx0(nmat + 1, INT32_MAX), bx1(nmat + 1, -1), by0(nmat + 1, INT32_MAX), by1(nmat + 1, -1),
             bz0(nmat + 1, INT32_MAX), bz1(nmat + 1, -1);
         if (d->geometry) {
-            // padded copy of the map and each material's bounding box, z-planes split over
-            // host threads (per-thread boxes merged after)
-            gpad.assign((size_t)Np, 0);
+            // each material's bounding box, z-planes split over host threads (per-thread
+            // boxes merged after); the map goes to its padded device layout in one 2-D copy
+            // below, with no host copy
             std::mutex mu;
             bool bad = false;
             parallel_ranges(nz, 4, [&](long long z0, long long z1) {
@@ -605,8 +604,6 @@ class Engine : public HandleBase {
                 for (int iz = (int)z0; iz < (int)z1; ++iz)
                     for (int iy = 0; iy < ny; ++iy) {
                         const uint8_t* row = d->geometry + (size_t)nx * (iy + (size_t)ny * iz);
-                        uint8_t* prow = gpad.data() + (size_t)px * iy + (size_t)sz * iz;
-                        std::memcpy(prow, row, (size_t)nx);
                         uint8_t orv = 0;
                         for (int ix = 0; ix < nx; ++ix) orv |= row[ix];
                         if (!orv) continue;
@@ -643,7 +640,11 @@ class Engine : public HandleBase {
             }
         }
         if (any_geom) {
-            if (!geom) geom = upload(gpad.data(), gpad.size());
+            if (!geom) {   // the caller's map, rows of nx bytes, into rows of px (the padding stays 0)
+                geom = dalloc<uint8_t>((size_t)Np, false);
+                MFD_CK(cudaMemcpy2DAsync(geom, (size_t)px, d->geometry, (size_t)nx, (size_t)nx, (size_t)ny * nz,
+                                         cudaMemcpyHostToDevice, st));
+            }
             E2 = dalloc<T>(Np);
         }
         const int nc = ndim;   // field components per vector quantity
