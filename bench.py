@@ -21,6 +21,8 @@ TFSF injection, monitor gather; the DFT accumulation runs every 64 staged steps)
             alongside), algorithmic bytes per update / its mean time from CUDA events around
             each update, measured over the K steps after the timed ones (the timed steps
             themselves carry no per-launch events), against the measured HBM copy bandwidth.
+  dft_fold: the same for the DFT fold of one spectral face monitor (the tensor-core fold in
+            the tolerance mode): its spectra read and written once, its 64 staged steps read.
 
 Multi-GPU: replicas (the path does not shard); each rank runs the same workload on its own
 GPU, scaling "weak".  ``--impl reference`` times the CPU oracle (the restatement of the
@@ -266,6 +268,18 @@ def run_gpu(args):
     e_gbs = e_bytes / (e_ms * 1e-3) / 1e9
     h_gbs = h_bytes / (h_ms * 1e-3) / 1e9
     per_kernel = {k: {"ms": round(kt1[k][0] - kt0[k][0], 4), "launches": int(kt1[k][1] - kt0[k][1])} for k in kt1}
+    # the DFT fold of one spectral face monitor per launch (every 64 steps): its spectra read
+    # and written once (complex128) and its staged samples (6 components x 64 steps) read once
+    spec = [m for m in meta["monitors"] if m["kind"] == 1 and not m["sum"]]
+    fold = None
+    if spec and per_kernel["dft"]["launches"]:
+        fold_ms = (kt1["dft"][0] - kt0["dft"][0]) / (kt1["dft"][1] - kt0["dft"][1])
+        fold_bytes = int(np.mean([len(m["cells"]) * 6 * (m["dft"].Nw * 32 + 64 * 4) for m in spec]))
+        fold_gbs = fold_bytes / (fold_ms * 1e-3) / 1e9
+        fold = {"kernel": ("monitor_dft_tc_kernel (tcgen05.mma kind::tf32, TMEM accumulators)" if args.mode == "fast"
+                           else "monitor_dft_kernel (FP64)"),
+                "mean_launch_ms": round(fold_ms, 5), "algorithmic_bytes_per_launch": fold_bytes,
+                "achieved": round(fold_gbs, 1), "unit": "GB/s", "frac": round(fold_gbs / peaks()[0], 4)}
 
     # the other arithmetic mode on the same workload: the same window on its own handle
     other = "exact" if args.mode == "fast" else "fast"
@@ -347,6 +361,7 @@ def run_gpu(args):
                                       "traffic": NCU_TRAFFIC_256.get((args.mode, "H")) if args.size == 256 else None,
                                       "algorithmic_bytes_per_launch": h_bytes, "mean_launch_ms": round(h_ms, 5)}},
             "kernels": per_kernel,
+            "dft_fold": fold,
             "plain_stepper": plain,
             "gpu_launches": launches,
             "device_bytes": dev_bytes,
