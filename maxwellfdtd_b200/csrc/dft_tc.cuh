@@ -226,7 +226,11 @@ __global__ void __launch_bounds__(TC_THREADS, 2) monitor_dft_tc_kernel(const Mon
             }
             phase ^= 1u;
         }
-        if (failed) { atomicOr(fault, 1); break; }
+        failed = __syncthreads_or(failed);   // one decision for the whole block
+        if (failed) {
+            if (tid == 0) atomicOr(fault, 1);
+            break;
+        }
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
         // Epilogue: warp (quarter q, half h) holds lanes 32q.. and frequencies 16h.. of the tile.
