@@ -411,10 +411,16 @@ class Engine : public HandleBase {
     // layered; the exact mode's layer code needs 80 registers and measured slower, 38.0
     // against 40.2).
     bool lay_H = true, lay_E = true;
-    // planes per block of a z-layer launch (12-plane layers at 256^3 plasmonics, side streams
-    // at the highest priority: 12 gave 44.26, 6 gave 44.08-44.10, 4 gave 43.86 Gcell/s; before
-    // the priority streams 6 gave 43.9 and 12 gave 42.2)
-    int zc_lay = 12;
+    // Planes per block of a z-layer launch of n planes: the whole layer in one march up to 16
+    // planes, else even chunks of at most 12.  At 256^3 plasmonics (13-plane layers, side
+    // streams at the highest priority): 13 gave 44.64-44.65 against 44.31-44.32 for chunks of
+    // 12 + 1 (same box); 6 + 6 + 1 gave 44.08-44.10 and 4 43.86 Gcell/s; before the priority
+    // streams 6 gave 43.9 and 12 gave 42.2.
+    static int zc_layer(int n) {
+        if (n <= 16) return std::max(1, n);
+        const int chunks = (n + 11) / 12;
+        return (n + chunks - 1) / chunks;
+    }
     bool mat_in_layers = false;       // some material cell lies in a y or z layer
     // single-precision 3-D updates split into core rows and CPML slabs (yee3d_split.cuh)
     bool use_split = false;
@@ -1306,8 +1312,9 @@ class Engine : public HandleBase {
             const int za = side ? sbox.zr : 0, zb = side ? nz : sbox.zl;
             if (zb <= za) continue;
             prefer_shared((const void*)h3d_core_async_kernel<MATH, FAST, ACC, E2S, 2>);
-            const SplitBox sl{0, ny, za, zb, zc_lay, 0};
-            const dim3 grd((nx + AS_TX - 1) / AS_TX, (ny + AS_TY - 1) / AS_TY, (zb - za + zc_lay - 1) / zc_lay);
+            const int zc = zc_layer(zb - za);
+            const SplitBox sl{0, ny, za, zb, zc, 0};
+            const dim3 grd((nx + AS_TX - 1) / AS_TX, (ny + AS_TY - 1) / AS_TY, (zb - za + zc - 1) / zc);
             h3d_core_async_kernel<MATH, FAST, ACC, E2S, 2><<<grd, blk, 0, sz_>>>(p, d3, sl);
             kcount++;
         }
@@ -1404,8 +1411,9 @@ class Engine : public HandleBase {
             const int za = side ? sbox.zr : 0, zb = side ? nz : sbox.zl;
             if (zb <= za) continue;
             prefer_shared((const void*)e3d_core_async_kernel<R, MAT, FAST, 2>);
-            const SplitBox sl{0, ny, za, zb, zc_lay, 0};
-            const dim3 grd((nx + AS_TX - 1) / AS_TX, (ny + AS_TY - 1) / AS_TY, (zb - za + zc_lay - 1) / zc_lay);
+            const int zc = zc_layer(zb - za);
+            const SplitBox sl{0, ny, za, zb, zc, 0};
+            const dim3 grd((nx + AS_TX - 1) / AS_TX, (ny + AS_TY - 1) / AS_TY, (zb - za + zc - 1) / zc);
             e3d_core_async_kernel<R, MAT, FAST, 2><<<grd, blk, 0, sz_>>>(p, d3, sl, none);
             kcount++;
         }
