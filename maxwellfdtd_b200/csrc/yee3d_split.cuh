@@ -376,6 +376,29 @@ __global__ void __launch_bounds__(256, RESP ? 2 : (sizeof(T) == 4 ? MFD_CORE_MIN
         D0 = mad<FAST>(Md1, D0, Md2 * (dHzy - dHyz));
         D1 = mad<FAST>(Md1, D1, Md2 * (dHxz - dHzx));
         D2 = mad<FAST>(Md1, D2, Md2 * (dHyx - dHxy));
+        if (RESP && !simple) {
+            // The response before this cell's D stores (it takes D from registers).  In
+            // single precision the pole count is a template argument: every load it makes
+            // (E^n, both buffers of every pole, the plasma state) is then issued at once
+            // instead of one pole buffer per round trip.  Double precision keeps the pole
+            // loop (the unrolled form spills there).
+            const MatDev<T, R>* mm = p.mats + (ld.g - 1);
+            T* Ep[3] = {Ex, Ey, Ez};
+            const T Dv[3] = {D0, D1, D2};
+            if constexpr (sizeof(T) == 4) {
+                const long long bi = (long long)(ix - mm->bx0) +
+                                     (long long)mm->bnx * ((long long)(iy - mm->by0) + (long long)mm->bny * (iz - mm->bz0));
+                switch (mm->nq) {
+                    case 0: material_cell_n<T, R, 3, 0>(mm, bi, Ep, c, Dv, cur, p.dt); break;
+                    case 1: material_cell_n<T, R, 3, 1>(mm, bi, Ep, c, Dv, cur, p.dt); break;
+                    case 2: material_cell_n<T, R, 3, 2>(mm, bi, Ep, c, Dv, cur, p.dt); break;
+                    case 3: material_cell_n<T, R, 3, 3>(mm, bi, Ep, c, Dv, cur, p.dt); break;
+                    default: material_cell<T, R, 3>(mm, ix, iy, iz, Ep, c, Dv, cur, p.dt); break;
+                }
+            } else {
+                material_cell<T, R, 3>(mm, ix, iy, iz, Ep, c, Dv, cur, p.dt);
+            }
+        }
         Dx[c] = D0;
         Dy[c] = D1;
         Dz[c] = D2;
@@ -383,10 +406,6 @@ __global__ void __launch_bounds__(256, RESP ? 2 : (sizeof(T) == 4 ? MFD_CORE_MIN
             Ex[c] = D0 * Me;
             Ey[c] = D1 * Me;
             Ez[c] = D2 * Me;
-        } else if (RESP) {
-            T* Ep[3] = {Ex, Ey, Ez};
-            const T Dv[3] = {D0, D1, D2};
-            material_cell<T, R, 3>(p.mats + (ld.g - 1), ix, iy, iz, Ep, c, Dv, cur, p.dt);
         }
         hx_zm = hx;
         hy_zm = hy;
