@@ -218,6 +218,18 @@ __global__ void __launch_bounds__(TC_THREADS, 2) monitor_dft_tc_kernel(const Mon
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
                          :: "r"(tc_saddr(bar)) : "memory");
         }
+        // The spectra this thread adds to do not depend on the products: its first 8 are
+        // loaded while the tensor core works.
+        const int q = warp & 3, h = warp >> 2;     // TMEM lane quarter, frequency half
+        const long long p = p0 + 32 * q + lane;
+        const int wb = wt * TC_W + 16 * h;
+        const bool mine = p < npts && wb < nw;
+        const int wn = mine ? min(16, nw - wb) : 0;
+        double2* S = M.S + ((long long)k * nw + wb) * npts + p;
+        double2 v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j < wn) v[j] = S[(long long)j * npts];
         // every thread waits for the products (bounded)
         {
             unsigned polls = 0;
@@ -234,7 +246,6 @@ __global__ void __launch_bounds__(TC_THREADS, 2) monitor_dft_tc_kernel(const Mon
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
         // Epilogue: warp (quarter q, half h) holds lanes 32q.. and frequencies 16h.. of the tile.
-        const int q = warp & 3, h = warp >> 2;
         const uint32_t lane_base = (uint32_t)(32 * q) << 16;
         float re[16], imv[16];
         tmem_ld16(tmem + lane_base + (uint32_t)(16 * h), re);
@@ -242,17 +253,14 @@ __global__ void __launch_bounds__(TC_THREADS, 2) monitor_dft_tc_kernel(const Mon
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
 
-        const long long p = p0 + 32 * q + lane;
-        const int wb = wt * TC_W + 16 * h;
-        if (p < npts && wb < nw) {
-            double2* S = M.S + ((long long)k * nw + wb) * npts + p;
-            const int wn = min(16, nw - wb);
+        if (mine) {
 #pragma unroll
             for (int j0 = 0; j0 < 16; j0 += 8) {
-                double2 v[8];
+                if (j0) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    if (j0 + j < wn) v[j] = S[(long long)(j0 + j) * npts];
+                    for (int j = 0; j < 8; ++j)
+                        if (j0 + j < wn) v[j] = S[(long long)(j0 + j) * npts];
+                }
 #pragma unroll
                 for (int j = 0; j < 8; ++j)
                     if (j0 + j < wn) {
