@@ -294,16 +294,19 @@ constexpr int EA_SLOTS = (AS_NE + EA_NO + AS_TX * AS_TY - 1) / (AS_TX * AS_TY);
 constexpr int EA_NST = 5, EA_AHEAD = EA_NST - 3;   // the copy issued at plane iz lands in the stage last read at iz - 2
 
 #define MFD_EASYNC_MINB (1024 / (32 * MFD_AS_TY))   // 1024 resident threads per SM (64 registers)
-// The tolerance mode's E layer launches fit 9 blocks per SM (56 registers, at most 4 bytes of
-// spill): 256^3 plasmonics 45.19 against 44.97-44.99 Gcell/s at 8 (the H layer code spills
-// 32-116 bytes there and measured slower: 44.78-44.79 with both at 9).
+// The tolerance mode's E layer launches without a material map fit 9 blocks per SM (56
+// registers, at most 4 bytes of spill): 256^3 plasmonics 45.19 against 44.97-44.99 Gcell/s
+// at 8 (the H layer code spills 32-116 bytes there and measured slower: 44.78-44.79 with
+// both at 9).  With the map (materials in a layer) the z-layer code would spill 84 bytes at
+// 56 registers, so those keep 8 blocks.
 #define MFD_EASYNC_MINB_LAY_RECIP 9
 
 // skip: the tiles of the materials' columns, rows and planes, left to another kernel (the
 // register march with the material map).
 // LAY as for h3d_core_async_kernel: the rows of a y layer (1) or the planes of a z layer (2).
 template <typename R, bool MAT, int FAST, int LAY = 0>
-__global__ void __launch_bounds__(AS_TX * AS_TY, LAY ? (FAST == DIV_RECIP ? MFD_EASYNC_MINB_LAY_RECIP : MFD_ASYNC_MINB_LAY)
+__global__ void __launch_bounds__(AS_TX * AS_TY, LAY ? (FAST == DIV_RECIP ? (MAT ? MFD_EASYNC_MINB : MFD_EASYNC_MINB_LAY_RECIP)
+                                                                            : MFD_ASYNC_MINB_LAY)
                                                       : (FAST == DIV_RECIP ? MFD_ASYNC_MINB_RECIP : MFD_EASYNC_MINB))
     e3d_core_async_kernel(const __grid_constant__ EParams<float, R> p, const Div3 D3, const SplitBox s, const TileSkip skip) {
     __shared__ __align__(16) EAStage S[EA_NST];
