@@ -215,3 +215,25 @@ def test_tensor_core_fold_against_fp64_sum(gpu_lib):
             continue
         rel = float(np.linalg.norm(got - ref) / den)
         assert rel <= 1e-5, (c, rel)
+
+
+def test_fast_mode_widened_y_layers_with_material(oracle_lib, gpu_lib):
+    """The tolerance mode widens each y-layer launch to whole tiles of 4 rows; here the
+    5-row CPML layers become 8-row launches, and a Drude+Lorentz ball lies in the rows that
+    move from the core launch to the layer launch and in the core rows next to them (rows
+    5-9), so the layer launches run with the material map and the response runs apart."""
+    g = C.grid3((40, 38, 24))
+    src = M.SoftSource(geometry=C._plane(3, -250e-9), waveform=C._src_wave(3, 2e8), component="Ex")
+    dt = 0.5 / C.C0 / np.sqrt(3 / (50e-9) ** 2)
+    ball = C._ball(3, 120e-9, (0.0, -575e-9, 0.0))
+    m = M.Material(geometry=ball, eps=3.0, chi=[M.DrudeSusceptibility(wp=1.37e16, gamma=1.07e14),
+                                                M.LorentzSusceptibility(deps=1.1, w0=4.2e15, delta=5e14)])
+    model = M.Model(g, src, tmax=(60 - 0.5) * dt, pml=200e-9, material=[m])
+    mons = C.monitors(3)
+    ref = C.run_all(model, oracle_lib, np.float32, mons)
+    got = C.run_all(model, gpu_lib, np.float32, mons, mode="fast")
+    _check(ref, got, np.float32, lambda: C.run_all(model, oracle_lib, np.float64, mons))
+    exact = C.run_all(model, gpu_lib, np.float32, mons)   # the exact mode keeps the layer bounds
+    for k in ref:
+        if k.startswith("field/") or k in ("Sa", "E2"):
+            assert np.array_equal(np.asarray(ref[k]), np.asarray(exact[k])), k
