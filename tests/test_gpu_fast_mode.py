@@ -237,3 +237,17 @@ def test_fast_mode_widened_y_layers_with_material(oracle_lib, gpu_lib):
     for k in ref:
         if k.startswith("field/") or k in ("Sa", "E2"):
             assert np.array_equal(np.asarray(ref[k]), np.asarray(exact[k])), k
+
+
+def test_fast_mode_thick_z_layers(oracle_lib, gpu_lib):
+    """z CPML layers of 19 planes, which the tolerance mode's z-layer launches split into
+    blocks of 10 and 9 planes (layers of at most 16 planes go in one march per block)."""
+    g = C.grid3((24, 20, 56))
+    src = M.SoftSource(geometry=C._plane(3, -250e-9), waveform=C._src_wave(3, 2e8), component="Ex")
+    dt = 0.5 / C.C0 / np.sqrt(3 / (50e-9) ** 2)
+    model = M.Model(g, src, tmax=(60 - 0.5) * dt, pml=(100e-9, 100e-9, 100e-9, 100e-9, 900e-9, 900e-9))
+    assert model.pml[4].nb == 19 and model.pml[5].nb == 19
+    mons = C.monitors(3)
+    ref = C.run_all(model, oracle_lib, np.float32, mons)
+    got = C.run_all(model, gpu_lib, np.float32, mons, mode="fast")
+    _check(ref, got, np.float32, lambda: C.run_all(model, oracle_lib, np.float64, mons))
