@@ -8,7 +8,7 @@
 //
 // i.e. D[p][n] = sum_s A[p][s] B[n][s] with A the ring tile (points x slots) and B the
 // factor tile (n = 32 frequencies x (re, im), slots).  The exact mode folds it with FP64
-// fused-free multiply-adds (monitor_dft_kernel), one point at a time in the reference's
+// multiplies and adds, unfused (monitor_dft_kernel), one point at a time in the reference's
 // order.  Here one CTA takes tiles of 128 points x 32 frequencies:
 //
 //   * A (Float32 samples) and B (FP64 factors, scaled by a power of two) are split into a
@@ -18,9 +18,9 @@
 //     next to each other);
 //   * one thread issues tcgen05.mma kind::tf32, M = 128, N = 64, K = 8 per instruction:
 //     hi*hi + hi*lo + lo*hi for each 8 slots, accumulating in TMEM (64 columns, FP32);
-//   * tcgen05.commit arrives on an mbarrier; every warp waits on it (bounded), reads its
-//     32 TMEM lanes x 32 columns with tcgen05.ld and adds the products, unscaled, to S in
-//     FP64.
+//   * tcgen05.commit arrives on an mbarrier; every warp waits on it (bounded; the first
+//     spectra it adds to are loaded meanwhile), reads its 32 TMEM lanes x 32 columns with
+//     tcgen05.ld and adds the products, unscaled, to S in FP64.
 //
 // The fold is bound by S's read-modify-write (16 B per point, component and frequency); the
 // products take about a microsecond per tile.  Per fold, the partial sums carry the TF32x3
