@@ -3,11 +3,11 @@
 - plasmonics at full size: the 256^3 FP32 workload the headline is measured on (Drude +
   Lorentz sphere, 12-cell CPML, TFSF plane wave, DFT monitors on six box faces at 64
   frequencies), 10 steps, bit-identical to the FP32 oracle; its distance to the FP64 oracle
-  is stated (printed) and bounded by the north-star tolerance 1e-5;
+  is stated (printed) and bounded by the tolerance 1e-5 (relative L2, Float32);
 - dielectric at full size: 100^3 FP64 with the sphere, 100 steps, the TFSF data made the
   reference's way (a vacuum record run), record and replay both bit-identical;
 - the nonlinear glass on a truncated grid (48 x 48 x 256, three Lorentz poles, Kerr, the
-  8-photon plasma with rho in FP64), within the north-star tolerance of the oracle;
+  8-photon plasma with rho in FP64), within the tolerance bound (relative L2 1e-5) of the oracle;
 - mid-size grids whose staged core tiles include blocks away from every face (the
   branch-free inner path of the staged H and E kernels) and whose sphere makes the E update
   split into the staged kernel and the material-map kernel for the sphere's rows and planes.

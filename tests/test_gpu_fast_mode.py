@@ -1,7 +1,7 @@
 """The tolerance mode (MFD_MODE_FAST) against the oracle's exact operation order.
 
 The field updates multiply by reciprocals and fuse multiply-adds, so results are no longer
-bit-identical; the north-star bound is relative L2 <= 1e-5 in Float32 and <= 1e-12 in
+bit-identical; the tolerance bound is relative L2 <= 1e-5 in Float32 and <= 1e-12 in
 Float64 for the fields, which the final fields and running sums meet against the oracle run
 in the same precision.  A monitor's time series or spectrum integrates rounding over every
 step at one place; where it is further than that from the same-precision oracle, the

@@ -3,7 +3,7 @@
 Paths without transcendental functions are compared bit for bit (the kernels follow the
 reference's operation order with no FMA contraction; both sides use IEEE division and
 square root).  Plasma (log10/pow/exp) and the summed monitors (a different summation
-order) are compared within the north-star tolerances: relative L2 <= 1e-5 in Float32 and
+order) are compared within the tolerance bounds: relative L2 <= 1e-5 in Float32 and
 <= 1e-12 in Float64.
 """
 import numpy as np
